@@ -1,0 +1,361 @@
+/*
+ * mutracer_b200 — B200-native progressive path-tracing megakernel behind the
+ * MuTracer buffer contract and C ABI.
+ *
+ * Two layers are exported, both plain C (no CUDA or torch types in any
+ * signature; device memory is passed as plain pointers, streams as void*):
+ *
+ *  1. mtc_*  — kernel-level entry points on caller-owned DEVICE buffers.  They
+ *     replace the reference's per-sample compute dispatch of the WGSL megakernel
+ *     (native/host/src/lib.rs:1466-1600 `dispatch_target`,
+ *     src/renderer/WGPURayTracePass.ts:1935-1939 `dispatchWorkgroups`) and read
+ *     exactly the bind-group buffers declared in
+ *     src/renderer/wgsl/chunks/rayTraceCore.wgsl.ts:320-338,383-386 and
+ *     src/renderer/wgsl/rayTrace.compute.ts:294-299.
+ *
+ *  2. mt_context_* / mt_job_* — the persistent host API of
+ *     native/include/mutracer-context.h:57-187 with the status codes of
+ *     native/include/mutracer-status.h:15-45.  commit takes the flattened
+ *     buffer bundle (mt_scene_bundle) instead of the scene descriptor v8.
+ *
+ * All entry points return an mt_status (0 = MT_OK).  Functions that take
+ * `char *error, size_t capacity` write a truncated NUL-terminated message.
+ */
+#ifndef MUTRACER_B200_H
+#define MUTRACER_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+/* Same values as native/include/mutracer-status.h:15-45. */
+typedef int32_t mt_status;
+enum {
+  MT_OK = 0,
+  MT_ERROR = 1,
+  MT_ERROR_INVALID_ARGUMENT = 2,
+  MT_ERROR_INVALID_HANDLE = 3,
+  MT_ERROR_BUSY = 4,
+  MT_ERROR_INVALID_STATE = 5,
+  MT_ERROR_FULL_COMMIT_REQUIRED = 6,
+  MT_ERROR_CANCELLED = 7,
+  MT_ERROR_BUFFER_TOO_SMALL = 8,
+  MT_ERROR_CONTEXT_FAILED = 9,
+  MT_ERROR_UNAVAILABLE = 10,
+  MT_ERROR_TIMEOUT = 11
+};
+/* mutracer-status.h mt_image_kind subset served by read_pixels. */
+enum { MT_IMAGE_HDR = 0, MT_IMAGE_NORMAL = 1, MT_IMAGE_ALBEDO = 2 };
+/* mutracer-status.h mt_context_state / mt_job_state / mt_sampling_pattern. */
+enum { MT_CONTEXT_EMPTY = 0, MT_CONTEXT_COMMITTED = 1, MT_CONTEXT_FAILED = 2,
+       MT_CONTEXT_JOB_ACTIVE = 3 };
+enum { MT_COMMIT_NONE = 0, MT_COMMIT_FULL = 1, MT_COMMIT_INCREMENTAL = 2 };
+enum { MT_JOB_QUEUED = 0, MT_JOB_RUNNING = 1, MT_JOB_COMPLETE = 2,
+       MT_JOB_CANCELLED = 3, MT_JOB_FAILED = 4, MT_JOB_CANCELLING = 5 };
+enum { MT_SAMPLING_SOBOL = 0, MT_SAMPLING_ZSOBOL = 1, MT_SAMPLING_RANDOM = 2 };
+
+/* ------------------------------------------------------- buffer contract */
+/* Light / choice / material constants: src/renderer/lightConstants.ts:1-15. */
+enum { MTC_LIGHT_DIRECTIONAL = 1, MTC_LIGHT_SPHERE = 2, MTC_LIGHT_RECT = 3,
+       MTC_LIGHT_SPOT = 4, MTC_LIGHT_DISK = 5, MTC_LIGHT_CYLINDER = 6 };
+enum { MTC_CHOICE_ENVIRONMENT = 1, MTC_CHOICE_ANALYTIC = 2,
+       MTC_CHOICE_EMISSIVE_TRIANGLE = 3 };
+/* Scene feature bits of RayTraceUniform.sceneFeatureFlags
+ * (src/renderer/WGPUSceneFeatures.ts:4-12). */
+enum { MTC_FEATURE_USE_ENVMAP = 1u, MTC_FEATURE_HAS_THIN_FILM = 1u << 10,
+       MTC_FEATURE_HAS_COAT = 1u << 11, MTC_FEATURE_HAS_FUZZ = 1u << 12,
+       MTC_FEATURE_HAS_SUBSURFACE = 1u << 13,
+       MTC_FEATURE_HAS_SHADOW_CATCHER = 1u << 14 };
+/* backgroundFlags bits (rayTrace.compute.ts:1268-1276). */
+enum { MTC_BACKGROUND_COLOR = 1, MTC_BACKGROUND_MAP = 2, MTC_BACKGROUND_GROUNDED = 4 };
+
+#define MTC_INSTANCE_VEC4_STRIDE 10   /* bvhAccel.ts:16 */
+#define MTC_MATERIAL_VEC4_ROWS 26     /* materialLayoutSchema.ts:23-150 */
+#define MTC_LIGHT_VEC4_ROWS 6         /* wgpuSceneUniform.ts:11 PIXELS_PER_LIGHT */
+#define MTC_ENERGY_LUT_WIDTH 32       /* decodeOpenPbrEnergyLut.ts:20-33 */
+#define MTC_ENERGY_LUT_HEIGHT 2177
+#define MTC_MAX_STACK 64              /* bvhAccel.ts:80 MAX_TRAVERSAL_STACK_SIZE */
+
+/* RayTraceUniform, byte-identical to the WGSL struct of
+ * rayTraceCore.wgsl.ts:281-318 as written by wgpuSceneUniform.ts:13-55
+ * (320 bytes, offsets in comments). */
+typedef struct mtc_trace_uniform {
+  float output_size[2];                 /*   0 */
+  float sample_count;                   /*   8 */
+  float _pad0;                          /*  12 */
+  float scale_offset[4];                /*  16 */
+  int32_t lights_count;                 /*  32 */
+  float transmissive_output_alpha_min;  /*  36 */
+  float jitter[2];                      /*  40 */
+  float background_color[4];            /*  48 */
+  float grounded_background_params[4];  /*  64 */
+  float grounded_background_center[2];  /*  80 */
+  int32_t blas_offset;                  /*  88 */
+  int32_t is_empty;                     /*  92 */
+  int32_t bevel;                        /*  96 */
+  int32_t dispersion_wavelengths;       /* 100 */
+  float env_light_pmf;                  /* 104 */
+  int32_t light_choice_count;           /* 108 */
+  float light_weight_total;             /* 112 */
+  int32_t light_sampling_texture_width; /* 116 */
+  int32_t light_choice_texel_offset;    /* 120 */
+  int32_t bounces;                      /* 124 */
+  int32_t variance_moments;             /* 128 */
+  int32_t adaptive_sampling;            /* 132 */
+  float clamping;                       /* 136 */
+  int32_t direct_light_candidates;      /* 140 */
+  int32_t background_flags;             /* 144 */
+  uint32_t loop_unroll_guard;           /* 148 */
+  uint32_t scene_feature_flags;         /* 152 */
+  uint32_t sequence_seed;               /* 156 */
+  uint32_t zsobol_log_spp;              /* 160 */
+  uint32_t sample_sequence_offset;      /* 164 */
+  int32_t shadow_catcher_choice_offset; /* 168 */
+  int32_t shadow_catcher_choice_count;  /* 172 */
+  float environment_rotation[16];       /* 176 */
+  float background_map_transform[4];    /* 240 */
+  float background_map_rotation[16];    /* 256 */
+} mtc_trace_uniform;                    /* 320 */
+
+/* CameraUniform, rayTraceCore.wgsl.ts:274-279 (column-major mat4). */
+typedef struct mtc_camera_uniform {
+  float view_projection_inv[16];
+  float view_inv[16];
+  float aperture_radius;
+  float focus_distance;
+  float _pad[2];
+} mtc_camera_uniform;
+
+/* Compact vertex layout of attrBuffers (src/renderer/compactVertices.ts:7-28):
+ * u32 words, position f32x3 at word 0, normal at normal_offset (oct-encoded
+ * u32, or f32x3 when normal_float != 0).  UV/color/tangent words may be present
+ * in the stride; this build's synthetic scenes carry none. */
+typedef struct mtc_vertex_layout {
+  uint32_t stride;
+  uint32_t normal_offset;
+  uint32_t normal_float;
+  uint32_t _pad;
+} mtc_vertex_layout;
+
+/* Device-side view of the bind groups (all pointers are device pointers). */
+typedef struct mtc_scene_view {
+  uint32_t struct_size;
+  uint32_t flags;                  /* MTC_SCENE_* below */
+  /* G0 */
+  const void *bvh;                 /* binding 0: vec4f[], TLAS at 0, BLASes after blas_offset */
+  uint64_t bvh_vec4_count;
+  const void *instances;           /* binding 1: vec4f[10 * instance_count] */
+  uint32_t instance_count;
+  uint32_t material_count;
+  const void *attributes;          /* binding 2: u32 words */
+  uint64_t attribute_words;
+  mtc_vertex_layout vertex_layout;
+  const void *materials;           /* binding 3: vec4f[26 * material_count] */
+  /* G1 */
+  const void *env_map;             /* binding 4: RGBA32F env_width x env_height */
+  const void *env_distribution;    /* binding 5: RG32F (env_width+2) x (env_height+1) */
+  uint32_t env_width, env_height;
+  const void *light_sampling;      /* binding 8: RGBA32F, width in the uniform */
+  uint32_t light_sampling_texels;
+  int32_t blas_offset;             /* vec4 index of the first BLAS (RayTraceUniform.blasOffset) */
+  const void *energy_lut;          /* binding 9: R32F 32 x 2177 */
+  /* G2 */
+  const void *analytic_lights;     /* binding 2: vec4f[6 * lights_count] */
+  uint32_t tlas_stack_size;        /* TLAS_STACK_SIZE (1..64) */
+  uint32_t blas_stack_size;        /* BLAS_STACK_SIZE (1..64) */
+} mtc_scene_view;
+/* flags: shader specialisation constants that are not in the uniform
+ * (HAS_MEDIUM, SPECTRAL and SAMPLING_PATTERN of wgpuMaterialConstants.ts:40-70).
+ * The sampling pattern (MT_SAMPLING_*) occupies bits 4..5. */
+enum { MTC_SCENE_HAS_MEDIUM = 1u, MTC_SCENE_SPECTRAL = 2u,
+       MTC_SCENE_PATTERN_SHIFT = 4u, MTC_SCENE_PATTERN_MASK = 0x30u };
+
+/* G3 accumulation outputs (rayTrace.compute.ts:294-299; never overwritten,
+ * always accumulated).  shadow_catcher holds 3 vec4 per pixel
+ * {mask, background, moments} (shadowCatcherAccumulation.wgsl.ts:9-15). */
+typedef struct mtc_outputs {
+  void *color;
+  void *normal;
+  void *albedo;
+  void *shadow_catcher;
+} mtc_outputs;
+
+/* First-hit record of querySceneSoftware (intersect.wgsl.ts:660-684). */
+typedef struct mtc_hit {
+  int32_t hit;
+  int32_t instance;
+  int32_t record;
+  float t;
+  float barycentric[3];
+  float _pad;
+} mtc_hit;
+
+/* Runtime counters (extension+shadow rays, path samples), for Mrays/s. */
+typedef struct mtc_counters {
+  unsigned long long path_samples;
+  unsigned long long extension_rays;
+  unsigned long long shadow_rays;
+  unsigned long long _pad;
+} mtc_counters;
+
+/* Library ABI version of this header. */
+#define MTC_ABI_VERSION 1u
+uint32_t mtc_abi_version(void);
+
+/* One progressive pass per sample over the whole image: for each of
+ * `samples` passes, every pixel (x, y) with x < output_size.x and
+ * y < output_size.y traces one path sample and adds to `out`.  The per-pixel
+ * sample index is read from out->normal[idx].w + sample_sequence_offset,
+ * exactly as rayTrace.compute.ts:1187-1193.  Replaces the per-sample dispatch
+ * loop of native/host/src/lib.rs:1506-1560.  counters may be NULL. */
+mt_status mtc_trace_samples(const mtc_scene_view *scene,
+                            const mtc_camera_uniform *camera,
+                            const mtc_trace_uniform *uniform,
+                            const mtc_outputs *out, uint32_t samples,
+                            mtc_counters *counters, void *stream);
+
+/* Raw first-hit query over `count` rays (8 floats each: o.xyz, pad, d.xyz,
+ * pad; device memory), writing `hits` (device memory).  The contract of
+ * querySceneSoftware, intersect.wgsl.ts:660-684 (bounces 0, single-sided). */
+mt_status mtc_query_first_hit(const mtc_scene_view *scene, const float *rays,
+                              uint32_t count, mtc_hit *hits, void *stream);
+
+/* Full TLAS refit on the device: rewrites the instance records (inverse
+ * transform, transform, BLAS placement) and every TLAS node box from the
+ * per-source-instance transforms, following bvhAccel.ts:579-740 refitTLAS with
+ * no dirty set.  transforms: f64[16 * n] column-major (device); local_bounds:
+ * f32[6 * n] BLAS-local AABB per source instance (device); blas_offsets and
+ * vertex_offsets: i32 per source instance; materials: packed i32 per source
+ * instance; colors f32[3 * n].  tlas/instances are the device buffers to
+ * update in place; tlas_vec4_count bounds the TLAS node range. */
+mt_status mtc_refit_tlas(void *tlas, uint64_t tlas_vec4_count, void *instances,
+                         uint32_t instance_count, const double *transforms,
+                         const float *local_bounds, const int32_t *blas_offsets,
+                         const int32_t *blas_layouts, const int32_t *vertex_offsets,
+                         const int32_t *materials, const float *colors,
+                         void *stream);
+
+/* ------------------------------------------------------ batched form */
+/* One render job of a batched launch: its own scene view, camera, uniform
+ * and outputs.  All jobs of a batch run in one persistent kernel that pulls
+ * (job, pixel-tile, sample) work items from a global queue. */
+typedef struct mtc_job_desc {
+  mtc_scene_view scene;
+  mtc_camera_uniform camera;
+  mtc_trace_uniform uniform;
+  mtc_outputs out;
+  uint32_t samples;        /* samples to add in this launch */
+  uint32_t _pad[3];
+} mtc_job_desc;
+
+/* Tuning knobs chosen by the autotuner (0 selects the built-in default). */
+typedef struct mtc_batch_config {
+  uint32_t struct_size;
+  uint32_t block_threads;  /* threads per CTA of the persistent kernel */
+  uint32_t tile_pixels;    /* pixels per work item */
+  uint32_t ctas_per_sm;    /* resident CTAs per SM (grid = 148 * ctas_per_sm) */
+} mtc_batch_config;
+
+/* Runs `job_count` jobs (descriptors in DEVICE memory) to completion in one
+ * persistent launch.  `queue_state` is caller-provided device scratch of
+ * mtc_batch_scratch_bytes(job_count) bytes, zeroed by the call on `stream`.
+ * status_out (device, may be NULL) receives 0 on success or a nonzero code if
+ * the kernel's bounded queue loop gave up.  Work is pulled with one atomic per
+ * work item; results are identical to running each job alone. */
+size_t mtc_batch_scratch_bytes(uint32_t job_count);
+mt_status mtc_trace_batch(const mtc_job_desc *jobs_device, uint32_t job_count,
+                          const mtc_batch_config *config, void *queue_state,
+                          uint32_t *status_out, mtc_counters *counters,
+                          void *stream);
+
+/* ------------------------------------------------------- host context */
+typedef uint64_t mt_context;
+typedef uint64_t mt_render_job;
+
+/* Flattened host buffer bundle: the same arrays as mtc_scene_view, in host
+ * memory, plus camera and uniform defaults.  commit copies everything. */
+typedef struct mt_scene_bundle {
+  uint32_t struct_size;
+  uint32_t width, height;
+  uint32_t flags;                  /* MTC_SCENE_* */
+  const float *bvh; uint64_t bvh_vec4_count;
+  const float *instances; uint32_t instance_count;
+  uint32_t material_count;
+  const uint32_t *attributes; uint64_t attribute_words;
+  mtc_vertex_layout vertex_layout;
+  const float *materials;
+  const float *env_map; uint32_t env_width, env_height;
+  const float *env_distribution;
+  const float *light_sampling; uint32_t light_sampling_texels;
+  uint32_t lights_count;
+  const float *energy_lut;
+  const float *analytic_lights;
+  uint32_t tlas_stack_size, blas_stack_size;
+  mtc_camera_uniform camera;
+  mtc_trace_uniform uniform;       /* settings fields are overwritten by mt_render_settings */
+} mt_scene_bundle;
+
+/* mutracer-context.h:86-100 */
+typedef struct mt_render_settings {
+  uint32_t struct_size, sampling_pattern, seed, max_samples;
+  uint32_t bounces, direct_light_candidates, bevel_samples, sample_sequence_offset;
+  double clamping, transmissive_output_alpha_min;
+  uint32_t caustic_flags;
+  uint32_t light_photons, photon_map_photons;
+  float photon_map_radius;
+} mt_render_settings;
+
+/* mutracer-context.h:63-68 */
+typedef struct mt_context_snapshot {
+  uint32_t struct_size;
+  uint32_t width, height, samples;
+  uint32_t state;
+  uint32_t last_commit;
+} mt_context_snapshot;
+
+/* mutracer-context.h:176-180 */
+typedef struct mt_job_snapshot {
+  uint32_t struct_size;
+  uint32_t state;
+  uint32_t requested_samples, submitted_samples, completed_samples, base_samples;
+} mt_job_snapshot;
+
+/* mutracer-context.h:77 */
+int32_t mt_context_create(mt_context *output, char *error, size_t capacity);
+/* mutracer-context.h:81 */
+int32_t mt_context_destroy(mt_context handle, char *error, size_t capacity);
+/* mutracer-context.h:101 */
+int32_t mt_render_settings_default(mt_render_settings *output);
+/* mutracer-context.h:91 (commit) and :102-103 (commit_with_settings): the
+ * descriptor argument is the flattened bundle. settings may be NULL. */
+int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *bundle,
+                                 const mt_render_settings *settings, char *error,
+                                 size_t capacity);
+/* mutracer-context.h:104 */
+int32_t mt_context_render(mt_context handle, uint32_t additional_samples, char *error,
+                          size_t capacity);
+/* mutracer-context.h:105 */
+int32_t mt_context_reset(mt_context handle, char *error, size_t capacity);
+/* mutracer-context.h:112 */
+#define MT_WAIT_INDEFINITELY UINT32_MAX
+int32_t mt_context_wait(mt_context handle, uint32_t timeout_ms, char *error, size_t capacity);
+/* mutracer-context.h:113 */
+int32_t mt_context_info(mt_context handle, mt_context_snapshot *info, char *error,
+                        size_t capacity);
+/* mutracer-context.h:114-115: f32 RGBA, bottom row first, divided by the
+ * per-pixel completed sample count. pixels=NULL,size=0 queries the size. */
+int32_t mt_context_read_pixels(mt_context handle, uint32_t kind, void *pixels, size_t size,
+                               size_t *written, char *error, size_t capacity);
+/* mutracer-context.h:181-185 */
+int32_t mt_context_submit(mt_context handle, uint32_t additional_samples, mt_render_job *job,
+                          char *error, size_t capacity);
+int32_t mt_job_poll(mt_render_job job, uint32_t max_new_samples, char *error, size_t capacity);
+int32_t mt_job_info(mt_render_job job, mt_job_snapshot *info, char *error, size_t capacity);
+int32_t mt_job_cancel(mt_render_job job, char *error, size_t capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,459 @@
+// Persistent host API of native/include/mutracer-context.h:57-187 on CUDA:
+// contexts own device copies of a committed buffer bundle plus the four
+// accumulation buffers; render adds samples through mtc_trace_samples; jobs
+// are caller-polled with at most one batch in flight (a CUDA event), like
+// native/host/src/context.rs:2002-2256 (submit/poll_job/advance_job).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/mutracer_b200.h"
+
+namespace {
+
+void setError(char *error, size_t capacity, const std::string &msg) {
+  if (!error || capacity == 0) return;
+  size_t n = std::min(msg.size(), capacity - 1);
+  std::memcpy(error, msg.data(), n);
+  error[n] = '\0';
+}
+
+struct DeviceBuffer {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  ~DeviceBuffer() { if (ptr) cudaFree(ptr); }
+  cudaError_t upload(const void *host, size_t n) {
+    if (!host || n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) { ptr = nullptr; return e; }
+    bytes = n;
+    return cudaMemcpy(ptr, host, n, cudaMemcpyHostToDevice);
+  }
+};
+
+struct SceneResources {
+  DeviceBuffer bvh, ins, attr, mats, env, envDist, lightData, lut, lights;
+  DeviceBuffer color, normal, albedo, catcher;
+  mtc_scene_view view{};
+  uint32_t width = 0, height = 0;
+};
+
+struct Job {
+  uint64_t handle = 0;
+  uint32_t state = MT_JOB_QUEUED;
+  uint32_t requested = 0, submitted = 0, completed = 0, base = 0;
+  uint32_t inflight = 0;
+};
+
+struct Context {
+  std::mutex m;
+  uint64_t handle = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t event = nullptr;
+  std::unique_ptr<SceneResources> scene;
+  mtc_camera_uniform camera{};
+  mtc_trace_uniform uniform{};
+  uint32_t samples = 0;  // completed samples
+  bool failed = false;
+  uint32_t lastCommit = MT_COMMIT_NONE;
+  std::unique_ptr<Job> job;
+  ~Context() {
+    if (stream) cudaStreamSynchronize(stream);
+    scene.reset();
+    if (event) cudaEventDestroy(event);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+std::mutex gRegistry;
+std::map<uint64_t, std::shared_ptr<Context>> gContexts;
+std::map<uint64_t, uint64_t> gJobs;  // job handle -> context handle
+uint64_t gNextHandle = 1;
+
+std::shared_ptr<Context> findContext(uint64_t h) {
+  std::lock_guard<std::mutex> g(gRegistry);
+  auto it = gContexts.find(h);
+  return it == gContexts.end() ? nullptr : it->second;
+}
+
+bool activeJob(const Context &c) {
+  return c.job && (c.job->state == MT_JOB_QUEUED || c.job->state == MT_JOB_RUNNING || c.job->state == MT_JOB_CANCELLING);
+}
+
+void expireJob(Context &c) {
+  if (!c.job) return;
+  std::lock_guard<std::mutex> g(gRegistry);
+  gJobs.erase(c.job->handle);
+  c.job.reset();
+}
+
+int32_t failContext(Context &c, cudaError_t e, char *error, size_t capacity) {
+  c.failed = true;
+  setError(error, capacity, std::string("CUDA failure: ") + cudaGetErrorString(e));
+  cudaGetLastError();
+  return MT_ERROR_CONTEXT_FAILED;
+}
+
+uint32_t logSpp(uint32_t maxSamples) {
+  // sceneAssembly.ts:34-37 traceSampling (ZSobol uses max_samples - 1).
+  uint32_t n = std::max(1u, maxSamples);
+  uint32_t l = 0;
+  while ((1u << l) < n && l < 16) l++;
+  return std::min(16u, l);
+}
+
+void applySettings(Context &c, const mt_render_settings &s) {
+  c.uniform.sequence_seed = s.seed;
+  c.uniform.bounces = int32_t(std::min(20u, std::max(1u, s.bounces)));
+  c.uniform.direct_light_candidates = int32_t(std::min(16u, std::max(1u, s.direct_light_candidates)));
+  c.uniform.sample_sequence_offset = s.sample_sequence_offset;
+  c.uniform.clamping = float(s.clamping);
+  c.uniform.transmissive_output_alpha_min = float(s.transmissive_output_alpha_min);
+  c.uniform.zsobol_log_spp = logSpp(s.sampling_pattern == MT_SAMPLING_ZSOBOL ? std::max(1u, s.max_samples - 1) : s.max_samples);
+}
+
+int32_t launch(Context &c, uint32_t samples) {
+  mtc_outputs out{c.scene->color.ptr, c.scene->normal.ptr, c.scene->albedo.ptr, c.scene->catcher.ptr};
+  return mtc_trace_samples(&c.scene->view, &c.camera, &c.uniform, &out, samples, nullptr, c.stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t mt_render_settings_default(mt_render_settings *o) {
+  if (!o) return MT_ERROR_INVALID_ARGUMENT;
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = sizeof(mt_render_settings);
+  o->sampling_pattern = MT_SAMPLING_SOBOL;
+  o->seed = 12345;
+  o->max_samples = 64;
+  o->bounces = 6;
+  o->direct_light_candidates = 2;
+  o->bevel_samples = 8;
+  o->sample_sequence_offset = 0;
+  o->clamping = 0.0;
+  o->transmissive_output_alpha_min = 1.0;
+  return MT_OK;
+}
+
+int32_t mt_context_create(mt_context *output, char *error, size_t capacity) {
+  if (!output) { setError(error, capacity, "output is NULL"); return MT_ERROR_INVALID_ARGUMENT; }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    setError(error, capacity, "no CUDA device");
+    return MT_ERROR_UNAVAILABLE;
+  }
+  auto c = std::make_shared<Context>();
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->event, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    setError(error, capacity, "stream creation failed");
+    return MT_ERROR_UNAVAILABLE;
+  }
+  std::lock_guard<std::mutex> g(gRegistry);
+  c->handle = gNextHandle++;
+  gContexts[c->handle] = c;
+  *output = c->handle;
+  return MT_OK;
+}
+
+int32_t mt_context_destroy(mt_context handle, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (activeJob(*c)) { setError(error, capacity, "active render job: cancel/poll it first"); return MT_ERROR_INVALID_STATE; }
+  expireJob(*c);
+  std::lock_guard<std::mutex> g(gRegistry);
+  gContexts.erase(handle);
+  return MT_OK;
+}
+
+int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, const mt_render_settings *settings,
+                                 char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  if (!b || b->struct_size != sizeof(mt_scene_bundle)) { setError(error, capacity, "bundle struct_size"); return MT_ERROR_INVALID_ARGUMENT; }
+  if (settings && settings->struct_size != sizeof(mt_render_settings)) { setError(error, capacity, "settings struct_size"); return MT_ERROR_INVALID_ARGUMENT; }
+  if (b->width == 0 || b->height == 0 || b->width > 16384 || b->height > 16384 || !b->bvh || !b->instances ||
+      !b->attributes || !b->materials || !b->energy_lut || !b->light_sampling || b->vertex_layout.stride < 4 ||
+      (b->env_map && !b->env_distribution) || (b->lights_count && !b->analytic_lights)) {
+    setError(error, capacity, "invalid buffer bundle");
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  if (settings && (!std::isfinite(settings->clamping) || !std::isfinite(settings->transmissive_output_alpha_min) ||
+                   settings->sampling_pattern > MT_SAMPLING_RANDOM)) {
+    setError(error, capacity, "invalid settings");
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  auto r = std::make_unique<SceneResources>();
+  size_t px = size_t(b->width) * b->height;
+  cudaError_t e = cudaSuccess;
+  auto up = [&](DeviceBuffer &d, const void *h, size_t n) { if (e == cudaSuccess) e = d.upload(h, n); };
+  up(r->bvh, b->bvh, b->bvh_vec4_count * 16);
+  up(r->ins, b->instances, size_t(b->instance_count) * MTC_INSTANCE_VEC4_STRIDE * 16);
+  up(r->attr, b->attributes, b->attribute_words * 4);
+  up(r->mats, b->materials, size_t(b->material_count) * MTC_MATERIAL_VEC4_ROWS * 16);
+  if (b->env_map) {
+    up(r->env, b->env_map, size_t(b->env_width) * b->env_height * 16);
+    up(r->envDist, b->env_distribution, size_t(b->env_width + 2) * (b->env_height + 1) * 8);
+  }
+  up(r->lightData, b->light_sampling, size_t(b->light_sampling_texels) * 16);
+  up(r->lut, b->energy_lut, size_t(MTC_ENERGY_LUT_WIDTH) * MTC_ENERGY_LUT_HEIGHT * 4);
+  if (b->lights_count) up(r->lights, b->analytic_lights, size_t(b->lights_count) * MTC_LIGHT_VEC4_ROWS * 16);
+  for (DeviceBuffer *d : {&r->color, &r->normal, &r->albedo, &r->catcher}) {
+    size_t bytes = px * 16 * (d == &r->catcher ? 3 : 1);
+    if (e == cudaSuccess) e = cudaMalloc(&d->ptr, bytes);
+    if (e == cudaSuccess) { d->bytes = bytes; e = cudaMemset(d->ptr, 0, bytes); }
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    setError(error, capacity, std::string("device allocation failed: ") + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? MT_ERROR_UNAVAILABLE : MT_ERROR;
+  }
+  mtc_scene_view &v = r->view;
+  v.struct_size = sizeof(mtc_scene_view);
+  v.flags = b->flags;
+  v.bvh = r->bvh.ptr; v.bvh_vec4_count = b->bvh_vec4_count;
+  v.instances = r->ins.ptr; v.instance_count = b->instance_count; v.material_count = b->material_count;
+  v.attributes = r->attr.ptr; v.attribute_words = b->attribute_words; v.vertex_layout = b->vertex_layout;
+  v.materials = r->mats.ptr;
+  v.env_map = r->env.ptr; v.env_distribution = r->envDist.ptr; v.env_width = b->env_width; v.env_height = b->env_height;
+  v.light_sampling = r->lightData.ptr; v.light_sampling_texels = b->light_sampling_texels;
+  v.blas_offset = b->uniform.blas_offset;
+  v.energy_lut = r->lut.ptr;
+  v.analytic_lights = r->lights.ptr;
+  v.tlas_stack_size = b->tlas_stack_size; v.blas_stack_size = b->blas_stack_size;
+  r->width = b->width; r->height = b->height;
+  // Publish: the previous job expires, accumulation restarts.
+  expireJob(*c);
+  cudaStreamSynchronize(c->stream);
+  c->scene = std::move(r);
+  c->camera = b->camera;
+  c->uniform = b->uniform;
+  c->uniform.output_size[0] = float(b->width);
+  c->uniform.output_size[1] = float(b->height);
+  if (settings) {
+    applySettings(*c, *settings);
+    c->scene->view.flags = (c->scene->view.flags & ~uint32_t(MTC_SCENE_PATTERN_MASK)) |
+                           (settings->sampling_pattern << MTC_SCENE_PATTERN_SHIFT);
+  }
+  c->samples = 0;
+  c->failed = false;
+  c->lastCommit = MT_COMMIT_FULL;
+  return MT_OK;
+}
+
+int32_t mt_context_render(mt_context handle, uint32_t additional, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (!c->scene || c->failed) { setError(error, capacity, "no healthy committed scene"); return MT_ERROR_INVALID_STATE; }
+  if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
+  if (additional == 0 || uint64_t(c->samples) + additional > 16384u) {
+    setError(error, capacity, "render total must stay within 1..16384 samples");
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  expireJob(*c);
+  int32_t st = launch(*c, additional);
+  if (st != MT_OK) { setError(error, capacity, "launch rejected"); return st; }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return failContext(*c, e, error, capacity);
+  c->samples += additional;
+  return MT_OK;
+}
+
+int32_t mt_context_reset(mt_context handle, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (!c->scene || c->failed) { setError(error, capacity, "no healthy committed scene"); return MT_ERROR_INVALID_STATE; }
+  if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
+  expireJob(*c);
+  cudaError_t e = cudaSuccess;
+  for (DeviceBuffer *d : {&c->scene->color, &c->scene->normal, &c->scene->albedo, &c->scene->catcher})
+    if (e == cudaSuccess) e = cudaMemsetAsync(d->ptr, 0, d->bytes, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return failContext(*c, e, error, capacity);
+  c->samples = 0;
+  return MT_OK;
+}
+
+int32_t mt_context_wait(mt_context handle, uint32_t timeout_ms, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (!c->scene || c->failed) { setError(error, capacity, "no healthy committed scene"); return MT_ERROR_INVALID_STATE; }
+  if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
+  auto start = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(c->stream);
+    if (e == cudaSuccess) return MT_OK;
+    if (e != cudaErrorNotReady) return failContext(*c, e, error, capacity);
+    auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start).count();
+    if (timeout_ms != MT_WAIT_INDEFINITELY && uint64_t(ms) >= timeout_ms) {
+      setError(error, capacity, "timeout");
+      return MT_ERROR_TIMEOUT;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(200));
+  }
+}
+
+int32_t mt_context_info(mt_context handle, mt_context_snapshot *info, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  if (!info || info->struct_size != sizeof(mt_context_snapshot)) { setError(error, capacity, "struct_size"); return MT_ERROR_INVALID_ARGUMENT; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  info->width = c->scene ? c->scene->width : 0;
+  info->height = c->scene ? c->scene->height : 0;
+  info->samples = c->samples;
+  info->state = !c->scene ? MT_CONTEXT_EMPTY : c->failed ? MT_CONTEXT_FAILED : activeJob(*c) ? MT_CONTEXT_JOB_ACTIVE : MT_CONTEXT_COMMITTED;
+  info->last_commit = c->lastCommit;
+  return MT_OK;
+}
+
+int32_t mt_context_read_pixels(mt_context handle, uint32_t kind, void *pixels, size_t size, size_t *written,
+                               char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  if (!written || kind > MT_IMAGE_ALBEDO) { setError(error, capacity, "invalid argument"); return MT_ERROR_INVALID_ARGUMENT; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (!c->scene || c->failed) { setError(error, capacity, "no healthy committed scene"); return MT_ERROR_INVALID_STATE; }
+  size_t px = size_t(c->scene->width) * c->scene->height;
+  size_t need = px * 16;
+  *written = need;
+  if (!pixels && size == 0) return MT_OK;
+  if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
+  if (c->samples == 0) { setError(error, capacity, "no completed samples"); return MT_ERROR_INVALID_STATE; }
+  if (!pixels || size < need) { setError(error, capacity, "destination too small"); return MT_ERROR_BUFFER_TOO_SMALL; }
+  std::vector<float> src(px * 4), cnt(px * 4);
+  const void *buf = kind == MT_IMAGE_HDR ? c->scene->color.ptr : kind == MT_IMAGE_NORMAL ? c->scene->normal.ptr : c->scene->albedo.ptr;
+  cudaError_t e = cudaMemcpyAsync(src.data(), buf, need, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt.data(), c->scene->normal.ptr, need, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return failContext(*c, e, error, capacity);
+  float *o = static_cast<float *>(pixels);
+  for (size_t i = 0; i < px; i++) {
+    float n = cnt[i * 4 + 3];
+    float inv = n > 0.0f ? 1.0f / n : 0.0f;
+    for (int k = 0; k < 4; k++) o[i * 4 + k] = src[i * 4 + k] * inv;
+  }
+  return MT_OK;
+}
+
+int32_t mt_context_submit(mt_context handle, uint32_t additional, mt_render_job *job, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  if (!job) { setError(error, capacity, "job is NULL"); return MT_ERROR_INVALID_ARGUMENT; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (!c->scene || c->failed) { setError(error, capacity, "no healthy committed scene"); return MT_ERROR_INVALID_STATE; }
+  if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
+  if (additional == 0 || uint64_t(c->samples) + additional > 16384u) {
+    setError(error, capacity, "render total must stay within 1..16384 samples");
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  expireJob(*c);
+  auto j = std::make_unique<Job>();
+  j->requested = additional;
+  j->base = c->samples;
+  {
+    std::lock_guard<std::mutex> g(gRegistry);
+    j->handle = gNextHandle++;
+    gJobs[j->handle] = c->handle;
+  }
+  *job = j->handle;
+  c->job = std::move(j);
+  return MT_OK;
+}
+
+static std::shared_ptr<Context> contextOfJob(uint64_t job) {
+  std::lock_guard<std::mutex> g(gRegistry);
+  auto it = gJobs.find(job);
+  if (it == gJobs.end()) return nullptr;
+  auto c = gContexts.find(it->second);
+  return c == gContexts.end() ? nullptr : c->second;
+}
+
+int32_t mt_job_poll(mt_render_job handle, uint32_t max_new_samples, char *error, size_t capacity) {
+  auto c = contextOfJob(handle);
+  if (!c) { setError(error, capacity, "unknown or expired job"); return MT_ERROR_INVALID_HANDLE; }
+  if (max_new_samples > 64) { setError(error, capacity, "max_new_samples must be 0..64"); return MT_ERROR_INVALID_ARGUMENT; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  Job *j = c->job.get();
+  if (!j || j->handle != handle) { setError(error, capacity, "unknown or expired job"); return MT_ERROR_INVALID_HANDLE; }
+  if (j->inflight) {
+    cudaError_t e = cudaEventQuery(c->event);
+    if (e == cudaErrorNotReady) return MT_OK;
+    if (e != cudaSuccess) {
+      j->state = MT_JOB_FAILED;
+      j->inflight = 0;
+      return failContext(*c, e, error, capacity);
+    }
+    j->completed += j->inflight;
+    c->samples += j->inflight;
+    j->inflight = 0;
+  }
+  if (j->completed >= j->requested) { j->state = MT_JOB_COMPLETE; return MT_OK; }
+  if (j->state == MT_JOB_CANCELLING || j->state == MT_JOB_CANCELLED) { j->state = MT_JOB_CANCELLED; return MT_OK; }
+  if (max_new_samples == 0) return MT_OK;
+  uint32_t n = std::min(max_new_samples, j->requested - j->submitted);
+  int32_t st = launch(*c, n);
+  if (st != MT_OK) { j->state = MT_JOB_FAILED; setError(error, capacity, "launch rejected"); return st; }
+  cudaError_t e = cudaEventRecord(c->event, c->stream);
+  if (e != cudaSuccess) { j->state = MT_JOB_FAILED; return failContext(*c, e, error, capacity); }
+  j->submitted += n;
+  j->inflight = n;
+  j->state = MT_JOB_RUNNING;
+  return MT_OK;
+}
+
+int32_t mt_job_info(mt_render_job handle, mt_job_snapshot *info, char *error, size_t capacity) {
+  auto c = contextOfJob(handle);
+  if (!c) { setError(error, capacity, "unknown or expired job"); return MT_ERROR_INVALID_HANDLE; }
+  if (!info || info->struct_size != sizeof(mt_job_snapshot)) { setError(error, capacity, "struct_size"); return MT_ERROR_INVALID_ARGUMENT; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  Job *j = c->job.get();
+  if (!j || j->handle != handle) { setError(error, capacity, "unknown or expired job"); return MT_ERROR_INVALID_HANDLE; }
+  info->state = j->state;
+  info->requested_samples = j->requested;
+  info->submitted_samples = j->submitted;
+  info->completed_samples = j->completed;
+  info->base_samples = j->base;
+  return MT_OK;
+}
+
+int32_t mt_job_cancel(mt_render_job handle, char *error, size_t capacity) {
+  auto c = contextOfJob(handle);
+  if (!c) { setError(error, capacity, "unknown or expired job"); return MT_ERROR_INVALID_HANDLE; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  Job *j = c->job.get();
+  if (!j || j->handle != handle) { setError(error, capacity, "unknown or expired job"); return MT_ERROR_INVALID_HANDLE; }
+  if (j->state == MT_JOB_COMPLETE || j->state == MT_JOB_CANCELLED || j->state == MT_JOB_FAILED) return MT_OK;
+  j->state = j->inflight ? MT_JOB_CANCELLING : MT_JOB_CANCELLED;
+  return MT_OK;
+}
+
+}  // extern "C"

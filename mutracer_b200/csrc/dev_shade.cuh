@@ -1,0 +1,1143 @@
+// Device lights, environment, material resolve, next-event estimation with
+// RIS + MIS, and the RGB integrator of the megakernel.  Function-by-function
+// restatement of rayTrace.compute.ts, sampleMaterial.wgsl.ts,
+// sampleLight.wgsl.ts, envMap.wgsl.ts, background.wgsl.ts and
+// materialBuffer.wgsl.ts (paths relative to src/renderer/wgsl/).
+#pragma once
+#include "dev_bsdf.cuh"
+#include "dev_trace.cuh"
+
+namespace mt {
+
+MTD V3 kLuminance() { return {0.2126f, 0.7152f, 0.0722f}; }
+MTD bool feature(const JobData &J, uint32_t bit) { return (J.u.scene_feature_flags & bit) != 0u; }
+MTD bool useEnvmap(const JobData &J) { return feature(J, MTC_FEATURE_USE_ENVMAP) && J.s.env != nullptr; }
+MTD bool isSpectral(const JobData &J) { return (J.s.flags & MTC_SCENE_SPECTRAL) != 0u; }
+
+struct Ray { V3 o, d; };
+
+// ------------------------------------------------------------ environment
+// envMap.wgsl.ts:10-31
+MTD float4 textureLinear(const float4 *tex, uint32_t w, uint32_t h, V2 uv) {
+  float ux = uv.x * float(w) - 0.5f, uy = uv.y * float(h) - 0.5f;
+  float fx = floorf(ux), fy = floorf(uy);
+  float tx = ux - fx, ty = uy - fy;
+  int ix = int(fx), iy = int(fy);
+  int x0 = min(max(ix, 0), int(w) - 1), x1 = min(max(ix + 1, 0), int(w) - 1);
+  int y0 = min(max(iy, 0), int(h) - 1), y1 = min(max(iy + 1, 0), int(h) - 1);
+  float4 s1 = ld4(tex + size_t(y0) * w + x0), s2 = ld4(tex + size_t(y0) * w + x1);
+  float4 s3 = ld4(tex + size_t(y1) * w + x0), s4 = ld4(tex + size_t(y1) * w + x1);
+  auto mix4 = [](float4 a, float4 b, float t) {
+    return make_float4(a.x * (1.0f - t) + b.x * t, a.y * (1.0f - t) + b.y * t, a.z * (1.0f - t) + b.z * t,
+                       a.w * (1.0f - t) + b.w * t);
+  };
+  return mix4(mix4(s1, s2, tx), mix4(s3, s4, tx), ty);
+}
+// envMap.wgsl.ts:33-49
+MTD V2 cartesianToEquirect(V3 p) {
+  float phi = atan2f(-p.z, -p.x);
+  if (phi < 0.0f) phi += TWOPI;
+  float theta = acosf(clampf(p.y, -1.0f, 1.0f));
+  return {phi * 0.5f * INVPI, theta * INVPI};
+}
+MTD V3 envRotCol(const JobData &J, int c) {
+  const float *m = J.u.environment_rotation;
+  return {m[c * 4 + 0], m[c * 4 + 1], m[c * 4 + 2]};
+}
+MTD V2 environmentUv(const JobData &J, V3 d) {
+  return cartesianToEquirect({dot(envRotCol(J, 0), d), dot(envRotCol(J, 1), d), dot(envRotCol(J, 2), d)});
+}
+MTD float2 distAt(const JobData &J, int x, int y) { return __ldg(J.s.envDist + size_t(y) * (J.s.envW + 2) + x); }
+// envMap.wgsl.ts:51-99
+MTD float getEnvmapV(const JobData &J, float u, int &vOffset, V2 &pdf) {
+  int left = 0, right = int(J.s.envH) + 1;
+  while (left < right) {
+    int mid = (left + right) >> 1;
+    if (distAt(J, 0, mid).x <= u) left = mid + 1; else right = mid;
+  }
+  vOffset = left - 1;
+  float2 s0 = distAt(J, 0, vOffset), s1 = distAt(J, 0, vOffset + 1);
+  pdf.y = s0.y;
+  return (float(vOffset) + (u - s0.x) / (s1.x - s0.x)) / float(J.s.envH);
+}
+MTD float getEnvmapU(const JobData &J, float u, int vOffset, V2 &pdf) {
+  int left = 0, right = int(J.s.envW) + 1;
+  while (left < right) {
+    int mid = (left + right) >> 1;
+    if (distAt(J, 1 + mid, vOffset).x <= u) left = mid + 1; else right = mid;
+  }
+  int uOffset = left - 1;
+  float2 s0 = distAt(J, 1 + uOffset, vOffset), s1 = distAt(J, 1 + uOffset + 1, vOffset);
+  pdf.x = s0.y;
+  return (float(uOffset) + (u - s0.x) / (s1.x - s0.x)) / float(J.s.envW);
+}
+// envMap.wgsl.ts:103-141
+MTD float envMapSolidAnglePdf(V2 partial, float v) {
+  if (!(v > 0.0f && v < 1.0f)) return 0.0f;
+  float sinTheta = sinf(fminf(v, 1.0f - v) * PI);
+  return partial.x * partial.y * INVPI2 / (2.0f * sinTheta);
+}
+MTD V3 sampleEnvmap(const JobData &J, V2 rnd, V2 &uv, float &pdf) {
+  V2 partial = {0.0f, 0.0f};
+  int vOffset;
+  uv.y = getEnvmapV(J, rnd.x, vOffset, partial);
+  uv.x = getEnvmapU(J, rnd.y, vOffset, partial);
+  float phi = uv.x * TWOPI, theta = uv.y * PI;
+  float st, ct, sp, cp;
+  sincosf(theta, &st, &ct);
+  sincosf(phi, &sp, &cp);
+  V3 dir = {-st * cp, ct, -st * sp};
+  pdf = envMapSolidAnglePdf(partial, uv.y);
+  return envRotCol(J, 0) * dir.x + envRotCol(J, 1) * dir.y + envRotCol(J, 2) * dir.z;
+}
+MTD float envMapPdf(const JobData &J, V2 uv) {
+  int x = int(uv.x * float(J.s.envW)), y = int(uv.y * float(J.s.envH));
+  x = min(max(x, 0), int(J.s.envW) - 1);
+  y = min(max(y, 0), int(J.s.envH) - 1);
+  return envMapSolidAnglePdf({distAt(J, 1 + x, y).y, distAt(J, 0, y).y}, uv.y);
+}
+// background.wgsl.ts:84-99 (no background map)
+MTD float4 sampleSceneBackground(const JobData &J, V3 d) {
+  if (J.u.background_flags & MTC_BACKGROUND_COLOR) {
+    const float *c = J.u.background_color;
+    return make_float4(c[0], c[1], c[2], c[3]);
+  }
+  if (useEnvmap(J)) return textureLinear(J.s.env, J.s.envW, J.s.envH, environmentUv(J, d));
+  return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+MTD V3 spectralFilter(V3 rgb, int channel) {
+  if (channel == 0) return rgb;
+  V3 f = v3(0.0f);
+  setcomp(f, channel - 1, comp(rgb, channel - 1));
+  return f;
+}
+
+// ------------------------------------------------------------------ lights
+struct Light {
+  V3 position; float litType; V3 emission; float area; V3 u; float radiusOrSpread; V3 v; float textureIndex;
+  float selectionPmf;
+};
+MTD Light loadLight(const JobData &J, int i) {
+  const float4 *L = J.s.lights + size_t(i) * MTC_LIGHT_VEC4_ROWS;
+  float4 a = ld4(L), b = ld4(L + 1), c = ld4(L + 2), d = ld4(L + 3), e = ld4(L + 4);
+  return {xyz(a), a.w, xyz(b), b.w, xyz(c), c.w, xyz(d), d.w, e.x};
+}
+struct LightSample {
+  V3 normal, emission, direction;
+  float dist, pdf, selectionPmf;
+  bool isDelta;
+  uint32_t sourceType, sourceIndex;
+};
+MTD LightSample zeroLightSample() {
+  LightSample ls;
+  ls.normal = v3(0.0f); ls.emission = v3(0.0f); ls.direction = v3(0.0f);
+  ls.dist = 0.0f; ls.pdf = 0.0f; ls.selectionPmf = 0.0f; ls.isDelta = false; ls.sourceType = 0; ls.sourceIndex = 0;
+  return ls;
+}
+// intersect.wgsl.ts:894-949
+MTD float intersectSphere(float rad, V3 pos, const Ray &r) {
+  V3 op = pos - r.o;
+  float b = dot(op, r.d);
+  float det = b * b - dot(op, op) + rad * rad;
+  if (det < 0.0f) return INF;
+  det = sqrtf(det);
+  float t1 = b - det;
+  if (t1 > 0.001f) return t1;
+  float t2 = b + det;
+  if (t2 > 0.001f) return t2;
+  return INF;
+}
+MTD float intersectRect(V3 pos, V3 u, V3 v, V3 n, const Ray &r) {
+  float dt = dot(r.d, n);
+  float t = (dot(n, pos) - dot(n, r.o)) / dt;
+  if (t > EPS) {
+    V3 p = r.o + r.d * t;
+    V3 vi = p - pos;
+    float a1 = dot(u / dot(u, u), vi);
+    if (a1 >= 0.0f && a1 <= 1.0f) {
+      float a2 = dot(v / dot(v, v), vi);
+      if (a2 >= 0.0f && a2 <= 1.0f) return t;
+    }
+  }
+  return INF;
+}
+MTD float sphereSolidAnglePdf(V3 origin, V3 center, float radius) {
+  float cd = distance(origin, center);
+  if (cd <= radius) return INV4PI;
+  float s2 = fminf(1.0f, radius * radius / (cd * cd));
+  float ct = sqrtf(fmaxf(0.0f, 1.0f - s2));
+  return 1.0f / fmaxf(TWOPI * (s2 / (1.0f + ct)), 1e-8f);
+}
+MTD float spotEmissionMultiplier(const Light &L, V3 lightToSurface) {
+  float cosTheta = dot(normalize(L.u), lightToSurface);
+  float cone = cosTheta >= L.v.x ? 1.0f : 0.0f;
+  if (L.v.y > L.v.x + 1e-6f) cone = smoothstepf(L.v.x, L.v.y, cosTheta);
+  return cone;
+}
+// intersect.wgsl.ts:976-1131
+MTD float intersectLight(const Ray &r, const Light &L, LightSample &ls) {
+  float d = INF;
+  ls.direction = r.d; ls.normal = -r.d; ls.dist = INF; ls.pdf = 0.0f; ls.emission = v3(0.0f); ls.isDelta = false;
+  V3 u = L.u, v = L.v;
+  int type = int(L.litType);
+  if (type == MTC_LIGHT_RECT) {
+    V3 pos = L.position - u * 0.5f - v * 0.5f;
+    V3 normal = normalize(cross(u, v));
+    if (dot(normal, r.d) > 0.0f) return INF;
+    d = intersectRect(pos, u, v, normal, r);
+    if (d < 0.0f) d = INF;
+    else {
+      float cosTheta = dot(-r.d, normal);
+      if (cosTheta >= cosf(L.radiusOrSpread * PI / 2.0f)) {
+        ls.direction = r.d; ls.normal = normal; ls.dist = d;
+        ls.pdf = (d * d) / (L.area * cosTheta);
+        ls.emission = L.emission; ls.isDelta = false;
+      } else d = INF;
+    }
+  } else if (type == MTC_LIGHT_DISK) {
+    V3 normal = normalize(cross(u, v));
+    if (dot(normal, r.d) >= 0.0f) return INF;
+    d = dot(L.position - r.o, normal) / dot(normal, r.d);
+    V3 hit = r.o + r.d * d - L.position;
+    float radius = fmaxf(length(u), 1e-8f);
+    if (d <= EPS || dot(hit, hit) > radius * radius) return INF;
+    float cosine = dot(-r.d, normal);
+    ls.direction = r.d; ls.normal = normal; ls.dist = d;
+    ls.pdf = d * d / fmaxf(L.area * cosine, 1e-8f);
+    ls.emission = L.emission;
+  } else if (type == MTC_LIGHT_CYLINDER) {
+    V3 axis = normalize(u);
+    float halfLength = 0.5f * length(u);
+    V3 oc = r.o - L.position;
+    V3 rd = r.d - axis * dot(r.d, axis);
+    V3 od = oc - axis * dot(oc, axis);
+    float a = dot(rd, rd), b = dot(od, rd), c = dot(od, od) - L.radiusOrSpread * L.radiusOrSpread;
+    float disc = b * b - a * c;
+    if (a <= 1e-12f || disc < 0.0f) return INF;
+    float root = sqrtf(disc);
+    float nearT = (-b - root) / a, farT = (-b + root) / a;
+    d = nearT > EPS ? nearT : farT;
+    float axial = dot(oc + r.d * d, axis);
+    if (d <= EPS || fabsf(axial) > halfLength) return INF;
+    V3 normal = normalize(r.o + r.d * d - L.position - axis * axial);
+    float cosine = dot(-r.d, normal);
+    if (cosine <= 0.0f) return INF;
+    ls.direction = r.d; ls.normal = normal; ls.dist = d;
+    ls.pdf = d * d / fmaxf(L.area * cosine, 1e-8f);
+    ls.emission = L.emission;
+  } else if (type == MTC_LIGHT_SPHERE || type == MTC_LIGHT_SPOT) {
+    if (L.radiusOrSpread <= 0.0f) {
+      V3 toPoint = L.position - r.o;
+      float proj = dot(toPoint, r.d);
+      V3 perp = toPoint - r.d * proj;
+      if (proj <= EPS || dot(perp, perp) > 1e-8f) return INF;
+      d = proj;
+      ls.direction = r.d; ls.normal = -r.d; ls.dist = d; ls.pdf = 1.0f; ls.isDelta = true;
+    } else {
+      d = intersectSphere(L.radiusOrSpread, L.position, r);
+      ls.isDelta = false;
+      if (type == MTC_LIGHT_SPHERE && d > 0.0f && d != INF) {
+        ls.direction = r.d; ls.dist = d;
+        ls.normal = normalize(r.o + r.d * d - L.position);
+        ls.pdf = sphereSolidAnglePdf(r.o, L.position, L.radiusOrSpread);
+      }
+    }
+    if (type == MTC_LIGHT_SPHERE) {
+      if (d < 0.0f) d = INF;
+      else {
+        ls.direction = r.d; ls.dist = d;
+        ls.emission = L.radiusOrSpread <= 0.0f ? L.emission / fmaxf(d * d, 1e-8f) : L.emission;
+      }
+    } else if (d != INF) {
+      V3 hitPt = r.o + r.d * d;
+      float mult = spotEmissionMultiplier(L, normalize(r.o - hitPt));
+      if (mult <= 0.0f) return INF;
+      if (L.radiusOrSpread > 0.0f) {
+        ls.direction = r.d; ls.dist = d;
+        ls.normal = normalize(r.o + r.d * d - L.position);
+        ls.pdf = sphereSolidAnglePdf(r.o, L.position, L.radiusOrSpread);
+      }
+      ls.emission = L.emission * mult * (L.radiusOrSpread <= 0.0f ? 1.0f / fmaxf(d * d, 1e-8f) : 1.0f);
+    }
+  } else {
+    d = INF;
+  }
+  return d;
+}
+// sampleLight.wgsl.ts:10-87
+MTD void lightSampleSphere(const Light &L, V3 p, V2 rnd, LightSample &ls) {
+  V3 co = L.position - p;
+  float cd = length(co);
+  if (L.radiusOrSpread <= 0.0f) {
+    if (cd <= 1e-6f) {
+      ls.direction = {0, 0, 1}; ls.normal = {0, 0, -1}; ls.dist = 0; ls.pdf = 1; ls.emission = v3(0.0f); ls.isDelta = true;
+      return;
+    }
+    ls.direction = co / cd; ls.normal = -ls.direction; ls.dist = cd; ls.pdf = 1.0f;
+    ls.emission = L.emission / fmaxf(cd * cd, 1e-8f); ls.isDelta = true;
+    return;
+  }
+  float radius = fmaxf(L.radiusOrSpread, 1e-6f);
+  ls.isDelta = false;
+  V3 sd;
+  if (cd <= radius) {
+    float z = 1.0f - 2.0f * rnd.x;
+    float radial = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    float sa, ca;
+    sincosf(TWOPI * rnd.y, &sa, &ca);
+    sd = {radial * ca, radial * sa, z};
+    ls.pdf = INV4PI;
+  } else {
+    V3 axis = co / cd;
+    float s2 = fminf(1.0f, radius * radius / (cd * cd));
+    float ctm = sqrtf(fmaxf(0.0f, 1.0f - s2));
+    float omctm = s2 / (1.0f + ctm);
+    float omct = rnd.x * omctm;
+    float ct = 1.0f - omct;
+    float st = sqrtf(fmaxf(0.0f, omct * (2.0f - omct)));
+    float sa, ca;
+    sincosf(TWOPI * rnd.y, &sa, &ca);
+    V3 t, b;
+    orthonormalBasis(axis, t, b);
+    sd = axis * ct + t * (st * ca) + b * (st * sa);
+    ls.pdf = 1.0f / fmaxf(TWOPI * omctm, 1e-8f);
+  }
+  float cp = dot(sd, co);
+  float disc = cp * cp - dot(co, co) + radius * radius;
+  float nearT = cp - sqrtf(fmaxf(0.0f, disc));
+  float farT = cp + sqrtf(fmaxf(0.0f, disc));
+  ls.dist = nearT > 1e-6f ? nearT : farT;
+  ls.direction = sd;
+  ls.normal = normalize(p + sd * ls.dist - L.position);
+  ls.emission = L.emission;
+}
+// sampleLight.wgsl.ts:108-161 (no light texture)
+MTD void lightSampleRect(const Light &L, V3 p, V2 rnd, LightSample &ls) {
+  V3 normal = normalize(cross(L.u, L.v));
+  V3 lowerLeft = L.position - (L.u + L.v) * 0.5f;
+  float spread = clampf(L.radiusOrSpread, 0.0f, 1.0f);
+  if (spread <= 0.001f) {
+    float pd = dot(normal, p - L.position);
+    V3 rel = p - normal * pd - lowerLeft;
+    float w = length(L.u), h = length(L.v);
+    V2 uv = {dot(rel, L.u / w) / w, dot(rel, L.v / h) / h};
+    if (pd <= 0.0f || uv.x < 0.0f || uv.y < 0.0f || uv.x > 1.0f || uv.y > 1.0f) {
+      ls.emission = v3(0.0f); ls.pdf = 0.0f; return;
+    }
+    ls.direction = -normal; ls.dist = pd; ls.normal = normal; ls.emission = L.emission; ls.pdf = 1.0f; ls.isDelta = true;
+    return;
+  }
+  V3 sp = lowerLeft + L.u * rnd.x + L.v * rnd.y;
+  V3 off = sp - p;
+  float d2 = dot(off, off);
+  ls.dist = sqrtf(d2);
+  ls.direction = off / ls.dist;
+  ls.normal = normal;
+  float ec = dot(-ls.direction, normal);
+  if (ec <= 0.0f || ec < cosf(0.5f * PI * spread)) { ls.emission = v3(0.0f); ls.pdf = 0.0f; return; }
+  ls.emission = L.emission;
+  ls.pdf = d2 / fmaxf(L.area * ec, 1e-8f);
+}
+// sampleLight.wgsl.ts:163-195
+MTD void lightSampleDiskOrCylinder(const Light &L, V3 p, V2 rnd, LightSample &ls, bool cylinder) {
+  V3 sp, normal;
+  if (!cylinder) {
+    float r = sqrtf(rnd.x);
+    float sa, ca;
+    sincosf(TWOPI * rnd.y, &sa, &ca);
+    sp = L.position + L.u * (r * ca) + L.v * (r * sa);
+    normal = normalize(cross(L.u, L.v));
+  } else {
+    V3 axis = normalize(L.u), r0 = normalize(L.v);
+    V3 r1 = normalize(cross(axis, r0));
+    float sa, ca;
+    sincosf(TWOPI * rnd.y, &sa, &ca);
+    normal = r0 * ca + r1 * sa;
+    sp = L.position + L.u * (rnd.x - 0.5f) + normal * L.radiusOrSpread;
+  }
+  V3 off = sp - p;
+  float d2 = dot(off, off);
+  ls.dist = sqrtf(d2);
+  ls.direction = off / fmaxf(ls.dist, 1e-8f);
+  ls.normal = normal;
+  float ec = dot(-ls.direction, normal);
+  if (ec <= 0.0f) { ls.emission = v3(0.0f); ls.pdf = 0.0f; return; }
+  ls.emission = L.emission;
+  ls.pdf = d2 / fmaxf(L.area * ec, 1e-8f);
+}
+// sampleLight.wgsl.ts:197-244
+MTD void sampleAnalyticLight(const Light &L, V3 p, V2 rnd, LightSample &ls) {
+  int type = int(L.litType);
+  if (type == MTC_LIGHT_RECT) { lightSampleRect(L, p, rnd, ls); return; }
+  if (type == MTC_LIGHT_SPHERE) { lightSampleSphere(L, p, rnd, ls); return; }
+  if (type == MTC_LIGHT_SPOT) {
+    lightSampleSphere(L, p, rnd, ls);
+    V3 surf = p + ls.direction * ls.dist;
+    ls.emission *= spotEmissionMultiplier(L, normalize(p - surf));
+    return;
+  }
+  if (type == MTC_LIGHT_DIRECTIONAL) {
+    ls.direction = normalize(-L.u); ls.normal = -ls.direction; ls.emission = L.emission;
+    ls.dist = INF; ls.pdf = 1.0f; ls.isDelta = true;
+    return;
+  }
+  if (type == MTC_LIGHT_DISK) { lightSampleDiskOrCylinder(L, p, rnd, ls, false); return; }
+  if (type == MTC_LIGHT_CYLINDER) lightSampleDiskOrCylinder(L, p, rnd, ls, true);
+}
+// sampleLight.wgsl.ts:319-357
+MTD void sampleEmissiveTriangle(const JobData &J, int index, V3 p, V2 rnd, LightSample &ls) {
+  const float4 *t = J.s.lightData + size_t(index) * 6;
+  float4 a = ld4(t), b = ld4(t + 1), c = ld4(t + 2);
+  V3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(c);
+  float su = sqrtf(rnd.x);
+  V3 bc = {1.0f - su, su * (1.0f - rnd.y), su * rnd.y};
+  V3 lp = p0 * bc.x + p1 * bc.y + p2 * bc.z;
+  V3 normal = normalize(cross(p1 - p0, p2 - p0));
+  ls.direction = lp - p;
+  ls.dist = length(ls.direction);
+  if (ls.dist <= EPS) { ls.emission = v3(0.0f); ls.pdf = 0.0f; return; }
+  ls.direction /= ls.dist;
+  ls.normal = normal;
+  float cl = dot(normal, -ls.direction);
+  if (cl <= 0.0f) { ls.emission = v3(0.0f); ls.pdf = 0.0f; return; }
+  ls.emission = xyz(ld4(J.s.mats + size_t(int(c.w)) * MTC_MATERIAL_VEC4_ROWS + 3));
+  ls.selectionPmf = a.w;
+  ls.pdf = a.w * (ls.dist * ls.dist) / fmaxf(b.w * cl, 1e-8f);
+}
+// sampleLight.wgsl.ts:359-420 sampleLightChoiceTable
+MTD void sampleLightChoiceTable(const JobData &J, V3 p, V3 rnd, LightSample &ls) {
+  ls.emission = v3(0.0f); ls.pdf = 0.0f; ls.selectionPmf = 0.0f; ls.dist = INF; ls.isDelta = false;
+  ls.sourceType = 0; ls.sourceIndex = 0xffffffffu;
+  int count = J.u.light_choice_count;
+  if (count <= 0) return;
+  float scaled = rnd.z * float(count);
+  int column = min(int(scaled), count - 1);
+  float4 cc = ld4(J.s.lightData + J.u.light_choice_texel_offset + column);
+  int selected = fractf(scaled) < cc.x ? column : asi(cc.y);
+  float4 ch = ld4(J.s.lightData + J.u.light_choice_texel_offset + selected);
+  int type = asi(ch.z), src = asi(ch.w);
+  if (useEnvmap(J) && type == MTC_CHOICE_ENVIRONMENT) {
+    ls.sourceType = 0; ls.sourceIndex = uint32_t(src);
+    V2 uv;
+    float pdf;
+    ls.direction = sampleEnvmap(J, {rnd.x, rnd.y}, uv, pdf);
+    ls.pdf = pdf;
+    ls.emission = xyz(textureLinear(J.s.env, J.s.envW, J.s.envH, uv));
+    ls.dist = INF;
+    ls.selectionPmf = J.u.env_light_pmf;
+    ls.pdf *= J.u.env_light_pmf;
+  } else if (type == MTC_CHOICE_ANALYTIC) {
+    ls.sourceType = 2; ls.sourceIndex = uint32_t(src);
+    Light L = loadLight(J, src);
+    sampleAnalyticLight(L, p, {rnd.x, rnd.y}, ls);
+    ls.selectionPmf = L.selectionPmf;
+    ls.pdf *= L.selectionPmf;
+  } else if (type == MTC_CHOICE_EMISSIVE_TRIANGLE) {
+    ls.sourceType = 1; ls.sourceIndex = uint32_t(src);
+    sampleEmissiveTriangle(J, src, p, {rnd.x, rnd.y}, ls);
+  }
+}
+
+// --------------------------------------------------------------- material
+// materialBuffer.wgsl.ts:170-257 getMaterial (no texture maps)
+MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, Material &m) {
+  // A miss keeps the previous hit's indices (zero before the first hit);
+  // clamp so an empty or single-material scene never reads past its buffers.
+  if (materialIndex < 0 || uint32_t(materialIndex) >= J.s.matCount) materialIndex = 0;
+  if (uint32_t(max(instanceIndex, 0)) >= J.s.insCount) instanceIndex = -1;
+  const float4 *d = J.s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  float4 r0 = ld4(d), r1 = ld4(d + 1), r2 = ld4(d + 2), r3 = ld4(d + 3), r4 = ld4(d + 4), r5 = ld4(d + 5);
+  float4 r9 = ld4(d + 9), r10 = ld4(d + 10), r11 = ld4(d + 11), r12 = ld4(d + 12), r14 = ld4(d + 14);
+  float4 r15 = ld4(d + 15), r16 = ld4(d + 16), r17 = ld4(d + 17), r18 = ld4(d + 18), r20 = ld4(d + 20);
+  float4 r21 = ld4(d + 21), r22 = ld4(d + 22), r23 = ld4(d + 23), r24 = ld4(d + 24), r25 = ld4(d + 25);
+  m.baseColor = xyz(r0);
+  m.materialType = int(r0.w);
+  m.specularRoughness = r1.x;
+  m.baseMetalness = r2.x;
+  m.specularAnisotropy = clampf(r2.y, 0.0f, 1.0f);
+  m.emission = xyz(r3);
+  m.inside = false;
+  m.specularIor = r4.x;
+  m.transmissionWeight = r4.y;
+  m.thinWalled = r4.w > 0.5f;
+  m.bevel = r5.x;
+  m.transmissionDispersionScale = r5.y;
+  m.dispersionAbbeNumber = fmaxf(r18.y, 1e-6f);
+  m.mediumExtinction = vmax(xyz(r20), v3(0.0f));
+  m.mediumScattering = vmax(xyz(r21), v3(0.0f));
+  m.mediumAnisotropy = clampf(r20.w, -1.0f, 1.0f);
+  m.mediumType = maxc(m.mediumExtinction) > 0.0f ? 1 : 0;
+  m.alpha = r9.x;
+  m.alphaMode = int(r23.w);
+  m.thinFilmThickness = r5.z * 1000.0f;
+  m.thinFilmIor = r9.z;
+  m.thinFilmWeight = feature(J, MTC_FEATURE_HAS_THIN_FILM) ? clampf(r18.x, 0.0f, 1.0f) : 0.0f;
+  m.baseWeight = clampf(r10.x, 0.0f, 1.0f);
+  m.diffuseRoughness = clampf(r10.y, 0.0f, 1.0f);
+  m.specularWeight = fmaxf(r10.z, 0.0f);
+  m.specularColor = vmax(xyz(r11), v3(0.0f));
+  m.subsurfaceWeight = feature(J, MTC_FEATURE_HAS_SUBSURFACE) ? clampf(r10.w, 0.0f, 1.0f) : 0.0f;
+  m.subsurfaceColor = vmax(xyz(r14), v3(0.0f));
+  m.transmissionColor = vmax(xyz(r12), v3(0.0f));
+  m.fuzzWeight = feature(J, MTC_FEATURE_HAS_FUZZ) ? clampf(r11.w, 0.0f, 1.0f) : 0.0f;
+  m.fuzzColor = vmax(xyz(r15), v3(0.0f));
+  m.fuzzRoughness = clampf(r15.w, 0.0f, 1.0f);
+  m.coatWeight = feature(J, MTC_FEATURE_HAS_COAT) ? clampf(r16.w, 0.0f, 1.0f) : 0.0f;
+  m.coatColor = vmax(xyz(r16), v3(0.0f));
+  m.coatRoughness = clampf(r17.x, ROUGHNESS_MIN, 1.0f);
+  m.coatAnisotropy = clampf(r17.y, 0.0f, 1.0f);
+  m.coatIor = fmaxf(r17.z, 1.0f);
+  m.coatDarkening = clampf(r17.w, 0.0f, 1.0f);
+  if (m.alphaMode == 0) m.alpha = 1.0f;
+  else if (m.alphaMode == 1) m.alpha = m.alpha >= r22.w ? 1.0f : 0.0f;
+  m.anisotropyDirection = {1.0f, 0.0f};
+  m.anisotropyDirectionEnabled = r24.y != 0.0f;
+  m.coatAnisotropyRotation = r25.x;
+  if (r25.y > 0.5f && m.specularAnisotropy > 0.0f) {
+    float roughness = clampf(m.specularRoughness, 0.0f, 1.0f), strength = m.specularAnisotropy;
+    float u = roughness * roughness;
+    float a = u + (1.0f - u) * strength * strength;
+    if (a == 0.0f) { m.specularRoughness = 0.0f; m.specularAnisotropy = 0.0f; }
+    else {
+      m.specularRoughness = powf((a * a + u * u) * 0.5f, 0.25f);
+      m.specularAnisotropy = clampf(1.0f - u / a, 0.0f, 1.0f);
+    }
+  }
+  if (m.anisotropyDirectionEnabled) {
+    float st, ct;
+    sincosf(r24.y, &st, &ct);
+    V2 dd = m.anisotropyDirection;
+    m.anisotropyDirection = {ct * dd.x - st * dd.y, st * dd.x + ct * dd.y};
+  }
+  if (m.coatWeight > 0.0f && m.coatRoughness > 0.0f) {
+    float br2 = m.specularRoughness * m.specularRoughness;
+    float cr2 = m.coatRoughness * m.coatRoughness;
+    m.specularRoughness = mixf(m.specularRoughness, powf(fminf(1.0f, br2 * br2 + 2.0f * cr2 * cr2), 0.25f), m.coatWeight);
+  }
+  V3 color = v3(1.0f);
+  if (instanceIndex >= 0) color = xyz(ld4(J.s.ins + size_t(instanceIndex) * MTC_INSTANCE_VEC4_STRIDE + 9));
+  m.baseColor *= color;
+  if (m.materialType == 2) m.emission *= color;
+  m.specularRoughness = clampf(m.specularRoughness, ROUGHNESS_MIN, 1.0f);
+  m.baseMetalness = clampf(m.baseMetalness, 0.0f, 1.0f);
+  V2 a = roughnessToAlpha(m.specularRoughness, m.specularAnisotropy);
+  m.alphaX = a.x;
+  m.alphaY = a.y;
+  m.directionTangent = v3(0.0f); m.directionBitangent = v3(0.0f);
+  m.geometryTangent = v3(0.0f); m.geometryBitangent = v3(0.0f);
+  m.relativeIor = 0.0f;
+}
+
+// ------------------------------------------------------------- surface hit
+struct SurfaceInteraction {
+  V3 position; bool albedoSampled;
+  V3 normal, vertexNormal, shadowOffset, faceNormal; bool hit;
+  int32_t triangleIndex, instanceIndex, materialIndex;
+  float wavelength; int32_t spectralChannel;
+  int32_t mediumType; V3 mediumExtinction, mediumScattering; float mediumAnisotropy;
+};
+
+// fetchAttributes + completeSurfaceInteraction (intersect.wgsl.ts:1233-1419,
+// 1539-1601) for compact vertices without UV/tangent words.
+MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, const TraversalHit &h, V3 rayO, V3 rayD) {
+  const DevScene &s = J.s;
+  const float4 *insv = s.ins + size_t(h.insIdx) * MTC_INSTANCE_VEC4_STRIDE;
+  float4 insData = ld4(insv);
+  float4 w0 = ld4(insv + 1), w1 = ld4(insv + 2), w2 = ld4(insv + 3), w3 = ld4(insv + 4);
+  float4 l0 = ld4(insv + 5), l1 = ld4(insv + 6), l2 = ld4(insv + 7), l3 = ld4(insv + 8);
+  V3 o = xmat4(w0, w1, w2, w3, rayO, 1.0f);
+  V3 d = xmat4(w0, w1, w2, w3, rayD, 0.0f);
+  V3 position = o + d * h.tMax;
+  si.instanceIndex = h.insIdx;
+  si.materialIndex = asi(insData.z) >> 8;
+  si.hit = true;
+  int32_t vertexOffset = asi(insData.y);
+  float4 rec = ld4(s.bvh + h.triangleIndex);
+  int32_t i0 = asi(rec.x) + vertexOffset, i1 = asi(rec.y) + vertexOffset, i2 = asi(rec.z) + vertexOffset;
+  V3 p0 = vertexPosition(s, i0), p1 = vertexPosition(s, i1), p2 = vertexPosition(s, i2);
+  V3 n0 = vertexNormal(s, i0), n1 = vertexNormal(s, i1), n2 = vertexNormal(s, i2);
+  V3 bary = h.hitBary;
+  V3 smoothNormal = n0 * bary.x + n1 * bary.y + n2 * bary.z;
+  V3 normal = normalize(smoothNormal);
+  // Cycles shadow-terminator offset (intersect.wgsl.ts:1376-1407).
+  V3 geometricNormal = normalize(cross(p1 - p0, p2 - p0));
+  float a = dot(n2 - n0, p0 - p2);
+  float b = dot(n2 - n1, p1 - p2);
+  float c = dot(n1 - n0, p1 - p0);
+  float hh = a * bary.x * (bary.x - 1.0f) + (a + b + c) * bary.x * bary.y + b * bary.y * (bary.y - 1.0f);
+  if (dot(smoothNormal, geometricNormal) > 0.0f) {
+    float h0 = fmaxf(fmaxf(dot(p1 - p0, n0), dot(p2 - p0, n0)), 0.0f);
+    float h1 = fmaxf(fmaxf(dot(p0 - p1, n1), dot(p2 - p1, n1)), 0.0f);
+    float h2 = fmaxf(fmaxf(dot(p0 - p2, n2), dot(p1 - p2, n2)), 0.0f);
+    h0 = fmaxf(dot(p0 - position, n0) + h0, 0.0f);
+    h1 = fmaxf(dot(p1 - position, n1) + h1, 0.0f);
+    h2 = fmaxf(dot(p2 - position, n2) + h2, 0.0f);
+    hh = fmaxf(fminf(fminf(h0, h1), h2), hh * 0.5f);
+  } else {
+    float h0 = fmaxf(fmaxf(dot(p0 - p1, n0), dot(p0 - p2, n0)), 0.0f);
+    float h1 = fmaxf(fmaxf(dot(p1 - p0, n1), dot(p1 - p2, n1)), 0.0f);
+    float h2 = fmaxf(fmaxf(dot(p2 - p0, n2), dot(p2 - p1, n2)), 0.0f);
+    h0 = fmaxf(dot(position - p0, n0) + h0, 0.0f);
+    h1 = fmaxf(dot(position - p1, n1) + h1, 0.0f);
+    h2 = fmaxf(dot(position - p2, n2) + h2, 0.0f);
+    hh = fminf(-fminf(fminf(h0, h1), h2), hh * 0.5f);
+  }
+  V3 shadowOffset = smoothNormal * hh;
+  auto nt = [&](V3 v) { return V3{dot(xyz(w0), v), dot(xyz(w1), v), dot(xyz(w2), v)}; };
+  si.faceNormal = normalize(nt(h.hitNormal));
+  si.normal = normalize(nt(normal));
+  si.vertexNormal = si.normal;
+  si.shadowOffset = mat4v(l0, l1, l2, l3, shadowOffset, 0.0f);
+  si.position = mat4v(l0, l1, l2, l3, position, 1.0f);
+}
+
+// intersect.wgsl.ts:696-740
+MTD bool intersectScene(const JobData &J, const Ray &r, SurfaceInteraction &si, int bounces, bool doubleSided,
+                        Counters &cnt) {
+  si.hit = false;
+  if (J.u.is_empty > 0) return false;
+  cnt.ext++;
+  TraversalHit h;
+  h.tMax = RAY_MAX_DISTANCE;
+  h.triangleIndex = -1;
+  h.insIdx = -1;
+  traverse<false>(J.s, J.u.blas_offset, r.o, r.d, bounces, doubleSided, si.triangleIndex, si.instanceIndex, h);
+  if (h.insIdx >= 0) {
+    si.triangleIndex = h.triangleIndex;
+    completeSurfaceInteraction(J, si, h, r.o, r.d);
+  }
+  return si.hit;
+}
+// intersect.wgsl.ts:829-879
+MTD bool intersectSceneShadow(const JobData &J, const Ray &r, float lightDistance, int32_t tri, int32_t ins,
+                              Counters &cnt) {
+  if (J.u.is_empty > 0) return false;
+  cnt.shadow++;
+  TraversalHit h;
+  h.tMax = fminf(fmaxf(lightDistance, 0.0f), RAY_MAX_DISTANCE);
+  return traverse<true>(J.s, J.u.blas_offset, r.o, r.d, 1, true, tri, ins, h);
+}
+
+// ------------------------------------------------------------- integrator
+struct Path {
+  bool scatteringMediumEntered;
+  Ray ray;
+  V3 li; float alpha; V3 beta;
+  bool fromEye, abort;
+  float scatteringPdf; bool scatteringIsDelta, isNextRefraction;
+};
+struct Aux { V3 albedo; V3 normal; bool isBlank; };
+
+struct Ctx {
+  const JobData &J;
+  Sampler smp;
+  BsdfContext bc;
+  Counters cnt;
+  MTD uint32_t candidateCount() const { return uint32_t(max(J.u.direct_light_candidates, 1)); }
+};
+
+// rayTrace.compute.ts:264-284
+MTD float neeMISWeight(const Ctx &c, float lightPdf, float scatteringPdf) {
+  uint32_t n = c.candidateCount();
+  if (n <= 1u) return powerHeuristic(lightPdf, scatteringPdf);
+  float w = float(n) * lightPdf;
+  return w / fmaxf(w + scatteringPdf, 1e-20f);
+}
+MTD float bsdfMISWeight(const Ctx &c, float scatteringPdf, float lightPdf) {
+  uint32_t n = c.candidateCount();
+  if (n <= 1u) return powerHeuristic(scatteringPdf, lightPdf);
+  float w = float(n) * lightPdf;
+  return scatteringPdf / fmaxf(scatteringPdf + w, 1e-20f);
+}
+// common.wgsl.ts:14-20
+MTD V3 offsetSurfaceRay(V3 p, V3 gn, V3 dir) {
+  V3 n = dot(gn, dir) >= 0.0f ? gn : -gn;
+  V3 r;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float pc = comp(p, k), nc = comp(n, k);
+    int io = int(256.0f * nc);
+    int sh = __float_as_int(pc) + (pc < 0.0f ? -io : io);
+    setcomp(r, k, fabsf(pc) < 1.0f / 32.0f ? pc + nc / 65536.0f : __int_as_float(sh));
+  }
+  return r;
+}
+// rayTrace.compute.ts:592-600
+MTD Ray initCameraRay(const JobData &J, V2 coord) {
+  const float *m = J.cam.view_projection_inv;
+  float x = coord.x * 2.0f - 1.0f, y = coord.y * 2.0f - 1.0f;
+  float ox = m[0] * x + m[4] * y + m[8] * -1.0f + m[12];
+  float oy = m[1] * x + m[5] * y + m[9] * -1.0f + m[13];
+  float oz = m[2] * x + m[6] * y + m[10] * -1.0f + m[14];
+  float ow = m[3] * x + m[7] * y + m[11] * -1.0f + m[15];
+  float cx = m[0] * x + m[4] * y + m[8] + m[12];
+  float cy = m[1] * x + m[5] * y + m[9] + m[13];
+  float cz = m[2] * x + m[6] * y + m[10] + m[14];
+  float cw = m[3] * x + m[7] * y + m[11] + m[15];
+  Ray r;
+  r.o = {ox / ow, oy / ow, oz / ow};
+  r.d = normalize(V3{cx * ow - ox * cw, cy * ow - oy * cw, cz * ow - oz * cw});
+  return r;
+}
+MTD V3 cameraEye(const JobData &J) { return {J.cam.view_inv[12], J.cam.view_inv[13], J.cam.view_inv[14]}; }
+
+struct ShadowWork {
+  Ray ray; float maxDistance; int32_t triangleIndex; V3 contribution;
+  float risTarget, lightSelectionPmf; bool valid;
+};
+// sampleMaterial.wgsl.ts:32-151
+MTD bool finishDirectLight(Ctx &c, const SurfaceInteraction &si, Path &path, V3 ffnormal, bool isSurface,
+                           const LightSample &ls, V3 f, float scatteringPdf, ShadowWork &w) {
+  w.valid = false; w.lightSelectionPmf = 0.0f; w.risTarget = 0.0f;
+  V3 Li = ls.emission;
+  V3 lightDir = ls.direction;
+  float lightPdf = ls.pdf, lsp = ls.selectionPmf;
+  float cosThetaL = dot(ffnormal, lightDir);
+  if (lightPdf <= 0.0f || lsp <= 0.0f || maxc(Li) <= 0.0f) return false;
+  if (scatteringPdf <= 0.0f || maxc(f) <= 0.0f) return false;
+  V3 shadowOrigin = si.position + lightDir * EPS;
+  if (isSurface) {
+    shadowOrigin = offsetSurfaceRay(si.position, si.faceNormal, lightDir);
+    const float cutoff = 0.1f;
+    float nl = dot(si.normal, lightDir);
+    V3 gn = nl < 0.0f ? -si.faceNormal : si.faceNormal;
+    nl = fabsf(nl);
+    float gl = dot(gn, lightDir);
+    float off = nl < cutoff ? clampf(2.0f - (gl + nl) / cutoff, 0.0f, 1.0f) : clampf(1.0f - gl / cutoff, 0.0f, 1.0f);
+    shadowOrigin += si.shadowOffset * off;
+  }
+  V3 visDir = lightDir;
+  float visDist = ls.dist - EPS;
+  if (ls.sourceType == 1u) {
+    V3 to = si.position + ls.direction * ls.dist + ls.normal * EPS - shadowOrigin;
+    visDist = length(to);
+    visDir = normalize(to);
+  }
+  if (isSurface && cosThetaL < 0.0f && ls.sourceType == 0u) {
+    float4 bg = sampleSceneBackground(c.J, visDir);
+    Li = V3{bg.x, bg.y, bg.z} * bg.w;
+  }
+  if (isSpectral(c.J)) Li = spectralFilter(Li, si.spectralChannel);
+  float mis = ls.isDelta ? 1.0f : neeMISWeight(c, lightPdf, scatteringPdf);
+  if (mis > 0.0f) {
+    V3 un = Li * f / lightPdf * path.beta;
+    w.risTarget = fmaxf(dot(vmax(un * lsp, v3(0.0f)), kLuminance()), 0.0f);
+    w.ray = {shadowOrigin, visDir};
+    w.maxDistance = visDist;
+    w.triangleIndex = si.triangleIndex;
+    w.contribution = un * mis;
+    w.lightSelectionPmf = lsp;
+    w.valid = true;
+    return true;
+  }
+  return false;
+}
+
+struct Scattering { V3 direction, response; float pdf; bool transmission; };
+
+MTD bool isDiscrete(const Prepared &p) {
+  return !p.material.thinWalled && fabsf(p.material.relativeIor - 1.0f) <= 1e-6f &&
+         p.probabilities[LOBE_TRANSMISSION] >= 1.0f - 1e-6f;
+}
+
+// sampleMaterial.wgsl.ts:160-277
+MTD Scattering sampleScattering(Ctx &c, SurfaceInteraction &si, const Material &ma, const Prepared &prepared,
+                                Path &path, V3 ffnormal, bool isSurface) {
+  uint32_t count = c.candidateCount();
+  ShadowWork selected;
+  selected.valid = false;
+  float selectedTarget = 0.0f, scalarWeightSum = 0.0f;
+  Scattering result = {v3(0.0f), v3(0.0f), 0.0f, false};
+  for (uint32_t event = 0; event <= count; event++) {
+    bool continuation = event == count;
+    LightSample ls = zeroLightSample();
+    V3 lightDir = v3(0.0f);
+    float scatteringPdf = 0.0f;
+    V3 response = v3(0.0f);
+    bool discrete = false;
+    if (continuation) {
+      float ucw = 1.0f;
+      bool valid = selected.valid;
+      if (count > 1u) {
+        valid = valid && selectedTarget > 0.0f;
+        if (valid) ucw = selected.lightSelectionPmf * scalarWeightSum / (float(count) * selectedTarget);
+      }
+      if (valid && !intersectSceneShadow(c.J, selected.ray, selected.maxDistance, selected.triangleIndex,
+                                         si.instanceIndex, c.cnt))
+        path.li += selected.contribution * ucw;
+      if (!isSurface) {
+        result.direction = henyeyGreenstein(-path.ray.d, si.mediumAnisotropy, c.smp.s2(c.smp.bounceDim(6)));
+        result.pdf = henyeyGreensteinPhase(dot(result.direction, -path.ray.d), si.mediumAnisotropy);
+        return result;
+      }
+      V2 dr = c.smp.s2(c.smp.bounceDim(3));
+      float lobe = c.smp.s1(c.smp.bounceDim(2));
+      discrete = isDiscrete(prepared);
+      if (discrete) {
+        lightDir = toWorld(prepared.basis, -prepared.viewLocal);
+        response = transmissionTint(c.bc, prepared.material) * coatBaseScale(c.bc, prepared, -prepared.viewLocal.z);
+        scatteringPdf = 1.0f;
+        result.transmission = true;
+      } else {
+        bool transmission = false;
+        if (!sampleDirection(c.bc, prepared, {dr.x, dr.y, lobe}, lightDir, transmission)) return result;
+        result.transmission = transmission;
+      }
+    } else {
+      V2 lr = c.smp.s2(c.smp.lightDim(event, 1u));
+      float lz = c.smp.s1(c.smp.lightDim(event, 0u));
+      V3 rnd = {lr.x, lr.y, (lz + float(min(event, count - 1u))) / float(max(count, 1u))};
+      sampleLightChoiceTable(c.J, si.position, rnd, ls);
+      lightDir = ls.direction;
+      if (ls.pdf <= 0.0f || ls.selectionPmf <= 0.0f || maxc(ls.emission) <= 0.0f) continue;
+      float cosThetaL = dot(ffnormal, lightDir);
+      if (isSurface && cosThetaL <= 0.0f && ma.transmissionWeight <= 0.0f && ma.subsurfaceWeight <= 0.0f) continue;
+    }
+    if (!discrete) {
+      if (isSurface) response = evalPrepared(c.bc, prepared, lightDir, scatteringPdf);
+      else {
+        scatteringPdf = henyeyGreensteinPhase(dot(-path.ray.d, lightDir), si.mediumAnisotropy);
+        response = v3(scatteringPdf);
+      }
+    }
+    if (continuation) {
+      result.direction = lightDir; result.response = response; result.pdf = scatteringPdf;
+      return result;
+    }
+    ShadowWork cand;
+    if (!finishDirectLight(c, si, path, ffnormal, isSurface, ls, response, scatteringPdf, cand)) continue;
+    if (count == 1u) { selected = cand; continue; }
+    float sw = cand.risTarget / fmaxf(cand.lightSelectionPmf, 1e-20f);
+    if (!(sw > 0.0f) || sw != sw) continue;
+    scalarWeightSum += sw;
+    if (!selected.valid || c.smp.lightCandidateRandom(event) * scalarWeightSum <= sw) {
+      selected = cand;
+      selectedTarget = cand.risTarget;
+    }
+  }
+  return result;
+}
+
+// sampleMaterial.wgsl.ts:279-303
+MTD float emissiveHitMisWeight(Ctx &c, const SurfaceInteraction &si, const Path &path, float4 row0, float4 row3,
+                               float doubleSided) {
+  float cosLight = dot(si.faceNormal, -path.ray.d);
+  if (cosLight <= 0.0f && doubleSided < 0.5f) return 0.0f;
+  if (path.fromEye || c.J.u.light_weight_total <= 0.0f || int(row0.w) == 2) return 1.0f;
+  float lum = dot(xyz(row3), kLuminance());
+  if (lum <= 0.0f || cosLight <= 0.0f) return 1.0f;
+  float hd = distance(si.position, path.ray.o);
+  float lightPdf = lum / c.J.u.light_weight_total * hd * hd / fmaxf(cosLight, 1e-8f);
+  return bsdfMISWeight(c, path.scatteringPdf, lightPdf);
+}
+
+// sampleMaterial.wgsl.ts:316-508
+MTD void sampleMaterial(Ctx &c, SurfaceInteraction &si, Material &ma, Path &path) {
+  const bool hasMedium = (c.J.s.flags & MTC_SCENE_HAS_MEDIUM) != 0u;
+  float ndv1 = -dot(si.faceNormal, path.ray.d);
+  float ndv2 = -dot(si.normal, path.ray.d);
+  if ((ma.transmissionWeight > 0.0f || ma.subsurfaceWeight > 0.0f) && ma.thinWalled) {
+    if (ndv1 < 0.0f) { si.faceNormal = -si.faceNormal; ndv1 = -ndv1; }
+    if (ndv2 < 0.0f) { si.normal = -si.normal; ndv2 = -ndv2; }
+  }
+  bool useFaceN = ndv1 >= 0.0f && ndv2 < 0.0f;
+  float ndv = useFaceN ? ndv1 : ndv2;
+  V3 N = useFaceN ? si.faceNormal : si.normal;
+  ma.inside = ndv <= 0.0f && !ma.thinWalled;
+  ma.relativeIor = ndv > 0.0f ? 1.0f / ma.specularIor : ma.specularIor;
+  V3 ffnormal = ndv >= 0.0f ? N : -N;
+  path.scatteringIsDelta = false;
+  bool mediumSampled = false, crossedBoundary = false;
+  if (hasMedium) {
+    float d = distance(si.position, path.ray.o);
+    V3 segmentOrigin = path.ray.o;
+    V3 ext = si.mediumExtinction;
+    V3 scat = vmin(si.mediumScattering, ext);
+    float majorant = maxc(ext);
+    if (si.mediumType > 0 && majorant > 0.0f) {
+      int ch = min(int(c.smp.s1(c.smp.bounceDim(4)) * 3.0f), 2);
+      float ce = comp(ext, ch);
+      float sd = ce > 0.0f ? fminf(-logf(fmaxf(c.smp.s1(c.smp.bounceDim(5)), 1e-7f)) / ce, d) : d;
+      mediumSampled = sd < d;
+      V3 T = {expf(-ext.x * sd), expf(-ext.y * sd), expf(-ext.z * sd)};
+      V3 density = mediumSampled ? ext * T : T;
+      float mp = fmaxf((density.x + density.y + density.z) / 3.0f, 1e-8f);
+      if (mediumSampled) {
+        path.beta *= T * scat / mp;
+        if (path.beta.x == 0.0f && path.beta.y == 0.0f && path.beta.z == 0.0f) { path.abort = true; return; }
+        path.ray.o = segmentOrigin + path.ray.d * sd;
+        si.position = path.ray.o;
+        si.triangleIndex = -1;
+        si.instanceIndex = -1;
+      } else {
+        path.beta *= T / mp;
+        if (path.beta.x == 0.0f && path.beta.y == 0.0f && path.beta.z == 0.0f) { path.abort = true; return; }
+      }
+    }
+  }
+  if (!mediumSampled) {
+    int mi = uint32_t(si.materialIndex) < c.J.s.matCount ? si.materialIndex : 0;
+    const float4 *md = c.J.s.mats + size_t(mi) * MTC_MATERIAL_VEC4_ROWS;
+    V3 se = ma.emission;
+    if (se.x != 0.0f || se.y != 0.0f || se.z != 0.0f) {
+      if (isSpectral(c.J)) se = spectralFilter(se, si.spectralChannel);
+      float w = emissiveHitMisWeight(c, si, path, ld4(md), ld4(md + 3), ld4(md + 23).z);
+      path.li += se * w * path.beta;
+    }
+  }
+  if (ma.materialType == 2) { path.abort = true; return; }
+  Prepared prepared;
+  if (!mediumSampled) prepared = prepare(c.bc, v3(0.0f), ma, -path.ray.d, ffnormal);
+  else prepared = Prepared{};
+  Scattering sc = sampleScattering(c, si, ma, prepared, path, ffnormal, !mediumSampled);
+  V3 scatterDir = sc.direction;
+  float scatteringPdf = sc.pdf;
+  if (!mediumSampled) {
+    V3 f = sc.response;
+    bool nextRefraction = sc.transmission;
+    bool finite = f.x == f.x && f.y == f.y && f.z == f.z && fabsf(f.x) < 3.402823e38f &&
+                  fabsf(f.y) < 3.402823e38f && fabsf(f.z) < 3.402823e38f;
+    if (!(scatteringPdf > 0.0f) || !finite || dot(scatterDir, scatterDir) < 0.5f) {
+      path.scatteringPdf = 0.0f;
+      path.abort = true;
+      return;
+    }
+    path.scatteringIsDelta = isDiscrete(prepared);
+    path.beta *= f / scatteringPdf;
+    if (path.beta.x == 0.0f && path.beta.y == 0.0f && path.beta.z == 0.0f) { path.abort = true; return; }
+    crossedBoundary = nextRefraction && !ma.thinWalled;
+    path.isNextRefraction = nextRefraction;
+    path.ray.o = si.position + scatterDir * EPS;
+  }
+  path.scatteringPdf = scatteringPdf;
+  path.ray.d = scatterDir;
+  if (mediumSampled) path.isNextRefraction = false;
+  path.fromEye = false;
+  if (hasMedium && !mediumSampled && crossedBoundary && ma.mediumType > 0) {
+    if (ndv1 >= 0.0f) {
+      si.mediumType = ma.mediumType;
+      si.mediumExtinction = ma.mediumExtinction;
+      si.mediumScattering = ma.mediumScattering;
+      path.scatteringMediumEntered = path.scatteringMediumEntered || ma.mediumScattering.x > 0.0f ||
+                                     ma.mediumScattering.y > 0.0f || ma.mediumScattering.z > 0.0f;
+      si.mediumAnisotropy = ma.mediumAnisotropy;
+    } else {
+      si.mediumType = 0;
+      si.mediumExtinction = v3(0.0f);
+      si.mediumScattering = v3(0.0f);
+      si.mediumAnisotropy = 0.0f;
+    }
+  }
+}
+
+// rayTrace.compute.ts:341-512 shadeVertex (no shadow catcher, no bevel)
+MTD void shadeVertex(Ctx &c, V2 uv, Path &path, int &depth, SurfaceInteraction &si, Material &ma, Aux &aux,
+                     bool &sampleIgnored) {
+  sampleIgnored = false;
+  c.smp.bounce = uint32_t(max(depth, 0));
+  int matType = ma.materialType;
+  const mtc_trace_uniform &u = c.J.u;
+  if (!si.hit) {
+    float4 bg = sampleSceneBackground(c.J, path.ray.d);
+    if (isSpectral(c.J)) {
+      V3 f = spectralFilter({bg.x, bg.y, bg.z}, si.spectralChannel);
+      bg = make_float4(f.x, f.y, f.z, bg.w);
+    }
+    if (path.fromEye) {
+      path.li = path.beta * V3{bg.x, bg.y, bg.z} * bg.w;
+      path.alpha = bg.w;
+      aux.isBlank = bg.w < 0.001f || ((u.background_flags & MTC_BACKGROUND_COLOR) && !(u.background_flags & MTC_BACKGROUND_MAP));
+    } else {
+      Ray cam = initCameraRay(c.J, uv);
+      bool towardsCam = dot(cam.d, path.ray.d) > 0.0f;
+      if (u.transmissive_output_alpha_min < 1.0f) {
+        if (towardsCam) path.alpha = fmaxf(path.alpha, bg.w); else path.alpha = 1.0f;
+      }
+      if (!useEnvmap(c.J) && towardsCam)
+        path.li += path.beta * bsdfMISWeight(c, path.scatteringPdf, 1.0f) * V3{bg.x, bg.y, bg.z};
+    }
+    path.abort = true;
+    return;
+  }
+  if (matType == 0 || matType == 2) {
+    float alpha = clampf(ma.alpha, 0.0f, 1.0f);
+    if (alpha < 1.0f) {
+      if (alpha <= 0.0f || c.smp.hashedSample(3u) > alpha) sampleIgnored = true;
+    }
+    if (!sampleIgnored && u.transmissive_output_alpha_min < 1.0f) {
+      float oa = fmaxf(1.0f - ma.transmissionWeight, 1.0f - powf(1.0f - u.transmissive_output_alpha_min, float(depth)));
+      path.alpha = fmaxf(oa, path.alpha);
+    }
+    if (!sampleIgnored) sampleMaterial(c, si, ma, path);
+    else path.ray.o = si.position + path.ray.d * EPS;
+  }
+  if (!si.albedoSampled && !sampleIgnored) {
+    if (matType == 0 || matType == 2) {
+      if (!(ma.transmissionWeight > 0.5f || (ma.specularRoughness <= 0.02f && ma.baseMetalness > 0.98f))) {
+        aux.albedo = ma.baseColor;
+        aux.normal = dot(si.normal, si.position - cameraEye(c.J)) > 0.0f ? -si.normal : si.normal;
+        si.albedoSampled = true;
+      }
+      if (depth > 4) si.albedoSampled = true;
+    }
+  }
+  if (depth >= (path.scatteringMediumEntered ? 12 : 2) && !sampleIgnored) {
+    float q = fmaxf(0.0f, 1.0f - maxc(path.beta));
+    if (c.smp.s1(c.smp.bounceDim(7)) < q) { path.alpha = 1.0f; path.abort = true; }
+    else path.beta /= 1.0f - q;
+  }
+}
+
+// rayTrace.compute.ts:514-589 completeVertex
+MTD void completeVertex(Ctx &c, Path &path, int &depth, SurfaceInteraction &si, Material &ma, bool sampleIgnored) {
+  const bool spectral = isSpectral(c.J);
+  if (spectral && ma.transmissionWeight > 0.001f)
+    ma.specularIor = cauchyIor(si.wavelength, ma.specularIor, ma.transmissionDispersionScale, ma.dispersionAbbeNumber);
+  if (sampleIgnored) return;
+  bool isAlphaOccluded = ma.alpha >= 1.0f ? (c.smp.hashed += 1u, true) : c.smp.hashedSample(3u) < ma.alpha;
+  for (int i = 0; i < c.J.u.lights_count; i++) {
+    Light L = loadLight(c.J, i);
+    LightSample ls = zeroLightSample();
+    float d = intersectLight(path.ray, L, ls);
+    ls.pdf *= L.selectionPmf;
+    bool occluded = si.hit && d > distance(si.position, path.ray.o);
+    if (d != INF && !(occluded && isAlphaOccluded)) {
+      float mis = bsdfMISWeight(c, path.scatteringPdf, ls.pdf);
+      if (spectral) ls.emission = spectralFilter(ls.emission, si.spectralChannel);
+      path.li += path.beta * ls.emission * mis;
+      path.alpha = 1.0f;
+      path.abort = true;
+    }
+  }
+  if (useEnvmap(c.J) && !(si.hit && isAlphaOccluded)) {
+    if (path.isNextRefraction) {
+      float4 bg = sampleSceneBackground(c.J, path.ray.d);
+      V3 rgb = {bg.x, bg.y, bg.z};
+      if (spectral) rgb = spectralFilter(rgb, si.spectralChannel);
+      float w = path.scatteringIsDelta ? 1.0f
+                : bsdfMISWeight(c, path.scatteringPdf, envMapPdf(c.J, environmentUv(c.J, path.ray.d)) * c.J.u.env_light_pmf);
+      path.li += path.beta * rgb * (w * bg.w);
+      path.alpha = fmaxf(path.alpha, bg.w);
+      path.abort = true;
+      return;
+    }
+    V2 euv = environmentUv(c.J, path.ray.d);
+    V3 emission = xyz(textureLinear(c.J.s.env, c.J.s.envW, c.J.s.envH, euv));
+    float mis = bsdfMISWeight(c, path.scatteringPdf, envMapPdf(c.J, euv) * c.J.u.env_light_pmf);
+    if (spectral) emission = spectralFilter(emission, si.spectralChannel);
+    if (!(c.J.u.background_flags & MTC_BACKGROUND_COLOR)) path.alpha = 1.0f;
+    path.li += path.beta * emission * mis;
+    path.abort = true;
+  }
+  depth = depth + 1;
+}
+
+// rayTrace.compute.ts:891-946 (RGB integrator, no alpha split)
+MTD float4 integrateRgb(Ctx &c, V2 uv, const Ray &ray, Aux &aux) {
+  SurfaceInteraction si;
+  si.albedoSampled = false; si.hit = false; si.triangleIndex = 0; si.instanceIndex = 0; si.materialIndex = 0;
+  si.wavelength = 0.0f; si.spectralChannel = 0; si.mediumType = 0; si.mediumExtinction = v3(0.0f);
+  si.mediumScattering = v3(0.0f); si.mediumAnisotropy = 0.0f;
+  si.position = v3(0.0f); si.normal = v3(0.0f); si.vertexNormal = v3(0.0f); si.shadowOffset = v3(0.0f);
+  si.faceNormal = v3(0.0f);
+  Material ma;
+  Path path;
+  path.scatteringMediumEntered = false;
+  path.ray = ray;
+  path.li = v3(0.0f);
+  path.alpha = c.J.u.transmissive_output_alpha_min < 1.0f ? 0.0f : 1.0f;
+  path.beta = v3(1.0f);
+  path.fromEye = true;
+  path.abort = false;
+  path.scatteringPdf = 0.0f;
+  path.scatteringIsDelta = false;
+  path.isNextRefraction = false;
+  int bounceLimit = max(c.J.u.bounces, 0);
+  int eventLimit = min(bounceLimit * 3, 20);
+  bool isNotTransparent = false;
+  int depth = 0;
+  bool sampleIgnored = false;
+  for (int event = 0; event <= eventLimit; event++) {
+    intersectScene(c.J, path.ray, si, depth, event != 0, c.cnt);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, ma);
+    if (event == 0) {
+      if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
+        aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+        aux.normal = dot(si.normal, si.position - cameraEye(c.J)) > 0.0f ? -si.normal : si.normal;
+        si.albedoSampled = ma.transmissionWeight > 0.5f;
+      }
+      isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
+    } else {
+      completeVertex(c, path, depth, si, ma, sampleIgnored);
+    }
+    if (isNotTransparent && event > bounceLimit) path.abort = true;
+    if (path.abort || event >= eventLimit) break;
+    shadeVertex(c, uv, path, depth, si, ma, aux, sampleIgnored);
+    if (path.abort) break;
+  }
+  return make_float4(path.li.x, path.li.y, path.li.z, path.alpha);
+}
+
+// rayTrace.compute.ts:1157-1263 main: one path sample for pixel (x, y),
+// accumulated into the job's outputs.
+MTD void tracePixel(const JobData &J, uint32_t x, uint32_t y, Counters &cnt) {
+  const mtc_trace_uniform &u = J.u;
+  uint32_t W = J.width;
+  uint32_t idx = x + y * W;
+  Ctx c{J, Sampler(), BsdfContext{J.s.lut, (J.s.flags & MTC_SCENE_HAS_MEDIUM) != 0u, feature(J, MTC_FEATURE_HAS_THIN_FILM)},
+        Counters()};
+  float4 nrm = J.outNormal[idx];
+  V2 outputSize = {u.output_size[0], u.output_size[1]};
+  V2 uv = {(float(x) + 0.5f) / outputSize.x, (float(y) + 0.5f) / outputSize.y};
+  c.smp.px = x; c.smp.py = y; c.smp.width = W;
+  c.smp.index = uint32_t(nrm.w) + u.sample_sequence_offset;
+  c.smp.bounce = 0; c.smp.hashed = 0;
+  c.smp.seed = u.sequence_seed; c.smp.logspp = u.zsobol_log_spp;
+  c.smp.pattern = int((J.s.flags & MTC_SCENE_PATTERN_MASK) >> MTC_SCENE_PATTERN_SHIFT);
+  V2 jitter = {u.jitter[0], u.jitter[1]};
+  if (c.smp.pattern == 0 || c.smp.pattern == 1) {
+    V2 j = c.smp.s2(0u);
+    jitter = {(j.x - 0.5f) / outputSize.x, (j.y - 0.5f) / outputSize.y};
+  }
+  c.smp.s0 = make_uint4(x, y, c.smp.index ^ sampleHash(u.sequence_seed), x + y);
+  V2 coord = {uv.x + jitter.x, uv.y + jitter.y};
+  Ray cam = initCameraRay(J, coord);
+  if (J.cam.aperture_radius > 0.0f) {
+    const float *vi = J.cam.view_inv;
+    V3 eye = cameraEye(J);
+    V3 forward = -normalize(V3{vi[8], vi[9], vi[10]});
+    V3 focus = eye + cam.d * (J.cam.focus_distance / dot(cam.d, forward));
+    V2 ip = c.smp.s2(1u);
+    V2 pp = {2.0f * ip.x - 1.0f, 2.0f * ip.y - 1.0f};
+    bool greater = fabsf(pp.x) > fabsf(pp.y);
+    float r = greater ? pp.x : pp.y;
+    float theta = greater ? 0.25f * PI * pp.y / pp.x : PI * (0.5f - 0.25f * pp.x / pp.y);
+    float st, ct;
+    sincosf(theta, &st, &ct);
+    float lx = J.cam.aperture_radius * r * ct, ly = J.cam.aperture_radius * r * st;
+    V3 origin = {vi[0] * lx + vi[4] * ly + vi[12], vi[1] * lx + vi[5] * ly + vi[13], vi[2] * lx + vi[6] * ly + vi[14]};
+    cam = {origin, normalize(focus - origin)};
+  }
+  Aux aux = {v3(0.0f), v3(0.0f), false};
+  float4 li = integrateRgb(c, coord, cam, aux);
+  if (u.clamping > 0.0f) {
+    float cl = u.clamping;
+    li = make_float4(clampf(li.x, -cl, cl), clampf(li.y, -cl, cl), clampf(li.z, -cl, cl), li.w);
+  }
+  if (!(li.x < INF && li.x > -EPS)) li = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+  float4 col = J.outColor[idx];
+  J.outColor[idx] = make_float4(col.x + li.x, col.y + li.y, col.z + li.z, col.w + li.w);
+  float4 alb = J.outAlbedo[idx];
+  J.outAlbedo[idx] = make_float4(alb.x + aux.albedo.x, alb.y + aux.albedo.y, alb.z + aux.albedo.z,
+                                 alb.w + (aux.isBlank ? 0.0f : 1.0f));
+  float lum = dot(V3{li.x, li.y, li.z}, kLuminance());
+  if (u.variance_moments != 0) J.outNormal[idx] = make_float4(nrm.x + lum * lum, nrm.y, nrm.z, nrm.w + 1.0f);
+  else J.outNormal[idx] = make_float4(nrm.x + aux.normal.x, nrm.y + aux.normal.y, nrm.z + aux.normal.z, nrm.w + 1.0f);
+  float4 *mom = J.outCatcher + size_t(idx) * 3 + 2;
+  float4 m = *mom;
+  *mom = make_float4(m.x + lum, m.y + lum * lum, m.z, m.w);
+  cnt.ext += c.cnt.ext;
+  cnt.shadow += c.cnt.shadow;
+}
+
+}  // namespace mt

@@ -1,0 +1,335 @@
+// Device sampler (Owen-scrambled Sobol, ZSobol, PCG4D) and two-level BVH2
+// traversal with the watertight FP32 triangle test.
+#pragma once
+#include "../../include/mutracer_b200.h"
+#include "dev_math.cuh"
+
+namespace mt {
+
+// Device copy of the bind groups; all pointers are device pointers.
+struct DevScene {
+  const float4 *bvh;
+  const float4 *ins;
+  const uint32_t *attr;
+  const float4 *mats;
+  const float4 *env;
+  const float2 *envDist;
+  const float4 *lightData;
+  const float *lut;
+  const float4 *lights;
+  uint32_t envW, envH;
+  uint32_t vstride, vnormalOff, vnormalFloat;
+  uint32_t flags;
+  uint32_t insCount, matCount;
+};
+
+// One render job: scene, uniforms, outputs (the plain kernel takes one as a
+// __grid_constant__ parameter; the batched kernel reads a table of them).
+struct JobData {
+  DevScene s;
+  mtc_trace_uniform u;
+  mtc_camera_uniform cam;
+  float4 *outColor, *outNormal, *outAlbedo, *outCatcher;
+  uint32_t samples;
+  uint32_t width, height;
+  uint32_t tilesX, tilesY;
+  uint32_t firstItem;  // first global work item of this job (batched kernel)
+  uint32_t items;      // tiles * samples
+  uint32_t _pad;
+};
+
+struct Counters {
+  uint32_t ext = 0, shadow = 0;
+};
+
+// ------------------------------------------------------------------ sampler
+// sobol.wgsl.ts:23-45
+MTD uint32_t sampleHash(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du;
+  x ^= x >> 15; x *= 0x846ca68bu;
+  return x ^ (x >> 16);
+}
+MTD uint32_t sampleSeed(uint32_t a, uint32_t b) { return sampleHash(a ^ sampleHash(b + 0x9e3779b9u)); }
+MTD uint32_t lkPermute(uint32_t v, uint32_t seed) {
+  uint32_t x = v + seed;
+  x ^= x * 0x6c50b47cu; x ^= x * 0xb82f1e52u;
+  x ^= x * 0xc7afe638u; x ^= x * 0x8d22f6e6u;
+  return x;
+}
+MTD uint32_t owen(uint32_t x, uint32_t seed) { return __brev(lkPermute(__brev(x), seed)); }
+MTD uint32_t sobolD1(uint32_t v) {
+  uint32_t r = __brev(v);
+  r ^= (r << 1) & 0xaaaaaaaau;
+  r ^= (r << 2) & 0xccccccccu;
+  r ^= (r << 4) & 0xf0f0f0f0u;
+  r ^= (r << 8) & 0xff00ff00u;
+  r ^= (r << 16) & 0xffff0000u;
+  return r;
+}
+MTD uint32_t morton2(uint32_t x, uint32_t y) {
+  uint32_t vx = x & 255u, vy = y & 255u;
+  vx = (vx | (vx << 4)) & 0x0f0fu; vy = (vy | (vy << 4)) & 0x0f0fu;
+  vx = (vx | (vx << 2)) & 0x3333u; vy = (vy | (vy << 2)) & 0x3333u;
+  vx = (vx | (vx << 1)) & 0x5555u; vy = (vy | (vy << 1)) & 0x5555u;
+  return vx | (vy << 1);
+}
+// Packed pbrt-v4 ZSobol digit permutations (src/renderer/sampling.ts:23-28).
+__device__ __constant__ static const uint32_t kZPermWords[6] = {
+    0x78d8b4e4u, 0xb1e19c6cu, 0x8d2d39c9u, 0x72d236c6u, 0x87271e4eu, 0x93634b1bu};
+MTD uint32_t zSobolPermutation(uint32_t perm) {
+  return (kZPermWords[perm >> 2] >> ((perm & 3u) * 8u)) & 255u;
+}
+MTD uint32_t zSobolIndex(uint32_t morton, uint32_t dim, uint32_t logSPP) {
+  uint32_t odd = logSPP & 1u;
+  uint32_t digits = 8u + ((logSPP + 1u) >> 1);
+  uint32_t result = 0;
+  for (int digit = int(digits) - 1; digit >= int(odd); digit--) {
+    uint32_t shift = 2u * uint32_t(digit) - odd;
+    uint32_t higher = shift < 30u ? morton >> (shift + 2u) : 0u;
+    uint32_t perm = (sampleHash(higher ^ (0x55555555u * dim)) >> 24) % 24u;
+    uint32_t d = (morton >> shift) & 3u;
+    result |= ((zSobolPermutation(perm) >> (2u * d)) & 3u) << shift;
+  }
+  if (odd != 0u) result |= (morton & 1u) ^ (sampleHash((morton >> 1) ^ (0x55555555u * dim)) & 1u);
+  return result;
+}
+
+struct Sampler {
+  uint32_t px, py, width, index, bounce, hashed, seed, logspp;
+  int pattern;
+  uint4 s0;
+  MTD V2 structured(uint32_t dim) const {
+    uint32_t pixelID = px + py * width;
+    uint32_t sd = sampleSeed(sampleSeed(pixelID, dim), seed);
+    uint32_t idx = index;
+    if (pattern == 1) {
+      uint32_t lg = logspp;
+      if (idx == 0u) lg = 0u; else idx -= 1u;
+      uint32_t block = idx >> lg;
+      uint32_t mask = (1u << lg) - 1u;
+      uint32_t morton = (morton2(px, py) << lg) | (idx & mask);
+      idx = zSobolIndex(morton, dim, lg);
+      sd = sampleSeed(sampleSeed(dim, seed), sampleSeed(px >> 8, py >> 8));
+      if (index != 0u) block += 1u;
+      sd = sampleSeed(sd, block);
+    }
+    uint32_t i = owen(idx, sampleSeed(sd, 0u));
+    uint32_t x = __brev(lkPermute(i, sampleSeed(sd, 1u)));
+    uint32_t y = owen(sobolD1(i), sampleSeed(sd, 2u));
+    float fx = float(x >> 8) * (1.0f / 16777216.0f);
+    float fy = float(y >> 8) * (1.0f / 16777216.0f);
+    return {EPS + 0.999f * fx, EPS + 0.999f * fy};
+  }
+  MTD float rnd() {
+    s0.x = s0.x * 1664525u + 1013904223u; s0.y = s0.y * 1664525u + 1013904223u;
+    s0.z = s0.z * 1664525u + 1013904223u; s0.w = s0.w * 1664525u + 1013904223u;
+    s0.x += s0.y * s0.w; s0.y += s0.z * s0.x; s0.z += s0.x * s0.y; s0.w += s0.y * s0.z;
+    s0.x ^= s0.x >> 16; s0.y ^= s0.y >> 16; s0.z ^= s0.z >> 16; s0.w ^= s0.w >> 16;
+    s0.x += s0.y * s0.w; s0.y += s0.z * s0.x; s0.z += s0.x * s0.y; s0.w += s0.y * s0.z;
+    return float(s0.x) / float(0xffffffffu);
+  }
+  MTD float s1(uint32_t dim) {
+    if (pattern == 2) return EPS + 0.999f * rnd();
+    return structured(dim).x;
+  }
+  MTD V2 s2(uint32_t dim) {
+    if (pattern == 2) { float a = s1(dim); float b = s1(dim); return {a, b}; }
+    return structured(dim);
+  }
+  MTD float hashedSample(uint32_t slot) {
+    uint32_t dim = sampleSeed(sampleSeed(bounce, slot), hashed) | 0x80000000u;
+    hashed += 1u;
+    if (pattern == 2) return EPS + 0.999f * rnd();
+    uint32_t pixelID = px + py * width;
+    uint32_t sd = sampleSeed(sampleSeed(pixelID, dim), seed);
+    uint32_t i = owen(index, sampleSeed(sd, 0u));
+    uint32_t x = __brev(lkPermute(i, sampleSeed(sd, 1u)));
+    return EPS + 0.999f * (float(x >> 8) * (1.0f / 16777216.0f));
+  }
+  MTD float lightCandidateRandom(uint32_t salt) {
+    if (pattern == 2) (void)rnd();
+    uint32_t pixelID = px + py * width;
+    uint32_t key = sampleSeed(sampleSeed(pixelID, index), seed);
+    uint32_t dimension = sampleSeed(bounce, salt) ^ 0xa511e9b3u;
+    return float(sampleHash(key ^ dimension) >> 8) * (1.0f / 16777216.0f);
+  }
+  MTD uint32_t bounceDim(uint32_t slot) const { return 3u + 8u + bounce * 64u + slot; }
+  MTD uint32_t lightDim(uint32_t c, uint32_t slot) const {
+    if (c == 0u) return slot == 2u ? bounceDim(8u) : bounceDim(slot);
+    return bounceDim(9u + (c - 1u) * 3u + slot);
+  }
+};
+
+// ---------------------------------------------------------------- traversal
+// intersect.wgsl.ts:1500-1521 (every operation rounded, fminf/fmaxf)
+MTD V3 traversalInverse(V3 d) { return {__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z)}; }
+MTD float intersectBox(V3 o, V3 bmin, V3 bmax, V3 invD, float tMax) {
+  V3 tBot = xmul3(xsub3(bmin, o), invD);
+  V3 tTop = xmul3(xsub3(bmax, o), invD);
+  float t0 = fmaxf(fminf(tBot.x, tTop.x), fmaxf(fminf(tBot.y, tTop.y), fminf(tBot.z, tTop.z)));
+  float t1 = fminf(fmaxf(tBot.x, tTop.x), fminf(fmaxf(tBot.y, tTop.y), fmaxf(tBot.z, tTop.z)));
+  if (t0 > t1 || t0 > tMax) return -1.0f;
+  return t0 > 0.0f ? t0 : t1;
+}
+MTD int maxDimension(V3 v) {
+  if (v.x > v.y) return v.x > v.z ? 0 : 2;
+  return v.y > v.z ? 1 : 2;
+}
+MTD V3 getShear(V3 d, int maxDim) {
+  if (maxDim == 0) return {xd(-d.y, d.x), xd(-d.z, d.x), __frcp_rn(d.x)};
+  if (maxDim == 1) return {xd(-d.z, d.y), xd(-d.x, d.y), __frcp_rn(d.y)};
+  return {xd(-d.x, d.z), xd(-d.y, d.z), __frcp_rn(d.z)};
+}
+// intersect.wgsl.ts:1430-1493; returns t (0 for a miss) and barycentrics.
+MTD float intersectTriangle(V3 o, V3 p0, V3 p1, V3 p2, int maxDim, V3 shear, float tMax, V3 &bary) {
+  V3 a = xsub3(p0, o), b = xsub3(p1, o), c = xsub3(p2, o);
+  if (maxDim == 0) { a = {a.y, a.z, a.x}; b = {b.y, b.z, b.x}; c = {c.y, c.z, c.x}; }
+  else if (maxDim == 1) { a = {a.z, a.x, a.y}; b = {b.z, b.x, b.y}; c = {c.z, c.x, c.y}; }
+  a.x = xa(a.x, xm(shear.x, a.z)); a.y = xa(a.y, xm(shear.y, a.z));
+  b.x = xa(b.x, xm(shear.x, b.z)); b.y = xa(b.y, xm(shear.y, b.z));
+  c.x = xa(c.x, xm(shear.x, c.z)); c.y = xa(c.y, xm(shear.y, c.z));
+  V3 e = {xs(xm(b.x, c.y), xm(b.y, c.x)), xs(xm(c.x, a.y), xm(c.y, a.x)), xs(xm(a.x, b.y), xm(a.y, b.x))};
+  bool anyNeg = e.x < 0.0f || e.y < 0.0f || e.z < 0.0f;
+  bool anyPos = e.x > 0.0f || e.y > 0.0f || e.z > 0.0f;
+  if (anyNeg && anyPos) return 0.0f;
+  float det = xa(xa(e.x, e.y), e.z);
+  float az = xm(a.z, shear.z), bz = xm(b.z, shear.z), cz = xm(c.z, shear.z);
+  float tScaled = xa(xa(xm(e.x, az), xm(e.y, bz)), xm(e.z, cz));
+  if (fabsf(tScaled) > fabsf(xm(tMax, det))) return 0.0f;
+  float invDet = __frcp_rn(det);
+  bary = {xm(e.x, invDet), xm(e.y, invDet), xm(e.z, invDet)};
+  return xm(tScaled, invDet);
+}
+
+MTD V3 vertexPosition(const DevScene &s, int32_t i) {
+  const uint32_t *w = s.attr + size_t(i) * s.vstride;
+  if (s.vstride == 4) {
+    float4 q = __ldg(reinterpret_cast<const float4 *>(w));
+    return {q.x, q.y, q.z};
+  }
+  return {asf(__ldg(w)), asf(__ldg(w + 1)), asf(__ldg(w + 2))};
+}
+// vertexAttributes.wgsl.ts:14-28
+MTD V3 vertexNormal(const DevScene &s, int32_t i) {
+  const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vnormalOff;
+  if (s.vnormalFloat) return {asf(__ldg(w)), asf(__ldg(w + 1)), asf(__ldg(w + 2))};
+  uint32_t word = __ldg(w);
+  int32_t a = int32_t(word << 16) >> 16;
+  int32_t b = int32_t(word) >> 16;
+  if (a == -32768 && b == -32768) return v3(0.0f);
+  V3 v = {float(a) / 32767.0f, float(b) / 32767.0f, 0.0f};
+  v.z = 1.0f - fabsf(v.x) - fabsf(v.y);
+  if (v.z < 0.0f) {
+    float nx = (1.0f - fabsf(v.y)) * (v.x >= 0.0f ? 1.0f : -1.0f);
+    float ny = (1.0f - fabsf(v.x)) * (v.y >= 0.0f ? 1.0f : -1.0f);
+    v.x = nx; v.y = ny;
+  }
+  return normalize(v);
+}
+
+struct TraversalHit {
+  float tMax;
+  V3 hitNormal, hitBary;
+  int32_t triangleIndex, insIdx;
+};
+
+// getBVHTraverseCode, intersect.wgsl.ts:213-629 for the BVH2 layout.  With
+// `shadow` the first accepted hit ends the query (returns true).
+template <bool shadow>
+__device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 rayO, V3 rayD, int bounces,
+                                      bool doubleSided, int32_t currentTri, int32_t currentIns, TraversalHit &h) {
+  int32_t tlasStack[MTC_MAX_STACK];
+  int32_t blasStack[MTC_MAX_STACK];
+  int tlasTop = -1;
+  const float4 *bvh = s.bvh;
+  V3 invD = traversalInverse(rayD);
+  if (intersectBox(rayO, xyz(ld4(bvh)), xyz(ld4(bvh + 1)), invD, h.tMax) > 0.0f) {
+    tlasTop = 0;
+    tlasStack[0] = 0;
+  }
+  while (tlasTop >= 0) {
+    int32_t tlasNode = tlasStack[tlasTop--];
+    float4 r1 = ld4(bvh + tlasNode);
+    int32_t ptr = asi(r1.w);
+    if (ptr >= 0) {
+      int32_t left = tlasNode + 2, right = ptr;
+      float d0 = intersectBox(rayO, xyz(ld4(bvh + left)), xyz(ld4(bvh + left + 1)), invD, h.tMax);
+      float d1 = intersectBox(rayO, xyz(ld4(bvh + right)), xyz(ld4(bvh + right + 1)), invD, h.tMax);
+      if (d0 > d1) {
+        if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
+        if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
+      } else {
+        if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
+        if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
+      }
+      continue;
+    }
+    int32_t tlasCount = -ptr;
+    for (int32_t io = tlasCount - 1; io >= 0; io--) {
+      float4 rec = ld4(bvh + tlasNode + 2 + io);
+      int32_t insIdx = asi(rec.x);
+      int32_t blasRoot = asi(rec.y);
+      const float4 *insv = s.ins + size_t(insIdx) * MTC_INSTANCE_VEC4_STRIDE;
+      float4 insData = ld4(insv);
+      float4 c0 = ld4(insv + 1), c1 = ld4(insv + 2), c2 = ld4(insv + 3), c3 = ld4(insv + 4);
+      V3 o = xmat4(c0, c1, c2, c3, rayO, 1.0f);
+      V3 d = xmat4(c0, c1, c2, c3, rayD, 0.0f);
+      V3 linvD = traversalInverse(d);
+      int maxDim = maxDimension(vabs(d));
+      V3 shear = getShear(d, maxDim);
+      uint32_t encoded = asu(insData.x);
+      if ((encoded >> 30) != 0u) continue;
+      int32_t blasOffset = int32_t(encoded & 0x3fffffffu);
+      int32_t vertexOffset = asi(insData.y);
+      int32_t sideMaterial = asi(insData.z) >> 8;
+      int blasTop = 0;
+      blasStack[0] = blasRoot;
+      while (blasTop >= 0) {
+        int32_t node = blasStack[blasTop--];
+        int32_t i = node + blasBase;
+        float4 n1 = ld4(bvh + i);
+        int32_t p = asi(n1.w);
+        if (p >= 0) {
+          int32_t left = node + 2, right = p + blasOffset;
+          float d0 = intersectBox(o, xyz(ld4(bvh + left + blasBase)), xyz(ld4(bvh + left + 1 + blasBase)), linvD, h.tMax);
+          float d1 = intersectBox(o, xyz(ld4(bvh + right + blasBase)), xyz(ld4(bvh + right + 1 + blasBase)), linvD, h.tMax);
+          if (d0 > d1) {
+            if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
+            if (d1 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = right;
+          } else {
+            if (d1 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = right;
+            if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
+          }
+          continue;
+        }
+        int32_t primitiveCount = -p;
+        int32_t primitiveOffset = i + 2;
+        for (int32_t k = 0; k < primitiveCount; k++) {
+          int32_t triangleIndex = primitiveOffset + k;
+          if (bounces > 0 && triangleIndex == currentTri && insIdx == currentIns) continue;
+          float4 r3 = ld4(bvh + triangleIndex);
+          V3 p0 = vertexPosition(s, asi(r3.x) + vertexOffset);
+          V3 p1 = vertexPosition(s, asi(r3.y) + vertexOffset);
+          V3 p2 = vertexPosition(s, asi(r3.z) + vertexOffset);
+          V3 bary;
+          float t = intersectTriangle(o, p0, p1, p2, maxDim, shear, h.tMax, bary);
+          if (!(t > 0.0f)) continue;
+          V3 candidateNormal = xnormalize(xcross(xsub3(p1, p0), xsub3(p2, p0)));
+          if (!doubleSided) {
+            bool matDoubleSided = __ldg(&s.mats[size_t(sideMaterial) * MTC_MATERIAL_VEC4_ROWS + 23].z) > 0.5f;
+            if (!matDoubleSided && xdot(candidateNormal, d) > 0.0f) continue;
+          }
+          h.hitNormal = candidateNormal;
+          h.tMax = t;
+          h.hitBary = bary;
+          if (shadow) return true;
+          h.triangleIndex = triangleIndex;
+          h.insIdx = insIdx;
+        }
+      }
+    }
+  }
+  return false;
+}
+
+}  // namespace mt

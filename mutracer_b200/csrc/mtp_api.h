@@ -1,0 +1,39 @@
+// Scene-preparation C API of mutracer_b200 (host memory only).  Produces the
+// flattened buffer bundle that mt_context_commit_bundle and the mtc_* entry
+// points consume, from seeded synthetic generators.
+#pragma once
+#include <stdint.h>
+#include "../../include/mutracer_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mtp_scene_info {
+  uint64_t triangles, unique_triangles;
+  uint32_t instances, blases, tlas_vec4, _pad;
+  uint64_t bvh_vec4, vertices;
+  float world_bounds[6];
+  float _pad2[2];
+} mtp_scene_info_t;
+
+void *mtp_scene_make(const char *kind, uint32_t width, uint32_t height, uint64_t seed, const uint32_t *params,
+                     uint32_t nparams);
+void mtp_scene_free(void *scene);
+int mtp_scene_bundle(void *scene, mt_scene_bundle *out);
+int mtp_scene_info(void *scene, mtp_scene_info_t *info);
+int mtp_scene_set_uniform(void *scene, const mtc_trace_uniform *u, const mtc_camera_uniform *cam, uint32_t flags);
+int mtp_scene_refit_inputs(void *scene, double *transforms, float *localBounds, int32_t *blasOffsets,
+                           int32_t *blasLayouts, int32_t *vertexOffsets, int32_t *materials, float *colors);
+int mtp_scene_set_transforms(void *scene, const double *transforms, uint32_t count);
+int mtp_scene_refit_host(void *scene);
+int mtp_build_binned_sah(const float *aabbs, uint32_t count, int bins, uint32_t *nodeCount, float *bounds,
+                         uint32_t *leftFirst, uint32_t *primCount, uint32_t *primIndices);
+int mtp_build_blas(const float *positions, uint32_t vertexCount, const uint32_t *indices, uint32_t triCount, int bins,
+                   float *out, uint64_t capacity, uint64_t *vec4Count, uint32_t *maxDepth);
+int mtp_energy_lut(float *out);
+int mtp_env_distribution(const float *image, uint32_t width, uint32_t height, float *distribution, double *power);
+
+#ifdef __cplusplus
+}
+#endif

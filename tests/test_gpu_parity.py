@@ -1,0 +1,209 @@
+"""GPU parity of the CUDA path against the CPU oracle, through the C ABI.
+
+Bars: first-hit instance/record/t bit-exact (ties counted), image relMSE
+<= 1e-3 and mean luminance within 0.5 % at the same seed, TLAS refit
+bit-exact, batched jobs bit-identical to the same jobs alone.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mutracer_b200 import abi, scene, trace
+from tests import oracle_lib
+
+pytestmark = pytest.mark.gpu
+
+REL_MSE_BAR = 1e-3
+LUMA_BAR = 0.005
+
+
+def _hits_equal(gpu, ref):
+    g, r = gpu.view(np.int32), ref.view(np.int32)
+    same = (g[:, 0] == r[:, 0]) & (g[:, 1] == r[:, 1]) & (g[:, 2] == r[:, 2]) & (g[:, 3] == r[:, 3])
+    # A tie: both report a hit at the same t on different primitives.
+    tie = (~same) & (g[:, 0] == 1) & (r[:, 0] == 1) & (g[:, 3] == r[:, 3])
+    return same, tie
+
+
+def _first_hit_case(cuda, host, n, seed):
+    import torch
+    dev = scene.DeviceScene(host, cuda)
+    rays = oracle_lib.seeded_rays(host, n, seed=seed)
+    ref = oracle_lib.first_hits(host, rays)
+    gpu = trace.query_first_hit(dev, torch.from_numpy(rays).to(cuda)).cpu().numpy()
+    torch.cuda.synchronize()
+    same, tie = _hits_equal(gpu, ref)
+    mismatches = int((~same).sum())
+    ties = int(tie.sum())
+    assert ref[:, 0].sum() > n // 4, "ray set should mostly hit the scene"
+    assert mismatches == ties, f"{mismatches} hit mismatches, of which {ties} are ties"
+    hit = ref[:, 0] == 1
+    # barycentrics are bit-exact wherever the record matches
+    both = same & hit
+    assert np.array_equal(gpu[both, 4:7], ref[both, 4:7])
+    return mismatches, ties
+
+
+def test_first_hit_bitexact_cornell(cuda):
+    host = scene.SceneHost("cornell", 64, 64, 1)
+    _first_hit_case(cuda, host, 200_000, seed=3)
+
+
+def test_first_hit_bitexact_large_1m(cuda):
+    host = scene.make_workload("instanced_spheres", width=64, height=64)
+    assert host.info.triangles > 4_000_000
+    _first_hit_case(cuda, host, 1_000_000, seed=11)
+
+
+def _render_pair(cuda, host, spp):
+    import torch
+    dev = scene.DeviceScene(host, cuda)
+    acc = trace.Accumulation(host.width, host.height, cuda)
+    trace.trace_samples(dev, acc, spp)
+    torch.cuda.synchronize()
+    gpu = acc.resolved().cpu().numpy()
+    ref_acc = oracle_lib.Accum(host.width, host.height)
+    oracle_lib.trace(host, ref_acc, spp)
+    ref = ref_acc.resolved()
+    return gpu, ref, acc, ref_acc
+
+
+def _image_metrics(gpu, ref):
+    a, b = gpu[..., :3].astype(np.float64), ref[..., :3].astype(np.float64)
+    rel_mse = float(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-30))
+    w = np.array([0.2126, 0.7152, 0.0722])
+    la, lb = float((a @ w).mean()), float((b @ w).mean())
+    return rel_mse, abs(la - lb) / max(lb, 1e-30)
+
+
+def test_image_parity_cornell(cuda):
+    host = scene.SceneHost("cornell", 128, 128, 1)
+    gpu, ref, acc, ref_acc = _render_pair(cuda, host, 64)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert np.isfinite(gpu).all()
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma
+    # per-pixel sample counts are exact
+    assert np.array_equal(acc.normal[:, 3].cpu().numpy(), ref_acc.normal[:, 3])
+
+
+def test_image_parity_instanced(cuda):
+    host = scene.make_workload("instanced_spheres", width=160, height=90)
+    gpu, ref, _, _ = _render_pair(cuda, host, 8)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma
+
+
+def test_image_parity_zsobol_two_candidates(cuda):
+    host = scene.SceneHost("cornell", 96, 96, 5)
+    u = abi.TraceUniform.from_buffer_copy(host.uniform)
+    u.direct_light_candidates = 3
+    u.sequence_seed = 99
+    host.set_uniform(u, None, (host.flags & ~abi.MTC_SCENE_PATTERN_MASK) | (1 << abi.MTC_SCENE_PATTERN_SHIFT))
+    gpu, ref, _, _ = _render_pair(cuda, host, 32)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma
+
+
+def test_refit_device_matches_host(cuda):
+    import torch
+    host = scene.make_workload("instanced_spheres", width=32, height=32, params=(64, 4, 8, 256, 2))
+    inputs = host.refit_inputs()
+    rng = np.random.default_rng(5)
+    t = inputs["transforms"].reshape(-1, 4, 4).copy()
+    t[:, 3, :3] += rng.normal(scale=0.5, size=(t.shape[0], 3))  # move every instance
+    t = t.reshape(-1, 16)
+    host.set_transforms(t)
+    inputs["transforms"] = t
+    dev = scene.DeviceScene(host, cuda)          # uploads the pre-refit buffers
+    host.refit_host()                            # reference refit on the host
+    host.refresh()
+    dinputs = {k: torch.from_numpy(np.ascontiguousarray(v)).to(cuda) for k, v in inputs.items()}
+    trace.refit_tlas(dev, dinputs)
+    torch.cuda.synchronize()
+    tlas_vec4 = host.info.tlas_vec4
+    got_tlas = dev.bvh[: tlas_vec4 * 4].cpu().numpy()
+    want_tlas = host.bvh[: tlas_vec4 * 4]
+    assert np.array_equal(got_tlas.view(np.uint32), want_tlas.view(np.uint32))
+    assert np.array_equal(dev.instances.cpu().numpy().view(np.uint32), host.instances.view(np.uint32))
+
+
+def test_batch_matches_alone(cuda):
+    import torch
+    hosts = [scene.SceneHost("cornell", 64, 48, 1), scene.SceneHost("cornell", 40, 72, 2),
+             scene.make_workload("instanced_spheres", width=48, height=32, params=(32, 4, 6, 256, 2))]
+    spps = [5, 9, 3]
+    devs = [scene.DeviceScene(h, cuda) for h in hosts]
+    alone = []
+    for d, s in zip(devs, spps):
+        acc = trace.Accumulation(d.width, d.height, cuda)
+        trace.trace_samples(d, acc, s)
+        alone.append(acc)
+    batched = [trace.Accumulation(d.width, d.height, cuda) for d in devs]
+    jobs = (abi.JobDesc * len(devs))()
+    for i, (d, s, acc) in enumerate(zip(devs, spps, batched)):
+        jobs[i].scene = d.view
+        jobs[i].camera = d.camera
+        jobs[i].uniform = d.uniform
+        jobs[i].out = acc.outputs
+        jobs[i].samples = s
+    scratch = torch.zeros(abi.lib().mtc_batch_scratch_bytes(len(devs)), dtype=torch.uint8, device=cuda)
+    st = abi.lib().mtc_trace_batch(jobs, len(devs), None, C.c_void_p(scratch.data_ptr()), None, None,
+                                   C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    abi.check(st)
+    torch.cuda.synchronize()
+    for a, b in zip(alone, batched):
+        for x, y in ((a.color, b.color), (a.normal, b.normal), (a.albedo, b.albedo), (a.catcher, b.catcher)):
+            assert torch.equal(x, y)
+
+
+def test_context_api_render_and_jobs(cuda):
+    from mutracer_b200.context import Context
+    host = scene.SceneHost("cornell", 48, 40, 1)
+    ctx = Context()
+    try:
+        with pytest.raises(abi.MtError):
+            ctx.render(1)                       # nothing committed yet
+        ctx.commit(host)
+        with pytest.raises(abi.MtError) as e:
+            ctx.read_pixels()                   # no completed sample
+        assert e.value.status == abi.MT_ERROR_INVALID_STATE
+        ctx.render(4)
+        img = ctx.read_pixels()
+        assert img.shape == (40, 48, 4) and np.isfinite(img).all()
+        # the same samples through the device-buffer entry point match exactly
+        import torch
+        dev = scene.DeviceScene(host, cuda)
+        acc = trace.Accumulation(48, 40, cuda)
+        trace.trace_samples(dev, acc, 4)
+        torch.cuda.synchronize()
+        ref = acc.resolved().cpu().numpy()
+        assert np.array_equal(img, ref)
+        job = ctx.submit(10)
+        with pytest.raises(abi.MtError):
+            ctx.render(1)                       # active job rejects blocking render
+        for _ in range(10000):
+            job.poll(3)
+            if job.info().state == abi.MT_JOB_COMPLETE:
+                break
+        info = job.info()
+        assert info.state == abi.MT_JOB_COMPLETE and info.completed_samples == 10 and info.base_samples == 4
+        assert ctx.info().samples == 14
+        job2 = ctx.submit(8)
+        job.__init__(job.handle)
+        with pytest.raises(abi.MtError) as e:
+            job.poll(1)                         # expired handle
+        assert e.value.status == abi.MT_ERROR_INVALID_HANDLE
+        job2.poll(2)
+        job2.cancel()
+        for _ in range(10000):
+            job2.poll(0)
+            if job2.info().state in (abi.MT_JOB_CANCELLED, abi.MT_JOB_COMPLETE):
+                break
+        assert job2.info().state == abi.MT_JOB_CANCELLED
+        assert ctx.info().samples == 16
+    finally:
+        ctx.destroy()
