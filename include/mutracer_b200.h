@@ -258,14 +258,16 @@ typedef struct mtc_batch_config {
   uint32_t ctas_per_sm;    /* resident CTAs per SM (grid = 148 * ctas_per_sm) */
 } mtc_batch_config;
 
-/* Runs `job_count` jobs (descriptors in DEVICE memory) to completion in one
- * persistent launch.  `queue_state` is caller-provided device scratch of
- * mtc_batch_scratch_bytes(job_count) bytes, zeroed by the call on `stream`.
- * status_out (device, may be NULL) receives 0 on success or a nonzero code if
- * the kernel's bounded queue loop gave up.  Work is pulled with one atomic per
- * work item; results are identical to running each job alone. */
+/* Runs `job_count` jobs (descriptors in HOST memory; their buffers are device
+ * pointers) to completion in one persistent launch.  `queue_state` is
+ * caller-provided device scratch of mtc_batch_scratch_bytes(job_count) bytes
+ * that receives the job table and the work-queue counter (reset by the call
+ * on `stream`).  status_out (device, may be NULL) is set to 0.  Work is
+ * pulled with one atomic per 32-pixel tile; every sample of a tile runs in
+ * order on one warp, so each job's outputs are bit-identical to running it
+ * alone through mtc_trace_samples. */
 size_t mtc_batch_scratch_bytes(uint32_t job_count);
-mt_status mtc_trace_batch(const mtc_job_desc *jobs_device, uint32_t job_count,
+mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count,
                           const mtc_batch_config *config, void *queue_state,
                           uint32_t *status_out, mtc_counters *counters,
                           void *stream);
