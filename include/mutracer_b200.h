@@ -272,6 +272,27 @@ mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count,
                           uint32_t *status_out, mtc_counters *counters,
                           void *stream);
 
+/* No counterpart in the reference.  For callers that cannot let the library
+ * allocate device memory (a host that owns a fixed device budget and its own
+ * allocator, a plugin inside such a host, a serving loop that cannot afford a
+ * synchronising cudaMalloc): the same batched launch as mtc_trace_batch, but
+ * its scratch (job table and work-queue counter) lives in one fixed array
+ * inside the library's device image, sized for MTC_BATCH_NOALLOC_MAX_JOBS
+ * jobs, so the call allocates nothing; a larger job_count returns
+ * MT_ERROR_INVALID_ARGUMENT.  The caller still passes the jobs with their
+ * scene buffers and accumulation outputs.  The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture.  Every call on a
+ * device shares the one array (each call rewrites the table and clears the
+ * counter), so calls whose work overlaps on the same device race: serialise
+ * them, for example on one stream.  The array stays resident on every device
+ * that loads the library until the process exits. */
+#define MTC_BATCH_NOALLOC_MAX_JOBS 64
+mt_status mtc_trace_batch_noalloc(const mtc_job_desc *jobs, uint32_t job_count,
+                                  const mtc_batch_config *config,
+                                  uint32_t *status_out, mtc_counters *counters,
+                                  void *stream);
+
 /* ------------------------------------------------------- host context */
 typedef uint64_t mt_context;
 typedef uint64_t mt_render_job;

@@ -35,6 +35,7 @@ MTC_MATERIAL_VEC4_ROWS = 26
 MTC_LIGHT_VEC4_ROWS = 6
 MTC_ENERGY_LUT_WIDTH = 32
 MTC_ENERGY_LUT_HEIGHT = 2177
+MTC_BATCH_NOALLOC_MAX_JOBS = 64
 
 
 class MtError(RuntimeError):
@@ -172,6 +173,7 @@ def _declare(lib):
         "mtc_query_first_hit": (C.c_int32, [C.POINTER(SceneView), P, C.c_uint32, P, P]),
         "mtc_batch_scratch_bytes": (C.c_size_t, [C.c_uint32]),
         "mtc_trace_batch": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P, P]),
+        "mtc_trace_batch_noalloc": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
         "mtc_refit_tlas": (C.c_int32, [P, C.c_uint64, P, C.c_uint32, P, P, P, P, P, P, P, P]),
         "mtp_scene_make": (P, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), C.c_uint32]),
         "mtp_scene_free": (None, [P]),
