@@ -250,12 +250,16 @@ typedef struct mtc_job_desc {
   uint32_t _pad[3];
 } mtc_job_desc;
 
-/* Tuning knobs chosen by the autotuner (0 selects the built-in default). */
+/* Tuning knobs of the persistent batched kernel, chosen by the autotuner
+ * (0 selects the built-in default).  None changes any job's result. */
 typedef struct mtc_batch_config {
   uint32_t struct_size;
-  uint32_t block_threads;  /* threads per CTA of the persistent kernel */
-  uint32_t tile_pixels;    /* pixels per work item */
-  uint32_t ctas_per_sm;    /* resident CTAs per SM (grid = 148 * ctas_per_sm) */
+  uint32_t block_threads;    /* threads per CTA: 32, 64, 96 or 128 (default 128) */
+  uint32_t tile_width;       /* warp tile width in pixels: 1, 2, 4, 8, 16 or 32;
+                                height = 32 / width (default 8, an 8x4 tile) */
+  uint32_t ctas_per_sm;      /* grid = SM count * ctas_per_sm (default 2) */
+  uint32_t items_per_fetch;  /* warp tiles taken per queue atomic, 1..16 (default 1) */
+  uint32_t _pad[3];
 } mtc_batch_config;
 
 /* Runs `job_count` jobs (descriptors in HOST memory; their buffers are device
@@ -271,6 +275,23 @@ mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count,
                           const mtc_batch_config *config, void *queue_state,
                           uint32_t *status_out, mtc_counters *counters,
                           void *stream);
+
+/* The two halves of mtc_trace_batch, for replay.  mtc_batch_prepare builds
+ * the device job table of `jobs` into caller HOST memory `table` of
+ * mtc_batch_table_bytes(job_count) bytes and reports the number of work items
+ * (host only, no CUDA call); `config` must be the one later given to
+ * mtc_batch_launch.  mtc_batch_launch copies that table into
+ * `queue_state`, clears the work counter and launches the persistent kernel,
+ * all ordered on `stream`; with `table` in pinned host memory the three
+ * operations can be captured in a CUDA graph and replayed after the table is
+ * rewritten in place. */
+size_t mtc_batch_table_bytes(uint32_t job_count);
+mt_status mtc_batch_prepare(const mtc_job_desc *jobs, uint32_t job_count,
+                            const mtc_batch_config *config, void *table,
+                            uint32_t *total_items);
+mt_status mtc_batch_launch(const void *table, uint32_t job_count, uint32_t total_items,
+                           const mtc_batch_config *config, void *queue_state,
+                           mtc_counters *counters, void *stream);
 
 /* No counterpart in the reference.  For callers that cannot let the library
  * allocate device memory (a host that owns a fixed device budget and its own

@@ -7,7 +7,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libmutracer_b200.so")
+LIB_PATH = os.environ.get("MUTRACER_B200_LIB") or os.path.join(HERE, "_lib", "libmutracer_b200.so")
 
 # Status codes (mutracer-status.h).
 MT_OK = 0
@@ -109,8 +109,16 @@ class JobDesc(C.Structure):
 
 
 class BatchConfig(C.Structure):
-    _fields_ = [("struct_size", C.c_uint32), ("block_threads", C.c_uint32), ("tile_pixels", C.c_uint32),
-                ("ctas_per_sm", C.c_uint32)]
+    _fields_ = [("struct_size", C.c_uint32), ("block_threads", C.c_uint32), ("tile_width", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("items_per_fetch", C.c_uint32), ("_pad", C.c_uint32 * 3)]
+
+    @classmethod
+    def make(cls, block_threads=0, tile_width=0, ctas_per_sm=0, items_per_fetch=0):
+        c = cls()
+        c.struct_size = C.sizeof(cls)
+        c.block_threads, c.tile_width, c.ctas_per_sm, c.items_per_fetch = (block_threads, tile_width, ctas_per_sm,
+                                                                          items_per_fetch)
+        return c
 
 
 class SceneBundle(C.Structure):
@@ -173,6 +181,10 @@ def _declare(lib):
         "mtc_query_first_hit": (C.c_int32, [C.POINTER(SceneView), P, C.c_uint32, P, P]),
         "mtc_batch_scratch_bytes": (C.c_size_t, [C.c_uint32]),
         "mtc_trace_batch": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P, P]),
+        "mtc_batch_table_bytes": (C.c_size_t, [C.c_uint32]),
+        "mtc_batch_prepare": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P,
+                                           C.POINTER(C.c_uint32)]),
+        "mtc_batch_launch": (C.c_int32, [P, C.c_uint32, C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
         "mtc_trace_batch_noalloc": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
         "mtc_refit_tlas": (C.c_int32, [P, C.c_uint64, P, C.c_uint32, P, P, P, P, P, P, P, P]),
         "mtp_scene_make": (P, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), C.c_uint32]),

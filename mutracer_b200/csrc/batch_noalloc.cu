@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(128)
     uint32_t tx = local % J.tilesX, ty = local / J.tilesX;
     uint32_t x = tx * kWarpTileW + (lane % kWarpTileW), y = ty * kWarpTileH + (lane / kWarpTileW);
     if (x < J.width && y < J.height) {
-      for (uint32_t s = 0; s < J.samples; s++) tracePixel(J, x, y, cnt);
+      tracePixelSamples(J, x, y, J.samples, cnt);
       paths += J.samples;
     }
   }

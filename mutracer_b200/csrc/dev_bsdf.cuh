@@ -32,7 +32,11 @@ enum { LOBE_FUZZ = 0, LOBE_COAT = 1, LOBE_METAL = 2, LOBE_SPECULAR = 3,
 
 // OpenPbrPreparedBsdf, openPbrBsdf.wgsl.ts:45-75.
 struct Prepared {
-  Material material;
+  // The resolved material by reference (the WGSL copies it into the prepared
+  // struct; on the GPU that copy only costs registers) plus the one field
+  // prepare() overrides.
+  const Material *mat;
+  float relativeIor;
   Basis basis, coatBasis;
   bool directionFrames;
   V3 viewLocal, diffuseColor;
@@ -439,11 +443,11 @@ MTD V3 finalTransmissionTint(const BsdfContext &c, const Material &m, float ci, 
   return {powf(t.x, e), powf(t.y, e), powf(t.z, e)};
 }
 // openPbrBsdf.wgsl.ts:732-748
-MTD V3 evalSubsurfaceBoundary(const Material &m, V3 view, V3 light, float &pdf) {
+MTD V3 evalSubsurfaceBoundary(float relativeIor, V3 view, V3 light, float &pdf) {
   pdf = 0.0f;
   if (view.z <= 0.0f || light.z >= 0.0f) return v3(0.0f);
   float tc = -light.z;
-  float ef = dielectricFresnel(view.z, m.relativeIor);
+  float ef = dielectricFresnel(view.z, relativeIor);
   pdf = tc * INVPI;
   return v3(1.0f - ef) * INVPI;
 }
@@ -484,7 +488,7 @@ MTD float coatEnergy(const BsdfContext &c, const Material &m, float cosine) {
 }
 // openPbrBsdf.wgsl.ts:805-823
 MTD V3 coatDarkening(const Prepared &p) {
-  const Material &m = p.material;
+  const Material &m = *p.mat;
   float dielectric = 1.0f - m.baseMetalness;
   float opaque = dielectric * (1.0f - m.transmissionWeight) * (1.0f - m.subsurfaceWeight);
   float sss = dielectric * (1.0f - m.transmissionWeight) * m.subsurfaceWeight;
@@ -504,9 +508,9 @@ MTD V3 coatDarkening(const Prepared &p) {
 // openPbrBsdf.wgsl.ts:825-833
 MTD V3 coatBaseScale(const BsdfContext &c, const Prepared &p, float lightCosine) {
   (void)c;
-  if (p.material.coatWeight <= 0.0f) return v3(1.0f);
-  if (p.material.inside) return coatPassage(p.material, -lightCosine);
-  return p.coatBaseScale * coatPassage(p.material, lightCosine);
+  if (p.mat->coatWeight <= 0.0f) return v3(1.0f);
+  if (p.mat->inside) return coatPassage(*p.mat, -lightCosine);
+  return p.coatBaseScale * coatPassage(*p.mat, lightCosine);
 }
 // openPbrBsdf.wgsl.ts:837-850
 MTD Basis directionBasis(const Basis &fallback, V3 tangent, V3 bitangent, V2 direction) {
@@ -534,7 +538,8 @@ MTD V2 roughnessToAlpha(float roughness, float anisotropy) {
 // openPbrBsdf.wgsl.ts:853-1080
 MTD Prepared prepare(const BsdfContext &c, V3 tangent, const Material &material, V3 viewDirection, V3 normal) {
   Prepared p = {};
-  p.material = material;
+  p.mat = &material;
+  p.relativeIor = material.relativeIor;
   p.basis = makeBasis(tangent, normal, fmaxf(material.specularAnisotropy, material.coatAnisotropy));
   p.coatBasis = p.basis;
   p.directionFrames = false;
@@ -561,9 +566,9 @@ MTD Prepared prepare(const BsdfContext &c, V3 tangent, const Material &material,
   p.weights[LOBE_SUBSURFACE] = opaqueDielectric * material.subsurfaceWeight;
 
   p.specularEtaTOverEtaI = applySpecularWeightToIor(1.0f / material.relativeIor, material.specularWeight);
-  p.material.relativeIor = 1.0f / p.specularEtaTOverEtaI;
+  p.relativeIor = 1.0f / p.specularEtaTOverEtaI;
   p.refractionEtaTOverEtaI = p.specularEtaTOverEtaI;
-  p.transmissionReflectionIor = p.material.relativeIor;
+  p.transmissionReflectionIor = p.relativeIor;
   if (material.coatWeight > 0.0f) {
     float weightedCoatIor = 1.0f;
     if (!material.inside) weightedCoatIor = mixf(1.0f, material.coatIor, material.coatWeight);
@@ -577,7 +582,7 @@ MTD Prepared prepare(const BsdfContext &c, V3 tangent, const Material &material,
       p.refractionEtaTOverEtaI = 1.0f / weightedBaseIor;
       p.transmissionReflectionIor = weightedBaseIor;
     }
-    p.material.relativeIor = 1.0f / p.refractionEtaTOverEtaI;
+    p.relativeIor = 1.0f / p.refractionEtaTOverEtaI;
   }
   p.thinFilmExteriorIor = 1.0f;
   p.thinFilmBaseIor = p.specularEtaTOverEtaI;
@@ -661,21 +666,21 @@ MTD Prepared prepare(const BsdfContext &c, V3 tangent, const Material &material,
 
 // openPbrBsdf.wgsl.ts:1083-1091
 MTD float substrateFresnel(const Prepared &p, float cosine, bool reflection) {
-  if (p.material.coatWeight <= 0.0f) return opDielectricFresnel(cosine, p.material.relativeIor);
+  if (p.mat->coatWeight <= 0.0f) return opDielectricFresnel(cosine, p.relativeIor);
   float trans = opDielectricFresnel(cosine, p.transmissionReflectionIor);
   if (!reflection) return trans;
   float opaque = opDielectricFresnel(cosine, 1.0f / p.specularEtaTOverEtaI);
-  float nonOpaque = p.material.transmissionWeight + (1.0f - p.material.transmissionWeight) * p.material.subsurfaceWeight;
+  float nonOpaque = p.mat->transmissionWeight + (1.0f - p.mat->transmissionWeight) * p.mat->subsurfaceWeight;
   return mixf(opaque, trans, nonOpaque);
 }
 
 // openPbrBsdf.wgsl.ts:1092-1422 with allowedLobe = -1 (all lobes)
 MTD V3 evalPrepared(const BsdfContext &c, const Prepared &p, V3 lightDirection, float &pdfOut) {
-  const Material &m = p.material;
+  const Material &m = *p.mat;
   V3 view = p.viewLocal;
   V3 light = toLocal(p.basis, lightDirection);
   bool reflection = light.z * view.z > 0.0f;
-  V3 h = reflection ? normalize(light + view) : normalize(light + view * m.relativeIor);
+  V3 h = reflection ? normalize(light + view) : normalize(light + view * p.relativeIor);
   if (h.z < 0.0f) h = -h;
   V3 response = v3(0.0f);
   float pdf = 0.0f, lobePdf = 0.0f;
@@ -745,7 +750,7 @@ MTD V3 evalPrepared(const BsdfContext &c, const Prepared &p, V3 lightDirection, 
         response += evalMicrofacetReflection(m.alphaX, m.alphaY, view, mirrored, thinWallHalf, tint * (v3(1.0f) - window), lobePdf) *
                     p.weights[LOBE_TRANSMISSION];
       } else {
-        response += evalMicrofacetRefraction(m.alphaX, m.alphaY, m.relativeIor, transmissionTint(c, m), view, light, h, subF, lobePdf) *
+        response += evalMicrofacetRefraction(m.alphaX, m.alphaY, p.relativeIor, transmissionTint(c, m), view, light, h, subF, lobePdf) *
                     p.weights[LOBE_TRANSMISSION];
       }
       if (p.dielectricMsProbability > 0.0f) lobePdf *= 1.0f - p.dielectricMsProbability;
@@ -757,7 +762,7 @@ MTD V3 evalPrepared(const BsdfContext &c, const Prepared &p, V3 lightDirection, 
         response += evalDiffuse(m, m.subsurfaceColor, view, flipped, dsec, lobePdf) * (0.5f * p.weights[LOBE_SUBSURFACE]);
         lobePdf *= 0.5f;
       } else {
-        response += evalSubsurfaceBoundary(m, view, light, lobePdf) * p.weights[LOBE_SUBSURFACE];
+        response += evalSubsurfaceBoundary(p.relativeIor, view, light, lobePdf) * p.weights[LOBE_SUBSURFACE];
       }
       pdf += p.probabilities[LOBE_SUBSURFACE] * lobePdf;
     }
@@ -804,7 +809,7 @@ MTD V3 evalPrepared(const BsdfContext &c, const Prepared &p, V3 lightDirection, 
 // openPbrBsdf.wgsl.ts:1450-1657
 MTD bool sampleDirection(const BsdfContext &c, const Prepared &p, V3 rnd, V3 &lightDirection, bool &isTransmission) {
   (void)c;
-  const Material &m = p.material;
+  const Material &m = *p.mat;
   V3 view = p.viewLocal;
   float rx = rnd.x, ry = rnd.y, lobeSample = rnd.z;
   isTransmission = false;
@@ -854,7 +859,7 @@ MTD bool sampleDirection(const BsdfContext &c, const Prepared &p, V3 rnd, V3 &li
         V3 r = normalize(reflect(-view, hv));
         light = {r.x, r.y, -r.z};
       } else {
-        light = refract(-view, hv, p.material.relativeIor);
+        light = refract(-view, hv, p.relativeIor);
         if (dot(light, light) <= 1e-8f) { isTransmission = false; return false; }
         light = normalize(light);
       }

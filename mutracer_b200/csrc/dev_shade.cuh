@@ -628,11 +628,22 @@ struct Path {
 };
 struct Aux { V3 albedo; V3 normal; bool isBlank; };
 
+// The NEE shadow ray selected at a vertex, traced after shading returns
+// (outside the shading code's branches, and out of its register pressure).
+struct ShadowQuery {
+  Ray ray;
+  float maxDistance;
+  int32_t triangleIndex, instanceIndex;
+  V3 contribution;  // added to the path radiance when unoccluded
+  bool valid;
+};
+
 struct Ctx {
   const JobData &J;
   Sampler smp;
   BsdfContext bc;
   Counters cnt;
+  ShadowQuery shadow;
   MTD uint32_t candidateCount() const { return uint32_t(max(J.u.direct_light_candidates, 1)); }
 };
 
@@ -736,7 +747,7 @@ MTD bool finishDirectLight(Ctx &c, const SurfaceInteraction &si, Path &path, V3 
 struct Scattering { V3 direction, response; float pdf; bool transmission; };
 
 MTD bool isDiscrete(const Prepared &p) {
-  return !p.material.thinWalled && fabsf(p.material.relativeIor - 1.0f) <= 1e-6f &&
+  return !p.mat->thinWalled && fabsf(p.relativeIor - 1.0f) <= 1e-6f &&
          p.probabilities[LOBE_TRANSMISSION] >= 1.0f - 1e-6f;
 }
 
@@ -762,9 +773,17 @@ MTD Scattering sampleScattering(Ctx &c, SurfaceInteraction &si, const Material &
         valid = valid && selectedTarget > 0.0f;
         if (valid) ucw = selected.lightSelectionPmf * scalarWeightSum / (float(count) * selectedTarget);
       }
-      if (valid && !intersectSceneShadow(c.J, selected.ray, selected.maxDistance, selected.triangleIndex,
-                                         si.instanceIndex, c.cnt))
-        path.li += selected.contribution * ucw;
+      // The shadow ray is traced after shading returns (resolveShadow); no
+      // other radiance is added to the path between here and there, so the
+      // sum is formed in the same order.
+      if (valid) {
+        c.shadow.ray = selected.ray;
+        c.shadow.maxDistance = selected.maxDistance;
+        c.shadow.triangleIndex = selected.triangleIndex;
+        c.shadow.instanceIndex = si.instanceIndex;
+        c.shadow.contribution = selected.contribution * ucw;
+        c.shadow.valid = true;
+      }
       if (!isSurface) {
         result.direction = henyeyGreenstein(-path.ray.d, si.mediumAnisotropy, c.smp.s2(c.smp.bounceDim(6)));
         result.pdf = henyeyGreensteinPhase(dot(result.direction, -path.ray.d), si.mediumAnisotropy);
@@ -775,7 +794,7 @@ MTD Scattering sampleScattering(Ctx &c, SurfaceInteraction &si, const Material &
       discrete = isDiscrete(prepared);
       if (discrete) {
         lightDir = toWorld(prepared.basis, -prepared.viewLocal);
-        response = transmissionTint(c.bc, prepared.material) * coatBaseScale(c.bc, prepared, -prepared.viewLocal.z);
+        response = transmissionTint(c.bc, *prepared.mat) * coatBaseScale(c.bc, prepared, -prepared.viewLocal.z);
         scatteringPdf = 1.0f;
         result.transmission = true;
       } else {
@@ -888,7 +907,7 @@ MTD void sampleMaterial(Ctx &c, SurfaceInteraction &si, Material &ma, Path &path
   if (ma.materialType == 2) { path.abort = true; return; }
   Prepared prepared;
   if (!mediumSampled) prepared = prepare(c.bc, v3(0.0f), ma, -path.ray.d, ffnormal);
-  else prepared = Prepared{};
+  else { prepared = Prepared{}; prepared.mat = &ma; }
   Scattering sc = sampleScattering(c, si, ma, prepared, path, ffnormal, !mediumSampled);
   V3 scatterDir = sc.direction;
   float scatteringPdf = sc.pdf;
@@ -1032,65 +1051,32 @@ MTD void completeVertex(Ctx &c, Path &path, int &depth, SurfaceInteraction &si, 
   depth = depth + 1;
 }
 
-// rayTrace.compute.ts:891-946 (RGB integrator, no alpha split)
-MTD float4 integrateRgb(Ctx &c, V2 uv, const Ray &ray, Aux &aux) {
+// One path sample in flight: the locals of the RGB integrator
+// (rayTrace.compute.ts:891-946) kept across events, so that a thread can
+// advance its path one event at a time and start its pixel's next sample as
+// soon as the current one ends, without waiting for the other lanes.
+struct PathSample {
   SurfaceInteraction si;
-  si.albedoSampled = false; si.hit = false; si.triangleIndex = 0; si.instanceIndex = 0; si.materialIndex = 0;
-  si.wavelength = 0.0f; si.spectralChannel = 0; si.mediumType = 0; si.mediumExtinction = v3(0.0f);
-  si.mediumScattering = v3(0.0f); si.mediumAnisotropy = 0.0f;
-  si.position = v3(0.0f); si.normal = v3(0.0f); si.vertexNormal = v3(0.0f); si.shadowOffset = v3(0.0f);
-  si.faceNormal = v3(0.0f);
-  Material ma;
   Path path;
-  path.scatteringMediumEntered = false;
-  path.ray = ray;
-  path.li = v3(0.0f);
-  path.alpha = c.J.u.transmissive_output_alpha_min < 1.0f ? 0.0f : 1.0f;
-  path.beta = v3(1.0f);
-  path.fromEye = true;
-  path.abort = false;
-  path.scatteringPdf = 0.0f;
-  path.scatteringIsDelta = false;
-  path.isNextRefraction = false;
-  int bounceLimit = max(c.J.u.bounces, 0);
-  int eventLimit = min(bounceLimit * 3, 20);
-  bool isNotTransparent = false;
-  int depth = 0;
-  bool sampleIgnored = false;
-  for (int event = 0; event <= eventLimit; event++) {
-    intersectScene(c.J, path.ray, si, depth, event != 0, c.cnt);
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, ma);
-    if (event == 0) {
-      if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
-        aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
-        aux.normal = dot(si.normal, si.position - cameraEye(c.J)) > 0.0f ? -si.normal : si.normal;
-        si.albedoSampled = ma.transmissionWeight > 0.5f;
-      }
-      isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
-    } else {
-      completeVertex(c, path, depth, si, ma, sampleIgnored);
-    }
-    if (isNotTransparent && event > bounceLimit) path.abort = true;
-    if (path.abort || event >= eventLimit) break;
-    shadeVertex(c, uv, path, depth, si, ma, aux, sampleIgnored);
-    if (path.abort) break;
-  }
-  return make_float4(path.li.x, path.li.y, path.li.z, path.alpha);
-}
+  Aux aux;
+  V2 coord;
+  int depth, event;
+  bool sampleIgnored, isNotTransparent;
+};
 
-// rayTrace.compute.ts:1157-1263 main: one path sample for pixel (x, y),
-// accumulated into the job's outputs.
-MTD void tracePixel(const JobData &J, uint32_t x, uint32_t y, Counters &cnt) {
+// rayTrace.compute.ts:1157-1208 main up to the integrator call: sampler
+// state for (x, y, outNormal.a + sampleSequenceOffset), Sobol jitter, camera
+// ray and thin lens, then integrator() locals (:891-905).
+MTD void beginSample(Ctx &c, uint32_t x, uint32_t y, PathSample &ps) {
+  const JobData &J = c.J;
   const mtc_trace_uniform &u = J.u;
   uint32_t W = J.width;
   uint32_t idx = x + y * W;
-  Ctx c{J, Sampler(), BsdfContext{J.s.lut, (J.s.flags & MTC_SCENE_HAS_MEDIUM) != 0u, feature(J, MTC_FEATURE_HAS_THIN_FILM)},
-        Counters()};
-  float4 nrm = J.outNormal[idx];
+  float count = J.outNormal[idx].w;
   V2 outputSize = {u.output_size[0], u.output_size[1]};
   V2 uv = {(float(x) + 0.5f) / outputSize.x, (float(y) + 0.5f) / outputSize.y};
   c.smp.px = x; c.smp.py = y; c.smp.width = W;
-  c.smp.index = uint32_t(nrm.w) + u.sample_sequence_offset;
+  c.smp.index = uint32_t(count) + u.sample_sequence_offset;
   c.smp.bounce = 0; c.smp.hashed = 0;
   c.smp.seed = u.sequence_seed; c.smp.logspp = u.zsobol_log_spp;
   c.smp.pattern = int((J.s.flags & MTC_SCENE_PATTERN_MASK) >> MTC_SCENE_PATTERN_SHIFT);
@@ -1118,8 +1104,77 @@ MTD void tracePixel(const JobData &J, uint32_t x, uint32_t y, Counters &cnt) {
     V3 origin = {vi[0] * lx + vi[4] * ly + vi[12], vi[1] * lx + vi[5] * ly + vi[13], vi[2] * lx + vi[6] * ly + vi[14]};
     cam = {origin, normalize(focus - origin)};
   }
-  Aux aux = {v3(0.0f), v3(0.0f), false};
-  float4 li = integrateRgb(c, coord, cam, aux);
+  ps.coord = coord;
+  ps.aux = {v3(0.0f), v3(0.0f), false};
+  SurfaceInteraction &si = ps.si;
+  si.albedoSampled = false; si.hit = false; si.triangleIndex = 0; si.instanceIndex = 0; si.materialIndex = 0;
+  si.wavelength = 0.0f; si.spectralChannel = 0; si.mediumType = 0; si.mediumExtinction = v3(0.0f);
+  si.mediumScattering = v3(0.0f); si.mediumAnisotropy = 0.0f;
+  si.position = v3(0.0f); si.normal = v3(0.0f); si.vertexNormal = v3(0.0f); si.shadowOffset = v3(0.0f);
+  si.faceNormal = v3(0.0f);
+  Path &path = ps.path;
+  path.scatteringMediumEntered = false;
+  path.ray = cam;
+  path.li = v3(0.0f);
+  path.alpha = u.transmissive_output_alpha_min < 1.0f ? 0.0f : 1.0f;
+  path.beta = v3(1.0f);
+  path.fromEye = true;
+  path.abort = false;
+  path.scatteringPdf = 0.0f;
+  path.scatteringIsDelta = false;
+  path.isNextRefraction = false;
+  ps.depth = 0;
+  ps.event = 0;
+  ps.sampleIgnored = false;
+  ps.isNotTransparent = false;
+}
+
+// One iteration of the integrator's event loop (rayTrace.compute.ts:906-944):
+// extension ray, material, primary guides or completeVertex, shadeVertex.
+// Returns true when the path has ended.
+MTD bool stepPath(Ctx &c, PathSample &ps) {
+  Path &path = ps.path;
+  SurfaceInteraction &si = ps.si;
+  const int bounceLimit = max(c.J.u.bounces, 0);
+  const int eventLimit = min(bounceLimit * 3, 20);
+  const int event = ps.event;
+  Material ma;
+  intersectScene(c.J, path.ray, si, ps.depth, event != 0, c.cnt);
+  getMaterial(c.J, si.materialIndex, si.instanceIndex, ma);
+  if (event == 0) {
+    if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
+      ps.aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+      ps.aux.normal = dot(si.normal, si.position - cameraEye(c.J)) > 0.0f ? -si.normal : si.normal;
+      si.albedoSampled = ma.transmissionWeight > 0.5f;
+    }
+    ps.isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
+  } else {
+    completeVertex(c, path, ps.depth, si, ma, ps.sampleIgnored);
+  }
+  if (ps.isNotTransparent && event > bounceLimit) path.abort = true;
+  if (path.abort || event >= eventLimit) return true;
+  shadeVertex(c, ps.coord, path, ps.depth, si, ma, ps.aux, ps.sampleIgnored);
+  if (path.abort) return true;
+  ps.event = event + 1;
+  return false;
+}
+
+// The deferred NEE visibility test of sampleScattering (sampleMaterial.wgsl.ts
+// :238-245): unoccluded -> the selected candidate's contribution.
+MTD void resolveShadow(Ctx &c, PathSample &ps) {
+  if (!c.shadow.valid) return;
+  c.shadow.valid = false;
+  if (!intersectSceneShadow(c.J, c.shadow.ray, c.shadow.maxDistance, c.shadow.triangleIndex,
+                            c.shadow.instanceIndex, c.cnt))
+    ps.path.li += c.shadow.contribution;
+}
+
+// rayTrace.compute.ts:1209-1262: clamp, NaN guard and accumulation of the
+// finished sample into the job's outputs.
+MTD void endSample(const JobData &J, uint32_t idx, const PathSample &ps) {
+  const mtc_trace_uniform &u = J.u;
+  float4 li = make_float4(ps.path.li.x, ps.path.li.y, ps.path.li.z, ps.path.alpha);
+  const Aux &aux = ps.aux;
   if (u.clamping > 0.0f) {
     float cl = u.clamping;
     li = make_float4(clampf(li.x, -cl, cl), clampf(li.y, -cl, cl), clampf(li.z, -cl, cl), li.w);
@@ -1131,11 +1186,45 @@ MTD void tracePixel(const JobData &J, uint32_t x, uint32_t y, Counters &cnt) {
   J.outAlbedo[idx] = make_float4(alb.x + aux.albedo.x, alb.y + aux.albedo.y, alb.z + aux.albedo.z,
                                  alb.w + (aux.isBlank ? 0.0f : 1.0f));
   float lum = dot(V3{li.x, li.y, li.z}, kLuminance());
+  float4 nrm = J.outNormal[idx];
   if (u.variance_moments != 0) J.outNormal[idx] = make_float4(nrm.x + lum * lum, nrm.y, nrm.z, nrm.w + 1.0f);
   else J.outNormal[idx] = make_float4(nrm.x + aux.normal.x, nrm.y + aux.normal.y, nrm.z + aux.normal.z, nrm.w + 1.0f);
   float4 *mom = J.outCatcher + size_t(idx) * 3 + 2;
   float4 m = *mom;
   *mom = make_float4(m.x + lum, m.y + lum * lum, m.z, m.w);
+}
+
+// `samples` consecutive progressive passes of pixel (x, y), in order, each
+// accumulated before the next begins (the same sums as `samples` separate
+// dispatches).  The thread runs its own sample sequence in one event loop,
+// so a lane whose path ended early starts its next sample while the warp's
+// longer paths are still tracing.  Kept out of line so that every kernel that
+// traces pixels (plain, batched, allocation-free batched) calls the same
+// out-of-line function, compiled once per translation unit from this one
+// source, instead of an inlined copy shaped by its caller: inlined copies could
+// contract multiply-adds differently, and a job's image must be bit-identical
+// alone and in a batch.
+static __device__ __noinline__ void tracePixelSamples(const JobData &J, uint32_t x, uint32_t y, uint32_t samples, Counters &cnt) {
+  Ctx c{J, Sampler(), BsdfContext{J.s.lut, (J.s.flags & MTC_SCENE_HAS_MEDIUM) != 0u, feature(J, MTC_FEATURE_HAS_THIN_FILM)},
+        Counters(), ShadowQuery()};
+  c.shadow.valid = false;
+  const uint32_t idx = x + y * J.width;
+  PathSample ps;
+  uint32_t left = samples;
+  bool active = left > 0u;
+  if (active) beginSample(c, x, y, ps);
+  // No warp vote here: the traversal and shading are latency-bound, and
+  // lanes left free to diverge give the scheduler more independent loads in
+  // flight than a warp forced back together at every event.
+  while (active) {
+    bool ended = stepPath(c, ps);
+    resolveShadow(c, ps);
+    if (ended) {
+      endSample(J, idx, ps);
+      if (--left == 0u) active = false;
+      else beginSample(c, x, y, ps);
+    }
+  }
   cnt.ext += c.cnt.ext;
   cnt.shadow += c.cnt.shadow;
 }

@@ -31,6 +31,19 @@ void *mtp_scene_make(const char *kind, uint32_t width, uint32_t height, uint64_t
   return s;
 }
 
+int mtp_camera_look_at(uint32_t width, uint32_t height, const double *eye, const double *target, const double *up,
+                       double fov_y_deg, mtc_camera_uniform *out) {
+  if (!eye || !target || !up || !out || width == 0 || height == 0 || !(fov_y_deg > 0.0 && fov_y_deg < 180.0))
+    return MT_ERROR_INVALID_ARGUMENT;
+  SceneHost s;
+  s.width = width;
+  s.height = height;
+  CameraDesc c{{eye[0], eye[1], eye[2]}, {target[0], target[1], target[2]}, {up[0], up[1], up[2]}, fov_y_deg};
+  setCamera(s, c);
+  *out = s.camera;
+  return MT_OK;
+}
+
 void mtp_scene_free(void *scene) { delete static_cast<SceneHost *>(scene); }
 
 int mtp_scene_bundle(void *scene, mt_scene_bundle *b) {

@@ -9,6 +9,7 @@
 //  - k_first_hit:  querySceneSoftware (intersect.wgsl.ts:660-684);
 //  - k_refit_*:    TLAS refit (bvhAccel.ts:579-740) on the device.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -36,43 +37,52 @@ __device__ __forceinline__ void flushCounters(const Counters &cnt, uint32_t path
   }
 }
 
-__global__ void __launch_bounds__(kTileW *kTileH)
+#ifndef MT_TRACE_MIN_BLOCKS
+#define MT_TRACE_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
     k_trace(const __grid_constant__ JobData J, uint32_t samples, mtc_counters *counters) {
   uint32_t lx = threadIdx.x % kTileW, ly = threadIdx.x / kTileW;
   uint32_t x = blockIdx.x * kTileW + lx, y = blockIdx.y * kTileH + ly;
   Counters cnt;
   uint32_t paths = 0;
   if (x < J.width && y < J.height) {
-    for (uint32_t s = 0; s < samples; s++) tracePixel(J, x, y, cnt);
+    tracePixelSamples(J, x, y, samples, cnt);
     paths = samples;
   }
   flushCounters(cnt, paths, counters);
 }
 
 // Persistent batched kernel.  queue[0] is the next work item; items are
-// warp tiles laid out job after job (JobData.firstItem / .items).  The loop
-// ends when the counter passes total_items, so every warp exits.
+// warp tiles (tileW x 32/tileW pixels) laid out job after job
+// (JobData.firstItem / .items).  A warp takes `grain` consecutive items per
+// atomic.  The loop ends when the counter passes total_items, so every warp
+// exits.
 __global__ void __launch_bounds__(128)
     k_batch(const JobData *__restrict__ jobs, uint32_t job_count, uint32_t total_items, uint32_t *queue,
-            mtc_counters *counters) {
+            mtc_counters *counters, uint32_t tileW, uint32_t grain) {
   const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lx = lane % tileW, ly = lane / tileW, tileH = 32u / tileW;
   Counters cnt;
   uint32_t paths = 0;
   for (uint32_t guard = 0; guard < total_items + 1u; guard++) {
-    uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(queue, 1u);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= total_items) break;
-    // Jobs are few; a linear scan of the prefix table finds the owner.
+    uint32_t first = 0;
+    if (lane == 0) first = atomicAdd(queue, grain);
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (first >= total_items) break;
+    const uint32_t last = min(first + grain, total_items);
     uint32_t j = 0;
-    while (j + 1 < job_count && jobs[j + 1].firstItem <= item) j++;
-    const JobData &J = jobs[j];
-    uint32_t local = item - J.firstItem;
-    uint32_t tx = local % J.tilesX, ty = local / J.tilesX;
-    uint32_t x = tx * kWarpTileW + (lane % kWarpTileW), y = ty * kWarpTileH + (lane / kWarpTileW);
-    if (x < J.width && y < J.height) {
-      for (uint32_t s = 0; s < J.samples; s++) tracePixel(J, x, y, cnt);
-      paths += J.samples;
+    for (uint32_t item = first; item < last; item++) {
+      // Jobs are few; a forward scan of the prefix table finds the owner.
+      while (j + 1 < job_count && jobs[j + 1].firstItem <= item) j++;
+      const JobData &J = jobs[j];
+      uint32_t local = item - J.firstItem;
+      uint32_t tx = local % J.tilesX, ty = local / J.tilesX;
+      uint32_t x = tx * tileW + lx, y = ty * tileH + ly;
+      if (x < J.width && y < J.height) {
+        tracePixelSamples(J, x, y, J.samples, cnt);
+        paths += J.samples;
+      }
     }
   }
   flushCounters(cnt, paths, counters);
@@ -270,6 +280,35 @@ JobData makeJob(const mtc_scene_view *scene, const mtc_camera_uniform *camera, c
   return J;
 }
 
+struct BatchShape {
+  uint32_t blockThreads, tileW, tileH, ctasPerSm, grain;
+};
+// Resolves a (possibly NULL) mtc_batch_config to launch parameters; false for
+// out-of-range values.
+bool batchShape(const mtc_batch_config *c, BatchShape &out) {
+  out = BatchShape{128u, 8u, 4u, 2u, 1u};
+  if (!c) return true;
+  if (c->struct_size != sizeof(mtc_batch_config)) return false;
+  if (c->block_threads) {
+    if (c->block_threads > 128u || c->block_threads % 32u) return false;
+    out.blockThreads = c->block_threads;
+  }
+  if (c->tile_width) {
+    if (c->tile_width > 32u || (32u % c->tile_width)) return false;
+    out.tileW = c->tile_width;
+    out.tileH = 32u / c->tile_width;
+  }
+  if (c->ctas_per_sm) {
+    if (c->ctas_per_sm > 32u) return false;
+    out.ctasPerSm = c->ctas_per_sm;
+  }
+  if (c->items_per_fetch) {
+    if (c->items_per_fetch > 16u) return false;
+    out.grain = c->items_per_fetch;
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -303,40 +342,74 @@ size_t mtc_batch_scratch_bytes(uint32_t job_count) {
   return (size_t(job_count) * sizeof(JobData) + 255) / 256 * 256 + 256;
 }
 
-mt_status mtc_trace_batch(const mtc_job_desc *jobs_host, uint32_t job_count, const mtc_batch_config *config,
-                          void *queue_state, uint32_t *status_out, mtc_counters *counters, void *stream) {
-  if ((!jobs_host && job_count) || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
-  if (config && config->struct_size != sizeof(mtc_batch_config)) return MT_ERROR_INVALID_ARGUMENT;
-  if (job_count == 0) return MT_OK;
-  std::vector<JobData> table(job_count);
+size_t mtc_batch_table_bytes(uint32_t job_count) { return size_t(job_count) * sizeof(JobData); }
+
+mt_status mtc_batch_prepare(const mtc_job_desc *jobs, uint32_t job_count, const mtc_batch_config *config,
+                            void *table, uint32_t *total_items) {
+  if ((!jobs || !table) && job_count) return MT_ERROR_INVALID_ARGUMENT;
+  if (!total_items) return MT_ERROR_INVALID_ARGUMENT;
+  BatchShape shape;
+  if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
+  JobData *t = static_cast<JobData *>(table);
   uint64_t total = 0;
   for (uint32_t j = 0; j < job_count; j++) {
-    const mtc_job_desc &d = jobs_host[j];
+    const mtc_job_desc &d = jobs[j];
     if (!validScene(&d.scene) || !validUniform(&d.uniform) || !d.out.color || !d.out.normal || !d.out.albedo ||
         !d.out.shadow_catcher)
       return MT_ERROR_INVALID_ARGUMENT;
-    table[j] = makeJob(&d.scene, &d.camera, &d.uniform, &d.out, d.samples);
-    table[j].firstItem = uint32_t(total);
-    total += d.samples ? table[j].items : 0;
-    if (!d.samples) table[j].items = 0;
+    JobData J = makeJob(&d.scene, &d.camera, &d.uniform, &d.out, d.samples);
+    J.tilesX = (J.width + shape.tileW - 1) / shape.tileW;
+    J.tilesY = (J.height + shape.tileH - 1) / shape.tileH;
+    J.items = d.samples ? J.tilesX * J.tilesY : 0u;
+    J.firstItem = uint32_t(total);
+    total += J.items;
+    if (total >= 0x7fffffffull) return MT_ERROR_INVALID_ARGUMENT;
+    std::memcpy(&t[j], &J, sizeof(J));
   }
-  if (total >= 0xffffffffull) return MT_ERROR_INVALID_ARGUMENT;
+  *total_items = uint32_t(total);
+  return MT_OK;
+}
+
+mt_status mtc_batch_launch(const void *table, uint32_t job_count, uint32_t total_items, const mtc_batch_config *config,
+                           void *queue_state, mtc_counters *counters, void *stream) {
+  if ((!table && job_count) || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
+  BatchShape shape;
+  if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
+  if (job_count == 0 || total_items == 0) return MT_OK;
   cudaStream_t st = (cudaStream_t)stream;
   char *scratch = (char *)queue_state;
   size_t tableBytes = (size_t(job_count) * sizeof(JobData) + 255) / 256 * 256;
   uint32_t *queue = (uint32_t *)(scratch + tableBytes);
-  cudaError_t e = cudaMemcpyAsync(scratch, table.data(), size_t(job_count) * sizeof(JobData), cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaMemcpyAsync(scratch, table, size_t(job_count) * sizeof(JobData), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(queue, 0, 256, st);
   if (e != cudaSuccess) return cudaStatus(e);
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  uint32_t ctasPerSm = config && config->ctas_per_sm ? config->ctas_per_sm : 4u;
-  uint32_t grid = uint32_t(sms) * ctasPerSm;
-  k_batch<<<grid, 128, 0, st>>>((const JobData *)scratch, job_count, uint32_t(total), queue, counters);
-  if (status_out) cudaMemsetAsync(status_out, 0, sizeof(uint32_t), st);
-  // The pageable host table is staged by cudaMemcpyAsync before it returns.
+  // Never more CTAs than warps of work.
+  uint64_t warpsWanted = (uint64_t(total_items) + shape.grain - 1) / shape.grain;
+  uint64_t grid = uint64_t(sms) * shape.ctasPerSm;
+  grid = std::min<uint64_t>(grid, (warpsWanted + shape.blockThreads / 32 - 1) / (shape.blockThreads / 32));
+  k_batch<<<uint32_t(std::max<uint64_t>(grid, 1)), shape.blockThreads, 0, st>>>(
+      (const JobData *)scratch, job_count, total_items, queue, counters, shape.tileW, shape.grain);
   return cudaStatus(cudaGetLastError());
+}
+
+mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count, const mtc_batch_config *config,
+                          void *queue_state, uint32_t *status_out, mtc_counters *counters, void *stream) {
+  if ((!jobs && job_count) || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
+  if (config && config->struct_size != sizeof(mtc_batch_config)) return MT_ERROR_INVALID_ARGUMENT;
+  if (job_count == 0) return MT_OK;
+  std::vector<JobData> table(job_count);
+  uint32_t total = 0;
+  mt_status st = mtc_batch_prepare(jobs, job_count, config, table.data(), &total);
+  if (st != MT_OK) return st;
+  if (status_out) {
+    cudaError_t e = cudaMemsetAsync(status_out, 0, sizeof(uint32_t), (cudaStream_t)stream);
+    if (e != cudaSuccess) return cudaStatus(e);
+  }
+  // A pageable host table is staged by cudaMemcpyAsync before it returns.
+  return mtc_batch_launch(table.data(), job_count, total, config, queue_state, counters, stream);
 }
 
 mt_status mtc_refit_tlas(void *tlas, uint64_t tlas_vec4_count, void *instances, uint32_t instance_count,

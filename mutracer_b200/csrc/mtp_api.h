@@ -32,6 +32,10 @@ int mtp_build_binned_sah(const float *aabbs, uint32_t count, int bins, uint32_t 
 int mtp_build_blas(const float *positions, uint32_t vertexCount, const uint32_t *indices, uint32_t triCount, int bins,
                    float *out, uint64_t capacity, uint64_t *vec4Count, uint32_t *maxDepth);
 int mtp_energy_lut(float *out);
+/* CameraUniform of a perspective look-at camera for a width x height image
+ * (the generators' own camera construction). */
+int mtp_camera_look_at(uint32_t width, uint32_t height, const double *eye, const double *target, const double *up,
+                       double fov_y_deg, mtc_camera_uniform *out);
 int mtp_env_distribution(const float *image, uint32_t width, uint32_t height, float *distribution, double *power);
 
 #ifdef __cplusplus
