@@ -39,12 +39,26 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--width", type=int, default=1920)
-    p.add_argument("--height", type=int, default=1080)
-    p.add_argument("--spp", type=int, default=16)
+    p.add_argument("--workload", default=WORKLOAD, choices=["instanced_spheres", "cornell", "glass_spheres"])
+    p.add_argument("--width", type=int, default=None)
+    p.add_argument("--height", type=int, default=None)
+    p.add_argument("--spp", type=int, default=None)
+    p.add_argument("--form", default="megakernel", choices=["megakernel", "wavefront"],
+                   help="engine of the headline step: the plain drop-in megakernel (mtc_trace_samples) or the "
+                        "wavefront kernels (mtc_stream_run)")
+    p.add_argument("--slots", type=int, default=1 << 20, help="wavefront paths in flight")
+    p.add_argument("--refill-lanes", type=int, default=0, help="wavefront traversal refill threshold (0: default)")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--mixed-jobs", type=int, default=64)
+    p.add_argument("--mixed-spp-divisor", type=int, default=16,
+                   help="scale the mixed jobs' spp (log-uniform 4-256) down by this factor")
+    p.add_argument("--serve-requests", type=int, default=48)
+    p.add_argument("--serve-rate", type=float, default=20.0)
+    p.add_argument("--serve-scenes", type=int, default=8)
+    p.add_argument("--serve-spp-divisor", type=int, default=16,
+                   help="scale the requests' target spp (uniform 16-128) down by this factor")
     return p.parse_args()
 
 
@@ -149,12 +163,20 @@ def cpu_baseline(host, spp, seconds):
                       f"({done_paths} path samples, {elapsed:.1f} s)"}
 
 
+def workload_desc(name, host, spp):
+    b = host.bundle
+    env = f"{b.env_width}x{b.env_height} sky" if b.env_width else "no env map"
+    return (f"{name} {host.width}x{host.height} {spp} spp, bounces {b.uniform.bounces}, "
+            f"{host.info.triangles} instanced tris ({host.info.unique_triangles} unique), {env} + "
+            f"{b.lights_count} analytic lights")
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from mutracer_b200 import scene
-    host = scene.make_workload(WORKLOAD, width=args.width, height=args.height)
+    host = scene.make_workload(args.workload, width=args.width, height=args.height)
     spp = args.spp
     per_step = max(1.0, args.cpu_seconds / max(1, args.steps))
     for _ in range(args.warmup):
@@ -172,8 +194,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1000 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": f"{WORKLOAD} {args.width}x{args.height} {spp} spp depth 6, 4,014,080 instanced tris",
-                       "parallelism": "host threads"},
+            "config": {"workload": workload_desc(args.workload, host, spp), "parallelism": "host threads"},
             "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": os.cpu_count(), "kind": "port",
                              "sample": samples[-1]},
             "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -193,7 +214,7 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev_id = torch.device("cuda", local)
-    host = scene.make_workload(WORKLOAD, width=args.width, height=args.height)
+    host = scene.make_workload(args.workload, width=args.width, height=args.height)
     dev = scene.DeviceScene(host, dev_id)
     acc = trace.Accumulation(host.width, host.height, dev_id)
     spp = args.spp
@@ -202,9 +223,22 @@ def run_b200(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev_id)  # 256 MB > 126 MB L2
     paths_per_step = host.width * host.height * spp
 
-    def step():
-        acc.zero_()
-        trace.trace_samples(dev, acc, spp, counters=counters)
+    if args.form == "wavefront":
+        from mutracer_b200 import batch
+        job = batch.RenderJob(dev, spp, device=dev_id)
+        acc = job.acc
+        sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=args.slots, refill_lanes=args.refill_lanes),
+                               device=dev_id)
+        sb.counters = counters
+        sb.set_jobs([job])
+
+        def step():
+            acc.zero_()
+            sb.run()
+    else:
+        def step():
+            acc.zero_()
+            trace.trace_samples(dev, acc, spp, counters=counters)
 
     for _ in range(args.warmup):
         step()
@@ -239,13 +273,13 @@ def run_b200(args):
               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
               "data": "synthetic (seeded generator, random-init scene)",
-              "config": {"workload": f"{WORKLOAD} {host.width}x{host.height} {spp} spp depth 6, "
-                                     f"{host.info.triangles} instanced tris ({host.info.unique_triangles} unique), "
-                                     f"2048x1024 sky + 4 rect lights",
+              "config": {"workload": workload_desc(args.workload, host, spp),
                          "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                         "l2": "flushed between steps (256 MB write)", "form": "plain megakernel"},
+                         "l2": "flushed between steps (256 MB write)",
+                         "form": "plain megakernel (mtc_trace_samples)" if args.form == "megakernel"
+                         else f"wavefront (mtc_stream_run, {args.slots} slots)"},
               "mrays_per_s": round(rays_per_step / (ms_per_step / 1000.0) / 1e6, 2),
-              "gpu_launches": args.steps,
+              "gpu_launches": int(cnt[3]),
               "clocks": clocks.summary()}
     if rank != 0:
         if world > 1:
@@ -269,6 +303,11 @@ def run_b200(args):
         result["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     if not args.no_e2e:
         result["e2e"] = e2e_context(host, spp, max(1, min(args.steps, 3)))
+    if not args.no_batch:
+        del dev, acc, flush
+        torch.cuda.empty_cache()
+        result["batched"] = mixed_batch(args, dev_id)
+        result["served"] = served_stream(args, dev_id)
     print(json.dumps(result), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -300,8 +339,110 @@ def e2e_context(host, spp, steps):
             "ms_per_step": round(dt * 1000, 2), "path": "mt_context_commit_bundle + render + read_pixels"}
 
 
+def _timed(fn, stream):
+    import torch
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    fn()
+    e.record(stream)
+    e.synchronize()
+    return s.elapsed_time(e)
+
+
+def mixed_batch(args, dev_id):
+    """The mixed 64-job workload three ways, each job from zeroed buffers:
+    plain per-sample (one mtc_trace_samples launch per sample per job, the
+    reference host's dispatch pattern), plain per-job (one launch per job with
+    all its samples) and batched (all jobs in one persistent launch, replayed
+    from a captured CUDA graph, launch shape from the autotuner).  Every job's
+    image is bit-identical across the three (checked here on the first job)."""
+    import torch
+    from mutracer_b200 import batch
+    stream = torch.cuda.current_stream()
+    specs = batch.mixed_jobs(args.mixed_jobs, seed=0, spp_divisor=args.mixed_spp_divisor)
+    t0 = time.perf_counter()
+    jobs = batch.build_mixed(specs, dev_id)
+    build_s = time.perf_counter() - t0
+    paths = batch.total_paths(jobs)
+
+    def zero():
+        for j in jobs:
+            j.acc.zero_()
+
+    t0 = time.perf_counter()
+    cfg, timings = batch.autotune(jobs, probe_samples=1, repeats=1, device=dev_id)
+    tune_s = time.perf_counter() - t0
+    b = batch.Batch(len(jobs), cfg, dev_id)
+    b.set_jobs(jobs)
+    b.capture()
+    res = {}
+    ref_img = None
+    for name, fn in (("plain_per_sample", lambda: batch.run_plain(jobs, per_sample=True)),
+                     ("plain_per_job", lambda: batch.run_plain(jobs, per_sample=False)),
+                     ("batched_graph", b.replay)):
+        ms = []
+        for it in range(2):               # one warm-up, one timed
+            zero()
+            ms.append(_timed(fn, stream))
+        res[name] = {"ms": round(ms[-1], 2), "mpaths_per_s": round(paths / ms[-1] / 1e3, 3)}
+        img = jobs[0].acc.color.clone()
+        if ref_img is None:
+            ref_img = img
+        res[name]["bit_identical_to_plain"] = bool(torch.equal(img, ref_img))
+    b.release()
+    shape = (cfg.block_threads, cfg.ctas_per_sm, cfg.tile_width, cfg.items_per_fetch)
+    res.update({
+        "workload": f"{len(jobs)} jobs, resolution from {{256^2, 512^2, 1280x720, 1920x1080}}, spp log-uniform "
+                    f"[4,256] / {args.mixed_spp_divisor} (rounded up), instanced-sphere scenes 10k-2M tris, "
+                    f"1-8 rect lights + 512x256 sky, depth 6, seed 0",
+        "paths": int(paths), "scene_build_s": round(build_s, 1), "autotune_s": round(tune_s, 1),
+        "autotuned_shape": {"block_threads": shape[0], "ctas_per_sm": shape[1], "tile_width": shape[2],
+                            "items_per_fetch": shape[3]},
+        "autotune_probe_ms": {f"{k[0]}x{k[1]}/t{k[2]}/g{k[3]}": round(v, 2) for k, v in timings.items()},
+        "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["batched_graph"]["ms"], 3),
+        "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["batched_graph"]["ms"], 3),
+    })
+    del jobs
+    torch.cuda.empty_cache()
+    return res
+
+
+def served_stream(args, dev_id):
+    """Poisson request stream over a pool of resident scenes, served by
+    continuous batching; p50/p99 time-to-target-spp and sustained Mpaths/s."""
+    import torch
+    from mutracer_b200 import batch, scene, serve
+    pool = serve.ScenePool(dev_id)
+    specs = batch.mixed_jobs(args.serve_scenes, seed=7, tri_range=(10_000, 8_000_000))
+    for sp in specs:
+        pool.add(sp.job_id, scene.SceneHost("instanced_spheres", 256, 256, sp.seed, sp.scene_params()))
+    reqs = serve.poisson_requests(pool, args.serve_requests, args.serve_rate, seed=11,
+                                  spp_divisor=args.serve_spp_divisor)
+    budget = 12 * 1024 ** 3
+    srv = serve.Server(pool, hbm_budget_bytes=budget, max_jobs=64, quantum=2, device=dev_id)
+    warm = serve.poisson_requests(pool, 4, 1000.0, seed=12, spp_divisor=args.serve_spp_divisor)
+    srv.run(warm)
+    stats = srv.run(reqs)
+    srv.release()
+    stats.update({
+        "workload": f"{len(reqs)} requests, Poisson {args.serve_rate}/s, {len(pool)} resident scenes "
+                    f"({pool.device_bytes / 1e6:.0f} MB, 10k-8M tris), orbit cameras FOV 30-70, resolution from "
+                    f"{{256^2, 512^2, 1280x720, 1920x1080}}, target spp U[16,128] / {args.serve_spp_divisor}",
+        "hbm_budget_gb": budget / 1024 ** 3, "quantum_spp": 2, "max_jobs": 64,
+    })
+    for k in ("mpaths_per_s", "p50_s", "p99_s", "mean_s", "device_seconds"):
+        stats[k] = round(stats[k], 4)
+    return stats
+
+
 def main():
     args = parse()
+    from mutracer_b200 import scene
+    w = scene.WORKLOADS[args.workload]
+    args.width = args.width or w["width"]
+    args.height = args.height or w["height"]
+    args.spp = args.spp or w["spp"]
     if args.impl == "reference":
         run_reference(args)
     else:

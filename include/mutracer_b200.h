@@ -192,12 +192,13 @@ typedef struct mtc_hit {
   float _pad;
 } mtc_hit;
 
-/* Runtime counters (extension+shadow rays, path samples), for Mrays/s. */
+/* Runtime counters (extension+shadow rays, path samples, kernel launches
+ * that ran), for Mrays/s and launch counts. */
 typedef struct mtc_counters {
   unsigned long long path_samples;
   unsigned long long extension_rays;
   unsigned long long shadow_rays;
-  unsigned long long _pad;
+  unsigned long long kernel_launches;
 } mtc_counters;
 
 /* Library ABI version of this header. */
@@ -267,31 +268,65 @@ typedef struct mtc_batch_config {
  * caller-provided device scratch of mtc_batch_scratch_bytes(job_count) bytes
  * that receives the job table and the work-queue counter (reset by the call
  * on `stream`).  status_out (device, may be NULL) is set to 0.  Work is
- * pulled with one atomic per 32-pixel tile; every sample of a tile runs in
- * order on one warp, so each job's outputs are bit-identical to running it
- * alone through mtc_trace_samples. */
-size_t mtc_batch_scratch_bytes(uint32_t job_count);
+ * pulled with one atomic per warp tile (config->items_per_fetch tiles); every
+ * sample of a tile runs in order on one warp, so each job's outputs are
+ * bit-identical to running it alone through mtc_trace_samples. */
+size_t mtc_batch_scratch_bytes(uint32_t capacity);
 mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count,
                           const mtc_batch_config *config, void *queue_state,
                           uint32_t *status_out, mtc_counters *counters,
                           void *stream);
 
-/* The two halves of mtc_trace_batch, for replay.  mtc_batch_prepare builds
- * the device job table of `jobs` into caller HOST memory `table` of
- * mtc_batch_table_bytes(job_count) bytes and reports the number of work items
- * (host only, no CUDA call); `config` must be the one later given to
- * mtc_batch_launch.  mtc_batch_launch copies that table into
- * `queue_state`, clears the work counter and launches the persistent kernel,
- * all ordered on `stream`; with `table` in pinned host memory the three
- * operations can be captured in a CUDA graph and replayed after the table is
- * rewritten in place. */
-size_t mtc_batch_table_bytes(uint32_t job_count);
+/* The two halves of mtc_trace_batch, for replay.  mtc_batch_prepare writes
+ * the job table of `jobs` (a 256-byte header with the job count and work-item
+ * total, then one entry per job) into caller HOST memory `table` of at least
+ * mtc_batch_table_bytes(job_count) bytes and reports the item total (host
+ * only, no CUDA call).  mtc_batch_launch copies mtc_batch_table_bytes(capacity)
+ * bytes of `table` into `queue_state` (mtc_batch_scratch_bytes(capacity)
+ * bytes of device memory), clears the work counter and launches the
+ * persistent kernel, all ordered on `stream`.  The kernel reads the job count
+ * and total from the copied header, so with `table` in pinned host memory the
+ * three operations can be captured once in a CUDA graph and replayed after
+ * mtc_batch_prepare has rewritten the table with up to `capacity` other jobs.
+ * The tile shape is fixed by prepare's config; launch's config sets the
+ * block size, CTAs per SM and fetch grain. */
+size_t mtc_batch_table_bytes(uint32_t capacity);
 mt_status mtc_batch_prepare(const mtc_job_desc *jobs, uint32_t job_count,
                             const mtc_batch_config *config, void *table,
                             uint32_t *total_items);
-mt_status mtc_batch_launch(const void *table, uint32_t job_count, uint32_t total_items,
+mt_status mtc_batch_launch(const void *table, uint32_t capacity,
                            const mtc_batch_config *config, void *queue_state,
                            mtc_counters *counters, void *stream);
+
+/* Wavefront form of the batched launch.  The integrator's event loop is cut
+ * at its traversals into kernels over queues of in-flight path slots
+ * (closest-hit traversal, shading, NEE shadow traversal, accumulation and
+ * restart), so the latency-bound traversals run at the occupancy of their own
+ * small register budget instead of the shading code's.  A slot owns one
+ * pixel until all of its samples are done, so outputs are bit-identical to
+ * mtc_trace_samples and to mtc_trace_batch.  `table` is a HOST job table
+ * written by mtc_batch_prepare for up to `capacity` jobs; `state` is device
+ * memory of mtc_stream_state_bytes(capacity, config) bytes.  The call
+ * enqueues the work on `stream` and returns once the queues have drained
+ * (it waits on the stream); calls on one device are serialised.  No
+ * counterpart in the reference. */
+typedef struct mtc_stream_config {
+  uint32_t struct_size;
+  uint32_t slots;                 /* paths in flight, 1024..2^25 (default 2^20) */
+  uint32_t iterations_per_check;  /* event iterations between queue polls (default 8) */
+  uint32_t max_iterations;        /* MT_ERROR_TIMEOUT beyond this (default 2^20) */
+  uint32_t refill_lanes;          /* idle lanes of a warp that trigger fetching new
+                                     rays in the traversal kernels, 1..32 (default 8) */
+  uint32_t regroup_interval;      /* order the shading queue by material class every
+                                     N-th event iteration, 1..1024 (default 1);
+                                     MTC_REGROUP_OFF never */
+  uint32_t _pad[2];
+} mtc_stream_config;
+#define MTC_REGROUP_OFF 0xffffffffu
+size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config);
+mt_status mtc_stream_run(const void *table, uint32_t capacity,
+                         const mtc_stream_config *config, void *state,
+                         mtc_counters *counters, void *stream);
 
 /* No counterpart in the reference.  For callers that cannot let the library
  * allocate device memory (a host that owns a fixed device budget and its own

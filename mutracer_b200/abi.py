@@ -35,6 +35,7 @@ MTC_MATERIAL_VEC4_ROWS = 26
 MTC_LIGHT_VEC4_ROWS = 6
 MTC_ENERGY_LUT_WIDTH = 32
 MTC_ENERGY_LUT_HEIGHT = 2177
+MTC_REGROUP_OFF = 0xFFFFFFFF
 MTC_BATCH_NOALLOC_MAX_JOBS = 64
 
 
@@ -100,7 +101,7 @@ class Hit(C.Structure):
 
 class Counters(C.Structure):
     _fields_ = [("path_samples", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("_pad", C.c_uint64)]
+                ("kernel_launches", C.c_uint64)]
 
 
 class JobDesc(C.Structure):
@@ -118,6 +119,20 @@ class BatchConfig(C.Structure):
         c.struct_size = C.sizeof(cls)
         c.block_threads, c.tile_width, c.ctas_per_sm, c.items_per_fetch = (block_threads, tile_width, ctas_per_sm,
                                                                           items_per_fetch)
+        return c
+
+
+class StreamConfig(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("slots", C.c_uint32), ("iterations_per_check", C.c_uint32),
+                ("max_iterations", C.c_uint32), ("refill_lanes", C.c_uint32), ("regroup_interval", C.c_uint32),
+                ("_pad", C.c_uint32 * 2)]
+
+    @classmethod
+    def make(cls, slots=0, iterations_per_check=0, max_iterations=0, refill_lanes=0, regroup_interval=0):
+        c = cls()
+        c.struct_size = C.sizeof(cls)
+        c.slots, c.iterations_per_check, c.max_iterations = slots, iterations_per_check, max_iterations
+        c.refill_lanes, c.regroup_interval = refill_lanes, regroup_interval
         return c
 
 
@@ -166,7 +181,7 @@ class SceneInfo(C.Structure):
 
 
 STRUCT_ORDER = [TraceUniform, CameraUniform, SceneView, Outputs, Hit, Counters, JobDesc, BatchConfig,
-                SceneBundle, RenderSettings, ContextSnapshot, JobSnapshot, SceneInfo]
+                SceneBundle, RenderSettings, ContextSnapshot, JobSnapshot, SceneInfo, StreamConfig]
 
 _lib = None
 
@@ -182,9 +197,11 @@ def _declare(lib):
         "mtc_batch_scratch_bytes": (C.c_size_t, [C.c_uint32]),
         "mtc_trace_batch": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P, P]),
         "mtc_batch_table_bytes": (C.c_size_t, [C.c_uint32]),
+        "mtc_stream_state_bytes": (C.c_size_t, [C.c_uint32, C.POINTER(StreamConfig)]),
+        "mtc_stream_run": (C.c_int32, [P, C.c_uint32, C.POINTER(StreamConfig), P, P, P]),
         "mtc_batch_prepare": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P,
                                            C.POINTER(C.c_uint32)]),
-        "mtc_batch_launch": (C.c_int32, [P, C.c_uint32, C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
+        "mtc_batch_launch": (C.c_int32, [P, C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
         "mtc_trace_batch_noalloc": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
         "mtc_refit_tlas": (C.c_int32, [P, C.c_uint64, P, C.c_uint32, P, P, P, P, P, P, P, P]),
         "mtp_scene_make": (P, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), C.c_uint32]),
@@ -198,6 +215,8 @@ def _declare(lib):
         "mtp_build_binned_sah": (C.c_int, [P, C.c_uint32, C.c_int, P, P, P, P, P]),
         "mtp_build_blas": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.c_int, P, C.c_uint64, P, P]),
         "mtp_energy_lut": (C.c_int, [P]),
+        "mtp_camera_look_at": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), C.c_double, C.POINTER(CameraUniform)]),
         "mtp_env_distribution": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P]),
         "mt_render_settings_default": (C.c_int32, [C.POINTER(RenderSettings)]),
         "mt_context_create": (C.c_int32, [C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]),

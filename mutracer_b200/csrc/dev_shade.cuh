@@ -591,23 +591,6 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
   si.position = mat4v(l0, l1, l2, l3, position, 1.0f);
 }
 
-// intersect.wgsl.ts:696-740
-MTD bool intersectScene(const JobData &J, const Ray &r, SurfaceInteraction &si, int bounces, bool doubleSided,
-                        Counters &cnt) {
-  si.hit = false;
-  if (J.u.is_empty > 0) return false;
-  cnt.ext++;
-  TraversalHit h;
-  h.tMax = RAY_MAX_DISTANCE;
-  h.triangleIndex = -1;
-  h.insIdx = -1;
-  traverse<false>(J.s, J.u.blas_offset, r.o, r.d, bounces, doubleSided, si.triangleIndex, si.instanceIndex, h);
-  if (h.insIdx >= 0) {
-    si.triangleIndex = h.triangleIndex;
-    completeSurfaceInteraction(J, si, h, r.o, r.d);
-  }
-  return si.hit;
-}
 // intersect.wgsl.ts:829-879
 MTD bool intersectSceneShadow(const JobData &J, const Ray &r, float lightDistance, int32_t tri, int32_t ins,
                               Counters &cnt) {
@@ -1066,8 +1049,9 @@ struct PathSample {
 
 // rayTrace.compute.ts:1157-1208 main up to the integrator call: sampler
 // state for (x, y, outNormal.a + sampleSequenceOffset), Sobol jitter, camera
-// ray and thin lens, then integrator() locals (:891-905).
-MTD void beginSample(Ctx &c, uint32_t x, uint32_t y, PathSample &ps) {
+// ray and thin lens, then integrator() locals (:891-905).  Out of line, like
+// shadeStep and endSample, so every kernel runs one compiled copy.
+static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, PathSample &ps) {
   const JobData &J = c.J;
   const mtc_trace_uniform &u = J.u;
   uint32_t W = J.width;
@@ -1129,17 +1113,35 @@ MTD void beginSample(Ctx &c, uint32_t x, uint32_t y, PathSample &ps) {
   ps.isNotTransparent = false;
 }
 
-// One iteration of the integrator's event loop (rayTrace.compute.ts:906-944):
-// extension ray, material, primary guides or completeVertex, shadeVertex.
-// Returns true when the path has ended.
-MTD bool stepPath(Ctx &c, PathSample &ps) {
+// The traversal half of intersectScene (intersect.wgsl.ts:696-740) for the
+// path's current event: the closest hit of its extension ray.
+MTD void traceExtension(const JobData &J, const PathSample &ps, TraversalHit &h, Counters &cnt) {
+  h.tMax = RAY_MAX_DISTANCE;
+  h.triangleIndex = -1;
+  h.insIdx = -1;
+  if (J.u.is_empty > 0) return;
+  cnt.ext++;
+  traverse<false>(J.s, J.u.blas_offset, ps.path.ray.o, ps.path.ray.d, ps.depth, ps.event != 0, ps.si.triangleIndex,
+                  ps.si.instanceIndex, h);
+}
+
+// The rest of one iteration of the integrator's event loop
+// (rayTrace.compute.ts:906-944) once the extension ray's closest hit `h` is
+// known: surface interaction, material, primary guides or completeVertex,
+// shadeVertex.  Returns true when the path has ended.  Out of line so that
+// the megakernel and the wavefront shading kernel run one compiled copy.
+static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const TraversalHit &h) {
   Path &path = ps.path;
   SurfaceInteraction &si = ps.si;
   const int bounceLimit = max(c.J.u.bounces, 0);
   const int eventLimit = min(bounceLimit * 3, 20);
   const int event = ps.event;
+  si.hit = false;
+  if (h.insIdx >= 0) {
+    si.triangleIndex = h.triangleIndex;
+    completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
+  }
   Material ma;
-  intersectScene(c.J, path.ray, si, ps.depth, event != 0, c.cnt);
   getMaterial(c.J, si.materialIndex, si.instanceIndex, ma);
   if (event == 0) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
@@ -1159,6 +1161,13 @@ MTD bool stepPath(Ctx &c, PathSample &ps) {
   return false;
 }
 
+// One iteration of the integrator's event loop.
+MTD bool stepPath(Ctx &c, PathSample &ps) {
+  TraversalHit h;
+  traceExtension(c.J, ps, h, c.cnt);
+  return shadeStep(c, ps, h);
+}
+
 // The deferred NEE visibility test of sampleScattering (sampleMaterial.wgsl.ts
 // :238-245): unoccluded -> the selected candidate's contribution.
 MTD void resolveShadow(Ctx &c, PathSample &ps) {
@@ -1171,7 +1180,7 @@ MTD void resolveShadow(Ctx &c, PathSample &ps) {
 
 // rayTrace.compute.ts:1209-1262: clamp, NaN guard and accumulation of the
 // finished sample into the job's outputs.
-MTD void endSample(const JobData &J, uint32_t idx, const PathSample &ps) {
+static __device__ __noinline__ void endSample(const JobData &J, uint32_t idx, const PathSample &ps) {
   const mtc_trace_uniform &u = J.u;
   float4 li = make_float4(ps.path.li.x, ps.path.li.y, ps.path.li.z, ps.path.alpha);
   const Aux &aux = ps.aux;

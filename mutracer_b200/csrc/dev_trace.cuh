@@ -332,4 +332,160 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
   return false;
 }
 
+// getBVHTraverseCode (intersect.wgsl.ts:213-629) as a restartable state
+// machine, for kernels that keep a queue of rays and give a lane a new ray as
+// soon as its current one has finished.  Each step() does exactly one of:
+// one BLAS node of the current instance, entering the next instance of the
+// current TLAS leaf, or one TLAS node.  Visit order, box tests, the `>` tie
+// rule and the self-hit and backface rules are those of traverse(), so the
+// hits are bit-identical to it.
+template <bool shadow>
+struct RayTraversal {
+  const float4 *bvh, *ins, *mats;
+  const uint32_t *attr;
+  uint32_t vstride;
+  int32_t blasBase;
+  V3 rayO, rayD, invD;
+  int bounces;
+  bool doubleSided;
+  int32_t currentTri, currentIns;
+  int32_t tlasStack[MTC_MAX_STACK];
+  int32_t blasStack[MTC_MAX_STACK];
+  int tlasTop, blasTop;
+  int32_t leafNode, io;
+  V3 o, d, linvD, shear;
+  int maxDim;
+  int32_t blasOffset, vertexOffset, sideMaterial, insIdx;
+  bool found;
+  TraversalHit h;
+
+  MTD V3 position(int32_t i) const {
+    const uint32_t *w = attr + size_t(i) * vstride;
+    if (vstride == 4) {
+      float4 q = __ldg(reinterpret_cast<const float4 *>(w));
+      return {q.x, q.y, q.z};
+    }
+    return {asf(__ldg(w)), asf(__ldg(w + 1)), asf(__ldg(w + 2))};
+  }
+
+  // Starts a query; returns false when the root box is missed (nothing to do).
+  MTD bool begin(const DevScene &s, int32_t base, V3 ro, V3 rd, int b, bool ds, int32_t ct, int32_t ci, float tMax) {
+    bvh = s.bvh; ins = s.ins; mats = s.mats; attr = s.attr; vstride = s.vstride; blasBase = base;
+    rayO = ro; rayD = rd; bounces = b; doubleSided = ds; currentTri = ct; currentIns = ci;
+    h.tMax = tMax;
+    h.triangleIndex = -1;
+    h.insIdx = -1;
+    h.hitBary = v3(0.0f);
+    h.hitNormal = v3(0.0f);
+    found = false;
+    tlasTop = -1;
+    blasTop = -1;
+    io = -1;
+    leafNode = 0;
+    insIdx = -1;
+    invD = traversalInverse(rd);
+    if (intersectBox(rayO, xyz(ld4(bvh)), xyz(ld4(bvh + 1)), invD, h.tMax) > 0.0f) {
+      tlasTop = 0;
+      tlasStack[0] = 0;
+      return true;
+    }
+    return false;
+  }
+
+  // One traversal step; returns true when the query has finished.
+  MTD bool step() {
+    if (blasTop >= 0) {
+      int32_t node = blasStack[blasTop--];
+      int32_t i = node + blasBase;
+      float4 n1 = ld4(bvh + i);
+      int32_t p = asi(n1.w);
+      if (p >= 0) {
+        int32_t left = node + 2, right = p + blasOffset;
+        float d0 = intersectBox(o, xyz(ld4(bvh + left + blasBase)), xyz(ld4(bvh + left + 1 + blasBase)), linvD, h.tMax);
+        float d1 = intersectBox(o, xyz(ld4(bvh + right + blasBase)), xyz(ld4(bvh + right + 1 + blasBase)), linvD, h.tMax);
+        if (d0 > d1) {
+          if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
+          if (d1 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = right;
+        } else {
+          if (d1 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = right;
+          if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
+        }
+        return false;
+      }
+      int32_t primitiveCount = -p;
+      int32_t primitiveOffset = i + 2;
+      for (int32_t k = 0; k < primitiveCount; k++) {
+        int32_t triangleIndex = primitiveOffset + k;
+        if (bounces > 0 && triangleIndex == currentTri && insIdx == currentIns) continue;
+        float4 r3 = ld4(bvh + triangleIndex);
+        V3 p0 = position(asi(r3.x) + vertexOffset);
+        V3 p1 = position(asi(r3.y) + vertexOffset);
+        V3 p2 = position(asi(r3.z) + vertexOffset);
+        V3 bary;
+        float t = intersectTriangle(o, p0, p1, p2, maxDim, shear, h.tMax, bary);
+        if (!(t > 0.0f)) continue;
+        V3 candidateNormal = xnormalize(xcross(xsub3(p1, p0), xsub3(p2, p0)));
+        if (!doubleSided) {
+          bool matDoubleSided = __ldg(&mats[size_t(sideMaterial) * MTC_MATERIAL_VEC4_ROWS + 23].z) > 0.5f;
+          if (!matDoubleSided && xdot(candidateNormal, d) > 0.0f) continue;
+        }
+        h.hitNormal = candidateNormal;
+        h.tMax = t;
+        h.hitBary = bary;
+        if (shadow) {
+          found = true;
+          return true;
+        }
+        h.triangleIndex = triangleIndex;
+        h.insIdx = insIdx;
+      }
+      return false;
+    }
+    if (io >= 0) {
+      float4 rec = ld4(bvh + leafNode + 2 + io);
+      io--;
+      insIdx = asi(rec.x);
+      int32_t blasRoot = asi(rec.y);
+      const float4 *insv = ins + size_t(insIdx) * MTC_INSTANCE_VEC4_STRIDE;
+      float4 insData = ld4(insv);
+      uint32_t encoded = asu(insData.x);
+      if ((encoded >> 30) != 0u) return false;
+      float4 c0 = ld4(insv + 1), c1 = ld4(insv + 2), c2 = ld4(insv + 3), c3 = ld4(insv + 4);
+      o = xmat4(c0, c1, c2, c3, rayO, 1.0f);
+      d = xmat4(c0, c1, c2, c3, rayD, 0.0f);
+      linvD = traversalInverse(d);
+      maxDim = maxDimension(vabs(d));
+      shear = getShear(d, maxDim);
+      blasOffset = int32_t(encoded & 0x3fffffffu);
+      vertexOffset = asi(insData.y);
+      sideMaterial = asi(insData.z) >> 8;
+      blasTop = 0;
+      blasStack[0] = blasRoot;
+      return false;
+    }
+    if (tlasTop >= 0) {
+      int32_t tlasNode = tlasStack[tlasTop--];
+      float4 r1 = ld4(bvh + tlasNode);
+      int32_t ptr = asi(r1.w);
+      if (ptr >= 0) {
+        int32_t left = tlasNode + 2, right = ptr;
+        float d0 = intersectBox(rayO, xyz(ld4(bvh + left)), xyz(ld4(bvh + left + 1)), invD, h.tMax);
+        float d1 = intersectBox(rayO, xyz(ld4(bvh + right)), xyz(ld4(bvh + right + 1)), invD, h.tMax);
+        if (d0 > d1) {
+          if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
+          if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
+        } else {
+          if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
+          if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
+        }
+      } else {
+        leafNode = tlasNode;
+        io = -ptr - 1;
+      }
+      return false;
+    }
+    return true;
+  }
+};
+
 }  // namespace mt

@@ -25,6 +25,7 @@ constexpr int kWarpTileW = 8, kWarpTileH = 4;  // batched kernel warp tile
 
 __device__ __forceinline__ void flushCounters(const Counters &cnt, uint32_t paths, mtc_counters *out) {
   if (!out) return;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(&out->kernel_launches, 1ull);
   unsigned mask = __activemask();
   uint32_t e = __reduce_add_sync(mask, cnt.ext);
   uint32_t s = __reduce_add_sync(mask, cnt.shadow);
@@ -53,14 +54,26 @@ __global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
   flushCounters(cnt, paths, counters);
 }
 
+// Header of a batched job table (host table and device scratch alike); the
+// JobData entries follow at kBatchTableOffset.  The kernel reads the job
+// count and item total from it, so a captured launch can be replayed after
+// the host table is rewritten with other jobs.
+struct BatchHeader {
+  uint32_t jobCount, totalItems, tileW, _pad[61];
+};
+static_assert(sizeof(BatchHeader) == 256, "batch header size");
+constexpr size_t kBatchTableOffset = sizeof(BatchHeader);
+
 // Persistent batched kernel.  queue[0] is the next work item; items are
 // warp tiles (tileW x 32/tileW pixels) laid out job after job
 // (JobData.firstItem / .items).  A warp takes `grain` consecutive items per
-// atomic.  The loop ends when the counter passes total_items, so every warp
-// exits.
+// atomic.  The loop ends when the counter passes the item total, so every
+// warp exits.
 __global__ void __launch_bounds__(128)
-    k_batch(const JobData *__restrict__ jobs, uint32_t job_count, uint32_t total_items, uint32_t *queue,
-            mtc_counters *counters, uint32_t tileW, uint32_t grain) {
+    k_batch(const BatchHeader *__restrict__ header, uint32_t *queue, mtc_counters *counters, uint32_t grain) {
+  const JobData *__restrict__ jobs =
+      reinterpret_cast<const JobData *>(reinterpret_cast<const char *>(header) + kBatchTableOffset);
+  const uint32_t job_count = header->jobCount, total_items = header->totalItems, tileW = header->tileW;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lx = lane % tileW, ly = lane / tileW, tileH = 32u / tileW;
   Counters cnt;
@@ -338,19 +351,18 @@ mt_status mtc_query_first_hit(const mtc_scene_view *scene, const float *rays, ui
   return cudaStatus(cudaGetLastError());
 }
 
-size_t mtc_batch_scratch_bytes(uint32_t job_count) {
-  return (size_t(job_count) * sizeof(JobData) + 255) / 256 * 256 + 256;
-}
+size_t mtc_batch_table_bytes(uint32_t capacity) { return kBatchTableOffset + size_t(capacity) * sizeof(JobData); }
 
-size_t mtc_batch_table_bytes(uint32_t job_count) { return size_t(job_count) * sizeof(JobData); }
+size_t mtc_batch_scratch_bytes(uint32_t capacity) {
+  return (mtc_batch_table_bytes(capacity) + 255) / 256 * 256 + 256;
+}
 
 mt_status mtc_batch_prepare(const mtc_job_desc *jobs, uint32_t job_count, const mtc_batch_config *config,
                             void *table, uint32_t *total_items) {
-  if ((!jobs || !table) && job_count) return MT_ERROR_INVALID_ARGUMENT;
-  if (!total_items) return MT_ERROR_INVALID_ARGUMENT;
+  if ((!jobs && job_count) || !table) return MT_ERROR_INVALID_ARGUMENT;
   BatchShape shape;
   if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
-  JobData *t = static_cast<JobData *>(table);
+  char *base = static_cast<char *>(table);
   uint64_t total = 0;
   for (uint32_t j = 0; j < job_count; j++) {
     const mtc_job_desc &d = jobs[j];
@@ -364,34 +376,37 @@ mt_status mtc_batch_prepare(const mtc_job_desc *jobs, uint32_t job_count, const 
     J.firstItem = uint32_t(total);
     total += J.items;
     if (total >= 0x7fffffffull) return MT_ERROR_INVALID_ARGUMENT;
-    std::memcpy(&t[j], &J, sizeof(J));
+    std::memcpy(base + kBatchTableOffset + size_t(j) * sizeof(JobData), &J, sizeof(J));
   }
-  *total_items = uint32_t(total);
+  BatchHeader h;
+  std::memset(&h, 0, sizeof(h));
+  h.jobCount = job_count;
+  h.totalItems = uint32_t(total);
+  h.tileW = shape.tileW;
+  std::memcpy(base, &h, sizeof(h));
+  if (total_items) *total_items = uint32_t(total);
   return MT_OK;
 }
 
-mt_status mtc_batch_launch(const void *table, uint32_t job_count, uint32_t total_items, const mtc_batch_config *config,
-                           void *queue_state, mtc_counters *counters, void *stream) {
-  if ((!table && job_count) || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
+mt_status mtc_batch_launch(const void *table, uint32_t capacity, const mtc_batch_config *config, void *queue_state,
+                           mtc_counters *counters, void *stream) {
+  if (!table || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
   BatchShape shape;
   if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
-  if (job_count == 0 || total_items == 0) return MT_OK;
   cudaStream_t st = (cudaStream_t)stream;
   char *scratch = (char *)queue_state;
-  size_t tableBytes = (size_t(job_count) * sizeof(JobData) + 255) / 256 * 256;
-  uint32_t *queue = (uint32_t *)(scratch + tableBytes);
-  cudaError_t e = cudaMemcpyAsync(scratch, table, size_t(job_count) * sizeof(JobData), cudaMemcpyHostToDevice, st);
+  size_t bytes = mtc_batch_table_bytes(capacity);
+  uint32_t *queue = (uint32_t *)(scratch + (bytes + 255) / 256 * 256);
+  cudaError_t e = cudaMemcpyAsync(scratch, table, bytes, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(queue, 0, 256, st);
   if (e != cudaSuccess) return cudaStatus(e);
   int device = 0, sms = 148;
-  cudaGetDevice(&device);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  // Never more CTAs than warps of work.
-  uint64_t warpsWanted = (uint64_t(total_items) + shape.grain - 1) / shape.grain;
-  uint64_t grid = uint64_t(sms) * shape.ctasPerSm;
-  grid = std::min<uint64_t>(grid, (warpsWanted + shape.blockThreads / 32 - 1) / (shape.blockThreads / 32));
-  k_batch<<<uint32_t(std::max<uint64_t>(grid, 1)), shape.blockThreads, 0, st>>>(
-      (const JobData *)scratch, job_count, total_items, queue, counters, shape.tileW, shape.grain);
+  e = cudaGetDevice(&device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return cudaStatus(e);
+  // A full persistent grid: the item total is only known on the device.
+  uint32_t grid = uint32_t(sms) * shape.ctasPerSm;
+  k_batch<<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain);
   return cudaStatus(cudaGetLastError());
 }
 
@@ -400,16 +415,16 @@ mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count, const mt
   if ((!jobs && job_count) || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
   if (config && config->struct_size != sizeof(mtc_batch_config)) return MT_ERROR_INVALID_ARGUMENT;
   if (job_count == 0) return MT_OK;
-  std::vector<JobData> table(job_count);
-  uint32_t total = 0;
-  mt_status st = mtc_batch_prepare(jobs, job_count, config, table.data(), &total);
+  std::vector<char> table(mtc_batch_table_bytes(job_count));
+  mt_status st = mtc_batch_prepare(jobs, job_count, config, table.data(), nullptr);
   if (st != MT_OK) return st;
   if (status_out) {
     cudaError_t e = cudaMemsetAsync(status_out, 0, sizeof(uint32_t), (cudaStream_t)stream);
     if (e != cudaSuccess) return cudaStatus(e);
   }
-  // A pageable host table is staged by cudaMemcpyAsync before it returns.
-  return mtc_batch_launch(table.data(), job_count, total, config, queue_state, counters, stream);
+  // cudaMemcpyAsync from pageable memory has finished reading the table
+  // when it returns, so the vector may go out of scope.
+  return mtc_batch_launch(table.data(), job_count, config, queue_state, counters, stream);
 }
 
 mt_status mtc_refit_tlas(void *tlas, uint64_t tlas_vec4_count, void *instances, uint32_t instance_count,

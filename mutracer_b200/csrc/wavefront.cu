@@ -1,0 +1,602 @@
+// Wavefront form of the batched path tracer (mtc_stream_run).
+//
+// The megakernel keeps a whole path sample in one thread: every kernel
+// register budget is the shading code's (255 registers, 8 warps per SM), so
+// the traversal loops, which are latency-bound chains of dependent node
+// loads, run with too few warps to hide that latency.  Here the integrator's
+// event loop (rayTrace.compute.ts:891-946) is cut at its traversals into
+// separate kernels that each see a queue of path slots:
+//
+//   k_wf_extend  closest hit of every queued extension ray (traverse<false>)
+//   k_wf_shade   surface interaction, material, completeVertex, shadeVertex
+//                (shadeStep, the same out-of-line code the megakernel calls);
+//                queues the NEE shadow ray and either the continuation or the
+//                finished sample
+//   k_wf_shadow  the NEE visibility tests (traverse<true>)
+//   k_wf_finish  accumulation of finished samples (endSample) and the start of
+//                the pixel's next sample or of a new pixel (beginSample)
+//
+// A slot owns one pixel of one job until all of that pixel's samples are
+// done, and starts sample k+1 only after sample k has been accumulated, so
+// every pixel receives the same sums in the same order as in the megakernel:
+// images are bit-identical to mtc_trace_samples.  Pixels (units) are handed
+// out from one counter in the warp-tile order of the mtc_batch_prepare table,
+// so neighbouring slots start on neighbouring pixels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "dev_shade.cuh"
+
+using namespace mt;
+
+namespace {
+
+struct Slot {
+  PathSample ps;
+  Sampler smp;
+  ShadowQuery shadow;
+  uint32_t job, x, y, left;  // pixel owned, samples still to start after the current one
+};
+
+// Queue state at the start of the stream state buffer (256 bytes).
+struct StreamQueues {
+  uint32_t unitNext;         // next unit (pixel) to hand out
+  uint32_t rayCount[2];      // extension-ray queue sizes (double-buffered)
+  uint32_t shadowCount;
+  uint32_t finishCount;
+  uint32_t extendNext;       // next extension ray to hand to a lane
+  uint32_t shadowNext;       // next shadow ray to hand to a lane
+  uint32_t _pad[57];
+};
+static_assert(sizeof(StreamQueues) == 256, "queue header size");
+
+// Same layout as the batched table header written by mtc_batch_prepare.
+struct TableHeader {
+  uint32_t jobCount, totalItems, tileW, _pad[61];
+};
+static_assert(sizeof(TableHeader) == 256, "table header size");
+
+struct StreamView {
+  const TableHeader *header;
+  const JobData *jobs;
+  StreamQueues *q;
+  Slot *slots;
+  TraversalHit *hits;
+  uint32_t *rayQueue[2];
+  uint32_t *shadowQueue, *finishQueue;
+  uint32_t *keys, *sortedQueue;   // material-class key per slot; extension queue ordered by key
+  uint32_t *classCount, *classCursor;  // kClasses each
+  uint32_t slotCount;
+  uint32_t refillLanes;  // idle lanes of a warp that trigger a ray refill
+  mtc_counters *counters;
+};
+
+constexpr uint32_t kStreamThreads = 128;
+
+__device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
+
+// Appends `value` to a queue with one atomic per converged group of lanes.
+__device__ __forceinline__ void enqueue(uint32_t *queue, uint32_t *count, uint32_t value) {
+  unsigned m = __activemask();
+  int leader = __ffs(m) - 1;
+  uint32_t rank = __popc(m & ((1u << laneId()) - 1u));
+  uint32_t base = 0;
+  if (int(laneId()) == leader) base = atomicAdd(count, uint32_t(__popc(m)));
+  base = __shfl_sync(m, base, leader);
+  queue[base + rank] = value;
+}
+
+__device__ __forceinline__ uint32_t takeUnit(uint32_t *counter) {
+  unsigned m = __activemask();
+  int leader = __ffs(m) - 1;
+  uint32_t rank = __popc(m & ((1u << laneId()) - 1u));
+  uint32_t base = 0;
+  if (int(laneId()) == leader) base = atomicAdd(counter, uint32_t(__popc(m)));
+  base = __shfl_sync(m, base, leader);
+  return base + rank;
+}
+
+__device__ __forceinline__ void flush(const StreamView &v, uint32_t ext, uint32_t shadow, uint32_t paths) {
+  if (!v.counters) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&v.counters->kernel_launches, 1ull);
+  unsigned m = __activemask();
+  uint32_t e = __reduce_add_sync(m, ext), s = __reduce_add_sync(m, shadow), p = __reduce_add_sync(m, paths);
+  if (int(laneId()) == __ffs(m) - 1) {
+    if (e) atomicAdd(&v.counters->extension_rays, (unsigned long long)e);
+    if (s) atomicAdd(&v.counters->shadow_rays, (unsigned long long)s);
+    if (p) atomicAdd(&v.counters->path_samples, (unsigned long long)p);
+  }
+}
+
+__device__ __forceinline__ BsdfContext bsdfContext(const JobData &J) {
+  return BsdfContext{J.s.lut, (J.s.flags & MTC_SCENE_HAS_MEDIUM) != 0u, feature(J, MTC_FEATURE_HAS_THIN_FILM)};
+}
+
+// Material classes for regrouping the shading queue: 0 = miss, else 1 + a
+// mask of the lobes the hit material switches on (metal, coat, transmission,
+// fuzz/subsurface/thin film, non-default material type), read from the
+// MaterialBuffer rows that getMaterial reads (materialLayoutSchema.ts:23-150).
+constexpr uint32_t kClasses = 64;
+
+__device__ __forceinline__ uint32_t materialClass(const JobData &J, const TraversalHit &h) {
+  if (h.insIdx < 0) return 0u;
+  const float4 *insv = J.s.ins + size_t(h.insIdx) * MTC_INSTANCE_VEC4_STRIDE;
+  int32_t mi = asi(ld4(insv).z) >> 8;
+  if (uint32_t(mi) >= J.s.matCount) mi = 0;
+  const float4 *d = J.s.mats + size_t(mi) * MTC_MATERIAL_VEC4_ROWS;
+  uint32_t k = 0;
+  if (ld4(d + 2).x > 0.0f) k |= 1u;                                   // base_metalness
+  if (ld4(d + 16).w > 0.0f) k |= 2u;                                  // coat_weight
+  if (ld4(d + 4).y > 0.0f) k |= 4u;                                   // transmission_weight
+  if (ld4(d + 11).w > 0.0f || ld4(d + 10).w > 0.0f || ld4(d + 18).x > 0.0f) k |= 8u;  // fuzz, subsurface, thin film
+  if (int(ld4(d).w) != 0) k |= 16u;                                   // material type
+  return 1u + k;
+}
+
+// Counts a finished extension ray in its material class (one atomic per
+// class present in the converged group of lanes).
+__device__ __forceinline__ void countClass(const StreamView &v, uint32_t s, uint32_t key) {
+  v.keys[s] = key;
+  unsigned m = __match_any_sync(__activemask(), key);
+  if (int(laneId()) == __ffs(m) - 1) atomicAdd(&v.classCount[key], uint32_t(__popc(m)));
+}
+
+// Gives slot `s` the next pixel that has samples to add, and starts its first
+// sample.  Returns false when the units are exhausted.
+__device__ bool claimPixel(const StreamView &v, uint32_t s) {
+  const uint32_t jobCount = v.header->jobCount;
+  const uint32_t totalUnits = v.header->totalItems * 32u;
+  const uint32_t tileW = v.header->tileW, tileH = 32u / tileW;
+  // Units outside their image (ragged edge tiles) are skipped; the loop ends
+  // at the first pixel with samples or when the units run out.
+  for (uint32_t guard = 0; guard <= totalUnits; guard++) {
+    uint32_t u = takeUnit(&v.q->unitNext);
+    if (u >= totalUnits) return false;
+    uint32_t item = u >> 5, lane = u & 31u;
+    // Binary search of the job owning warp tile `item` (firstItem ascending).
+    uint32_t lo = 0, hi = jobCount;
+    while (hi - lo > 1u) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (v.jobs[mid].firstItem <= item) lo = mid; else hi = mid;
+    }
+    const JobData &J = v.jobs[lo];
+    uint32_t local = item - J.firstItem;
+    uint32_t x = (local % J.tilesX) * tileW + lane % tileW;
+    uint32_t y = (local / J.tilesX) * tileH + lane / tileW;
+    if (x >= J.width || y >= J.height || J.samples == 0u) continue;
+    Slot &sl = v.slots[s];
+    sl.job = lo;
+    sl.x = x;
+    sl.y = y;
+    sl.left = J.samples - 1u;
+    Ctx c{J, Sampler(), bsdfContext(J), Counters(), ShadowQuery()};
+    PathSample ps;
+    beginSample(c, x, y, ps);
+    sl.ps = ps;
+    sl.smp = c.smp;
+    sl.shadow.valid = false;
+    return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.slotCount; s += gridDim.x * blockDim.x) {
+    if (claimPixel(v, s)) enqueue(v.rayQueue[0], &v.q->rayCount[0], s);
+  }
+  flush(v, 0, 0, 0);
+}
+
+// Closest hits of the queued extension rays.  Persistent: a lane whose ray
+// has finished takes the next queued ray at once, so a warp is not held by
+// its slowest ray (traversal lengths differ by an order of magnitude here).
+__global__ void __launch_bounds__(kStreamThreads) k_wf_extend(StreamView v, uint32_t cur, uint32_t regroup) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    v.q->rayCount[cur ^ 1u] = 0;
+    v.q->shadowCount = 0;
+    v.q->finishCount = 0;
+  }
+  const uint32_t n = v.q->rayCount[cur];
+  const uint32_t *queue = v.rayQueue[cur];
+  RayTraversal<false> rt;
+  uint32_t s = 0, ext = 0;
+  bool busy = false, exhausted = false;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !busy && !exhausted);
+    const unsigned live = __ballot_sync(0xffffffffu, busy);
+    if (!idle && !live) break;
+    // Refill once enough lanes wait (or none is left tracing).
+    if (idle && (uint32_t(__popc(idle)) >= v.refillLanes || !live)) {
+      if (busy || exhausted) continue;
+      uint32_t t = takeUnit(&v.q->extendNext);
+      if (t >= n) {
+        exhausted = true;
+      } else {
+        s = queue[t];
+        const Slot &sl = v.slots[s];
+        const JobData &J = v.jobs[sl.job];
+        // traceExtension: an empty scene is a miss without a traversal.
+        if (J.u.is_empty > 0) {
+          TraversalHit none;
+          none.tMax = RAY_MAX_DISTANCE;
+          none.triangleIndex = -1;
+          none.insIdx = -1;
+          v.hits[s] = none;
+          if (regroup) countClass(v, s, 0u);
+        } else {
+          ext++;
+          if (rt.begin(J.s, J.u.blas_offset, sl.ps.path.ray.o, sl.ps.path.ray.d, sl.ps.depth, sl.ps.event != 0,
+                       sl.ps.si.triangleIndex, sl.ps.si.instanceIndex, RAY_MAX_DISTANCE)) {
+            busy = true;
+          } else {
+            v.hits[s] = rt.h;
+            if (regroup) countClass(v, s, 0u);
+          }
+        }
+      }
+      continue;
+    }
+    if (busy && rt.step()) {
+      v.hits[s] = rt.h;
+      busy = false;
+      if (regroup) countClass(v, s, materialClass(v.jobs[v.slots[s].job], rt.h));
+    }
+  }
+  flush(v, ext, 0, 0);
+}
+
+// Orders the extension queue by material class (counting sort on the keys
+// counted by k_wf_extend), so that the warps shading at any one time run the
+// same BSDF code.  The order of slots inside a class is arbitrary; it cannot
+// change any result, since slots never share state.
+__global__ void __launch_bounds__(kStreamThreads) k_wf_regroup(StreamView v, uint32_t cur) {
+  __shared__ uint32_t offset[kClasses];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < kClasses; k++) {
+      offset[k] = acc;
+      acc += v.classCount[k];
+    }
+  }
+  __syncthreads();
+  const uint32_t n = v.q->rayCount[cur];
+  const uint32_t *queue = v.rayQueue[cur];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    uint32_t s = queue[t];
+    uint32_t key = v.keys[s];
+    unsigned m = __match_any_sync(__activemask(), key);
+    int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (int(laneId()) == leader) base = atomicAdd(&v.classCursor[key], uint32_t(__popc(m)));
+    base = __shfl_sync(m, base, leader);
+    v.sortedQueue[offset[key] + base + __popc(m & ((1u << laneId()) - 1u))] = s;
+  }
+}
+
+#ifndef MT_SHADE_MIN_BLOCKS
+#define MT_SHADE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
+    k_wf_shade(StreamView v, uint32_t cur, uint32_t regroup) {
+  if (blockIdx.x == 0) {
+    if (threadIdx.x == 0) v.q->extendNext = 0;
+    // The class counts of this iteration have been consumed by k_wf_regroup.
+    for (uint32_t k = threadIdx.x; k < kClasses && regroup; k += blockDim.x) {
+      v.classCount[k] = 0;
+      v.classCursor[k] = 0;
+    }
+  }
+  const uint32_t n = v.q->rayCount[cur];
+  const uint32_t *queue = regroup ? v.sortedQueue : v.rayQueue[cur];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    uint32_t s = queue[t];
+    if (s >= v.slotCount) continue;
+    Slot &sl = v.slots[s];
+    const JobData &J = v.jobs[sl.job];
+    Ctx c{J, sl.smp, bsdfContext(J), Counters(), ShadowQuery()};
+    c.shadow.valid = false;
+    PathSample ps = sl.ps;
+    TraversalHit h = v.hits[s];
+    bool ended = shadeStep(c, ps, h);
+    sl.ps = ps;
+    sl.smp = c.smp;
+    sl.shadow = c.shadow;
+    if (c.shadow.valid) enqueue(v.shadowQueue, &v.q->shadowCount, s);
+    if (ended) enqueue(v.finishQueue, &v.q->finishCount, s);
+    else enqueue(v.rayQueue[cur ^ 1u], &v.q->rayCount[cur ^ 1u], s);
+  }
+  flush(v, 0, 0, 0);
+}
+
+// NEE visibility of the queued shadow rays (intersectSceneShadow and
+// resolveShadow), persistent like k_wf_extend.
+__global__ void __launch_bounds__(kStreamThreads) k_wf_shadow(StreamView v) {
+  const uint32_t n = v.q->shadowCount;
+  RayTraversal<true> rt;
+  uint32_t s = 0, shadowRays = 0;
+  bool busy = false, exhausted = false;
+  for (;;) {
+    bool done = false;
+    const unsigned idle = __ballot_sync(0xffffffffu, !busy && !exhausted);
+    const unsigned live = __ballot_sync(0xffffffffu, busy);
+    if (!idle && !live) break;
+    const bool refill = idle && (uint32_t(__popc(idle)) >= v.refillLanes || !live);
+    if (refill && !busy && !exhausted) {
+      uint32_t t = takeUnit(&v.q->shadowNext);
+      if (t >= n) {
+        exhausted = true;
+      } else {
+        s = v.shadowQueue[t];
+        const Slot &sl = v.slots[s];
+        const JobData &J = v.jobs[sl.job];
+        const ShadowQuery &q = sl.shadow;
+        if (J.u.is_empty > 0) {
+          rt.found = false;
+          done = true;
+        } else {
+          shadowRays++;
+          float tMax = fminf(fmaxf(q.maxDistance, 0.0f), RAY_MAX_DISTANCE);
+          if (rt.begin(J.s, J.u.blas_offset, q.ray.o, q.ray.d, 1, true, q.triangleIndex, q.instanceIndex, tMax))
+            busy = true;
+          else
+            done = true;
+        }
+      }
+    }
+    if (!refill && busy && rt.step()) {
+      busy = false;
+      done = true;
+    }
+    if (done) {
+      Slot &sl = v.slots[s];
+      if (!rt.found) {
+        V3 li = sl.ps.path.li;
+        li += sl.shadow.contribution;
+        sl.ps.path.li = li;
+      }
+      sl.shadow.valid = false;
+    }
+  }
+  flush(v, 0, shadowRays, 0);
+}
+
+__global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint32_t cur) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) v.q->shadowNext = 0;
+  const uint32_t n = v.q->finishCount;
+  uint32_t paths = 0;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    uint32_t s = v.finishQueue[t];
+    Slot &sl = v.slots[s];
+    const JobData &J = v.jobs[sl.job];
+    PathSample ps = sl.ps;
+    endSample(J, sl.x + sl.y * J.width, ps);
+    paths++;
+    bool again;
+    if (sl.left > 0u) {
+      sl.left--;
+      Ctx c{J, Sampler(), bsdfContext(J), Counters(), ShadowQuery()};
+      beginSample(c, sl.x, sl.y, ps);
+      sl.ps = ps;
+      sl.smp = c.smp;
+      again = true;
+    } else {
+      again = claimPixel(v, s);
+    }
+    if (again) enqueue(v.rayQueue[cur ^ 1u], &v.q->rayCount[cur ^ 1u], s);
+  }
+  flush(v, 0, 0, paths);
+}
+
+size_t roundUp(size_t x) { return (x + 255) / 256 * 256; }
+
+struct StreamLayout {
+  size_t table, queues, slots, hits, rayQueues, shadowQueue, finishQueue, keys, sortedQueue, classes, total;
+};
+
+StreamLayout layout(uint32_t capacity, uint32_t slots) {
+  StreamLayout L;
+  size_t off = 0;
+  L.table = off;
+  off += roundUp(sizeof(TableHeader) + size_t(capacity) * sizeof(JobData));
+  L.queues = off;
+  off += sizeof(StreamQueues);
+  L.slots = off;
+  off += roundUp(size_t(slots) * sizeof(Slot));
+  L.hits = off;
+  off += roundUp(size_t(slots) * sizeof(TraversalHit));
+  L.rayQueues = off;
+  off += 2 * roundUp(size_t(slots) * 4);
+  L.shadowQueue = off;
+  off += roundUp(size_t(slots) * 4);
+  L.finishQueue = off;
+  off += roundUp(size_t(slots) * 4);
+  L.keys = off;
+  off += roundUp(size_t(slots) * 4);
+  L.sortedQueue = off;
+  off += roundUp(size_t(slots) * 4);
+  L.classes = off;
+  off += roundUp(2 * kClasses * 4);
+  L.total = off;
+  return L;
+}
+
+struct StreamShape {
+  uint32_t slots, iterationsPerCheck, maxIterations, refillLanes, regroupInterval;
+};
+
+bool streamShape(const mtc_stream_config *c, StreamShape &out) {
+  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u};
+  if (!c) return true;
+  if (c->struct_size != sizeof(mtc_stream_config)) return false;
+  if (c->slots) {
+    if (c->slots < 1024u || c->slots > (1u << 25)) return false;
+    out.slots = c->slots;
+  }
+  if (c->iterations_per_check) {
+    if (c->iterations_per_check > 256u) return false;
+    out.iterationsPerCheck = c->iterations_per_check;
+  }
+  if (c->max_iterations) out.maxIterations = c->max_iterations;
+  if (c->regroup_interval == MTC_REGROUP_OFF) {
+    out.regroupInterval = 0;
+  } else if (c->regroup_interval) {
+    if (c->regroup_interval > 1024u) return false;
+    out.regroupInterval = c->regroup_interval;
+  }
+  if (c->refill_lanes) {
+    if (c->refill_lanes > 32u) return false;
+    out.refillLanes = c->refill_lanes;
+  }
+  return true;
+}
+
+cudaError_t gridFor(const void *kernel, uint32_t &grid) {
+  int device = 0, sms = 0, perSm = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kStreamThreads, 0);
+  if (e != cudaSuccess) return e;
+  grid = uint32_t(std::max(1, sms * std::max(1, perSm)));
+  return cudaSuccess;
+}
+
+// Pinned words the host polls for the queue size (one pair per device), and
+// a per-device lock that serialises concurrent mtc_stream_run calls, which
+// share them.
+constexpr int kMaxDevices = 64;
+uint32_t *g_pinned[kMaxDevices];
+std::mutex g_pinnedMutex;
+std::mutex g_runMutex[kMaxDevices];
+
+cudaError_t pinnedWords(uint32_t **out) {
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(g_pinnedMutex);
+  if (!g_pinned[device]) {
+    void *p = nullptr;
+    e = cudaHostAlloc(&p, 64, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    std::memset(p, 0, 64);
+    g_pinned[device] = static_cast<uint32_t *>(p);
+  }
+  *out = g_pinned[device];
+  return cudaSuccess;
+}
+
+mt_status toStatus(cudaError_t e) {
+  if (e == cudaSuccess) return MT_OK;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return MT_ERROR_UNAVAILABLE;
+  return MT_ERROR;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config) {
+  StreamShape shape;
+  if (!streamShape(config, shape)) return 0;
+  return layout(capacity, shape.slots).total;
+}
+
+mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_config *config, void *state,
+                         mtc_counters *counters, void *stream) {
+  if (!table || !state || capacity == 0) return MT_ERROR_INVALID_ARGUMENT;
+  StreamShape shape;
+  if (!streamShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
+  TableHeader hdr;
+  std::memcpy(&hdr, table, sizeof(hdr));
+  if (hdr.jobCount > capacity || hdr.tileW == 0 || hdr.tileW > 32 || 32 % hdr.tileW) return MT_ERROR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  StreamLayout L = layout(capacity, shape.slots);
+  char *base = static_cast<char *>(state);
+  StreamView v;
+  v.header = reinterpret_cast<const TableHeader *>(base + L.table);
+  v.jobs = reinterpret_cast<const JobData *>(base + L.table + sizeof(TableHeader));
+  v.q = reinterpret_cast<StreamQueues *>(base + L.queues);
+  v.slots = reinterpret_cast<Slot *>(base + L.slots);
+  v.hits = reinterpret_cast<TraversalHit *>(base + L.hits);
+  v.rayQueue[0] = reinterpret_cast<uint32_t *>(base + L.rayQueues);
+  v.rayQueue[1] = reinterpret_cast<uint32_t *>(base + L.rayQueues + roundUp(size_t(shape.slots) * 4));
+  v.shadowQueue = reinterpret_cast<uint32_t *>(base + L.shadowQueue);
+  v.finishQueue = reinterpret_cast<uint32_t *>(base + L.finishQueue);
+  v.keys = reinterpret_cast<uint32_t *>(base + L.keys);
+  v.sortedQueue = reinterpret_cast<uint32_t *>(base + L.sortedQueue);
+  v.classCount = reinterpret_cast<uint32_t *>(base + L.classes);
+  v.classCursor = v.classCount + kClasses;
+  v.slotCount = shape.slots;
+  v.refillLanes = shape.refillLanes;
+  v.counters = counters;
+
+  cudaError_t e = cudaMemcpyAsync(base + L.table, table, sizeof(TableHeader) + size_t(capacity) * sizeof(JobData),
+                                  cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(v.q, 0, sizeof(StreamQueues), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(v.classCount, 0, 2 * kClasses * 4, st);
+  if (e != cudaSuccess) return toStatus(e);
+  if (hdr.totalItems == 0 || hdr.jobCount == 0) return MT_OK;
+
+  uint32_t gSeed, gExtend, gShade, gShadow, gFinish, gRegroup;
+  if ((e = gridFor((const void *)k_wf_seed, gSeed)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_extend, gExtend)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_shade, gShade)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_shadow, gShadow)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_finish, gFinish)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_regroup, gRegroup)) != cudaSuccess)
+    return toStatus(e);
+  uint32_t *pinned = nullptr;
+  if ((e = pinnedWords(&pinned)) != cudaSuccess) return toStatus(e);
+  int device = 0;
+  if ((e = cudaGetDevice(&device)) != cudaSuccess) return toStatus(e);
+  std::lock_guard<std::mutex> runLock(g_runMutex[device]);
+  cudaEvent_t ev[2];
+  if ((e = cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming)) != cudaSuccess) return toStatus(e);
+  if ((e = cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming)) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return toStatus(e);
+  }
+
+  k_wf_seed<<<gSeed, kStreamThreads, 0, st>>>(v);
+  e = cudaGetLastError();
+  uint32_t cur = 0, iterations = 0, chunk = 0;
+  mt_status status = MT_OK;
+  while (e == cudaSuccess) {
+    for (uint32_t k = 0; k < shape.iterationsPerCheck && e == cudaSuccess; k++) {
+      const uint32_t regroup = shape.regroupInterval && (iterations % shape.regroupInterval) == 0u ? 1u : 0u;
+      k_wf_extend<<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
+      if (regroup) k_wf_regroup<<<gRegroup, kStreamThreads, 0, st>>>(v, cur);
+      k_wf_shade<<<gShade, kStreamThreads, 0, st>>>(v, cur, regroup);
+      k_wf_shadow<<<gShadow, kStreamThreads, 0, st>>>(v);
+      k_wf_finish<<<gFinish, kStreamThreads, 0, st>>>(v, cur);
+      e = cudaGetLastError();
+      cur ^= 1u;
+      iterations++;
+    }
+    if (e != cudaSuccess) break;
+    // Rays queued for the next iteration; zero means every slot is idle.
+    e = cudaMemcpyAsync(&pinned[chunk & 1u], &v.q->rayCount[cur], 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[chunk & 1u], st);
+    if (e != cudaSuccess) break;
+    if (chunk > 0) {
+      e = cudaEventSynchronize(ev[(chunk - 1) & 1u]);
+      if (e != cudaSuccess) break;
+      if (pinned[(chunk - 1) & 1u] == 0u) break;
+    }
+    chunk++;
+    if (iterations >= shape.maxIterations) {
+      status = MT_ERROR_TIMEOUT;
+      break;
+    }
+  }
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev[(chunk) & 1u]);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (e != cudaSuccess) return toStatus(e);
+  return status;
+}
+
+}  // extern "C"

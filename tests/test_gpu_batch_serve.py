@@ -1,0 +1,147 @@
+"""The batched form (graph-captured persistent launch, autotuned shapes) and
+the served form (continuous batching over resident scenes) give every job
+the bit-identical outputs of the same job rendered alone through
+mtc_trace_samples."""
+import pytest
+
+from mutracer_b200 import abi, batch, scene, serve
+
+pytestmark = pytest.mark.gpu
+
+
+def _equal(a, b):
+    import torch
+    return all(torch.equal(x, y) for x, y in ((a.color, b.color), (a.normal, b.normal), (a.albedo, b.albedo),
+                                              (a.catcher, b.catcher)))
+
+
+def _small_jobs(cuda):
+    specs = [batch.JobSpec(0, 40, 24, 3, 20_000, 2, 11), batch.JobSpec(1, 33, 47, 5, 60_000, 5, 12),
+             batch.JobSpec(2, 64, 16, 2, 10_000, 1, 13), batch.JobSpec(3, 17, 9, 4, 120_000, 8, 14)]
+    return batch.build_mixed(specs, cuda, env_width=64)
+
+
+def test_graph_replay_matches_alone_and_picks_up_rewritten_table(cuda):
+    import torch
+    jobs = _small_jobs(cuda)
+    alone = _small_jobs(cuda)
+    b = batch.Batch(len(jobs), abi.BatchConfig.make(tile_width=4, items_per_fetch=2), cuda)
+    b.set_jobs(jobs)
+    b.capture()
+    b.replay()
+    torch.cuda.synchronize()
+    for j in alone:
+        j.render_alone()
+    torch.cuda.synchronize()
+    assert all(_equal(a.acc, j.acc) for a, j in zip(alone, jobs))
+    # Rewrite the pinned table in place (other sample counts, fewer jobs) and
+    # replay the same graph: the device reads the new header and entries.
+    b.set_jobs(jobs[1:], [2, 1, 3])
+    b.replay()
+    torch.cuda.synchronize()
+    for j, s in zip(alone[1:], [2, 1, 3]):
+        j.render_alone(samples=s)
+    torch.cuda.synchronize()
+    assert all(_equal(a.acc, j.acc) for a, j in zip(alone, jobs))
+    expected = sum(j.pixels * j.spp for j in jobs) + sum(j.pixels * s for j, s in zip(jobs[1:], [2, 1, 3]))
+    assert int(b.counters[0].item()) == expected
+    b.release()
+
+
+def test_every_autotune_shape_gives_the_same_images(cuda):
+    import torch
+    ref = _small_jobs(cuda)
+    for j in ref:
+        j.render_alone(per_sample=True)
+    torch.cuda.synchronize()
+    best, timings = batch.autotune(_small_jobs(cuda), probe_samples=1, repeats=1, device=cuda)
+    assert best is not None and len(timings) == len(batch.AUTOTUNE_SPACE)
+    for shape in batch.AUTOTUNE_SPACE:
+        jobs = _small_jobs(cuda)
+        b = batch.Batch(len(jobs), abi.BatchConfig.make(*shape), cuda)
+        b.set_jobs(jobs)
+        b.launch()
+        torch.cuda.synchronize()
+        assert all(_equal(a.acc, j.acc) for a, j in zip(ref, jobs)), shape
+
+
+def test_served_results_equal_alone(cuda):
+    import torch
+    pool = serve.ScenePool(cuda)
+    for sid, (kind, params) in enumerate((("cornell", ()), ("instanced_spheres", (12, 3, 6, 64, 2)),
+                                          ("instanced_spheres", (40, 4, 8, 64, 5)))):
+        pool.add(sid, scene.SceneHost(kind, 32, 32, sid + 1, params))
+    reqs = serve.poisson_requests(pool, 10, rate=400.0, seed=5, spp_range=(2, 9),
+                                  resolutions=((24, 16), (40, 40), (13, 31)))
+    srv = serve.Server(pool, hbm_budget_bytes=3 * 40 * 40 * serve.ACCUMULATION_BYTES_PER_PIXEL, max_jobs=3,
+                       quantum=2, device=cuda)
+    stats = srv.run(reqs, keep_outputs=True)
+    srv.release()
+    assert stats["requests"] == 10 and stats["rounds"] >= 5
+    assert stats["paths"] == sum(r.width * r.height * r.spp for r in reqs)
+    assert all(r.completed >= r.admitted - 1e-3 and r.latency > 0 for r in reqs)
+    for r in reqs:
+        alone = batch.RenderJob(pool[r.scene_id], r.spp, r.width, r.height, camera=r.camera, device=cuda)
+        alone.render_alone()
+        torch.cuda.synchronize()
+        assert _equal(alone.acc, r.job.acc), r.request_id
+
+
+def test_served_admission_respects_the_hbm_budget(cuda):
+    pool = serve.ScenePool(cuda)
+    pool.add(0, scene.SceneHost("cornell", 16, 16, 1))
+    reqs = [serve.Request(i, 0, 64, 64, 3, 0.0) for i in range(6)]
+    one = 64 * 64 * serve.ACCUMULATION_BYTES_PER_PIXEL
+    srv = serve.Server(pool, hbm_budget_bytes=2 * one, max_jobs=8, quantum=1, device=cuda)
+    stats = srv.run(reqs)
+    srv.release()
+    # At most two jobs fit at once, 3 samples each: 6 jobs need >= 9 rounds.
+    assert stats["rounds"] >= 9
+    with pytest.raises(RuntimeError):
+        serve.Server(pool, hbm_budget_bytes=one - 1, device=cuda).run([serve.Request(0, 0, 64, 64, 1, 0.0)])
+
+
+@pytest.mark.parametrize("slots", [1024, 1 << 16])
+def test_wavefront_matches_alone(cuda, slots):
+    import torch
+    jobs = _small_jobs(cuda)
+    extra = batch.build_mixed([batch.JobSpec(9, 96, 80, 6, 40_000, 3, 21)], cuda, env_width=64)
+    jobs += extra
+    alone = _small_jobs(cuda) + batch.build_mixed([batch.JobSpec(9, 96, 80, 6, 40_000, 3, 21)], cuda, env_width=64)
+    sb = batch.StreamBatch(len(jobs), abi.BatchConfig.make(tile_width=8),
+                           abi.StreamConfig.make(slots=slots, iterations_per_check=3), device=cuda)
+    sb.set_jobs(jobs)
+    sb.run()
+    torch.cuda.synchronize()
+    for j in alone:
+        j.render_alone()
+    torch.cuda.synchronize()
+    for a, j in zip(alone, jobs):
+        assert _equal(a.acc, j.acc), j.job_id
+    c = sb.counters.cpu().tolist()
+    assert c[0] == sum(j.pixels * j.spp for j in jobs)
+    # A second run adds the same number of samples again, continuing each
+    # pixel's sample sequence, like a second mtc_trace_samples call.
+    sb.set_jobs(jobs, [2] * len(jobs))
+    sb.run()
+    for a in alone:
+        a.render_alone(samples=2)
+    torch.cuda.synchronize()
+    for a, j in zip(alone, jobs):
+        assert _equal(a.acc, j.acc), j.job_id
+
+
+def test_wavefront_cornell_and_glass_scenes(cuda):
+    """Analytic-light hits, media and transmission through the wavefront."""
+    import torch
+    for kind, params in (("cornell", ()), ("glass_spheres", (6,))):
+        host = scene.SceneHost(kind, 48, 40, 3, params)
+        dev = scene.DeviceScene(host, cuda)
+        a = batch.RenderJob(dev, 5, device=cuda)
+        b = batch.RenderJob(dev, 5, device=cuda)
+        a.render_alone()
+        sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=2048), device=cuda)
+        sb.set_jobs([b])
+        sb.run()
+        torch.cuda.synchronize()
+        assert _equal(a.acc, b.acc), kind
