@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-scenes", type=int, default=8)
+    p.add_argument("--serve-quantum", type=int, default=4, help="samples per job per served round")
     p.add_argument("--serve-spp-divisor", type=int, default=16,
                    help="scale the requests' target spp (uniform 16-128) down by this factor")
     return p.parse_args()
@@ -351,12 +352,13 @@ def _timed(fn, stream):
 
 
 def mixed_batch(args, dev_id):
-    """The mixed 64-job workload three ways, each job from zeroed buffers:
+    """The mixed 64-job workload four ways, each job from zeroed buffers:
     plain per-sample (one mtc_trace_samples launch per sample per job, the
     reference host's dispatch pattern), plain per-job (one launch per job with
-    all its samples) and batched (all jobs in one persistent launch, replayed
-    from a captured CUDA graph, launch shape from the autotuner).  Every job's
-    image is bit-identical across the three (checked here on the first job)."""
+    all its samples), persistent (all jobs in one persistent-megakernel
+    launch replayed from a captured CUDA graph) and wavefront (all jobs in
+    one mtc_stream_run, knobs from the autotuner).  Every job's image is
+    bit-identical across the four (checked here on every job)."""
     import torch
     from mutracer_b200 import batch
     stream = torch.cuda.current_stream()
@@ -371,37 +373,41 @@ def mixed_batch(args, dev_id):
             j.acc.zero_()
 
     t0 = time.perf_counter()
-    cfg, timings = batch.autotune(jobs, probe_samples=1, repeats=1, device=dev_id)
+    scfg, timings = batch.autotune_stream(jobs, probe_samples=1, device=dev_id)
     tune_s = time.perf_counter() - t0
-    b = batch.Batch(len(jobs), cfg, dev_id)
-    b.set_jobs(jobs)
-    b.capture()
+    pb = batch.Batch(len(jobs), None, dev_id)
+    pb.set_jobs(jobs)
+    pb.capture()
+    sb = batch.StreamBatch(len(jobs), None, scfg, dev_id)
+    sb.set_jobs(jobs)
     res = {}
-    ref_img = None
+    ref = None
     for name, fn in (("plain_per_sample", lambda: batch.run_plain(jobs, per_sample=True)),
                      ("plain_per_job", lambda: batch.run_plain(jobs, per_sample=False)),
-                     ("batched_graph", b.replay)):
+                     ("persistent_graph", pb.replay),
+                     ("wavefront", sb.run)):
         ms = []
         for it in range(2):               # one warm-up, one timed
             zero()
             ms.append(_timed(fn, stream))
         res[name] = {"ms": round(ms[-1], 2), "mpaths_per_s": round(paths / ms[-1] / 1e3, 3)}
-        img = jobs[0].acc.color.clone()
-        if ref_img is None:
-            ref_img = img
-        res[name]["bit_identical_to_plain"] = bool(torch.equal(img, ref_img))
-    b.release()
-    shape = (cfg.block_threads, cfg.ctas_per_sm, cfg.tile_width, cfg.items_per_fetch)
+        imgs = [j.acc.color.clone() for j in jobs]
+        if ref is None:
+            ref = imgs
+        res[name]["bit_identical_to_plain"] = all(torch.equal(a, b) for a, b in zip(imgs, ref))
+        del imgs
+    pb.release()
+    del sb
     res.update({
         "workload": f"{len(jobs)} jobs, resolution from {{256^2, 512^2, 1280x720, 1920x1080}}, spp log-uniform "
                     f"[4,256] / {args.mixed_spp_divisor} (rounded up), instanced-sphere scenes 10k-2M tris, "
                     f"1-8 rect lights + 512x256 sky, depth 6, seed 0",
         "paths": int(paths), "scene_build_s": round(build_s, 1), "autotune_s": round(tune_s, 1),
-        "autotuned_shape": {"block_threads": shape[0], "ctas_per_sm": shape[1], "tile_width": shape[2],
-                            "items_per_fetch": shape[3]},
-        "autotune_probe_ms": {f"{k[0]}x{k[1]}/t{k[2]}/g{k[3]}": round(v, 2) for k, v in timings.items()},
-        "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["batched_graph"]["ms"], 3),
-        "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["batched_graph"]["ms"], 3),
+        "wavefront_config": {"slots": scfg.slots, "refill_lanes": scfg.refill_lanes,
+                             "regroup_interval": scfg.regroup_interval},
+        "autotune_probe_ms": {k: round(v, 2) for k, v in timings.items()},
+        "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["wavefront"]["ms"], 3),
+        "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["wavefront"]["ms"], 3),
     })
     del jobs
     torch.cuda.empty_cache()
@@ -420,7 +426,7 @@ def served_stream(args, dev_id):
     reqs = serve.poisson_requests(pool, args.serve_requests, args.serve_rate, seed=11,
                                   spp_divisor=args.serve_spp_divisor)
     budget = 12 * 1024 ** 3
-    srv = serve.Server(pool, hbm_budget_bytes=budget, max_jobs=64, quantum=2, device=dev_id)
+    srv = serve.Server(pool, hbm_budget_bytes=budget, max_jobs=64, quantum=args.serve_quantum, device=dev_id)
     warm = serve.poisson_requests(pool, 4, 1000.0, seed=12, spp_divisor=args.serve_spp_divisor)
     srv.run(warm)
     stats = srv.run(reqs)
@@ -429,7 +435,8 @@ def served_stream(args, dev_id):
         "workload": f"{len(reqs)} requests, Poisson {args.serve_rate}/s, {len(pool)} resident scenes "
                     f"({pool.device_bytes / 1e6:.0f} MB, 10k-8M tris), orbit cameras FOV 30-70, resolution from "
                     f"{{256^2, 512^2, 1280x720, 1920x1080}}, target spp U[16,128] / {args.serve_spp_divisor}",
-        "hbm_budget_gb": budget / 1024 ** 3, "quantum_spp": 2, "max_jobs": 64,
+        "hbm_budget_gb": budget / 1024 ** 3, "quantum_spp": args.serve_quantum, "max_jobs": 64,
+        "engine": "wavefront (mtc_stream_run per round)",
     })
     for k in ("mpaths_per_s", "p50_s", "p99_s", "mean_s", "device_seconds"):
         stats[k] = round(stats[k], 4)

@@ -258,6 +258,62 @@ def autotune(jobs, probe_samples=1, space=AUTOTUNE_SPACE, repeats=2, device="cud
     return best, timings
 
 
+# Wavefront knobs the autotuner walks one at a time (coordinate descent from
+# the defaults): paths in flight ("queue depth"), idle lanes that trigger a
+# ray refill in the traversal kernels, and how often the shading queue is
+# regrouped by material class (abi.MTC_REGROUP_OFF: never).
+STREAM_SPACE = {
+    "refill_lanes": (4, 8, 16),
+    "regroup_interval": (1, 2, abi.MTC_REGROUP_OFF),
+    "slots": (1 << 19, 1 << 20, 1 << 21),
+}
+STREAM_DEFAULT = {"slots": 1 << 20, "refill_lanes": 8, "regroup_interval": 1}
+
+
+def autotune_stream(jobs, probe_samples=1, space=STREAM_SPACE, device="cuda", batch_config=None):
+    """Coordinate-descent tuning of the wavefront knobs on probe runs of the
+    actual jobs (each at `probe_samples` samples).  Returns (best
+    StreamConfig, {setting: ms}).  The probes accumulate into the jobs'
+    buffers, which are cleared afterwards; no setting changes any result."""
+    import torch
+    best = dict(STREAM_DEFAULT)
+    timings = {}
+    cache = {}
+
+    def probe(setting):
+        key = tuple(sorted(setting.items()))
+        if key in cache:
+            return cache[key]
+        sb = StreamBatch(len(jobs), batch_config, abi.StreamConfig.make(**setting), device)
+        sb.set_jobs(jobs, [probe_samples] * len(jobs))
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        sb.run()
+        e.record()
+        e.synchronize()
+        ms = s.elapsed_time(e)
+        del sb
+        cache[key] = ms
+        timings[",".join(f"{k}={v}" for k, v in key)] = ms
+        return ms
+
+    probe(best)  # warm-up of the code paths; timed again below
+    cache.clear()
+    timings.clear()
+    for knob, values in space.items():
+        results = {}
+        for val in values:
+            trial = dict(best)
+            trial[knob] = val
+            results[val] = probe(trial)
+        best[knob] = min(results, key=results.get)
+    for j in jobs:
+        j.acc.zero_()
+    torch.cuda.synchronize()
+    return abi.StreamConfig.make(**best), timings
+
+
 def total_paths(jobs, samples=None):
     samples = samples if samples is not None else [j.spp for j in jobs]
     return sum(j.pixels * s for j, s in zip(jobs, samples))

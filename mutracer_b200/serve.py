@@ -3,12 +3,13 @@
 Requests (scene, camera, resolution, target spp) arrive over time.  Each
 round the loop admits waiting requests while the batch has a free slot and
 their accumulation buffers fit the HBM budget, then runs every admitted job
-for up to `quantum` more samples in ONE persistent batched launch (a replay
-of a captured CUDA graph).  Jobs that reach their target spp complete and
-free their slot and memory; requests that arrived meanwhile join the next
-round, so new and running jobs share the device (continuous batching at
-sample granularity, not a FIFO of whole renders).  Two job tables alternate
-so the host prepares round k+1 while round k runs.
+for up to `quantum` more samples in one batched pass: a wavefront run
+(mtc_stream_run, the default engine) or a replay of the captured persistent
+megakernel launch (two job tables alternate, so the host prepares round k+1
+while round k runs).  Jobs that reach their target spp complete and free
+their slot and memory; requests that arrived meanwhile join the next round,
+so new and running jobs share the device (continuous batching at sample
+granularity, not a FIFO of whole renders).
 
 A pixel's samples always run in order on one lane and each round resumes at
 the pixel's accumulated sample count, so a job's outputs are bit-identical to
@@ -114,14 +115,24 @@ class Server:
     """Continuous-batching render server over a ScenePool."""
 
     def __init__(self, pool, hbm_budget_bytes, max_jobs=64, quantum=8, config=None, use_graph=True,
-                 device="cuda"):
+                 engine="wavefront", stream_config=None, device="cuda"):
+        """engine "wavefront": each round is one mtc_stream_run over all
+        admitted jobs; "persistent": each round replays the captured
+        persistent-megakernel launch (two alternating tables, so the host
+        prepares round k+1 while round k runs)."""
         self.pool = pool
         self.budget = int(hbm_budget_bytes)
         self.max_jobs = int(max_jobs)
         self.quantum = int(quantum)
         self.device = device
         self.use_graph = use_graph
-        self.batches = [batch.Batch(max_jobs, config, device) for _ in range(2)]
+        self.engine = engine
+        if engine == "wavefront":
+            self.batches = [batch.StreamBatch(max_jobs, config, stream_config, device)]
+        elif engine == "persistent":
+            self.batches = [batch.Batch(max_jobs, config, device) for _ in range(2)]
+        else:
+            raise ValueError(f"engine {engine!r}")
 
     def _bytes(self, req):
         return req.width * req.height * ACCUMULATION_BYTES_PER_PIXEL
@@ -134,7 +145,6 @@ class Server:
         waiting = collections.deque()
         active = []
         used = 0
-        rounds = []                       # (end event, finished requests, batch index)
         start = torch.cuda.Event(enable_timing=True)
         stream = torch.cuda.current_stream()
         torch.cuda.synchronize()
@@ -177,13 +187,16 @@ class Server:
                 if waiting:
                     raise RuntimeError("a request does not fit the HBM budget on its own")
                 break
-            # Table `which` was last used two rounds ago; make sure it ran.
-            while len(in_flight) >= 2:
+            # The table about to be rewritten was last used len(batches)
+            # rounds ago; make sure that round has run.
+            while len(in_flight) >= len(self.batches):
                 retire_one()
-            b = self.batches[which]
+            b = self.batches[which % len(self.batches)]
             samples = [min(self.quantum, r.spp - r.job.done) for r in active]
             b.set_jobs([r.job for r in active], samples)
-            if self.use_graph:
+            if self.engine == "wavefront":
+                b.run(stream)
+            elif self.use_graph:
                 b.replay()
             else:
                 b.launch(stream)
@@ -197,7 +210,7 @@ class Server:
                     finished.append(r)
             active = [r for r in active if r.job.done < r.spp]
             in_flight.append((ev, finished))
-            which ^= 1
+            which += 1
             n_rounds += 1
         while in_flight:
             retire_one()

@@ -87,6 +87,24 @@ def test_served_results_equal_alone(cuda):
         assert _equal(alone.acc, r.job.acc), r.request_id
 
 
+@pytest.mark.parametrize("engine", ["wavefront", "persistent"])
+def test_served_results_equal_alone_both_engines(cuda, engine):
+    import torch
+    pool = serve.ScenePool(cuda)
+    pool.add(0, scene.SceneHost("instanced_spheres", 32, 32, 4, (20, 4, 6, 64, 3)))
+    pool.add(1, scene.SceneHost("glass_spheres", 32, 32, 2, (5,)))
+    reqs = serve.poisson_requests(pool, 6, rate=300.0, seed=9, spp_range=(1, 7),
+                                  resolutions=((20, 30), (33, 17)))
+    srv = serve.Server(pool, hbm_budget_bytes=1 << 30, max_jobs=4, quantum=3, engine=engine, device=cuda)
+    srv.run(reqs, keep_outputs=True)
+    srv.release()
+    for r in reqs:
+        alone = batch.RenderJob(pool[r.scene_id], r.spp, r.width, r.height, camera=r.camera, device=cuda)
+        alone.render_alone(per_sample=True)
+        torch.cuda.synchronize()
+        assert _equal(alone.acc, r.job.acc), (engine, r.request_id)
+
+
 def test_served_admission_respects_the_hbm_budget(cuda):
     pool = serve.ScenePool(cuda)
     pool.add(0, scene.SceneHost("cornell", 16, 16, 1))
@@ -101,15 +119,17 @@ def test_served_admission_respects_the_hbm_budget(cuda):
         serve.Server(pool, hbm_budget_bytes=one - 1, device=cuda).run([serve.Request(0, 0, 64, 64, 1, 0.0)])
 
 
-@pytest.mark.parametrize("slots", [1024, 1 << 16])
-def test_wavefront_matches_alone(cuda, slots):
+@pytest.mark.parametrize("slots,refill,regroup", [(1024, 1, 1), (1 << 16, 8, 1), (4096, 32, 3),
+                                                  (1 << 14, 16, abi.MTC_REGROUP_OFF)])
+def test_wavefront_matches_alone(cuda, slots, refill, regroup):
     import torch
     jobs = _small_jobs(cuda)
     extra = batch.build_mixed([batch.JobSpec(9, 96, 80, 6, 40_000, 3, 21)], cuda, env_width=64)
     jobs += extra
     alone = _small_jobs(cuda) + batch.build_mixed([batch.JobSpec(9, 96, 80, 6, 40_000, 3, 21)], cuda, env_width=64)
     sb = batch.StreamBatch(len(jobs), abi.BatchConfig.make(tile_width=8),
-                           abi.StreamConfig.make(slots=slots, iterations_per_check=3), device=cuda)
+                           abi.StreamConfig.make(slots=slots, iterations_per_check=3, refill_lanes=refill,
+                                                 regroup_interval=regroup), device=cuda)
     sb.set_jobs(jobs)
     sb.run()
     torch.cuda.synchronize()
