@@ -335,10 +335,12 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
 // getBVHTraverseCode (intersect.wgsl.ts:213-629) as a restartable state
 // machine, for kernels that keep a queue of rays and give a lane a new ray as
 // soon as its current one has finished.  Each step() does exactly one of:
-// one BLAS node of the current instance, entering the next instance of the
-// current TLAS leaf, or one TLAS node.  Visit order, box tests, the `>` tie
-// rule and the self-hit and backface rules are those of traverse(), so the
-// hits are bit-identical to it.
+// one node (a BLAS node of the current instance, or a TLAS node when no
+// instance is open: interior nodes of both levels run the same code, so lanes
+// at different levels stay together), or entering the next instance of the
+// current TLAS leaf.  Visit order, box tests, the `>` tie rule and the
+// self-hit and backface rules are those of traverse(), so the hits are
+// bit-identical to it.
 template <bool shadow>
 struct RayTraversal {
   const float4 *bvh, *ins, *mats;
@@ -349,8 +351,11 @@ struct RayTraversal {
   int bounces;
   bool doubleSided;
   int32_t currentTri, currentIns;
-  int32_t tlasStack[MTC_MAX_STACK];
-  int32_t blasStack[MTC_MAX_STACK];
+  // TLAS entries at [0, MTC_MAX_STACK), the current instance's BLAS entries
+  // at [MTC_MAX_STACK, 2 * MTC_MAX_STACK): two stacks of the reference's
+  // depth, addressed through one array so TLAS and BLAS node visits share
+  // one code path.
+  int32_t stack[2 * MTC_MAX_STACK];
   int tlasTop, blasTop;
   int32_t leafNode, io;
   V3 o, d, linvD, shear;
@@ -383,10 +388,11 @@ struct RayTraversal {
     io = -1;
     leafNode = 0;
     insIdx = -1;
+    blasOffset = 0;
     invD = traversalInverse(rd);
     if (intersectBox(rayO, xyz(ld4(bvh)), xyz(ld4(bvh + 1)), invD, h.tMax) > 0.0f) {
       tlasTop = 0;
-      tlasStack[0] = 0;
+      stack[0] = 0;
       return true;
     }
     return false;
@@ -394,97 +400,96 @@ struct RayTraversal {
 
   // One traversal step; returns true when the query has finished.
   MTD bool step() {
-    if (blasTop >= 0) {
-      int32_t node = blasStack[blasTop--];
-      int32_t i = node + blasBase;
-      float4 n1 = ld4(bvh + i);
-      int32_t p = asi(n1.w);
-      if (p >= 0) {
-        int32_t left = node + 2, right = p + blasOffset;
-        float d0 = intersectBox(o, xyz(ld4(bvh + left + blasBase)), xyz(ld4(bvh + left + 1 + blasBase)), linvD, h.tMax);
-        float d1 = intersectBox(o, xyz(ld4(bvh + right + blasBase)), xyz(ld4(bvh + right + 1 + blasBase)), linvD, h.tMax);
-        if (d0 > d1) {
-          if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
-          if (d1 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = right;
-        } else {
-          if (d1 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = right;
-          if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
-        }
-        return false;
+    const bool blas = blasTop >= 0;
+    if (!blas) {
+      if (io >= 0) return enterInstance();
+      if (tlasTop < 0) return true;
+    }
+    // Pop one node of the current level.
+    int top = blas ? blasTop : tlasTop;
+    const int stackBase = blas ? MTC_MAX_STACK : 0;
+    int32_t node = stack[stackBase + top];
+    top--;
+    const int32_t base = blas ? blasBase : 0;
+    float4 n1 = ld4(bvh + node + base);
+    int32_t p = asi(n1.w);
+    if (p >= 0) {
+      // Interior node at either level: box-test both children, push the
+      // nearer last (the `>` rule of intersect.wgsl.ts).
+      const V3 ro = blas ? o : rayO, id = blas ? linvD : invD;
+      int32_t left = node + 2, right = blas ? p + blasOffset : p;
+      float d0 = intersectBox(ro, xyz(ld4(bvh + left + base)), xyz(ld4(bvh + left + 1 + base)), id, h.tMax);
+      float d1 = intersectBox(ro, xyz(ld4(bvh + right + base)), xyz(ld4(bvh + right + 1 + base)), id, h.tMax);
+      int32_t first = right, second = left;
+      float df = d1, ds = d0;
+      if (d0 > d1) {
+        first = left; second = right;
+        df = d0; ds = d1;
       }
-      int32_t primitiveCount = -p;
-      int32_t primitiveOffset = i + 2;
-      for (int32_t k = 0; k < primitiveCount; k++) {
-        int32_t triangleIndex = primitiveOffset + k;
-        if (bounces > 0 && triangleIndex == currentTri && insIdx == currentIns) continue;
-        float4 r3 = ld4(bvh + triangleIndex);
-        V3 p0 = position(asi(r3.x) + vertexOffset);
-        V3 p1 = position(asi(r3.y) + vertexOffset);
-        V3 p2 = position(asi(r3.z) + vertexOffset);
-        V3 bary;
-        float t = intersectTriangle(o, p0, p1, p2, maxDim, shear, h.tMax, bary);
-        if (!(t > 0.0f)) continue;
-        V3 candidateNormal = xnormalize(xcross(xsub3(p1, p0), xsub3(p2, p0)));
-        if (!doubleSided) {
-          bool matDoubleSided = __ldg(&mats[size_t(sideMaterial) * MTC_MATERIAL_VEC4_ROWS + 23].z) > 0.5f;
-          if (!matDoubleSided && xdot(candidateNormal, d) > 0.0f) continue;
-        }
-        h.hitNormal = candidateNormal;
-        h.tMax = t;
-        h.hitBary = bary;
-        if (shadow) {
-          found = true;
-          return true;
-        }
-        h.triangleIndex = triangleIndex;
-        h.insIdx = insIdx;
-      }
+      if (df > 0.0f && top + 1 < MTC_MAX_STACK) stack[stackBase + (++top)] = first;
+      if (ds > 0.0f && top + 1 < MTC_MAX_STACK) stack[stackBase + (++top)] = second;
+      if (blas) blasTop = top; else tlasTop = top;
       return false;
     }
-    if (io >= 0) {
-      float4 rec = ld4(bvh + leafNode + 2 + io);
-      io--;
-      insIdx = asi(rec.x);
-      int32_t blasRoot = asi(rec.y);
-      const float4 *insv = ins + size_t(insIdx) * MTC_INSTANCE_VEC4_STRIDE;
-      float4 insData = ld4(insv);
-      uint32_t encoded = asu(insData.x);
-      if ((encoded >> 30) != 0u) return false;
-      float4 c0 = ld4(insv + 1), c1 = ld4(insv + 2), c2 = ld4(insv + 3), c3 = ld4(insv + 4);
-      o = xmat4(c0, c1, c2, c3, rayO, 1.0f);
-      d = xmat4(c0, c1, c2, c3, rayD, 0.0f);
-      linvD = traversalInverse(d);
-      maxDim = maxDimension(vabs(d));
-      shear = getShear(d, maxDim);
-      blasOffset = int32_t(encoded & 0x3fffffffu);
-      vertexOffset = asi(insData.y);
-      sideMaterial = asi(insData.z) >> 8;
-      blasTop = 0;
-      blasStack[0] = blasRoot;
+    if (blas) blasTop = top; else tlasTop = top;
+    if (!blas) {
+      leafNode = node;
+      io = -p - 1;
       return false;
     }
-    if (tlasTop >= 0) {
-      int32_t tlasNode = tlasStack[tlasTop--];
-      float4 r1 = ld4(bvh + tlasNode);
-      int32_t ptr = asi(r1.w);
-      if (ptr >= 0) {
-        int32_t left = tlasNode + 2, right = ptr;
-        float d0 = intersectBox(rayO, xyz(ld4(bvh + left)), xyz(ld4(bvh + left + 1)), invD, h.tMax);
-        float d1 = intersectBox(rayO, xyz(ld4(bvh + right)), xyz(ld4(bvh + right + 1)), invD, h.tMax);
-        if (d0 > d1) {
-          if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
-          if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
-        } else {
-          if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
-          if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
-        }
-      } else {
-        leafNode = tlasNode;
-        io = -ptr - 1;
+    int32_t primitiveCount = -p;
+    int32_t primitiveOffset = node + base + 2;
+    for (int32_t k = 0; k < primitiveCount; k++) {
+      int32_t triangleIndex = primitiveOffset + k;
+      if (bounces > 0 && triangleIndex == currentTri && insIdx == currentIns) continue;
+      float4 r3 = ld4(bvh + triangleIndex);
+      V3 p0 = position(asi(r3.x) + vertexOffset);
+      V3 p1 = position(asi(r3.y) + vertexOffset);
+      V3 p2 = position(asi(r3.z) + vertexOffset);
+      V3 bary;
+      float t = intersectTriangle(o, p0, p1, p2, maxDim, shear, h.tMax, bary);
+      if (!(t > 0.0f)) continue;
+      V3 candidateNormal = xnormalize(xcross(xsub3(p1, p0), xsub3(p2, p0)));
+      if (!doubleSided) {
+        bool matDoubleSided = __ldg(&mats[size_t(sideMaterial) * MTC_MATERIAL_VEC4_ROWS + 23].z) > 0.5f;
+        if (!matDoubleSided && xdot(candidateNormal, d) > 0.0f) continue;
       }
-      return false;
+      h.hitNormal = candidateNormal;
+      h.tMax = t;
+      h.hitBary = bary;
+      if (shadow) {
+        found = true;
+        return true;
+      }
+      h.triangleIndex = triangleIndex;
+      h.insIdx = insIdx;
     }
-    return true;
+    return false;
+  }
+
+  // Next instance entry of the current TLAS leaf (descending, as the WGSL's
+  // leaf loop): the ray in instance space and its watertight-test shear.
+  MTD bool enterInstance() {
+    float4 rec = ld4(bvh + leafNode + 2 + io);
+    io--;
+    insIdx = asi(rec.x);
+    int32_t blasRoot = asi(rec.y);
+    const float4 *insv = ins + size_t(insIdx) * MTC_INSTANCE_VEC4_STRIDE;
+    float4 insData = ld4(insv);
+    uint32_t encoded = asu(insData.x);
+    if ((encoded >> 30) != 0u) return false;
+    float4 c0 = ld4(insv + 1), c1 = ld4(insv + 2), c2 = ld4(insv + 3), c3 = ld4(insv + 4);
+    o = xmat4(c0, c1, c2, c3, rayO, 1.0f);
+    d = xmat4(c0, c1, c2, c3, rayD, 0.0f);
+    linvD = traversalInverse(d);
+    maxDim = maxDimension(vabs(d));
+    shear = getShear(d, maxDim);
+    blasOffset = int32_t(encoded & 0x3fffffffu);
+    vertexOffset = asi(insData.y);
+    sideMaterial = asi(insData.z) >> 8;
+    blasTop = 0;
+    stack[MTC_MAX_STACK] = blasRoot;
+    return false;
   }
 };
 

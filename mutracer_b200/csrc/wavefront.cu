@@ -193,7 +193,11 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v) {
 // Closest hits of the queued extension rays.  Persistent: a lane whose ray
 // has finished takes the next queued ray at once, so a warp is not held by
 // its slowest ray (traversal lengths differ by an order of magnitude here).
-__global__ void __launch_bounds__(kStreamThreads) k_wf_extend(StreamView v, uint32_t cur, uint32_t regroup) {
+#ifndef MT_TRAVERSE_MIN_BLOCKS
+#define MT_TRAVERSE_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
+    k_wf_extend(StreamView v, uint32_t cur, uint32_t regroup) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     v.q->rayCount[cur ^ 1u] = 0;
     v.q->shadowCount = 0;
@@ -277,7 +281,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_regroup(StreamView v, uin
 }
 
 #ifndef MT_SHADE_MIN_BLOCKS
-#define MT_SHADE_MIN_BLOCKS 3
+#define MT_SHADE_MIN_BLOCKS 4
 #endif
 __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
     k_wf_shade(StreamView v, uint32_t cur, uint32_t regroup) {
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
 
 // NEE visibility of the queued shadow rays (intersectSceneShadow and
 // resolveShadow), persistent like k_wf_extend.
-__global__ void __launch_bounds__(kStreamThreads) k_wf_shadow(StreamView v) {
+__global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS) k_wf_shadow(StreamView v) {
   const uint32_t n = v.q->shadowCount;
   RayTraversal<true> rt;
   uint32_t s = 0, shadowRays = 0;
