@@ -6,6 +6,7 @@
 #pragma once
 #include "dev_bsdf.cuh"
 #include "dev_trace.cuh"
+#include "spectrum_cdf.h"
 
 namespace mt {
 
@@ -110,6 +111,25 @@ MTD V3 spectralFilter(V3 rgb, int channel) {
   V3 f = v3(0.0f);
   setcomp(f, channel - 1, comp(rgb, channel - 1));
   return f;
+}
+
+// spectrum.ts:62-88: inverse CDFs of continuous wavelength sampling, one per
+// RGB channel and one for r+g+b (generated by gen_spectrum_cdf.py).
+static __constant__ float c_spectrumCdf[MT_SPECTRUM_CDF_SIZE] = {MT_SPECTRUM_CDF_VALUES};
+
+// spectrum.ts:133-141 spectrumSample + spectrumIorWavelength: the refracting
+// wavelength of a camera path that carries RGB channel `channel`.
+MTD float spectrumCameraWavelength(uint32_t channel, float u) {
+  const float *cdf = c_spectrumCdf + channel * (MT_SPECTRUM_BINS + 1);
+  uint32_t low = 0, high = MT_SPECTRUM_BINS;
+  while (high - low > 1u) {
+    uint32_t middle = (low + high) >> 1;
+    if (cdf[middle] <= u) low = middle; else high = middle;
+  }
+  float mass = cdf[low + 1] - cdf[low];
+  float wavelength = 400.0f + 5.0f * (float(low) + (u - cdf[low]) / mass);
+  if (wavelength >= 500.0f) return wavelength;
+  return 500.0f - 25.0f * (1.0f - expf((wavelength - 500.0f) / 25.0f));
 }
 
 // ------------------------------------------------------------------ lights
@@ -711,15 +731,22 @@ MTD bool finishDirectLight(Ctx &c, const SurfaceInteraction &si, Path &path, V3 
     float4 bg = sampleSceneBackground(c.J, visDir);
     Li = V3{bg.x, bg.y, bg.z} * bg.w;
   }
-  if (isSpectral(c.J)) Li = spectralFilter(Li, si.spectralChannel);
+  // Spectral scenes use channel-independent RIS (WGPURayTracePass.ts:1349,
+  // sampleMaterial.wgsl.ts:119-140): with three wavelengths the radiance is
+  // filtered after the target, and each RGB component weighs 1/3.
+  const bool spectral = isSpectral(c.J);
+  const bool threeWavelengths = spectral && c.J.u.dispersion_wavelengths != 1;
+  if (spectral && !threeWavelengths) Li = spectralFilter(Li, si.spectralChannel);
   float mis = ls.isDelta ? 1.0f : neeMISWeight(c, lightPdf, scatteringPdf);
   if (mis > 0.0f) {
     V3 un = Li * f / lightPdf * path.beta;
-    w.risTarget = fmaxf(dot(vmax(un * lsp, v3(0.0f)), kLuminance()), 0.0f);
+    const V3 targetWeights = threeWavelengths ? v3(1.0f / 3.0f) : kLuminance();
+    w.risTarget = fmaxf(dot(vmax(un * lsp, v3(0.0f)), targetWeights), 0.0f);
     w.ray = {shadowOrigin, visDir};
     w.maxDistance = visDist;
     w.triangleIndex = si.triangleIndex;
     w.contribution = un * mis;
+    if (threeWavelengths) w.contribution = spectralFilter(w.contribution, si.spectralChannel);
     w.lightSelectionPmf = lsp;
     w.valid = true;
     return true;
@@ -1047,11 +1074,27 @@ struct PathSample {
   bool sampleIgnored, isNotTransparent;
 };
 
+// Locals of the spectral integrator (rayTrace.compute.ts:947-1057) that live
+// across its three wavelength paths: the primary vertex they share, the
+// sampler state each restarts from, and the running sums.
+struct SpectralState {
+  SurfaceInteraction primarySi;
+  Aux primaryAux;        // the integrator's outAux: primary-hit guides
+  Ray cameraRay;
+  uint4 savedS0;
+  uint32_t savedHashed;
+  float wavelengthSample;
+  int wavelengthIndex, heroWavelengthIndex;
+  bool primaryReady, dispersivePrimary, allBlank;
+  V3 color, guideAlbedo, guideNormal;
+  float alpha;
+};
+
 // rayTrace.compute.ts:1157-1208 main up to the integrator call: sampler
 // state for (x, y, outNormal.a + sampleSequenceOffset), Sobol jitter, camera
 // ray and thin lens, then integrator() locals (:891-905).  Out of line, like
 // shadeStep and endSample, so every kernel runs one compiled copy.
-static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, PathSample &ps) {
+static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, PathSample &ps, SpectralState &sp) {
   const JobData &J = c.J;
   const mtc_trace_uniform &u = J.u;
   uint32_t W = J.width;
@@ -1111,10 +1154,29 @@ static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, 
   ps.event = 0;
   ps.sampleIgnored = false;
   ps.isNotTransparent = false;
+  if (isSpectral(J)) {
+    sp.primaryReady = false;
+    sp.primaryAux = {v3(0.0f), v3(0.0f), false};
+    sp.cameraRay = cam;
+    sp.wavelengthIndex = 0;
+    sp.heroWavelengthIndex = 0;
+    sp.dispersivePrimary = false;
+    sp.allBlank = true;
+    sp.color = v3(0.0f);
+    sp.guideAlbedo = v3(0.0f);
+    sp.guideNormal = v3(0.0f);
+    sp.alpha = 0.0f;
+  }
 }
 
 // The traversal half of intersectScene (intersect.wgsl.ts:696-740) for the
 // path's current event: the closest hit of its extension ray.
+// A spectral wavelength path after the first starts from the shared primary
+// vertex and traces nothing at its event 0 (rayTrace.compute.ts:978).
+MTD bool reusesPrimary(const JobData &J, const PathSample &ps, bool primaryReady) {
+  return isSpectral(J) && ps.event == 0 && primaryReady;
+}
+
 MTD void traceExtension(const JobData &J, const PathSample &ps, TraversalHit &h, Counters &cnt) {
   h.tMax = RAY_MAX_DISTANCE;
   h.triangleIndex = -1;
@@ -1161,11 +1223,130 @@ static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const Trav
   return false;
 }
 
-// One iteration of the integrator's event loop.
-MTD bool stepPath(Ctx &c, PathSample &ps) {
+// One step of the spectral integrator (rayTrace.compute.ts:947-1057) after
+// its extension ray (if any) has been traced: at event 0 the first wavelength
+// path resolves and keeps the primary vertex, and every wavelength path
+// restarts there with its own wavelength, Cauchy IOR and the sampler state
+// saved after the wavelength draw.  Returns true when the current wavelength
+// path has ended (finishWavelength then decides whether the sample has).
+static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, SpectralState &sp,
+                                                      const TraversalHit &h) {
+  Path &path = ps.path;
+  SurfaceInteraction &si = ps.si;
+  const mtc_trace_uniform &u = c.J.u;
+  const int bounceLimit = max(u.bounces, 0);
+  const int eventLimit = min(bounceLimit * 3, 20);
+  const int event = ps.event;
+  const bool singleWavelength = u.dispersion_wavelengths == 1;
+  Material ma;
+  if (!reusesPrimary(c.J, ps, sp.primaryReady)) {
+    si.hit = false;
+    if (h.insIdx >= 0) {
+      si.triangleIndex = h.triangleIndex;
+      completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
+    }
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, ma);
+  } else {
+    // The primary material is a pure function of the primary vertex.
+    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, ma);
+  }
+  if (event == 0) {
+    if (!sp.primaryReady) {
+      if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
+        sp.primaryAux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+        sp.primaryAux.normal = dot(si.normal, si.position - cameraEye(c.J)) > 0.0f ? -si.normal : si.normal;
+        si.albedoSampled = ma.transmissionWeight > 0.5f;
+      }
+      sp.primarySi = si;
+      sp.primaryReady = true;
+      sp.dispersivePrimary = si.hit && ma.transmissionWeight > 0.001f && ma.transmissionDispersionScale > 0.001f;
+      sp.wavelengthSample = c.smp.s1(2u);  // CAMERA_WAVELENGTH, sobol.wgsl.ts:5
+      if (singleWavelength) {
+        sp.heroWavelengthIndex = min(int(floorf(sp.wavelengthSample * 3.0f)), 2);
+        float w3 = sp.wavelengthSample * 3.0f;
+        sp.wavelengthSample = w3 - floorf(w3);
+      }
+      sp.savedS0 = c.smp.s0;
+      sp.savedHashed = c.smp.hashed;
+    }
+    si = sp.primarySi;
+    ps.aux = sp.primaryAux;
+    if (!singleWavelength) {
+      c.smp.s0 = sp.savedS0;
+      c.smp.hashed = sp.savedHashed;
+      c.smp.bounce = 0;
+      ps.aux.isBlank = false;
+    }
+    si.wavelength = 0.0f;
+    si.spectralChannel = 0;
+    if (!singleWavelength || sp.dispersivePrimary) {
+      int channel = singleWavelength ? sp.heroWavelengthIndex : sp.wavelengthIndex;
+      si.spectralChannel = channel + 1;
+      si.wavelength = spectrumCameraWavelength(uint32_t(channel), sp.wavelengthSample);
+      ma.specularIor = cauchyIor(si.wavelength, ma.specularIor, ma.transmissionDispersionScale,
+                                 ma.dispersionAbbeNumber);
+    }
+    path.scatteringMediumEntered = false;
+    path.ray = sp.cameraRay;
+    path.li = v3(0.0f);
+    path.alpha = u.transmissive_output_alpha_min < 1.0f ? 0.0f : 1.0f;
+    path.beta = v3(1.0f);
+    path.fromEye = true;
+    path.abort = false;
+    path.scatteringPdf = 0.0f;
+    path.scatteringIsDelta = false;
+    path.isNextRefraction = false;
+    ps.depth = 0;
+    ps.sampleIgnored = false;
+    ps.isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
+  } else if (!path.abort) {
+    completeVertex(c, path, ps.depth, si, ma, ps.sampleIgnored);
+  }
+  if (ps.isNotTransparent && event > bounceLimit) path.abort = true;
+  if (!path.abort && event < eventLimit) shadeVertex(c, ps.coord, path, ps.depth, si, ma, ps.aux, ps.sampleIgnored);
+  if (path.abort || event >= eventLimit) return true;
+  ps.event = event + 1;
+  return false;
+}
+
+// End of a spectral wavelength path, after its last NEE shadow ray has been
+// resolved (rayTrace.compute.ts:1036-1053).  Returns true when the sample is
+// complete; its radiance, alpha and guides are then in ps.path / ps.aux for
+// endSample.  Otherwise the next wavelength path starts at event 0.
+MTD bool finishWavelength(const JobData &J, PathSample &ps, SpectralState &sp) {
+  if (J.u.dispersion_wavelengths == 1) {
+    float scale = sp.dispersivePrimary ? 3.0f : 1.0f;
+    ps.path.li = ps.path.li * scale;
+    return true;
+  }
+  sp.color += ps.path.li;
+  sp.alpha = fmaxf(sp.alpha, ps.path.alpha);
+  sp.guideAlbedo += ps.aux.albedo;
+  sp.guideNormal += ps.aux.normal;
+  sp.allBlank = sp.allBlank && ps.aux.isBlank;
+  sp.wavelengthIndex++;
+  if (sp.wavelengthIndex >= 3) {
+    ps.path.li = sp.color;
+    ps.path.alpha = sp.alpha;
+    ps.aux.albedo = sp.guideAlbedo / 3.0f;
+    ps.aux.normal = sp.guideNormal / 3.0f;
+    ps.aux.isBlank = sp.allBlank;
+    return true;
+  }
+  ps.event = 0;
+  return false;
+}
+
+// One iteration of the integrator's event loop: true when the path (the
+// current wavelength path of a spectral sample) has ended.
+MTD bool stepPath(Ctx &c, PathSample &ps, SpectralState &sp) {
   TraversalHit h;
-  traceExtension(c.J, ps, h, c.cnt);
-  return shadeStep(c, ps, h);
+  h.tMax = RAY_MAX_DISTANCE;
+  h.triangleIndex = -1;
+  h.insIdx = -1;
+  const bool spectral = isSpectral(c.J);
+  if (!spectral || !reusesPrimary(c.J, ps, sp.primaryReady)) traceExtension(c.J, ps, h, c.cnt);
+  return spectral ? shadeStepSpectral(c, ps, sp, h) : shadeStep(c, ps, h);
 }
 
 // The deferred NEE visibility test of sampleScattering (sampleMaterial.wgsl.ts
@@ -1219,19 +1400,22 @@ static __device__ __noinline__ void tracePixelSamples(const JobData &J, uint32_t
   c.shadow.valid = false;
   const uint32_t idx = x + y * J.width;
   PathSample ps;
+  SpectralState sp;
+  const bool spectral = isSpectral(J);
   uint32_t left = samples;
   bool active = left > 0u;
-  if (active) beginSample(c, x, y, ps);
+  if (active) beginSample(c, x, y, ps, sp);
   // No warp vote here: the traversal and shading are latency-bound, and
   // lanes left free to diverge give the scheduler more independent loads in
   // flight than a warp forced back together at every event.
   while (active) {
-    bool ended = stepPath(c, ps);
+    bool ended = stepPath(c, ps, sp);
     resolveShadow(c, ps);
+    if (ended && spectral) ended = finishWavelength(J, ps, sp);
     if (ended) {
       endSample(J, idx, ps);
       if (--left == 0u) active = false;
-      else beginSample(c, x, y, ps);
+      else beginSample(c, x, y, ps, sp);
     }
   }
   cnt.ext += c.cnt.ext;

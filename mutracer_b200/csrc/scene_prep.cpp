@@ -824,7 +824,7 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   // Materials.
   s.materials.assign(materials.size() * MTC_MATERIAL_VEC4_ROWS * 4, 0.0f);
   uint32_t features = 0;
-  bool hasMedium = false;
+  bool hasMedium = false, spectral = false;
   for (size_t i = 0; i < materials.size(); i++) {
     packMaterial(materials[i], &s.materials[i * MTC_MATERIAL_VEC4_ROWS * 4]);
     const MaterialDesc &m = materials[i];
@@ -833,9 +833,12 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
     if (m.subsurfaceWeight > 0) features |= MTC_FEATURE_HAS_SUBSURFACE;
     if (m.thinFilmWeight > 0) features |= MTC_FEATURE_HAS_THIN_FILM;
     if (m.mediumExtinction[0] > 0 || m.mediumExtinction[1] > 0 || m.mediumExtinction[2] > 0) hasMedium = true;
+    // SPECTRAL: some material disperses (wgpuMaterialConstants.ts:14-15).
+    if (m.dispersionScale > 0) spectral = true;
   }
   if (!s.env.image.empty()) features |= MTC_FEATURE_USE_ENVMAP;
   if (hasMedium) s.flags |= MTC_SCENE_HAS_MEDIUM;
+  if (spectral) s.flags |= MTC_SCENE_SPECTRAL;
   // Light choices: environment, analytic lights (sceneAssembly.ts:42-82).
   std::vector<int> types, idx;
   std::vector<double> weights;

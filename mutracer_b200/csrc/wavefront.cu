@@ -64,6 +64,7 @@ struct StreamView {
   const JobData *jobs;
   StreamQueues *q;
   Slot *slots;
+  SpectralState *spectral;  // per slot, used by spectral jobs only
   TraversalHit *hits;
   uint32_t *rayQueue[2];
   uint32_t *shadowQueue, *finishQueue;
@@ -174,7 +175,7 @@ __device__ bool claimPixel(const StreamView &v, uint32_t s) {
     sl.left = J.samples - 1u;
     Ctx c{J, Sampler(), bsdfContext(J), Counters(), ShadowQuery()};
     PathSample ps;
-    beginSample(c, x, y, ps);
+    beginSample(c, x, y, ps, v.spectral[s]);
     sl.ps = ps;
     sl.smp = c.smp;
     sl.shadow.valid = false;
@@ -222,8 +223,10 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
         s = queue[t];
         const Slot &sl = v.slots[s];
         const JobData &J = v.jobs[sl.job];
-        // traceExtension: an empty scene is a miss without a traversal.
-        if (J.u.is_empty > 0) {
+        // traceExtension: an empty scene is a miss without a traversal, and a
+        // spectral wavelength path restarting at the shared primary vertex
+        // traces nothing.
+        if (J.u.is_empty > 0 || (isSpectral(J) && reusesPrimary(J, sl.ps, v.spectral[s].primaryReady))) {
           TraversalHit none;
           none.tMax = RAY_MAX_DISTANCE;
           none.triangleIndex = -1;
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
     c.shadow.valid = false;
     PathSample ps = sl.ps;
     TraversalHit h = v.hits[s];
-    bool ended = shadeStep(c, ps, h);
+    bool ended = isSpectral(J) ? shadeStepSpectral(c, ps, v.spectral[s], h) : shadeStep(c, ps, h);
     sl.ps = ps;
     sl.smp = c.smp;
     sl.shadow = c.shadow;
@@ -376,13 +379,19 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
     Slot &sl = v.slots[s];
     const JobData &J = v.jobs[sl.job];
     PathSample ps = sl.ps;
+    if (isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) {
+      // The next wavelength path of this sample starts at event 0.
+      sl.ps = ps;
+      enqueue(v.rayQueue[cur ^ 1u], &v.q->rayCount[cur ^ 1u], s);
+      continue;
+    }
     endSample(J, sl.x + sl.y * J.width, ps);
     paths++;
     bool again;
     if (sl.left > 0u) {
       sl.left--;
       Ctx c{J, Sampler(), bsdfContext(J), Counters(), ShadowQuery()};
-      beginSample(c, sl.x, sl.y, ps);
+      beginSample(c, sl.x, sl.y, ps, v.spectral[s]);
       sl.ps = ps;
       sl.smp = c.smp;
       again = true;
@@ -397,7 +406,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
 size_t roundUp(size_t x) { return (x + 255) / 256 * 256; }
 
 struct StreamLayout {
-  size_t table, queues, slots, hits, rayQueues, shadowQueue, finishQueue, keys, sortedQueue, classes, total;
+  size_t table, queues, slots, spectral, hits, rayQueues, shadowQueue, finishQueue, keys, sortedQueue, classes, total;
 };
 
 StreamLayout layout(uint32_t capacity, uint32_t slots) {
@@ -409,6 +418,8 @@ StreamLayout layout(uint32_t capacity, uint32_t slots) {
   off += sizeof(StreamQueues);
   L.slots = off;
   off += roundUp(size_t(slots) * sizeof(Slot));
+  L.spectral = off;
+  off += roundUp(size_t(slots) * sizeof(SpectralState));
   L.hits = off;
   off += roundUp(size_t(slots) * sizeof(TraversalHit));
   L.rayQueues = off;
@@ -524,6 +535,7 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
   v.jobs = reinterpret_cast<const JobData *>(base + L.table + sizeof(TableHeader));
   v.q = reinterpret_cast<StreamQueues *>(base + L.queues);
   v.slots = reinterpret_cast<Slot *>(base + L.slots);
+  v.spectral = reinterpret_cast<SpectralState *>(base + L.spectral);
   v.hits = reinterpret_cast<TraversalHit *>(base + L.hits);
   v.rayQueue[0] = reinterpret_cast<uint32_t *>(base + L.rayQueues);
   v.rayQueue[1] = reinterpret_cast<uint32_t *>(base + L.rayQueues + roundUp(size_t(shape.slots) * 4));

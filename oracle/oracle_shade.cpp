@@ -2,6 +2,9 @@
 //
 // Lights, environment, material resolve, next-event estimation and the RGB
 // integrator of the CPU oracle.
+#include <cstdio>
+#include <cstdlib>
+
 #include "oracle_bsdf.h"
 
 namespace oracle {
@@ -110,6 +113,91 @@ static V3 spectralFilter(V3 rgb, i32 channel) {
   V3 f = v3(0.0f);
   setcomp(f, channel - 1, comp(rgb, channel - 1));
   return f;
+}
+
+// --------------------------------------------------------------- spectrum
+// spectrum.ts:10-88: continuous wavelength sampling.  The inverse-CDF tables
+// are built in float64 exactly as the reference's module builds them when it
+// loads (Wyman-Sloan-Shirley CIE lobes -> linear sRGB, clamp, per-channel
+// scale rounded to 6 decimals, 60 bins x 20 midpoint substeps, every CDF value
+// rounded to 7 decimals), then read as f32 like the WGSL literals.
+namespace {
+struct SpectrumTables {
+  float cdf[4 * 61];
+  double scale[3];
+  static void unnormalized(double wl, double rgb[3]) {
+    static const double lobes[3][3][4] = {
+        {{1.056, 599.8, 37.9, 31.0}, {0.362, 442.0, 16.0, 26.7}, {-0.065, 501.1, 20.4, 26.2}},
+        {{0.821, 568.8, 46.9, 40.5}, {0.286, 530.9, 16.3, 31.1}, {0, 0, 0, 0}},
+        {{1.217, 437.0, 11.8, 36.0}, {0.681, 459.0, 26.0, 13.8}, {0, 0, 0, 0}}};
+    static const int counts[3] = {3, 2, 2};
+    static const double m[3][3] = {{3.2406, -1.5372, -0.4986}, {-0.9689, 1.8758, 0.0415}, {0.0557, -0.204, 1.057}};
+    double xyz[3];
+    for (int c = 0; c < 3; c++) {
+      double sum = 0;
+      for (int l = 0; l < counts[c]; l++) {
+        const double *L = lobes[c][l];
+        double t = (wl - L[1]) / (wl < L[1] ? L[2] : L[3]);
+        sum += L[0] * std::exp(-0.5 * t * t);
+      }
+      xyz[c] = sum;
+    }
+    for (int r = 0; r < 3; r++) rgb[r] = std::max(0.0, m[r][0] * xyz[0] + m[r][1] * xyz[1] + m[r][2] * xyz[2]);
+  }
+  static double rounded(double v, int digits) {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%.*f", digits, v);
+    return std::strtod(buf, nullptr);
+  }
+  SpectrumTables() {
+    const int steps = 3000;
+    double sum[3] = {0, 0, 0};
+    for (int i = 0; i < steps; i++) {
+      double rgb[3];
+      unnormalized(400.0 + (300.0 * (i + 0.5)) / steps, rgb);
+      for (int c = 0; c < 3; c++) sum[c] += rgb[c] / steps;
+    }
+    for (int c = 0; c < 3; c++) scale[c] = rounded(1.0 / sum[c], 6);
+    for (int d = 0; d <= 3; d++) {
+      double cdf[61];
+      cdf[0] = 0;
+      for (int b = 0; b < 60; b++) {
+        double mass = 0;
+        for (int i = 0; i < 20; i++) {
+          double rgb[3];
+          unnormalized(400.0 + (b + (i + 0.5) / 20) * 5.0, rgb);
+          for (int c = 0; c < 3; c++) rgb[c] *= scale[c];
+          mass += d == 3 ? rgb[0] + rgb[1] + rgb[2] : rgb[d];
+        }
+        cdf[b + 1] = cdf[b] + mass;
+      }
+      for (int b = 0; b <= 60; b++) {
+        char buf[64];
+        std::snprintf(buf, sizeof buf, "%.7f", cdf[b] / cdf[60]);
+        this->cdf[d * 61 + b] = std::strtof(buf, nullptr);
+      }
+    }
+  }
+};
+const SpectrumTables &spectrumTables() {
+  static const SpectrumTables t;
+  return t;
+}
+}  // namespace
+
+// spectrum.ts:133-141 spectrumSample + spectrumIorWavelength: the refracting
+// wavelength of a camera path that carries one RGB channel.
+static float spectrumCameraWavelength(u32 channel, float u) {
+  const float *cdf = spectrumTables().cdf + channel * 61u;
+  u32 low = 0, high = 60;
+  while (high - low > 1u) {
+    u32 middle = (low + high) / 2u;
+    if (cdf[middle] <= u) low = middle; else high = middle;
+  }
+  float mass = cdf[low + 1] - cdf[low];
+  float wavelength = 400.0f + 5.0f * (float(low) + (u - cdf[low]) / mass);
+  if (wavelength >= 500.0f) return wavelength;
+  return 500.0f - 25.0f * (1.0f - std::exp((wavelength - 500.0f) / 25.0f));
 }
 
 // ------------------------------------------------------------------ lights
@@ -646,15 +734,22 @@ static bool finishDirectLight(Ctx &c, SurfaceInteraction &si, const Material &ma
     V4 bg = sampleSceneBackground(c.s, lightRay);
     Li = V3{bg.x, bg.y, bg.z} * bg.w;
   }
-  if (c.s.flags & MTC_SCENE_SPECTRAL) Li = spectralFilter(Li, si.spectralChannel);
+  // Spectral scenes use channel-independent RIS (WGPURayTracePass.ts:1349,
+  // sampleMaterial.wgsl.ts:119-140): with three wavelengths the radiance is
+  // filtered after the target, and each RGB component weighs 1/3.
+  const bool spectral = (c.s.flags & MTC_SCENE_SPECTRAL) != 0;
+  const bool threeWavelengths = spectral && c.s.u->dispersion_wavelengths != 1;
+  if (spectral && !threeWavelengths) Li = spectralFilter(Li, si.spectralChannel);
   float mis = ls.isDelta ? 1.0f : neeMISWeight(c, lightPdf, scatteringPdf);
   if (mis > 0.0f) {
     V3 un = Li * f / lightPdf * path.beta;
-    w.risTarget = fmaxf(dot(vmax(un * lsp, v3(0.0f)), kLuminance), 0.0f);
+    const V3 targetWeights = threeWavelengths ? v3(1.0f / 3.0f) : kLuminance;
+    w.risTarget = fmaxf(dot(vmax(un * lsp, v3(0.0f)), targetWeights), 0.0f);
     w.ray = lightRay;
     w.maxDistance = visDist;
     w.triangleIndex = si.triangleIndex;
     w.contribution = un * mis;
+    if (threeWavelengths) w.contribution = spectralFilter(w.contribution, si.spectralChannel);
     w.lightSelectionPmf = lsp;
     w.valid = true;
     return true;
@@ -1002,6 +1097,120 @@ static V4 integrateRgb(Ctx &c, V2 uv, const Ray &ray, Aux &aux) {
   return {path.li.x, path.li.y, path.li.z, path.alpha};
 }
 
+// rayTrace.compute.ts:947-1057: the spectral integrator (independent
+// wavelength paths, shareSpectralPrefix off).  The primary hit is traced once
+// and reused by the three wavelength paths (or one hero wavelength when
+// dispersionWavelengths == 1); each path restarts from the primary vertex with
+// the sampler state saved after the wavelength draw, refracts with a Cauchy
+// IOR at its wavelength, and its radiance is filtered to its RGB channel.
+static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
+  SurfaceInteraction si, primarySi;
+  Material ma, primaryMa;
+  bool primaryReady = false;
+  Path path;
+  path.ray = ray;
+  const int bounceLimit = std::max(c.s.u->bounces, 0);
+  const int eventLimit = std::min(bounceLimit * 3, 20);
+  int depth = 0, event = 0;
+  bool sampleIgnored = false, isNotTransparent = false;
+  int wavelengthIndex = 0;
+  const bool singleWavelength = c.s.u->dispersion_wavelengths == 1;
+  bool dispersivePrimary = false;
+  int heroWavelengthIndex = 0;
+  float wavelengthSample = 0.0f;
+  u32 savedS0[4] = {0, 0, 0, 0};
+  u32 savedHashed = 0;
+  Aux wavelengthAux;
+  V3 color = v3(0.0f);
+  float alpha = 0.0f;
+  V3 guideAlbedo = v3(0.0f), guideNormal = v3(0.0f);
+  bool allBlank = true;
+  const int stepLimit = std::min((20 + 1) * 3, int(c.s.u->loop_unroll_guard * 16u));
+  for (int step = 0; step < stepLimit; step++) {
+    if (!primaryReady || (event != 0 && !path.abort)) {
+      intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
+      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex);
+      if (c.tr) c.tr->material_fetches++;
+    }
+    if (event == 0) {
+      if (!primaryReady) {
+        if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
+          outAux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+          outAux.normal = dot(si.normal, si.position - cameraEye(c.s)) > 0.0f ? -si.normal : si.normal;
+          si.albedoSampled = ma.transmissionWeight > 0.5f;
+        }
+        outAux.isShadowCatcher = false;
+        primarySi = si;
+        primaryMa = ma;
+        primaryReady = true;
+        dispersivePrimary = si.hit && ma.transmissionWeight > 0.001f && ma.transmissionDispersionScale > 0.001f;
+        wavelengthSample = c.smp.s1(2u);  // CAMERA_WAVELENGTH, sobol.wgsl.ts:5
+        if (singleWavelength) {
+          heroWavelengthIndex = std::min(int(std::floor(wavelengthSample * 3.0f)), 2);
+          float w3 = wavelengthSample * 3.0f;
+          wavelengthSample = w3 - std::floor(w3);
+        }
+        for (int k = 0; k < 4; k++) savedS0[k] = c.smp.s0[k];
+        savedHashed = c.smp.hashed;
+      }
+      si = primarySi;
+      ma = primaryMa;
+      wavelengthAux = outAux;
+      if (!singleWavelength) {
+        for (int k = 0; k < 4; k++) c.smp.s0[k] = savedS0[k];
+        c.smp.hashed = savedHashed;
+        c.smp.bounce = 0;
+        wavelengthAux.isBlank = false;
+        wavelengthAux.isShadowCatcher = false;
+      }
+      si.wavelength = 0.0f;
+      si.spectralChannel = 0;
+      if (!singleWavelength || dispersivePrimary) {
+        int channel = singleWavelength ? heroWavelengthIndex : wavelengthIndex;
+        si.spectralChannel = channel + 1;
+        si.wavelength = spectrumCameraWavelength(u32(channel), wavelengthSample);
+        ma.specularIor = cauchyIor(si.wavelength, ma.specularIor, ma.transmissionDispersionScale,
+                                   ma.dispersionAbbeNumber);
+      }
+      path = Path();
+      path.ray = ray;
+      path.beta = v3(1.0f);
+      path.fromEye = true;
+      path.alpha = c.s.u->transmissive_output_alpha_min < 1.0f ? 0.0f : 1.0f;
+      depth = 0;
+      sampleIgnored = false;
+      isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
+    } else if (!path.abort) {
+      completeVertex(c, path, depth, si, ma, sampleIgnored);
+    }
+    if (isNotTransparent && event > bounceLimit) path.abort = true;
+    if (!path.abort && event < eventLimit) shadeVertex(c, uv, path, depth, si, ma, wavelengthAux, sampleIgnored);
+    if (path.abort || event >= eventLimit) {
+      if (singleWavelength) {
+        outAux = wavelengthAux;
+        float scale = dispersivePrimary ? 3.0f : 1.0f;
+        return {path.li.x * scale, path.li.y * scale, path.li.z * scale, path.alpha};
+      }
+      color += path.li;
+      alpha = std::max(alpha, path.alpha);
+      guideAlbedo += wavelengthAux.albedo;
+      guideNormal += wavelengthAux.normal;
+      allBlank = allBlank && wavelengthAux.isBlank;
+      wavelengthIndex++;
+      if (wavelengthIndex >= 3) {
+        outAux.albedo = guideAlbedo / 3.0f;
+        outAux.normal = guideNormal / 3.0f;
+        outAux.isBlank = allBlank;
+        return {color.x, color.y, color.z, alpha};
+      }
+      event = 0;
+    } else {
+      event++;
+    }
+  }
+  return {0, 0, 0, 0};
+}
+
 // rayTrace.compute.ts:1157-1263 main, for one pixel and one sample.
 void tracePixel(const Scene &s, u32 x, u32 y, V4 *outColor, V4 *outNormal, V4 *outAlbedo, V4 *outCatcher,
                 Traffic *tr) {
@@ -1043,7 +1252,7 @@ void tracePixel(const Scene &s, u32 x, u32 y, V4 *outColor, V4 *outNormal, V4 *o
     cam = {origin, normalize(focus - origin)};
   }
   Aux aux;
-  V4 li = integrateRgb(c, coord, cam, aux);
+  V4 li = (s.flags & MTC_SCENE_SPECTRAL) ? integrateSpectral(c, coord, cam, aux) : integrateRgb(c, coord, cam, aux);
   if (tr) tr->paths++;
   if (u.clamping > 0.0f) {
     float cl = u.clamping;
@@ -1071,6 +1280,16 @@ void tracePixel(const Scene &s, u32 x, u32 y, V4 *outColor, V4 *outNormal, V4 *o
 // ----------------------------------------------------------- test exports
 // Environment and BSDF entry points for the known-answer tests.
 extern "C" {
+
+// The 4 x 61 wavelength-sampling CDFs and the spectrumCameraWavelength map.
+int oracle_spectrum_cdf(float *out, unsigned capacity) {
+  const auto &t = oracle::spectrumTables();
+  for (unsigned i = 0; i < 244 && i < capacity; i++) out[i] = t.cdf[i];
+  return 244;
+}
+float oracle_spectrum_camera_wavelength(unsigned channel, float u) {
+  return oracle::spectrumCameraWavelength(channel, u);
+}
 
 // envMapPdf(uv) and sampleEnvmap(rnd) over a scene's environment:
 // out = {envMapPdf(u, v), sampled pdf, envMapPdf(sampled uv), |direction|}

@@ -108,6 +108,25 @@ def test_image_parity_zsobol_two_candidates(cuda):
     assert luma <= LUMA_BAR, luma
 
 
+@pytest.mark.parametrize("wavelengths", [3, 1])
+def test_image_parity_spectral_glass(cuda, wavelengths):
+    """Spectral integrator (rayTrace.compute.ts:947-1057): dispersive glass
+    spheres with homogeneous interiors, three wavelength paths per sample (or
+    one hero wavelength)."""
+    host = scene.SceneHost("glass_spheres", 64, 48, 3, (8,))
+    assert host.flags & abi.MTC_SCENE_SPECTRAL
+    if wavelengths == 1:
+        u = abi.TraceUniform.from_buffer_copy(host.uniform)
+        u.dispersion_wavelengths = 1
+        host.set_uniform(u)
+    gpu, ref, acc, ref_acc = _render_pair(cuda, host, 16)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert np.isfinite(gpu).all()
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma
+    assert np.array_equal(acc.normal[:, 3].cpu().numpy(), ref_acc.normal[:, 3])
+
+
 def test_refit_device_matches_host(cuda):
     import torch
     host = scene.make_workload("instanced_spheres", width=32, height=32, params=(64, 4, 8, 256, 2))
