@@ -238,6 +238,14 @@ mt_status mtc_refit_tlas(void *tlas, uint64_t tlas_vec4_count, void *instances,
                          const int32_t *materials, const float *colors,
                          void *stream);
 
+/* read_average of native/host/src/lib.rs:343-364 on the device: out[i] =
+ * accum[i] / samples for the `pixels` float4 of an accumulation buffer
+ * (outColor, outNormal or outAlbedo), ordered on `stream`.  *nonfinite_flag
+ * (device) is cleared and then set to 1 if any result is not finite, which the
+ * reference treats as a failed read ("Non-finite native output"). */
+mt_status mtc_average_output(const void *accum, uint32_t pixels, uint32_t samples,
+                             void *out, uint32_t *nonfinite_flag, void *stream);
+
 /* ------------------------------------------------------ batched form */
 /* One render job of a batched launch: its own scene view, camera, uniform
  * and outputs.  All jobs of a batch run in one persistent kernel that pulls

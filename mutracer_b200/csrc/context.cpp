@@ -28,22 +28,39 @@ void setError(char *error, size_t capacity, const std::string &msg) {
   error[n] = '\0';
 }
 
+// Device allocation kept across commits: a commit of a scene that fits the
+// previous capacity reuses it instead of freeing and reallocating.
 struct DeviceBuffer {
   void *ptr = nullptr;
-  size_t bytes = 0;
+  size_t bytes = 0, capacity = 0;
   ~DeviceBuffer() { if (ptr) cudaFree(ptr); }
-  cudaError_t upload(const void *host, size_t n) {
-    if (!host || n == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&ptr, n);
-    if (e != cudaSuccess) { ptr = nullptr; return e; }
+  cudaError_t reserve(size_t n) {
     bytes = n;
-    return cudaMemcpy(ptr, host, n, cudaMemcpyHostToDevice);
+    if (n <= capacity) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    capacity = 0;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) { ptr = nullptr; bytes = 0; return e; }
+    capacity = n;
+    return cudaSuccess;
   }
+  // Copies `n` bytes of caller memory, ordered on `stream`; the caller's
+  // memory is no longer needed when the call returns (pageable sources are
+  // staged by the driver before cudaMemcpyAsync returns).
+  cudaError_t upload(const void *host, size_t n, cudaStream_t stream) {
+    if (!host || n == 0) { bytes = 0; return cudaSuccess; }
+    cudaError_t e = reserve(n);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(ptr, host, n, cudaMemcpyHostToDevice, stream);
+  }
+  void *data() const { return bytes ? ptr : nullptr; }
 };
 
 struct SceneResources {
   DeviceBuffer bvh, ins, attr, mats, env, envDist, lightData, lut, lights;
   DeviceBuffer color, normal, albedo, catcher;
+  DeviceBuffer average, flag;  // read_pixels staging: averaged image, non-finite flag
   mtc_scene_view view{};
   uint32_t width = 0, height = 0;
 };
@@ -200,48 +217,54 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   }
   std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
   if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
-  auto r = std::make_unique<SceneResources>();
+  // The previous job expires and nothing may still read the buffers that the
+  // new scene reuses.
+  expireJob(*c);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  std::unique_ptr<SceneResources> r = c->scene ? std::move(c->scene) : std::make_unique<SceneResources>();
   size_t px = size_t(b->width) * b->height;
-  cudaError_t e = cudaSuccess;
-  auto up = [&](DeviceBuffer &d, const void *h, size_t n) { if (e == cudaSuccess) e = d.upload(h, n); };
+  cudaStream_t st = c->stream;
+  auto up = [&](DeviceBuffer &d, const void *h, size_t n) { if (e == cudaSuccess) e = d.upload(h, n, st); };
   up(r->bvh, b->bvh, b->bvh_vec4_count * 16);
   up(r->ins, b->instances, size_t(b->instance_count) * MTC_INSTANCE_VEC4_STRIDE * 16);
   up(r->attr, b->attributes, b->attribute_words * 4);
   up(r->mats, b->materials, size_t(b->material_count) * MTC_MATERIAL_VEC4_ROWS * 16);
-  if (b->env_map) {
-    up(r->env, b->env_map, size_t(b->env_width) * b->env_height * 16);
-    up(r->envDist, b->env_distribution, size_t(b->env_width + 2) * (b->env_height + 1) * 8);
-  }
+  up(r->env, b->env_map, b->env_map ? size_t(b->env_width) * b->env_height * 16 : 0);
+  up(r->envDist, b->env_distribution, b->env_map ? size_t(b->env_width + 2) * (b->env_height + 1) * 8 : 0);
   up(r->lightData, b->light_sampling, size_t(b->light_sampling_texels) * 16);
   up(r->lut, b->energy_lut, size_t(MTC_ENERGY_LUT_WIDTH) * MTC_ENERGY_LUT_HEIGHT * 4);
-  if (b->lights_count) up(r->lights, b->analytic_lights, size_t(b->lights_count) * MTC_LIGHT_VEC4_ROWS * 16);
+  up(r->lights, b->analytic_lights, b->lights_count ? size_t(b->lights_count) * MTC_LIGHT_VEC4_ROWS * 16 : 0);
   for (DeviceBuffer *d : {&r->color, &r->normal, &r->albedo, &r->catcher}) {
     size_t bytes = px * 16 * (d == &r->catcher ? 3 : 1);
-    if (e == cudaSuccess) e = cudaMalloc(&d->ptr, bytes);
-    if (e == cudaSuccess) { d->bytes = bytes; e = cudaMemset(d->ptr, 0, bytes); }
+    if (e == cudaSuccess) e = d->reserve(bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d->ptr, 0, bytes, st);
   }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    setError(error, capacity, std::string("device allocation failed: ") + cudaGetErrorString(e));
-    return e == cudaErrorMemoryAllocation ? MT_ERROR_UNAVAILABLE : MT_ERROR;
+    // Reused buffers may hold part of the new scene: the context is failed
+    // until a later commit succeeds.
+    c->scene = std::move(r);
+    c->failed = true;
+    c->samples = 0;
+    setError(error, capacity, std::string("commit failed: ") + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? MT_ERROR_UNAVAILABLE : MT_ERROR_CONTEXT_FAILED;
   }
   mtc_scene_view &v = r->view;
   v.struct_size = sizeof(mtc_scene_view);
   v.flags = b->flags;
-  v.bvh = r->bvh.ptr; v.bvh_vec4_count = b->bvh_vec4_count;
-  v.instances = r->ins.ptr; v.instance_count = b->instance_count; v.material_count = b->material_count;
-  v.attributes = r->attr.ptr; v.attribute_words = b->attribute_words; v.vertex_layout = b->vertex_layout;
-  v.materials = r->mats.ptr;
-  v.env_map = r->env.ptr; v.env_distribution = r->envDist.ptr; v.env_width = b->env_width; v.env_height = b->env_height;
-  v.light_sampling = r->lightData.ptr; v.light_sampling_texels = b->light_sampling_texels;
+  v.bvh = r->bvh.data(); v.bvh_vec4_count = b->bvh_vec4_count;
+  v.instances = r->ins.data(); v.instance_count = b->instance_count; v.material_count = b->material_count;
+  v.attributes = r->attr.data(); v.attribute_words = b->attribute_words; v.vertex_layout = b->vertex_layout;
+  v.materials = r->mats.data();
+  v.env_map = r->env.data(); v.env_distribution = r->envDist.data(); v.env_width = b->env_width; v.env_height = b->env_height;
+  v.light_sampling = r->lightData.data(); v.light_sampling_texels = b->light_sampling_texels;
   v.blas_offset = b->uniform.blas_offset;
-  v.energy_lut = r->lut.ptr;
-  v.analytic_lights = r->lights.ptr;
+  v.energy_lut = r->lut.data();
+  v.analytic_lights = r->lights.data();
   v.tlas_stack_size = b->tlas_stack_size; v.blas_stack_size = b->blas_stack_size;
   r->width = b->width; r->height = b->height;
-  // Publish: the previous job expires, accumulation restarts.
-  expireJob(*c);
-  cudaStreamSynchronize(c->stream);
+  // Publish: accumulation restarts.
   c->scene = std::move(r);
   c->camera = b->camera;
   c->uniform = b->uniform;
@@ -345,18 +368,29 @@ int32_t mt_context_read_pixels(mt_context handle, uint32_t kind, void *pixels, s
   if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
   if (c->samples == 0) { setError(error, capacity, "no completed samples"); return MT_ERROR_INVALID_STATE; }
   if (!pixels || size < need) { setError(error, capacity, "destination too small"); return MT_ERROR_BUFFER_TOO_SMALL; }
-  std::vector<float> src(px * 4), cnt(px * 4);
-  const void *buf = kind == MT_IMAGE_HDR ? c->scene->color.ptr : kind == MT_IMAGE_NORMAL ? c->scene->normal.ptr : c->scene->albedo.ptr;
-  cudaError_t e = cudaMemcpyAsync(src.data(), buf, need, cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt.data(), c->scene->normal.ptr, need, cudaMemcpyDeviceToHost, c->stream);
+  // read_average (native/host/src/lib.rs:343-364): every value divided by the
+  // completed sample count on the device, then one copy to the caller; a
+  // non-finite value fails the read and marks the context failed.
+  SceneResources &r = *c->scene;
+  const void *buf = kind == MT_IMAGE_HDR ? r.color.ptr : kind == MT_IMAGE_NORMAL ? r.normal.ptr : r.albedo.ptr;
+  cudaError_t e = r.average.reserve(need);
+  if (e == cudaSuccess) e = r.flag.reserve(4);
+  if (e != cudaSuccess) return failContext(*c, e, error, capacity);
+  uint32_t nonFinite = 0;
+  int32_t st = mtc_average_output(buf, uint32_t(px), c->samples, r.average.ptr, static_cast<uint32_t *>(r.flag.ptr),
+                                  c->stream);
+  if (st != MT_OK) { c->failed = true; setError(error, capacity, "average launch failed"); return MT_ERROR_CONTEXT_FAILED; }
+  e = cudaMemcpyAsync(&nonFinite, r.flag.ptr, 4, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return failContext(*c, e, error, capacity);
-  float *o = static_cast<float *>(pixels);
-  for (size_t i = 0; i < px; i++) {
-    float n = cnt[i * 4 + 3];
-    float inv = n > 0.0f ? 1.0f / n : 0.0f;
-    for (int k = 0; k < 4; k++) o[i * 4 + k] = src[i * 4 + k] * inv;
+  if (nonFinite) {
+    c->failed = true;
+    setError(error, capacity, "Non-finite native output");
+    return MT_ERROR_CONTEXT_FAILED;
   }
+  e = cudaMemcpyAsync(pixels, r.average.ptr, need, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return failContext(*c, e, error, capacity);
   return MT_OK;
 }
 

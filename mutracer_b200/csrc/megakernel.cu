@@ -124,6 +124,22 @@ __global__ void k_first_hit(const __grid_constant__ DevScene s, int32_t blasBase
   hits[i] = out;
 }
 
+// read_average (native/host/src/lib.rs:343-364): each f32 of an accumulation
+// buffer divided by the completed sample count; any non-finite result raises
+// the flag.  HBM-bound: 16 B read + 16 B written per pixel.
+__global__ void k_average(const float4 *__restrict__ in, uint32_t pixels, float samples, float4 *__restrict__ out,
+                          uint32_t *nonFinite) {
+  bool bad = false;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pixels; i += gridDim.x * blockDim.x) {
+    float4 a = in[i];
+    float4 r = make_float4(__fdiv_rn(a.x, samples), __fdiv_rn(a.y, samples), __fdiv_rn(a.z, samples),
+                           __fdiv_rn(a.w, samples));
+    bad |= !isfinite(r.x) || !isfinite(r.y) || !isfinite(r.z) || !isfinite(r.w);
+    out[i] = r;
+  }
+  if (__any_sync(__activemask(), bad) && bad) atomicOr(nonFinite, 1u);
+}
+
 // ------------------------------------------------------------------ refit
 // One thread per TLAS leaf entry: world bounds of the instance's BLAS box
 // (computeBounds, scenePreparation.ts:19-47) and its instance record
@@ -348,6 +364,21 @@ mt_status mtc_query_first_hit(const mtc_scene_view *scene, const float *rays, ui
   int32_t blasBase = scene->blas_offset;
   k_first_hit<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(toDev(scene), blasBase, scene->instance_count == 0,
                                                                    (const float4 *)rays, count, hits);
+  return cudaStatus(cudaGetLastError());
+}
+
+mt_status mtc_average_output(const void *accum, uint32_t pixels, uint32_t samples, void *out,
+                             uint32_t *nonfinite_flag, void *stream) {
+  if (!accum || !out || !nonfinite_flag || samples == 0) return MT_ERROR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(nonfinite_flag, 0, sizeof(uint32_t), st);
+  if (e != cudaSuccess) return cudaStatus(e);
+  if (pixels == 0) return MT_OK;
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  uint32_t grid = std::min<uint32_t>((pixels + 255) / 256, uint32_t(sms) * 8u);
+  k_average<<<grid, 256, 0, st>>>((const float4 *)accum, pixels, float(samples), (float4 *)out, nonfinite_flag);
   return cudaStatus(cudaGetLastError());
 }
 

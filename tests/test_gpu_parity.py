@@ -224,5 +224,23 @@ def test_context_api_render_and_jobs(cuda):
                 break
         assert job2.info().state == abi.MT_JOB_CANCELLED
         assert ctx.info().samples == 16
+        # Recommits reuse (or grow) the context's device buffers: a larger
+        # scene, then the first one again, each from zeroed accumulation.
+        import torch
+        for h, spp in ((scene.make_workload("instanced_spheres", width=64, height=48, params=(24, 4, 6, 64, 3)), 3),
+                       (host, 2)):
+            ctx.commit(h)
+            assert ctx.info().samples == 0
+            ctx.render(spp)
+            d = scene.DeviceScene(h, cuda)
+            a = trace.Accumulation(h.width, h.height, cuda)
+            trace.trace_samples(d, a, spp)
+            torch.cuda.synchronize()
+            for kind, buf in ((abi.MT_IMAGE_HDR, a.color), (abi.MT_IMAGE_NORMAL, a.normal),
+                              (abi.MT_IMAGE_ALBEDO, a.albedo)):
+                # IEEE division by the sample count (torch divides by a
+                # scalar through its reciprocal, so compute on the host)
+                want = (buf.cpu().numpy() / np.float32(spp)).reshape(h.height, h.width, 4)
+                assert np.array_equal(ctx.read_pixels(kind), want), kind
     finally:
         ctx.destroy()
