@@ -142,6 +142,21 @@ def oracle_traffic(host, rows=8, spp=2):
     return oracle_lib.algorithmic_bytes(total), total
 
 
+def measured_traffic(args, host, spp):
+    """DRAM bytes (read + write) of one k_trace launch of this exact workload,
+    from the committed ncu summary, or None for another workload."""
+    if args.form != "megakernel" or args.workload != WORKLOAD or (host.width, host.height, spp) != (1920, 1080, 16):
+        return None
+    path = os.path.join(ROOT, "profiles", "k_trace_dram_instanced_spheres_1080p_16spp.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(host, spp, seconds):
     """The CPU oracle on all host cores over a bounded row sample (full spp)."""
     from tests import oracle_lib
@@ -291,10 +306,13 @@ def run_b200(args):
     try:
         bpp, traffic = oracle_traffic(host)
         achieved = bpp * paths_per_step / (ms_per_step / 1000.0) / 1e9
+        dram = measured_traffic(args, host, spp)
         result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                              "frac": round(achieved / peak, 4), "traffic": None,
+                              "frac": round(achieved / peak, 4), "traffic": dram,
                               "peak_source": peak_kind,
-                              "bytes_per_path": round(bpp, 1)}
+                              "bytes_per_path": round(bpp, 1),
+                              "traffic_source": "profiles/k_trace_dram_instanced_spheres_1080p_16spp.md"
+                              if dram is not None else None}
     except Exception as exc:  # the oracle library may be absent on a box
         result["roofline"] = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                               "traffic": None, "error": str(exc)[:200]}
@@ -305,6 +323,8 @@ def run_b200(args):
     if not args.no_e2e:
         result["e2e"] = e2e_context(host, spp, max(1, min(args.steps, 3)))
     if not args.no_batch:
+        if args.form == "megakernel":
+            result["wavefront_same_job"] = same_job_wavefront(dev, acc, spp, paths_per_step, dev_id, flush)
         del dev, acc, flush
         torch.cuda.empty_cache()
         result["batched"] = mixed_batch(args, dev_id)
@@ -349,6 +369,32 @@ def _timed(fn, stream):
     e.record(stream)
     e.synchronize()
     return s.elapsed_time(e)
+
+
+def same_job_wavefront(dev, acc, spp, paths, dev_id, flush):
+    """The headline job through mtc_stream_run (default knobs), timed like the
+    plain steps (L2 flushed, CUDA events), and checked bit-identical to the
+    plain megakernel's image of the last timed step."""
+    import torch
+    from mutracer_b200 import abi, batch
+    plain = acc.color.clone()
+    job = batch.RenderJob(dev, spp, device=dev_id)
+    sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(), device=dev_id)
+    sb.set_jobs([job])
+    stream = torch.cuda.current_stream()
+    times = []
+    for it in range(4):                   # one warm-up, three timed
+        job.acc.zero_()
+        flush_l2(flush)
+        ms = _timed(sb.run, stream)
+        if it:
+            times.append(ms)
+    ms = sum(times) / len(times)
+    out = {"ms_per_step": round(ms, 2), "mpaths_per_s": round(paths / ms / 1e3, 3),
+           "bit_identical_to_plain": bool(torch.equal(job.acc.color, plain)),
+           "config": "1M slots, refill at 8 idle lanes, regroup every iteration"}
+    del sb, job
+    return out
 
 
 def mixed_batch(args, dev_id):
