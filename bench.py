@@ -450,7 +450,7 @@ def mixed_batch(args, dev_id):
                     f"1-8 rect lights + 512x256 sky, depth 6, seed 0",
         "paths": int(paths), "scene_build_s": round(build_s, 1), "autotune_s": round(tune_s, 1),
         "wavefront_config": {"slots": scfg.slots, "refill_lanes": scfg.refill_lanes,
-                             "regroup_interval": scfg.regroup_interval},
+                             "regroup_interval": scfg.regroup_interval, "sort_rays": scfg.sort_rays},
         "autotune_probe_ms": {k: round(v, 2) for k, v in timings.items()},
         "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["wavefront"]["ms"], 3),
         "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["wavefront"]["ms"], 3),

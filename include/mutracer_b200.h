@@ -328,7 +328,9 @@ typedef struct mtc_stream_config {
   uint32_t regroup_interval;      /* order the shading queue by material class every
                                      N-th event iteration, 1..1024 (default 1);
                                      MTC_REGROUP_OFF never */
-  uint32_t _pad[2];
+  uint32_t sort_rays;             /* 1: order each extension queue by (job, direction
+                                     octant) before traversal (default 0) */
+  uint32_t _pad[1];
 } mtc_stream_config;
 #define MTC_REGROUP_OFF 0xffffffffu
 size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config);

@@ -260,14 +260,16 @@ def autotune(jobs, probe_samples=1, space=AUTOTUNE_SPACE, repeats=2, device="cud
 
 # Wavefront knobs the autotuner walks one at a time (coordinate descent from
 # the defaults): paths in flight ("queue depth"), idle lanes that trigger a
-# ray refill in the traversal kernels, and how often the shading queue is
-# regrouped by material class (abi.MTC_REGROUP_OFF: never).
+# ray refill in the traversal kernels, how often the shading queue is
+# regrouped by material class (abi.MTC_REGROUP_OFF: never), and whether the
+# extension queue is ordered by (job, direction octant) before traversal.
 STREAM_SPACE = {
     "refill_lanes": (4, 8, 16),
     "regroup_interval": (1, 2, abi.MTC_REGROUP_OFF),
+    "sort_rays": (0, 1),
     "slots": (1 << 19, 1 << 20, 1 << 21),
 }
-STREAM_DEFAULT = {"slots": 1 << 20, "refill_lanes": 8, "regroup_interval": 1}
+STREAM_DEFAULT = {"slots": 1 << 20, "refill_lanes": 8, "regroup_interval": 1, "sort_rays": 0}
 
 
 def autotune_stream(jobs, probe_samples=1, space=STREAM_SPACE, device="cuda", batch_config=None):

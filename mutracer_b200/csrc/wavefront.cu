@@ -70,6 +70,9 @@ struct StreamView {
   uint32_t *shadowQueue, *finishQueue;
   uint32_t *keys, *sortedQueue;   // material-class key per slot; extension queue ordered by key
   uint32_t *classCount, *classCursor;  // kClasses each
+  uint32_t *rayKeys, *sortedRays;  // (job, direction octant) key per slot; extension queue ordered by it
+  uint32_t *rayKeyCount[2], *rayKeyCursor;  // kRayKeys each, counts per queue parity
+  uint32_t sortRays;
   uint32_t slotCount;
   uint32_t refillLanes;  // idle lanes of a warp that trigger a ray refill
   mtc_counters *counters;
@@ -137,6 +140,29 @@ __device__ __forceinline__ uint32_t materialClass(const JobData &J, const Traver
   return 1u + k;
 }
 
+// Keys for ordering the extension queue: the job (mod 64) and the octant of
+// the ray direction, so that a warp traverses rays of one scene heading the
+// same way.
+constexpr uint32_t kRayKeys = 512;
+
+__device__ __forceinline__ uint32_t rayKey(uint32_t job, V3 d) {
+  uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  return (job & 63u) * 8u + oct;
+}
+
+// Appends slot `s` to the extension queue of parity `q` and, when the queue
+// is ordered before traversal, counts it under its ray key.
+__device__ __forceinline__ void enqueueRay(const StreamView &v, uint32_t q, uint32_t s) {
+  enqueue(v.rayQueue[q], &v.q->rayCount[q], s);
+  if (v.sortRays) {
+    const Slot &sl = v.slots[s];
+    uint32_t key = rayKey(sl.job, sl.ps.path.ray.d);
+    v.rayKeys[s] = key;
+    unsigned m = __match_any_sync(__activemask(), key);
+    if (int(laneId()) == __ffs(m) - 1) atomicAdd(&v.rayKeyCount[q][key], uint32_t(__popc(m)));
+  }
+}
+
 // Counts a finished extension ray in its material class (one atomic per
 // class present in the converged group of lanes).
 __device__ __forceinline__ void countClass(const StreamView &v, uint32_t s, uint32_t key) {
@@ -186,7 +212,7 @@ __device__ bool claimPixel(const StreamView &v, uint32_t s) {
 
 __global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v) {
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.slotCount; s += gridDim.x * blockDim.x) {
-    if (claimPixel(v, s)) enqueue(v.rayQueue[0], &v.q->rayCount[0], s);
+    if (claimPixel(v, s)) enqueueRay(v, 0u, s);
   }
   flush(v, 0, 0, 0);
 }
@@ -205,7 +231,14 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
     v.q->finishCount = 0;
   }
   const uint32_t n = v.q->rayCount[cur];
-  const uint32_t *queue = v.rayQueue[cur];
+  const uint32_t *queue = v.sortRays ? v.sortedRays : v.rayQueue[cur];
+  if (v.sortRays && blockIdx.x == 0) {
+    // The ray-key counts of this queue were consumed by k_wf_sort_rays.
+    for (uint32_t k = threadIdx.x; k < kRayKeys; k += blockDim.x) {
+      v.rayKeyCount[cur][k] = 0;
+      v.rayKeyCursor[k] = 0;
+    }
+  }
   RayTraversal<false> rt;
   uint32_t s = 0, ext = 0;
   bool busy = false, exhausted = false;
@@ -219,8 +252,9 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
       uint32_t t = takeUnit(&v.q->extendNext);
       if (t >= n) {
         exhausted = true;
+      } else if ((s = queue[t]) >= v.slotCount) {
+        // Not reachable with consistent queue counts; never index past the slots.
       } else {
-        s = queue[t];
         const Slot &sl = v.slots[s];
         const JobData &J = v.jobs[sl.job];
         // traceExtension: an empty scene is a miss without a traversal, and a
@@ -253,6 +287,32 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
     }
   }
   flush(v, ext, 0, 0);
+}
+
+// Orders the extension queue by ray key (counting sort, keys counted when
+// the rays were queued).  Slot order never changes a result.
+__global__ void __launch_bounds__(kStreamThreads) k_wf_sort_rays(StreamView v, uint32_t cur) {
+  __shared__ uint32_t offset[kRayKeys];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < kRayKeys; k++) {
+      offset[k] = acc;
+      acc += v.rayKeyCount[cur][k];
+    }
+  }
+  __syncthreads();
+  const uint32_t n = v.q->rayCount[cur];
+  const uint32_t *queue = v.rayQueue[cur];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    uint32_t s = queue[t];
+    uint32_t key = v.rayKeys[s];
+    unsigned m = __match_any_sync(__activemask(), key);
+    int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (int(laneId()) == leader) base = atomicAdd(&v.rayKeyCursor[key], uint32_t(__popc(m)));
+    base = __shfl_sync(m, base, leader);
+    v.sortedRays[offset[key] + base + __popc(m & ((1u << laneId()) - 1u))] = s;
+  }
 }
 
 // Orders the extension queue by material class (counting sort on the keys
@@ -313,7 +373,7 @@ __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
     sl.shadow = c.shadow;
     if (c.shadow.valid) enqueue(v.shadowQueue, &v.q->shadowCount, s);
     if (ended) enqueue(v.finishQueue, &v.q->finishCount, s);
-    else enqueue(v.rayQueue[cur ^ 1u], &v.q->rayCount[cur ^ 1u], s);
+    else enqueueRay(v, cur ^ 1u, s);
   }
   flush(v, 0, 0, 0);
 }
@@ -382,7 +442,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
     if (isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) {
       // The next wavelength path of this sample starts at event 0.
       sl.ps = ps;
-      enqueue(v.rayQueue[cur ^ 1u], &v.q->rayCount[cur ^ 1u], s);
+      enqueueRay(v, cur ^ 1u, s);
       continue;
     }
     endSample(J, sl.x + sl.y * J.width, ps);
@@ -398,7 +458,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
     } else {
       again = claimPixel(v, s);
     }
-    if (again) enqueue(v.rayQueue[cur ^ 1u], &v.q->rayCount[cur ^ 1u], s);
+    if (again) enqueueRay(v, cur ^ 1u, s);
   }
   flush(v, 0, 0, paths);
 }
@@ -406,7 +466,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
 size_t roundUp(size_t x) { return (x + 255) / 256 * 256; }
 
 struct StreamLayout {
-  size_t table, queues, slots, spectral, hits, rayQueues, shadowQueue, finishQueue, keys, sortedQueue, classes, total;
+  size_t table, queues, slots, spectral, hits, rayQueues, shadowQueue, finishQueue, keys, sortedQueue, classes, rayKeys, sortedRays, rayKeyCounts, total;
 };
 
 StreamLayout layout(uint32_t capacity, uint32_t slots) {
@@ -434,16 +494,22 @@ StreamLayout layout(uint32_t capacity, uint32_t slots) {
   off += roundUp(size_t(slots) * 4);
   L.classes = off;
   off += roundUp(2 * kClasses * 4);
+  L.rayKeys = off;
+  off += roundUp(size_t(slots) * 4);
+  L.sortedRays = off;
+  off += roundUp(size_t(slots) * 4);
+  L.rayKeyCounts = off;
+  off += roundUp(3 * kRayKeys * 4);
   L.total = off;
   return L;
 }
 
 struct StreamShape {
-  uint32_t slots, iterationsPerCheck, maxIterations, refillLanes, regroupInterval;
+  uint32_t slots, iterationsPerCheck, maxIterations, refillLanes, regroupInterval, sortRays;
 };
 
 bool streamShape(const mtc_stream_config *c, StreamShape &out) {
-  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u};
+  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u, 0u};
   if (!c) return true;
   if (c->struct_size != sizeof(mtc_stream_config)) return false;
   if (c->slots) {
@@ -461,6 +527,8 @@ bool streamShape(const mtc_stream_config *c, StreamShape &out) {
     if (c->regroup_interval > 1024u) return false;
     out.regroupInterval = c->regroup_interval;
   }
+  if (c->sort_rays > 1u) return false;
+  out.sortRays = c->sort_rays;
   if (c->refill_lanes) {
     if (c->refill_lanes > 32u) return false;
     out.refillLanes = c->refill_lanes;
@@ -545,6 +613,12 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
   v.sortedQueue = reinterpret_cast<uint32_t *>(base + L.sortedQueue);
   v.classCount = reinterpret_cast<uint32_t *>(base + L.classes);
   v.classCursor = v.classCount + kClasses;
+  v.rayKeys = reinterpret_cast<uint32_t *>(base + L.rayKeys);
+  v.sortedRays = reinterpret_cast<uint32_t *>(base + L.sortedRays);
+  v.rayKeyCount[0] = reinterpret_cast<uint32_t *>(base + L.rayKeyCounts);
+  v.rayKeyCount[1] = v.rayKeyCount[0] + kRayKeys;
+  v.rayKeyCursor = v.rayKeyCount[1] + kRayKeys;
+  v.sortRays = shape.sortRays;
   v.slotCount = shape.slots;
   v.refillLanes = shape.refillLanes;
   v.counters = counters;
@@ -553,16 +627,18 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
                                   cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(v.q, 0, sizeof(StreamQueues), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(v.classCount, 0, 2 * kClasses * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(v.rayKeyCount[0], 0, 3 * kRayKeys * 4, st);
   if (e != cudaSuccess) return toStatus(e);
   if (hdr.totalItems == 0 || hdr.jobCount == 0) return MT_OK;
 
-  uint32_t gSeed, gExtend, gShade, gShadow, gFinish, gRegroup;
+  uint32_t gSeed, gExtend, gShade, gShadow, gFinish, gRegroup, gSort;
   if ((e = gridFor((const void *)k_wf_seed, gSeed)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_extend, gExtend)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_shade, gShade)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_shadow, gShadow)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_finish, gFinish)) != cudaSuccess ||
-      (e = gridFor((const void *)k_wf_regroup, gRegroup)) != cudaSuccess)
+      (e = gridFor((const void *)k_wf_regroup, gRegroup)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_sort_rays, gSort)) != cudaSuccess)
     return toStatus(e);
   uint32_t *pinned = nullptr;
   if ((e = pinnedWords(&pinned)) != cudaSuccess) return toStatus(e);
@@ -583,6 +659,7 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
   while (e == cudaSuccess) {
     for (uint32_t k = 0; k < shape.iterationsPerCheck && e == cudaSuccess; k++) {
       const uint32_t regroup = shape.regroupInterval && (iterations % shape.regroupInterval) == 0u ? 1u : 0u;
+      if (v.sortRays) k_wf_sort_rays<<<gSort, kStreamThreads, 0, st>>>(v, cur);
       k_wf_extend<<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
       if (regroup) k_wf_regroup<<<gRegroup, kStreamThreads, 0, st>>>(v, cur);
       k_wf_shade<<<gShade, kStreamThreads, 0, st>>>(v, cur, regroup);

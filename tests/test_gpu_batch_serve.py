@@ -119,9 +119,9 @@ def test_served_admission_respects_the_hbm_budget(cuda):
         serve.Server(pool, hbm_budget_bytes=one - 1, device=cuda).run([serve.Request(0, 0, 64, 64, 1, 0.0)])
 
 
-@pytest.mark.parametrize("slots,refill,regroup", [(1024, 1, 1), (1 << 16, 8, 1), (4096, 32, 3),
-                                                  (1 << 14, 16, abi.MTC_REGROUP_OFF)])
-def test_wavefront_matches_alone(cuda, slots, refill, regroup):
+@pytest.mark.parametrize("slots,refill,regroup,sort", [(1024, 1, 1, 0), (1 << 16, 8, 1, 1), (4096, 32, 3, 1),
+                                                       (1 << 14, 16, abi.MTC_REGROUP_OFF, 0)])
+def test_wavefront_matches_alone(cuda, slots, refill, regroup, sort):
     import torch
     jobs = _small_jobs(cuda)
     extra = batch.build_mixed([batch.JobSpec(9, 96, 80, 6, 40_000, 3, 21)], cuda, env_width=64)
@@ -129,7 +129,7 @@ def test_wavefront_matches_alone(cuda, slots, refill, regroup):
     alone = _small_jobs(cuda) + batch.build_mixed([batch.JobSpec(9, 96, 80, 6, 40_000, 3, 21)], cuda, env_width=64)
     sb = batch.StreamBatch(len(jobs), abi.BatchConfig.make(tile_width=8),
                            abi.StreamConfig.make(slots=slots, iterations_per_check=3, refill_lanes=refill,
-                                                 regroup_interval=regroup), device=cuda)
+                                                 regroup_interval=regroup, sort_rays=sort), device=cuda)
     sb.set_jobs(jobs)
     sb.run()
     torch.cuda.synchronize()
