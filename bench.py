@@ -392,7 +392,8 @@ def same_job_wavefront(dev, acc, spp, paths, dev_id, flush):
     ms = sum(times) / len(times)
     out = {"ms_per_step": round(ms, 2), "mpaths_per_s": round(paths / ms / 1e3, 3),
            "bit_identical_to_plain": bool(torch.equal(job.acc.color, plain)),
-           "config": "1M slots, refill at 8 idle lanes, regroup every iteration"}
+           "config": "defaults: 1M slots, refill at 8 idle lanes, 8 steps per refill check, regroup every "
+                     "iteration"}
     del sb, job
     return out
 
@@ -450,7 +451,8 @@ def mixed_batch(args, dev_id):
                     f"1-8 rect lights + 512x256 sky, depth 6, seed 0",
         "paths": int(paths), "scene_build_s": round(build_s, 1), "autotune_s": round(tune_s, 1),
         "wavefront_config": {"slots": scfg.slots, "refill_lanes": scfg.refill_lanes,
-                             "regroup_interval": scfg.regroup_interval, "sort_rays": scfg.sort_rays},
+                             "regroup_interval": scfg.regroup_interval, "sort_rays": scfg.sort_rays,
+                             "steps_per_check": scfg.steps_per_check},
         "autotune_probe_ms": {k: round(v, 2) for k, v in timings.items()},
         "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["wavefront"]["ms"], 3),
         "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["wavefront"]["ms"], 3),

@@ -330,7 +330,8 @@ typedef struct mtc_stream_config {
                                      MTC_REGROUP_OFF never */
   uint32_t sort_rays;             /* 1: order each extension queue by (job, direction
                                      octant) before traversal (default 0) */
-  uint32_t _pad[1];
+  uint32_t steps_per_check;       /* traversal steps between refill checks, 1..64
+                                     (default 8) */
 } mtc_stream_config;
 #define MTC_REGROUP_OFF 0xffffffffu
 size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config);

@@ -261,15 +261,17 @@ def autotune(jobs, probe_samples=1, space=AUTOTUNE_SPACE, repeats=2, device="cud
 # Wavefront knobs the autotuner walks one at a time (coordinate descent from
 # the defaults): paths in flight ("queue depth"), idle lanes that trigger a
 # ray refill in the traversal kernels, how often the shading queue is
-# regrouped by material class (abi.MTC_REGROUP_OFF: never), and whether the
-# extension queue is ordered by (job, direction octant) before traversal.
+# regrouped by material class (abi.MTC_REGROUP_OFF: never), whether the
+# extension queue is ordered by (job, direction octant) before traversal, and
+# how many traversal steps a lane takes between refill checks.
 STREAM_SPACE = {
     "refill_lanes": (4, 8, 16),
     "regroup_interval": (1, 2, abi.MTC_REGROUP_OFF),
     "sort_rays": (0, 1),
+    "steps_per_check": (4, 8, 16),
     "slots": (1 << 19, 1 << 20, 1 << 21),
 }
-STREAM_DEFAULT = {"slots": 1 << 20, "refill_lanes": 8, "regroup_interval": 1, "sort_rays": 0}
+STREAM_DEFAULT = {"slots": 1 << 20, "refill_lanes": 8, "regroup_interval": 1, "sort_rays": 0, "steps_per_check": 8}
 
 
 def autotune_stream(jobs, probe_samples=1, space=STREAM_SPACE, device="cuda", batch_config=None):

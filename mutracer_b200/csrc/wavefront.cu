@@ -75,6 +75,7 @@ struct StreamView {
   uint32_t sortRays;
   uint32_t slotCount;
   uint32_t refillLanes;  // idle lanes of a warp that trigger a ray refill
+  uint32_t stepsPerCheck;  // traversal steps between refill checks
   mtc_counters *counters;
 };
 
@@ -280,7 +281,10 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
       }
       continue;
     }
-    if (busy && rt.step()) {
+    // Several steps between refill checks: the votes cost as much as a node.
+    bool finished = false;
+    for (uint32_t k = 0; k < v.stepsPerCheck && busy && !finished; k++) finished = rt.step();
+    if (finished) {
       v.hits[s] = rt.h;
       busy = false;
       if (regroup) countClass(v, s, materialClass(v.jobs[v.slots[s].job], rt.h));
@@ -413,9 +417,13 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS) k_wf_s
         }
       }
     }
-    if (!refill && busy && rt.step()) {
-      busy = false;
-      done = true;
+    if (!refill && busy) {
+      bool finished = false;
+      for (uint32_t k = 0; k < v.stepsPerCheck && !finished; k++) finished = rt.step();
+      if (finished) {
+        busy = false;
+        done = true;
+      }
     }
     if (done) {
       Slot &sl = v.slots[s];
@@ -505,11 +513,11 @@ StreamLayout layout(uint32_t capacity, uint32_t slots) {
 }
 
 struct StreamShape {
-  uint32_t slots, iterationsPerCheck, maxIterations, refillLanes, regroupInterval, sortRays;
+  uint32_t slots, iterationsPerCheck, maxIterations, refillLanes, regroupInterval, sortRays, stepsPerCheck;
 };
 
 bool streamShape(const mtc_stream_config *c, StreamShape &out) {
-  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u, 0u};
+  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u, 0u, 8u};
   if (!c) return true;
   if (c->struct_size != sizeof(mtc_stream_config)) return false;
   if (c->slots) {
@@ -529,6 +537,10 @@ bool streamShape(const mtc_stream_config *c, StreamShape &out) {
   }
   if (c->sort_rays > 1u) return false;
   out.sortRays = c->sort_rays;
+  if (c->steps_per_check) {
+    if (c->steps_per_check > 64u) return false;
+    out.stepsPerCheck = c->steps_per_check;
+  }
   if (c->refill_lanes) {
     if (c->refill_lanes > 32u) return false;
     out.refillLanes = c->refill_lanes;
@@ -621,6 +633,7 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
   v.sortRays = shape.sortRays;
   v.slotCount = shape.slots;
   v.refillLanes = shape.refillLanes;
+  v.stepsPerCheck = shape.stepsPerCheck;
   v.counters = counters;
 
   cudaError_t e = cudaMemcpyAsync(base + L.table, table, sizeof(TableHeader) + size_t(capacity) * sizeof(JobData),
