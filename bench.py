@@ -467,10 +467,7 @@ def served_stream(args, dev_id):
     continuous batching; p50/p99 time-to-target-spp and sustained Mpaths/s."""
     import torch
     from mutracer_b200 import batch, scene, serve
-    pool = serve.ScenePool(dev_id)
-    specs = batch.mixed_jobs(args.serve_scenes, seed=7, tri_range=(10_000, 8_000_000))
-    for sp in specs:
-        pool.add(sp.job_id, scene.SceneHost("instanced_spheres", 256, 256, sp.seed, sp.scene_params()))
+    pool = serve.build_pool(args.serve_scenes, seed=7, device=dev_id)
     reqs = serve.poisson_requests(pool, args.serve_requests, args.serve_rate, seed=11,
                                   spp_divisor=args.serve_spp_divisor)
     budget = 12 * 1024 ** 3

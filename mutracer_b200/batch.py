@@ -35,13 +35,14 @@ class JobSpec:
     lights: int      # rect lights
     seed: int
 
-    def scene_params(self, env_width=512):
+    def scene_params(self, env_width=512, max_base_meshes=16):
         """instanced_spheres parameters (instances, base meshes, icosphere
         frequency, sky width, rect lights) giving about `triangles` instanced
-        triangles: 20 * frequency^2 triangles per sphere."""
+        triangles: 20 * frequency^2 triangles per sphere, at most
+        `max_base_meshes` distinct (BLAS) meshes."""
         instances = int(min(512, max(4, round(self.triangles / 2000))))
         freq = int(min(28, max(2, round(math.sqrt(self.triangles / (20.0 * instances))))))
-        return (instances, min(16, instances), freq, env_width, self.lights)
+        return (instances, min(max_base_meshes, instances), freq, env_width, self.lights)
 
 
 def mixed_jobs(count=64, seed=0, spp_range=(4, 256), tri_range=(10_000, 2_000_000), light_range=(1, 8),

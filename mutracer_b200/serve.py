@@ -71,6 +71,17 @@ class ScenePool:
         return sum(s.device_bytes for s in self.scenes.values())
 
 
+def build_pool(count, seed=7, device="cuda", tri_range=(10_000, 8_000_000), max_base_meshes=16,
+               env_width=512):
+    """`count` seeded instanced-sphere scenes (triangles log-uniform in
+    tri_range, 1-8 rect lights), resident on the device."""
+    pool = ScenePool(device)
+    for sp in batch.mixed_jobs(count, seed=seed, tri_range=tri_range):
+        host = scene.SceneHost("instanced_spheres", 256, 256, sp.seed, sp.scene_params(env_width, max_base_meshes))
+        pool.add(sp.job_id, host)
+    return pool
+
+
 def orbit_camera(host, width, height, rng, fov_range=(30.0, 70.0)):
     """Camera at a random point of the scene's bounding sphere looking at its
     centre, vertical FOV uniform in fov_range."""
@@ -226,3 +237,39 @@ class Server:
     def release(self):
         for b in self.batches:
             b.release()
+
+
+def main(argv=None):
+    """Rate sweep of the served form: one JSON line per arrival rate."""
+    import argparse
+    import json
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--scenes", type=int, default=32)
+    p.add_argument("--base-meshes", type=int, default=64, help="distinct meshes per scene at most")
+    p.add_argument("--requests", type=int, default=64)
+    p.add_argument("--rates", default="5,10,20,50,100,200")
+    p.add_argument("--spp-divisor", type=int, default=16)
+    p.add_argument("--quantum", type=int, default=4)
+    p.add_argument("--budget-gb", type=float, default=24.0)
+    p.add_argument("--max-jobs", type=int, default=64)
+    a = p.parse_args(argv)
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t0 = time.perf_counter()
+    pool = build_pool(a.scenes, device=dev, max_base_meshes=a.base_meshes)
+    build_s = time.perf_counter() - t0
+    srv = Server(pool, hbm_budget_bytes=int(a.budget_gb * 1024 ** 3), max_jobs=a.max_jobs, quantum=a.quantum,
+                 device=dev)
+    srv.run(poisson_requests(pool, 4, 1000.0, seed=3, spp_divisor=a.spp_divisor))
+    for rate in (float(r) for r in a.rates.split(",")):
+        reqs = poisson_requests(pool, a.requests, rate, seed=11, spp_divisor=a.spp_divisor)
+        stats = srv.run(reqs)
+        stats.update(rate_per_s=rate, scenes=len(pool), pool_gb=round(pool.device_bytes / 1e9, 3),
+                     pool_build_s=round(build_s, 1), spp_divisor=a.spp_divisor, quantum=a.quantum,
+                     budget_gb=a.budget_gb, offered_s=round(reqs[-1].arrival, 3))
+        print(json.dumps({k: (round(v, 4) if isinstance(v, float) else v) for k, v in stats.items()}), flush=True)
+    srv.release()
+
+
+if __name__ == "__main__":
+    main()

@@ -116,3 +116,30 @@ def test_poisson_requests_rate_and_ranges():
     assert {(r.width, r.height) for r in reqs} <= set(batch.RESOLUTIONS)
     again = serve.poisson_requests(pool, 400, rate=50.0, seed=2)
     assert [bytes(r.camera) for r in again] == [bytes(r.camera) for r in reqs]
+
+
+def test_plain_entry_points_validate_before_touching_the_device():
+    """Argument checks of the C ABI run on the host: rejected calls and
+    zero-sample calls return without a CUDA call (this runs without a GPU)."""
+    L = abi.lib()
+    host = scene.SceneHost("cornell", 16, 16, 1)
+    view, cam, uni = host.host_view(), host.camera, host.uniform
+    out = abi.Outputs(0x1000, 0x2000, 0x3000, 0x4000)
+    assert L.mtc_trace_samples(C.byref(view), C.byref(cam), C.byref(uni), C.byref(out), 0, None, None) == abi.MT_OK
+    assert L.mtc_trace_samples(None, C.byref(cam), C.byref(uni), C.byref(out), 1, None, None) == \
+        abi.MT_ERROR_INVALID_ARGUMENT
+    bad = abi.Outputs(0x1000, 0, 0x3000, 0x4000)
+    assert L.mtc_trace_samples(C.byref(view), C.byref(cam), C.byref(uni), C.byref(bad), 1, None, None) == \
+        abi.MT_ERROR_INVALID_ARGUMENT
+    v2 = abi.SceneView.from_buffer_copy(view)
+    v2.struct_size = 4
+    assert L.mtc_trace_samples(C.byref(v2), C.byref(cam), C.byref(uni), C.byref(out), 1, None, None) == \
+        abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_query_first_hit(None, None, 0, None, None) == abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_average_output(None, 4, 1, None, None, None) == abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_average_output(C.c_void_p(16), 4, 0, C.c_void_p(16), C.c_void_p(16), None) == \
+        abi.MT_ERROR_INVALID_ARGUMENT
+    cfg = abi.StreamConfig.make(slots=100)                # below the 1024-slot minimum
+    assert L.mtc_stream_state_bytes(4, C.byref(cfg)) == 0
+    assert L.mtc_stream_run(None, 4, None, C.c_void_p(16), None, None) == abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_stream_state_bytes(4, None) > (1 << 20) * 400

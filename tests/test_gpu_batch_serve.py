@@ -165,3 +165,60 @@ def test_wavefront_cornell_and_glass_scenes(cuda):
         sb.run()
         torch.cuda.synchronize()
         assert _equal(a.acc, b.acc), kind
+
+
+def test_edge_jobs_zero_samples_tiny_and_ragged_images(cuda):
+    """Jobs with no samples, a 1x1 image and ragged image edges, through both
+    batched engines, against the jobs alone."""
+    import torch
+    specs = [batch.JobSpec(0, 1, 1, 3, 10_000, 1, 31), batch.JobSpec(1, 7, 3, 0, 10_000, 2, 32),
+             batch.JobSpec(2, 33, 17, 2, 20_000, 3, 33), batch.JobSpec(3, 5, 29, 1, 10_000, 1, 34)]
+
+    def fresh():
+        return batch.build_mixed(specs, cuda, env_width=64)
+
+    alone = fresh()
+    for j in alone:
+        if j.spp:
+            j.render_alone()
+    for engine in ("persistent", "wavefront"):
+        jobs = fresh()
+        if engine == "persistent":
+            b = batch.Batch(len(jobs), abi.BatchConfig.make(tile_width=32), cuda)
+            b.set_jobs(jobs)
+            b.launch()
+        else:
+            b = batch.StreamBatch(len(jobs), stream_config=abi.StreamConfig.make(slots=1024), device=cuda)
+            b.set_jobs(jobs)
+            b.run()
+        torch.cuda.synchronize()
+        for a, j in zip(alone, jobs):
+            assert _equal(a.acc, j.acc), (engine, j.job_id)
+        assert float(jobs[1].acc.normal[:, 3].sum()) == 0.0          # zero-sample job untouched
+        assert int(b.counters[0].item()) == sum(j.pixels * j.spp for j in jobs)
+
+
+def test_empty_batches_and_empty_scene(cuda):
+    import torch
+    sb = batch.StreamBatch(4, device=cuda)
+    sb.set_jobs([])
+    sb.run()                                             # nothing to do
+    b = batch.Batch(4, None, cuda)
+    b.set_jobs([])
+    b.launch()
+    torch.cuda.synchronize()
+    assert int(sb.counters[0].item()) == 0 and int(b.counters[0].item()) == 0
+    # A scene flagged empty (RayTraceUniform.isEmpty) only sees the background.
+    host = scene.SceneHost("instanced_spheres", 24, 16, 2, (8, 2, 4, 64, 1))
+    u = abi.TraceUniform.from_buffer_copy(host.uniform)
+    u.is_empty = 1
+    host.set_uniform(u)
+    dev = scene.DeviceScene(host, cuda)
+    a, w = batch.RenderJob(dev, 3, device=cuda), batch.RenderJob(dev, 3, device=cuda)
+    a.render_alone()
+    sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=1024), device=cuda)
+    sb.set_jobs([w])
+    sb.run()
+    torch.cuda.synchronize()
+    assert _equal(a.acc, w.acc)
+    assert int(sb.counters[1].item()) == 0               # no extension ray traced
