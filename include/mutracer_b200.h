@@ -168,9 +168,14 @@ typedef struct mtc_scene_view {
 } mtc_scene_view;
 /* flags: shader specialisation constants that are not in the uniform
  * (HAS_MEDIUM, SPECTRAL and SAMPLING_PATTERN of wgpuMaterialConstants.ts:40-70).
- * The sampling pattern (MT_SAMPLING_*) occupies bits 4..5. */
+ * The sampling pattern (MT_SAMPLING_*) occupies bits 4..5.  BLAS_GPU_LAYOUT is
+ * bit 2 (layout code 2) of the reference's blasLayoutMask: set it when any
+ * instance record carries BLAS layout code 2 (BVH_GPU); without it such
+ * instances are not traversed, as in a shader compiled without that layout.
+ * BVH2 (layout code 0) is always traversed. */
 enum { MTC_SCENE_HAS_MEDIUM = 1u, MTC_SCENE_SPECTRAL = 2u,
-       MTC_SCENE_PATTERN_SHIFT = 4u, MTC_SCENE_PATTERN_MASK = 0x30u };
+       MTC_SCENE_PATTERN_SHIFT = 4u, MTC_SCENE_PATTERN_MASK = 0x30u,
+       MTC_SCENE_BLAS_GPU_LAYOUT = 0x100u };
 
 /* G3 accumulation outputs (rayTrace.compute.ts:294-299; never overwritten,
  * always accumulated).  shadow_catcher holds 3 vec4 per pixel

@@ -29,6 +29,7 @@ MTC_SCENE_HAS_MEDIUM = 1
 MTC_SCENE_SPECTRAL = 2
 MTC_SCENE_PATTERN_SHIFT = 4
 MTC_SCENE_PATTERN_MASK = 0x30
+MTC_SCENE_BLAS_GPU_LAYOUT = 0x100
 MTC_FEATURE_USE_ENVMAP = 1
 MTC_INSTANCE_VEC4_STRIDE = 10
 MTC_MATERIAL_VEC4_ROWS = 26
@@ -215,6 +216,7 @@ def _declare(lib):
         "mtp_scene_refit_inputs": (C.c_int, [P, P, P, P, P, P, P, P]),
         "mtp_scene_set_transforms": (C.c_int, [P, P, C.c_uint32]),
         "mtp_scene_refit_host": (C.c_int, [P]),
+        "mtp_scene_set_blas_layout": (C.c_int, [P, C.c_uint32]),
         "mtp_build_binned_sah": (C.c_int, [P, C.c_uint32, C.c_int, P, P, P, P, P]),
         "mtp_build_blas": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.c_int, P, C.c_uint64, P, P]),
         "mtp_energy_lut": (C.c_int, [P]),

@@ -136,6 +136,7 @@ class _JobTable:
         self.jobs = []
         self.samples = []
         self.total_items = 0
+        self.layout_mask = 0
 
     def set_jobs(self, jobs, samples=None):
         """Writes the table for `jobs` (RenderJob list), each adding
@@ -152,6 +153,12 @@ class _JobTable:
         self.jobs = list(jobs)
         self.samples = list(samples)
         self.total_items = total.value
+        # The kernel specialisation (BLAS layouts present) is chosen from the
+        # table when a launch is issued or captured.
+        mask = 0
+        for j in jobs:
+            mask |= j.scene.view.flags & abi.MTC_SCENE_BLAS_GPU_LAYOUT
+        self.layout_mask = mask
 
 
 class Batch(_JobTable):
@@ -168,6 +175,7 @@ class Batch(_JobTable):
         self.scratch = torch.zeros(abi.lib().mtc_batch_scratch_bytes(self.capacity), dtype=torch.uint8,
                                    device=self.device)
         self.graph = None
+        self._graph_mask = None
 
     def launch(self, stream=None):
         abi.check(abi.lib().mtc_batch_launch(C.c_void_p(self.table.data_ptr()), self.capacity,
@@ -184,10 +192,11 @@ class Batch(_JobTable):
                 self.launch(side)
         torch.cuda.current_stream(self.device).wait_stream(side)
         self.graph = g
+        self._graph_mask = self.layout_mask
         return g
 
     def replay(self):
-        if self.graph is None:
+        if self.graph is None or self._graph_mask != self.layout_mask:
             self.capture()
         self.graph.replay()
 

@@ -50,6 +50,7 @@ cudaError_t scratchAddress(void **out) {
   return cudaSuccess;
 }
 
+template <bool kGpuLayout>
 __global__ void __launch_bounds__(128)
     k_batch_noalloc(const JobData *__restrict__ jobs, uint32_t job_count, uint32_t total_items, uint32_t *queue,
                     mtc_counters *counters) {
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(128)
     uint32_t tx = local % J.tilesX, ty = local / J.tilesX;
     uint32_t x = tx * kWarpTileW + (lane % kWarpTileW), y = ty * kWarpTileH + (lane / kWarpTileW);
     if (x < J.width && y < J.height) {
-      tracePixelSamples(J, x, y, J.samples, cnt);
+      tracePixelSamples<kGpuLayout>(J, x, y, J.samples, cnt);
       paths += J.samples;
     }
   }
@@ -163,8 +164,13 @@ extern "C" mt_status mtc_trace_batch_noalloc(const mtc_job_desc *jobs, uint32_t 
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   uint32_t ctasPerSm = config && config->ctas_per_sm ? config->ctas_per_sm : 4u;
-  k_batch_noalloc<<<uint32_t(sms) * ctasPerSm, 128, 0, st>>>((const JobData *)scratch, job_count, uint32_t(total),
-                                                             queue, counters);
+  uint32_t flagsUnion = 0;
+  for (uint32_t j = 0; j < job_count; j++) flagsUnion |= jobs[j].scene.flags;
+  const uint32_t grid = uint32_t(sms) * ctasPerSm;
+  if (flagsUnion & MTC_SCENE_BLAS_GPU_LAYOUT)
+    k_batch_noalloc<true><<<grid, 128, 0, st>>>((const JobData *)scratch, job_count, uint32_t(total), queue, counters);
+  else
+    k_batch_noalloc<false><<<grid, 128, 0, st>>>((const JobData *)scratch, job_count, uint32_t(total), queue, counters);
   e = cudaGetLastError();
   return e == cudaSuccess ? MT_OK : MT_ERROR;
 }

@@ -612,13 +612,14 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
 }
 
 // intersect.wgsl.ts:829-879
+template <bool kGpuLayout>
 MTD bool intersectSceneShadow(const JobData &J, const Ray &r, float lightDistance, int32_t tri, int32_t ins,
                               Counters &cnt) {
   if (J.u.is_empty > 0) return false;
   cnt.shadow++;
   TraversalHit h;
   h.tMax = fminf(fmaxf(lightDistance, 0.0f), RAY_MAX_DISTANCE);
-  return traverse<true>(J.s, J.u.blas_offset, r.o, r.d, 1, true, tri, ins, h);
+  return traverse<true, kGpuLayout>(J.s, J.u.blas_offset, r.o, r.d, 1, true, tri, ins, h);
 }
 
 // ------------------------------------------------------------- integrator
@@ -1177,13 +1178,15 @@ MTD bool reusesPrimary(const JobData &J, const PathSample &ps, bool primaryReady
   return isSpectral(J) && ps.event == 0 && primaryReady;
 }
 
+template <bool kGpuLayout>
 MTD void traceExtension(const JobData &J, const PathSample &ps, TraversalHit &h, Counters &cnt) {
   h.tMax = RAY_MAX_DISTANCE;
   h.triangleIndex = -1;
   h.insIdx = -1;
   if (J.u.is_empty > 0) return;
   cnt.ext++;
-  traverse<false>(J.s, J.u.blas_offset, ps.path.ray.o, ps.path.ray.d, ps.depth, ps.event != 0, ps.si.triangleIndex,
+  traverse<false, kGpuLayout>(J.s, J.u.blas_offset, ps.path.ray.o, ps.path.ray.d, ps.depth, ps.event != 0,
+                              ps.si.triangleIndex,
                   ps.si.instanceIndex, h);
 }
 
@@ -1339,22 +1342,24 @@ MTD bool finishWavelength(const JobData &J, PathSample &ps, SpectralState &sp) {
 
 // One iteration of the integrator's event loop: true when the path (the
 // current wavelength path of a spectral sample) has ended.
+template <bool kGpuLayout>
 MTD bool stepPath(Ctx &c, PathSample &ps, SpectralState &sp) {
   TraversalHit h;
   h.tMax = RAY_MAX_DISTANCE;
   h.triangleIndex = -1;
   h.insIdx = -1;
   const bool spectral = isSpectral(c.J);
-  if (!spectral || !reusesPrimary(c.J, ps, sp.primaryReady)) traceExtension(c.J, ps, h, c.cnt);
+  if (!spectral || !reusesPrimary(c.J, ps, sp.primaryReady)) traceExtension<kGpuLayout>(c.J, ps, h, c.cnt);
   return spectral ? shadeStepSpectral(c, ps, sp, h) : shadeStep(c, ps, h);
 }
 
 // The deferred NEE visibility test of sampleScattering (sampleMaterial.wgsl.ts
 // :238-245): unoccluded -> the selected candidate's contribution.
+template <bool kGpuLayout>
 MTD void resolveShadow(Ctx &c, PathSample &ps) {
   if (!c.shadow.valid) return;
   c.shadow.valid = false;
-  if (!intersectSceneShadow(c.J, c.shadow.ray, c.shadow.maxDistance, c.shadow.triangleIndex,
+  if (!intersectSceneShadow<kGpuLayout>(c.J, c.shadow.ray, c.shadow.maxDistance, c.shadow.triangleIndex,
                             c.shadow.instanceIndex, c.cnt))
     ps.path.li += c.shadow.contribution;
 }
@@ -1394,7 +1399,9 @@ static __device__ __noinline__ void endSample(const JobData &J, uint32_t idx, co
 // source, instead of an inlined copy shaped by its caller: inlined copies could
 // contract multiply-adds differently, and a job's image must be bit-identical
 // alone and in a batch.
-static __device__ __noinline__ void tracePixelSamples(const JobData &J, uint32_t x, uint32_t y, uint32_t samples, Counters &cnt) {
+template <bool kGpuLayout>
+static __device__ __noinline__ void tracePixelSamples(const JobData &J, uint32_t x, uint32_t y, uint32_t samples,
+                                                      Counters &cnt) {
   Ctx c{J, Sampler(), BsdfContext{J.s.lut, (J.s.flags & MTC_SCENE_HAS_MEDIUM) != 0u, feature(J, MTC_FEATURE_HAS_THIN_FILM)},
         Counters(), ShadowQuery()};
   c.shadow.valid = false;
@@ -1409,8 +1416,8 @@ static __device__ __noinline__ void tracePixelSamples(const JobData &J, uint32_t
   // lanes left free to diverge give the scheduler more independent loads in
   // flight than a warp forced back together at every event.
   while (active) {
-    bool ended = stepPath(c, ps, sp);
-    resolveShadow(c, ps);
+    bool ended = stepPath<kGpuLayout>(c, ps, sp);
+    resolveShadow<kGpuLayout>(c, ps);
     if (ended && spectral) ended = finishWavelength(J, ps, sp);
     if (ended) {
       endSample(J, idx, ps);

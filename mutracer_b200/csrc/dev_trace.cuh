@@ -235,7 +235,12 @@ struct TraversalHit {
 
 // getBVHTraverseCode, intersect.wgsl.ts:213-629 for the BVH2 layout.  With
 // `shadow` the first accepted hit ends the query (returns true).
-template <bool shadow>
+//
+// kGpuLayout mirrors the reference's blasLayoutMask specialisation
+// (getBVHTraverseCode's layout branches are compiled only for the layouts a
+// scene uses): without it only BVH2 (layout 0) BLASes are traversed and the
+// BVH_GPU (layout 2) code is not compiled in.
+template <bool shadow, bool kGpuLayout>
 __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 rayO, V3 rayD, int bounces,
                                       bool doubleSided, int32_t currentTri, int32_t currentIns, TraversalHit &h) {
   int32_t tlasStack[MTC_MAX_STACK];
@@ -278,7 +283,8 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
       int maxDim = maxDimension(vabs(d));
       V3 shear = getShear(d, maxDim);
       uint32_t encoded = asu(insData.x);
-      if ((encoded >> 30) != 0u) continue;
+      const uint32_t layout = encoded >> 30;
+      if (layout != 0u && !(kGpuLayout && layout == 2u)) continue;  // TinyBVH bvh4 / cwbvh are not consumed
       int32_t blasOffset = int32_t(encoded & 0x3fffffffu);
       int32_t vertexOffset = asi(insData.y);
       int32_t sideMaterial = asi(insData.z) >> 8;
@@ -287,12 +293,32 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
       while (blasTop >= 0) {
         int32_t node = blasStack[blasTop--];
         int32_t i = node + blasBase;
-        float4 n1 = ld4(bvh + i);
-        int32_t p = asi(n1.w);
+        int32_t p, left, right;
+        float d0 = 0.0f, d1 = 0.0f;
+        if (kGpuLayout && layout == 2u) {
+          // BVH_GPU node (intersect.wgsl.ts:453-497): both child boxes inline.
+          float4 g0 = ld4(bvh + i), g1 = ld4(bvh + i + 1), g2 = ld4(bvh + i + 2), g3 = ld4(bvh + i + 3);
+          int32_t count = int32_t(asu(g2.w));
+          p = count > 0 ? -count : 0;
+          left = blasOffset + int32_t(asu(g0.w) * 4u);
+          right = blasOffset + int32_t(asu(g1.w) * 4u);
+          if (p >= 0) {
+            d0 = intersectBox(o, xyz(g0), xyz(g1), linvD, h.tMax);
+            d1 = intersectBox(o, xyz(g2), xyz(g3), linvD, h.tMax);
+          } else {
+            i = blasBase + blasOffset + int32_t(asu(g3.w)) - 2;  // records at i + 2
+          }
+        } else {
+          float4 n1 = ld4(bvh + i);
+          p = asi(n1.w);
+          left = node + 2;
+          right = p + blasOffset;
+          if (p >= 0) {
+            d0 = intersectBox(o, xyz(ld4(bvh + left + blasBase)), xyz(ld4(bvh + left + 1 + blasBase)), linvD, h.tMax);
+            d1 = intersectBox(o, xyz(ld4(bvh + right + blasBase)), xyz(ld4(bvh + right + 1 + blasBase)), linvD, h.tMax);
+          }
+        }
         if (p >= 0) {
-          int32_t left = node + 2, right = p + blasOffset;
-          float d0 = intersectBox(o, xyz(ld4(bvh + left + blasBase)), xyz(ld4(bvh + left + 1 + blasBase)), linvD, h.tMax);
-          float d1 = intersectBox(o, xyz(ld4(bvh + right + blasBase)), xyz(ld4(bvh + right + 1 + blasBase)), linvD, h.tMax);
           if (d0 > d1) {
             if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
             if (d1 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = right;
@@ -341,7 +367,7 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
 // current TLAS leaf.  Visit order, box tests, the `>` tie rule and the
 // self-hit and backface rules are those of traverse(), so the hits are
 // bit-identical to it.
-template <bool shadow>
+template <bool shadow, bool kGpuLayout>
 struct RayTraversal {
   const float4 *bvh, *ins, *mats;
   const uint32_t *attr;
@@ -361,6 +387,7 @@ struct RayTraversal {
   V3 o, d, linvD, shear;
   int maxDim;
   int32_t blasOffset, vertexOffset, sideMaterial, insIdx;
+  uint32_t blasLayout;
   bool found;
   TraversalHit h;
 
@@ -389,6 +416,7 @@ struct RayTraversal {
     leafNode = 0;
     insIdx = -1;
     blasOffset = 0;
+    blasLayout = 0;
     invD = traversalInverse(rd);
     if (intersectBox(rayO, xyz(ld4(bvh)), xyz(ld4(bvh + 1)), invD, h.tMax) > 0.0f) {
       tlasTop = 0;
@@ -411,15 +439,43 @@ struct RayTraversal {
     int32_t node = stack[stackBase + top];
     top--;
     const int32_t base = blas ? blasBase : 0;
-    float4 n1 = ld4(bvh + node + base);
-    int32_t p = asi(n1.w);
-    if (p >= 0) {
+    // Decode the node: BVH2 (TLAS, BLAS layout 0) keeps each child's box in
+    // the child; BVH_GPU (BLAS layout 2, intersect.wgsl.ts:453-497) keeps both
+    // child boxes in the node itself.
+    bool interior;
+    int32_t left = 0, right = 0, primitiveCount = 0, primitiveOffset = 0;
+    float4 lmin, lmax, rmin, rmax;
+    if (kGpuLayout && blas && blasLayout == 2u) {
+      lmin = ld4(bvh + node + base);
+      lmax = ld4(bvh + node + base + 1);
+      rmin = ld4(bvh + node + base + 2);
+      rmax = ld4(bvh + node + base + 3);
+      int32_t count = int32_t(asu(rmin.w));
+      interior = count <= 0;
+      left = blasOffset + int32_t(asu(lmin.w) * 4u);
+      right = blasOffset + int32_t(asu(lmax.w) * 4u);
+      primitiveCount = count;
+      primitiveOffset = base + blasOffset + int32_t(asu(rmax.w));
+    } else {
+      int32_t p = asi(ld4(bvh + node + base).w);
+      interior = p >= 0;
+      left = node + 2;
+      right = blas ? p + blasOffset : p;
+      primitiveCount = -p;
+      primitiveOffset = node + base + 2;
+      if (interior) {
+        lmin = ld4(bvh + left + base);
+        lmax = ld4(bvh + left + 1 + base);
+        rmin = ld4(bvh + right + base);
+        rmax = ld4(bvh + right + 1 + base);
+      }
+    }
+    if (interior) {
       // Interior node at either level: box-test both children, push the
       // nearer last (the `>` rule of intersect.wgsl.ts).
       const V3 ro = blas ? o : rayO, id = blas ? linvD : invD;
-      int32_t left = node + 2, right = blas ? p + blasOffset : p;
-      float d0 = intersectBox(ro, xyz(ld4(bvh + left + base)), xyz(ld4(bvh + left + 1 + base)), id, h.tMax);
-      float d1 = intersectBox(ro, xyz(ld4(bvh + right + base)), xyz(ld4(bvh + right + 1 + base)), id, h.tMax);
+      float d0 = intersectBox(ro, xyz(lmin), xyz(lmax), id, h.tMax);
+      float d1 = intersectBox(ro, xyz(rmin), xyz(rmax), id, h.tMax);
       int32_t first = right, second = left;
       float df = d1, ds = d0;
       if (d0 > d1) {
@@ -434,11 +490,9 @@ struct RayTraversal {
     if (blas) blasTop = top; else tlasTop = top;
     if (!blas) {
       leafNode = node;
-      io = -p - 1;
+      io = primitiveCount - 1;
       return false;
     }
-    int32_t primitiveCount = -p;
-    int32_t primitiveOffset = node + base + 2;
     for (int32_t k = 0; k < primitiveCount; k++) {
       int32_t triangleIndex = primitiveOffset + k;
       if (bounces > 0 && triangleIndex == currentTri && insIdx == currentIns) continue;
@@ -477,7 +531,8 @@ struct RayTraversal {
     const float4 *insv = ins + size_t(insIdx) * MTC_INSTANCE_VEC4_STRIDE;
     float4 insData = ld4(insv);
     uint32_t encoded = asu(insData.x);
-    if ((encoded >> 30) != 0u) return false;
+    blasLayout = encoded >> 30;
+    if (blasLayout != 0u && !(kGpuLayout && blasLayout == 2u)) return false;  // TinyBVH bvh4 / cwbvh are not consumed
     float4 c0 = ld4(insv + 1), c1 = ld4(insv + 2), c2 = ld4(insv + 3), c3 = ld4(insv + 4);
     o = xmat4(c0, c1, c2, c3, rayO, 1.0f);
     d = xmat4(c0, c1, c2, c3, rayD, 0.0f);

@@ -44,6 +44,16 @@ int mtp_camera_look_at(uint32_t width, uint32_t height, const double *eye, const
   return MT_OK;
 }
 
+int mtp_scene_set_blas_layout(void *scene, uint32_t layout) {
+  if (!scene || (layout != 0 && layout != 2)) return MT_ERROR_INVALID_ARGUMENT;
+  try {
+    setBlasLayout(*static_cast<SceneHost *>(scene), layout);
+  } catch (...) {
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  return MT_OK;
+}
+
 void mtp_scene_free(void *scene) { delete static_cast<SceneHost *>(scene); }
 
 int mtp_scene_bundle(void *scene, mt_scene_bundle *b) {
@@ -116,7 +126,7 @@ int mtp_scene_refit_inputs(void *scene, double *transforms, float *localBounds, 
     if (transforms) std::memcpy(transforms + i * 16, ins.transform, sizeof(ins.transform));
     if (localBounds) std::memcpy(localBounds + i * 6, s.blases[ins.blasIndex].localBounds, 24);
     if (blasOffsets) blasOffsets[i] = int32_t(s.blasOffsets[ins.blasIndex]);
-    if (blasLayouts) blasLayouts[i] = 0;
+    if (blasLayouts) blasLayouts[i] = int32_t(s.blasLayout);
     if (vertexOffsets) vertexOffsets[i] = int32_t(s.vertexOffsets[ins.blasIndex]);
     if (materials) materials[i] = ins.material;
     if (colors) std::memcpy(colors + i * 3, ins.color, 12);
@@ -137,7 +147,8 @@ int mtp_scene_set_transforms(void *scene, const double *transforms, uint32_t cou
 int mtp_scene_refit_host(void *scene) {
   if (!scene) return MT_ERROR_INVALID_ARGUMENT;
   SceneHost &s = *static_cast<SceneHost *>(scene);
-  refitTlasHost(s.bvh.data(), s.instances.data(), s.sourceInstances, s.blases, s.blasOffsets, s.vertexOffsets);
+  refitTlasHost(s.bvh.data(), s.instances.data(), s.sourceInstances, s.blases, s.blasOffsets, s.vertexOffsets,
+                s.blasLayout);
   return MT_OK;
 }
 

@@ -41,6 +41,7 @@ __device__ __forceinline__ void flushCounters(const Counters &cnt, uint32_t path
 #ifndef MT_TRACE_MIN_BLOCKS
 #define MT_TRACE_MIN_BLOCKS 2
 #endif
+template <bool kGpuLayout>
 __global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
     k_trace(const __grid_constant__ JobData J, uint32_t samples, mtc_counters *counters) {
   uint32_t lx = threadIdx.x % kTileW, ly = threadIdx.x / kTileW;
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
   Counters cnt;
   uint32_t paths = 0;
   if (x < J.width && y < J.height) {
-    tracePixelSamples(J, x, y, samples, cnt);
+    tracePixelSamples<kGpuLayout>(J, x, y, samples, cnt);
     paths = samples;
   }
   flushCounters(cnt, paths, counters);
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
 // count and item total from it, so a captured launch can be replayed after
 // the host table is rewritten with other jobs.
 struct BatchHeader {
-  uint32_t jobCount, totalItems, tileW, _pad[61];
+  uint32_t jobCount, totalItems, tileW, flagsUnion, _pad[60];
 };
 static_assert(sizeof(BatchHeader) == 256, "batch header size");
 constexpr size_t kBatchTableOffset = sizeof(BatchHeader);
@@ -69,6 +70,7 @@ constexpr size_t kBatchTableOffset = sizeof(BatchHeader);
 // (JobData.firstItem / .items).  A warp takes `grain` consecutive items per
 // atomic.  The loop ends when the counter passes the item total, so every
 // warp exits.
+template <bool kGpuLayout>
 __global__ void __launch_bounds__(128)
     k_batch(const BatchHeader *__restrict__ header, uint32_t *queue, mtc_counters *counters, uint32_t grain) {
   const JobData *__restrict__ jobs =
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(128)
       uint32_t tx = local % J.tilesX, ty = local / J.tilesX;
       uint32_t x = tx * tileW + lx, y = ty * tileH + ly;
       if (x < J.width && y < J.height) {
-        tracePixelSamples(J, x, y, J.samples, cnt);
+        tracePixelSamples<kGpuLayout>(J, x, y, J.samples, cnt);
         paths += J.samples;
       }
     }
@@ -101,6 +103,7 @@ __global__ void __launch_bounds__(128)
   flushCounters(cnt, paths, counters);
 }
 
+template <bool kGpuLayout>
 __global__ void k_first_hit(const __grid_constant__ DevScene s, int32_t blasBase, int32_t isEmpty, const float4 *rays,
                             uint32_t count, mtc_hit *hits) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -115,7 +118,7 @@ __global__ void k_first_hit(const __grid_constant__ DevScene s, int32_t blasBase
     h.triangleIndex = -1;
     h.insIdx = -1;
     h.hitBary = v3(0.0f);
-    traverse<false>(s, blasBase, xyz(o4), xyz(d4), 0, false, -1, -1, h);
+    traverse<false, kGpuLayout>(s, blasBase, xyz(o4), xyz(d4), 0, false, -1, -1, h);
     if (h.insIdx >= 0) {
       out.hit = 1; out.instance = h.insIdx; out.record = h.triangleIndex; out.t = h.tMax;
       out.barycentric[0] = h.hitBary.x; out.barycentric[1] = h.hitBary.y; out.barycentric[2] = h.hitBary.z;
@@ -353,7 +356,10 @@ mt_status mtc_trace_samples(const mtc_scene_view *scene, const mtc_camera_unifor
   if (samples == 0) return MT_OK;
   JobData J = makeJob(scene, camera, uniform, out, samples);
   dim3 grid((J.width + kTileW - 1) / kTileW, (J.height + kTileH - 1) / kTileH);
-  k_trace<<<grid, kTileW * kTileH, 0, (cudaStream_t)stream>>>(J, samples, counters);
+  if (scene->flags & MTC_SCENE_BLAS_GPU_LAYOUT)
+    k_trace<true><<<grid, kTileW * kTileH, 0, (cudaStream_t)stream>>>(J, samples, counters);
+  else
+    k_trace<false><<<grid, kTileW * kTileH, 0, (cudaStream_t)stream>>>(J, samples, counters);
   return cudaStatus(cudaGetLastError());
 }
 
@@ -362,8 +368,12 @@ mt_status mtc_query_first_hit(const mtc_scene_view *scene, const float *rays, ui
   if (!validScene(scene) || (!rays && count) || (!hits && count)) return MT_ERROR_INVALID_ARGUMENT;
   if (count == 0) return MT_OK;
   int32_t blasBase = scene->blas_offset;
-  k_first_hit<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(toDev(scene), blasBase, scene->instance_count == 0,
-                                                                   (const float4 *)rays, count, hits);
+  if (scene->flags & MTC_SCENE_BLAS_GPU_LAYOUT)
+    k_first_hit<true><<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+        toDev(scene), blasBase, scene->instance_count == 0, (const float4 *)rays, count, hits);
+  else
+    k_first_hit<false><<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+        toDev(scene), blasBase, scene->instance_count == 0, (const float4 *)rays, count, hits);
   return cudaStatus(cudaGetLastError());
 }
 
@@ -414,6 +424,7 @@ mt_status mtc_batch_prepare(const mtc_job_desc *jobs, uint32_t job_count, const 
   h.jobCount = job_count;
   h.totalItems = uint32_t(total);
   h.tileW = shape.tileW;
+  for (uint32_t j = 0; j < job_count; j++) h.flagsUnion |= jobs[j].scene.flags;
   std::memcpy(base, &h, sizeof(h));
   if (total_items) *total_items = uint32_t(total);
   return MT_OK;
@@ -437,7 +448,12 @@ mt_status mtc_batch_launch(const void *table, uint32_t capacity, const mtc_batch
   if (e != cudaSuccess) return cudaStatus(e);
   // A full persistent grid: the item total is only known on the device.
   uint32_t grid = uint32_t(sms) * shape.ctasPerSm;
-  k_batch<<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain);
+  // The host copy of the header decides the BLAS-layout specialisation.
+  uint32_t flagsUnion = static_cast<const BatchHeader *>(table)->flagsUnion;
+  if (flagsUnion & MTC_SCENE_BLAS_GPU_LAYOUT)
+    k_batch<true><<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain);
+  else
+    k_batch<false><<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain);
   return cudaStatus(cudaGetLastError());
 }
 

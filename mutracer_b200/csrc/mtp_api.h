@@ -27,6 +27,8 @@ int mtp_scene_refit_inputs(void *scene, double *transforms, float *localBounds, 
                            int32_t *blasLayouts, int32_t *vertexOffsets, int32_t *materials, float *colors);
 int mtp_scene_set_transforms(void *scene, const double *transforms, uint32_t count);
 int mtp_scene_refit_host(void *scene);
+/* Re-encodes the scene's BLASes in layout code 0 (BVH2) or 2 (BVH_GPU). */
+int mtp_scene_set_blas_layout(void *scene, uint32_t layout);
 int mtp_build_binned_sah(const float *aabbs, uint32_t count, int bins, uint32_t *nodeCount, float *bounds,
                          uint32_t *leftFirst, uint32_t *primCount, uint32_t *primIndices);
 int mtp_build_blas(const float *positions, uint32_t vertexCount, const uint32_t *indices, uint32_t triCount, int bins,

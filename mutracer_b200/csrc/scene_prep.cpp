@@ -246,6 +246,98 @@ Blas buildBlas(const std::vector<float> &positions, const std::vector<uint32_t> 
   return b;
 }
 
+std::vector<float> blasToGpuLayout(const std::vector<float> &f) {
+  if (f.empty()) return {};
+  auto ptr = [&](uint32_t off) { return asInt(f[size_t(off) * 4 + 3]); };
+  // Depth-first preorder numbering of the BVH2 nodes (left before right).
+  std::vector<uint32_t> order;
+  std::vector<uint32_t> stack = {0};
+  while (!stack.empty()) {
+    uint32_t off = stack.back();
+    stack.pop_back();
+    order.push_back(off);
+    int32_t p = ptr(off);
+    if (p >= 0) {
+      stack.push_back(uint32_t(p));
+      stack.push_back(off + 2);
+    }
+  }
+  std::vector<int64_t> index(f.size() / 4, -1);
+  for (size_t k = 0; k < order.size(); k++) index[order[k]] = int64_t(k);
+  size_t nodeVec4 = order.size() * 4, records = 0;
+  for (uint32_t off : order)
+    if (ptr(off) < 0) records += size_t(-ptr(off));
+  std::vector<float> g((nodeVec4 + records) * 4, 0.0f);
+  size_t next = nodeVec4;  // next primitive record, vec4 units
+  for (size_t k = 0; k < order.size(); k++) {
+    uint32_t off = order[k];
+    float *n = &g[k * 16];
+    int32_t p = ptr(off);
+    if (p >= 0) {
+      uint32_t left = off + 2, right = uint32_t(p);
+      for (int c = 0; c < 3; c++) {
+        n[c] = f[size_t(left) * 4 + c];           // left min
+        n[4 + c] = f[size_t(left) * 4 + 4 + c];   // left max
+        n[8 + c] = f[size_t(right) * 4 + c];      // right min
+        n[12 + c] = f[size_t(right) * 4 + 4 + c]; // right max
+      }
+      n[3] = asFloat(int32_t(index[left]));
+      n[7] = asFloat(int32_t(index[right]));
+      n[11] = asFloat(int32_t(0));
+      n[15] = asFloat(int32_t(0));
+      continue;
+    }
+    uint32_t count = uint32_t(-p);
+    n[11] = asFloat(int32_t(count));
+    n[15] = asFloat(int32_t(next));
+    std::memcpy(&g[next * 4], &f[(size_t(off) + 2) * 4], size_t(count) * 16);
+    next += count;
+  }
+  return g;
+}
+
+void setBlasLayout(SceneHost &s, uint32_t layout) {
+  if (layout != 0 && layout != 2) throw std::runtime_error("BLAS layout must be 0 or 2");
+  std::vector<std::vector<float>> buffers(s.blases.size());
+  for (size_t m = 0; m < s.blases.size(); m++)
+    buffers[m] = layout == 2 ? blasToGpuLayout(s.blases[m].buffer) : s.blases[m].buffer;
+  std::vector<uint32_t> offsets;
+  uint32_t off = 0;
+  for (auto &b : buffers) {
+    offsets.push_back(off);
+    off += uint32_t(b.size() / 4);
+  }
+  std::vector<float> bvh(s.bvh.begin(), s.bvh.begin() + size_t(s.tlasVec4) * 4);
+  for (auto &b : buffers) bvh.insert(bvh.end(), b.begin(), b.end());
+  // TLAS leaf records (instanceSlot, blasRoot, sourceIndex, box): walk the
+  // TLAS and move each blasRoot to its BLAS's new start.
+  std::vector<uint32_t> stack;
+  if (s.tlasVec4) stack.push_back(0);
+  while (!stack.empty()) {
+    uint32_t node = stack.back();
+    stack.pop_back();
+    int32_t p = asInt(bvh[size_t(node) * 4 + 3]);
+    if (p >= 0) {
+      stack.push_back(node + 2);
+      stack.push_back(uint32_t(p));
+      continue;
+    }
+    for (int32_t i = 0; i < -p; i++) {
+      float *rec = &bvh[(size_t(node) + 2 + i) * 4];
+      int32_t source = asInt(rec[2]);
+      uint32_t m = s.sourceInstances[size_t(source)].blasIndex;
+      rec[1] = asFloat(int32_t(offsets[m]));
+      float *ins = &s.instances[size_t(asInt(rec[0])) * 40];
+      ins[0] = asFloat(int32_t(offsets[m] | (layout << 30)));  // as writeInstanceRecord
+    }
+  }
+  s.bvh.swap(bvh);
+  s.blasOffsets = offsets;
+  s.blasLayout = layout;
+  if (layout == 2) s.flags |= MTC_SCENE_BLAS_GPU_LAYOUT;
+  else s.flags &= ~uint32_t(MTC_SCENE_BLAS_GPU_LAYOUT);
+}
+
 // gl-matrix mat4 invert (cofactor expansion), float64, as called by
 // writeInstanceRecord (bvhAccel.ts:330-353).
 bool invert4(const double *a, double *out) {
@@ -299,10 +391,11 @@ void computeInstanceBounds(const Instance &ins, const float local[6], float out[
   for (int k = 0; k < 3; k++) { out[k] = mn[k]; out[3 + k] = mx[k]; }
 }
 
-// bvhAccel.ts:330-353 writeInstanceRecord (BVH2 layout code 0)
-void writeInstanceRecord(float *rec, const Instance &ins, uint32_t blasOffset, uint32_t vertexOffset) {
+// bvhAccel.ts:330-353 writeInstanceRecord: blasOffset | layout << 30
+void writeInstanceRecord(float *rec, const Instance &ins, uint32_t blasOffset, uint32_t vertexOffset,
+                         uint32_t blasLayout) {
   if (blasOffset > 0x3fffffffu) throw std::runtime_error("BLAS offset exceeds the packed 30-bit range");
-  rec[0] = asFloat(int32_t(blasOffset));
+  rec[0] = asFloat(int32_t(blasOffset | (blasLayout << 30)));
   rec[1] = asFloat(int32_t(vertexOffset));
   rec[2] = asFloat(ins.material);
   rec[3] = 0.0f;
@@ -356,7 +449,7 @@ Tlas buildTlas(const std::vector<Instance> &instances, const std::vector<Blas> &
 // bvhAccel.ts:579-740 refitTLAS with no dirty set (full refit, refitNode).
 void refitTlasHost(float *tlas, float *records, const std::vector<Instance> &instances,
                    const std::vector<Blas> &blases, const std::vector<uint32_t> &blasOffsets,
-                   const std::vector<uint32_t> &vertexOffsets) {
+                   const std::vector<uint32_t> &vertexOffsets, uint32_t blasLayout) {
   std::function<void(int32_t)> refitNode = [&](int32_t index) {
     size_t base = size_t(index) * 4;
     int32_t child = asInt(tlas[base + 3]);
@@ -379,7 +472,8 @@ void refitTlasHost(float *tlas, float *records, const std::vector<Instance> &ins
       computeInstanceBounds(ins, blases[ins.blasIndex].localBounds, b);
       for (int k = 0; k < 3; k++) { mn[k] = std::min(mn[k], b[k]); mx[k] = std::max(mx[k], b[3 + k]); }
       int32_t target = asInt(tlas[record]);
-      writeInstanceRecord(records + size_t(target) * 40, ins, blasOffsets[ins.blasIndex], vertexOffsets[ins.blasIndex]);
+      writeInstanceRecord(records + size_t(target) * 40, ins, blasOffsets[ins.blasIndex], vertexOffsets[ins.blasIndex],
+                          blasLayout);
     }
     for (int k = 0; k < 3; k++) { tlas[base + k] = mn[k]; tlas[base + 4 + k] = mx[k]; }
   };

@@ -53,14 +53,15 @@ struct Tlas {
 void computeInstanceBounds(const Instance &ins, const float local[6], float out[6]);
 Tlas buildTlas(const std::vector<Instance> &instances, const std::vector<Blas> &blases,
                const std::vector<uint32_t> &blasOffsets, const std::vector<uint32_t> &vertexOffsets, int bins);
-void writeInstanceRecord(float *record, const Instance &ins, uint32_t blasOffset, uint32_t vertexOffset);
+void writeInstanceRecord(float *record, const Instance &ins, uint32_t blasOffset, uint32_t vertexOffset,
+                         uint32_t blasLayout = 0);
 bool invert4(const double *a, double *out);
 
 // Full TLAS refit on the host (bvhAccel.ts:579-740 without a dirty set);
 // the oracle of the device refit kernel.
 void refitTlasHost(float *tlas, float *records, const std::vector<Instance> &instances,
                    const std::vector<Blas> &blases, const std::vector<uint32_t> &blasOffsets,
-                   const std::vector<uint32_t> &vertexOffsets);
+                   const std::vector<uint32_t> &vertexOffsets, uint32_t blasLayout = 0);
 
 struct MaterialDesc {
   float baseColor[3] = {0.8f, 0.8f, 0.8f};
@@ -121,9 +122,22 @@ struct SceneHost {
   std::vector<Blas> blases;
   std::vector<Instance> sourceInstances;
   std::vector<uint32_t> blasOffsets, vertexOffsets;
+  uint32_t blasLayout = 0;  // BLAS layout code of every instance (0 BVH2, 2 BVH_GPU)
   uint64_t triangleCount = 0, uniqueTriangleCount = 0;
   std::string name;
 };
+
+// Re-encodes every BLAS of an assembled scene in the given layout code
+// (0: BVH2 of bvhAccel.ts:248-275; 2: the two-children-per-node BVH_GPU
+// layout that intersect.wgsl.ts:453-497 traverses) and rewrites the TLAS leaf
+// records and instance records that point at them.  Same tree, same child
+// order: a ray visits the same nodes in the same order in either layout.
+void setBlasLayout(SceneHost &s, uint32_t layout);
+// A layout-0 BLAS buffer (vec4 words, offsets relative to its start) in the
+// BVH_GPU layout: 4 vec4 per node, (left min, left index) (left max, right
+// index) (right min, leaf count) (right max, first record), node k at vec4
+// 4k, leaf primitive records after the nodes.
+std::vector<float> blasToGpuLayout(const std::vector<float> &bvh2);
 
 struct CameraDesc {
   double eye[3], target[3], up[3];

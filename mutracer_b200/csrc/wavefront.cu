@@ -55,7 +55,7 @@ static_assert(sizeof(StreamQueues) == 256, "queue header size");
 
 // Same layout as the batched table header written by mtc_batch_prepare.
 struct TableHeader {
-  uint32_t jobCount, totalItems, tileW, _pad[61];
+  uint32_t jobCount, totalItems, tileW, flagsUnion, _pad[60];
 };
 static_assert(sizeof(TableHeader) == 256, "table header size");
 
@@ -224,6 +224,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v) {
 #ifndef MT_TRAVERSE_MIN_BLOCKS
 #define MT_TRAVERSE_MIN_BLOCKS 8
 #endif
+template <bool kGpuLayout>
 __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
     k_wf_extend(StreamView v, uint32_t cur, uint32_t regroup) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
       v.rayKeyCursor[k] = 0;
     }
   }
-  RayTraversal<false> rt;
+  RayTraversal<false, kGpuLayout> rt;
   uint32_t s = 0, ext = 0;
   bool busy = false, exhausted = false;
   for (;;) {
@@ -384,9 +385,10 @@ __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
 
 // NEE visibility of the queued shadow rays (intersectSceneShadow and
 // resolveShadow), persistent like k_wf_extend.
+template <bool kGpuLayout>
 __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS) k_wf_shadow(StreamView v) {
   const uint32_t n = v.q->shadowCount;
-  RayTraversal<true> rt;
+  RayTraversal<true, kGpuLayout> rt;
   uint32_t s = 0, shadowRays = 0;
   bool busy = false, exhausted = false;
   for (;;) {
@@ -646,9 +648,9 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
 
   uint32_t gSeed, gExtend, gShade, gShadow, gFinish, gRegroup, gSort;
   if ((e = gridFor((const void *)k_wf_seed, gSeed)) != cudaSuccess ||
-      (e = gridFor((const void *)k_wf_extend, gExtend)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_extend<false>, gExtend)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_shade, gShade)) != cudaSuccess ||
-      (e = gridFor((const void *)k_wf_shadow, gShadow)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_shadow<false>, gShadow)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_finish, gFinish)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_regroup, gRegroup)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_sort_rays, gSort)) != cudaSuccess)
@@ -665,6 +667,8 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
     return toStatus(e);
   }
 
+  // The BLAS-layout specialisation (blasLayoutMask) of the traversal kernels.
+  const bool gpuLayout = (hdr.flagsUnion & MTC_SCENE_BLAS_GPU_LAYOUT) != 0u;
   k_wf_seed<<<gSeed, kStreamThreads, 0, st>>>(v);
   e = cudaGetLastError();
   uint32_t cur = 0, iterations = 0, chunk = 0;
@@ -673,10 +677,12 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
     for (uint32_t k = 0; k < shape.iterationsPerCheck && e == cudaSuccess; k++) {
       const uint32_t regroup = shape.regroupInterval && (iterations % shape.regroupInterval) == 0u ? 1u : 0u;
       if (v.sortRays) k_wf_sort_rays<<<gSort, kStreamThreads, 0, st>>>(v, cur);
-      k_wf_extend<<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
+      if (gpuLayout) k_wf_extend<true><<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
+      else k_wf_extend<false><<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
       if (regroup) k_wf_regroup<<<gRegroup, kStreamThreads, 0, st>>>(v, cur);
       k_wf_shade<<<gShade, kStreamThreads, 0, st>>>(v, cur, regroup);
-      k_wf_shadow<<<gShadow, kStreamThreads, 0, st>>>(v);
+      if (gpuLayout) k_wf_shadow<true><<<gShadow, kStreamThreads, 0, st>>>(v);
+      else k_wf_shadow<false><<<gShadow, kStreamThreads, 0, st>>>(v);
       k_wf_finish<<<gFinish, kStreamThreads, 0, st>>>(v, cur);
       e = cudaGetLastError();
       cur ^= 1u;

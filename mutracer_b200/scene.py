@@ -123,6 +123,12 @@ class SceneHost:
         t = np.ascontiguousarray(transforms, dtype=np.float64)
         abi.check(abi.lib().mtp_scene_set_transforms(self._handle, t.ctypes.data, t.shape[0]))
 
+    def set_blas_layout(self, layout):
+        """Re-encodes every BLAS in layout code 0 (BVH2) or 2 (BVH_GPU: both
+        child boxes in the parent node) and refreshes the host arrays."""
+        abi.check(abi.lib().mtp_scene_set_blas_layout(self._handle, layout))
+        self.refresh()
+
     def refit_host(self):
         abi.check(abi.lib().mtp_scene_refit_host(self._handle))
 

@@ -282,18 +282,46 @@ static bool traverse(const Scene &s, const Ray &ray, int bounces, bool doubleSid
       u32 layout = encoded >> 30;
       i32 blasOffset = i32(encoded & 0x3fffffffu);
       i32 vertexOffset = asi(insData.y);
-      if (layout != 0u) continue;  // only the BVH2 layout is consumed
+      // BVH2 (code 0) and BVH_GPU (code 2) BLASes are consumed; the TinyBVH
+      // bvh4 and cwbvh layouts (codes 1 and 3) are not.
+      if (layout != 0u && layout != 2u) continue;
       int blasTop = 0;
       blasStack[0] = blasRoot;
       while (blasTop >= 0) {
         i32 node = blasStack[blasTop--];
         i32 i = node + bufferOff;
-        V4 n1 = s.bvh[i];
-        i32 p = asi(n1.w);
-        if (p >= 0) {
-          i32 left = node + 2, right = p + blasOffset;
-          float d0 = intersectBox(o, xyz(s.bvh[left + bufferOff]), xyz(s.bvh[left + 1 + bufferOff]), invD, h.tMax);
-          float d1 = intersectBox(o, xyz(s.bvh[right + bufferOff]), xyz(s.bvh[right + 1 + bufferOff]), invD, h.tMax);
+        i32 primitiveCount = 0, primitiveOffset = 0;
+        i32 left = 0, right = 0;
+        float d0 = 0.0f, d1 = 0.0f;
+        bool interior;
+        if (layout == 2u) {
+          // intersect.wgsl.ts:453-497: both child boxes live in the node.
+          V4 g0 = s.bvh[i], g1 = s.bvh[i + 1], g2 = s.bvh[i + 2], g3 = s.bvh[i + 3];
+          primitiveCount = i32(asu(g2.w));
+          interior = primitiveCount <= 0;
+          if (!interior) {
+            primitiveOffset = bufferOff + blasOffset + i32(asu(g3.w));
+          } else {
+            left = blasOffset + i32(asu(g0.w) * 4u);
+            right = blasOffset + i32(asu(g1.w) * 4u);
+            d0 = intersectBox(o, xyz(g0), xyz(g1), invD, h.tMax);
+            d1 = intersectBox(o, xyz(g2), xyz(g3), invD, h.tMax);
+          }
+        } else {
+          V4 n1 = s.bvh[i];
+          i32 p = asi(n1.w);
+          interior = p >= 0;
+          if (interior) {
+            left = node + 2;
+            right = p + blasOffset;
+            d0 = intersectBox(o, xyz(s.bvh[left + bufferOff]), xyz(s.bvh[left + 1 + bufferOff]), invD, h.tMax);
+            d1 = intersectBox(o, xyz(s.bvh[right + bufferOff]), xyz(s.bvh[right + 1 + bufferOff]), invD, h.tMax);
+          } else {
+            primitiveCount = -p;
+            primitiveOffset = i + 2;
+          }
+        }
+        if (interior) {
           if (tr) tr->box_tests += 2;
           if (d0 > d1) {
             if (d0 > 0.0f && blasTop + 1 < MTC_MAX_STACK) blasStack[++blasTop] = left;
@@ -304,8 +332,6 @@ static bool traverse(const Scene &s, const Ray &ray, int bounces, bool doubleSid
           }
           continue;
         }
-        i32 primitiveCount = -p;
-        i32 primitiveOffset = i + 2;
         for (i32 k = 0; k < primitiveCount; k++) {
           i32 triangleIndex = primitiveOffset + k;
           if (bounces > 0 && triangleIndex == currentTri && insIdx == currentIns) continue;

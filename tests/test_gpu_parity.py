@@ -244,3 +244,30 @@ def test_context_api_render_and_jobs(cuda):
                 assert np.array_equal(ctx.read_pixels(kind), want), kind
     finally:
         ctx.destroy()
+
+
+def test_first_hits_layout2_bit_exact(cuda):
+    """BVH_GPU BLASes (layout code 2) through the device traversal."""
+    host = scene.make_workload("instanced_spheres", width=64, height=64, params=(128, 8, 16, 256, 2))
+    host.set_blas_layout(2)
+    _first_hit_case(cuda, host, 200_000, seed=13)
+
+
+def test_layout2_images_equal_layout0_in_both_engines(cuda):
+    import torch
+    from mutracer_b200 import batch
+    params = (48, 6, 10, 128, 3)
+    a = scene.make_workload("instanced_spheres", width=72, height=40, params=params)
+    b = scene.make_workload("instanced_spheres", width=72, height=40, params=params)
+    b.set_blas_layout(2)
+    da, db = scene.DeviceScene(a, cuda), scene.DeviceScene(b, cuda)
+    ja, jb, jw = batch.RenderJob(da, 4, device=cuda), batch.RenderJob(db, 4, device=cuda), \
+        batch.RenderJob(db, 4, device=cuda)
+    ja.render_alone()
+    jb.render_alone()
+    sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=4096), device=cuda)
+    sb.set_jobs([jw])
+    sb.run()
+    torch.cuda.synchronize()
+    for x in (jb, jw):
+        assert torch.equal(ja.acc.color, x.acc.color) and torch.equal(ja.acc.normal, x.acc.normal)
