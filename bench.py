@@ -1,15 +1,20 @@
-"""Benchmark: converged Mpaths/s of the path-tracing megakernel on one B200.
+"""Benchmark: converged Mpaths/s of the B200 path tracer on one GPU.
 
-Workload (the large plain-method configuration): 256 seeded affine instances
-of 16 displaced icospheres (15,680 triangles each, 4,014,080 instanced
-triangles), 2048x1024 analytic sky plus 4 rect lights, 1920x1080, 16 spp,
-6 bounces, OpenPBR diffuse / F82 metal / coat.  One step renders the whole
-job (16 spp over 1080p) from zeroed accumulation buffers.
+Headline workload (the large plain-method configuration): 256 seeded affine
+instances of 16 displaced icospheres (15,680 triangles each, 4,014,080
+instanced triangles), 2048x1024 analytic sky plus 4 rect lights, 1920x1080,
+16 spp, 6 bounces, OpenPBR diffuse / F82 metal / coat.  One step renders the
+whole job from zeroed accumulation buffers through the wavefront engine
+(mtc_stream_run; `--form megakernel` times the plain drop-in megakernel
+mtc_trace_samples instead).  The other engine renders the same job beside it
+and must produce the same bits.
 
-Also reported on the same line: the batched form (mixed 64-job workload in one
-persistent launch vs. the plain kernel job by job), end-to-end throughput
-through the public context API with host buffers, the HBM roofline of the
-megakernel and the CPU oracle baseline.
+Also reported on the same line: the batched form (the mixed 64-job workload:
+plain megakernel job by job, one sample per launch as the reference's host
+dispatches, vs. the persistent and wavefront batched forms), the served form
+(Poisson requests over resident scenes: sustained Mpaths/s, p50/p99),
+end-to-end throughput through the public context API with host buffers, the
+HBM roofline and the CPU oracle baseline.
 
 `--impl reference` times the reference algorithm's CPU implementation (the
 C++ oracle restating the WGSL megakernel; the reference itself only runs
@@ -43,9 +48,9 @@ def parse():
     p.add_argument("--width", type=int, default=None)
     p.add_argument("--height", type=int, default=None)
     p.add_argument("--spp", type=int, default=None)
-    p.add_argument("--form", default="megakernel", choices=["megakernel", "wavefront"],
-                   help="engine of the headline step: the plain drop-in megakernel (mtc_trace_samples) or the "
-                        "wavefront kernels (mtc_stream_run)")
+    p.add_argument("--form", default="wavefront", choices=["megakernel", "wavefront"],
+                   help="engine of the headline step: the wavefront kernels (mtc_stream_run, the default, also "
+                        "what mt_context_render runs) or the plain drop-in megakernel (mtc_trace_samples)")
     p.add_argument("--slots", type=int, default=1 << 20, help="wavefront paths in flight")
     p.add_argument("--refill-lanes", type=int, default=0, help="wavefront traversal refill threshold (0: default)")
     p.add_argument("--no-batch", action="store_true")
@@ -142,19 +147,26 @@ def oracle_traffic(host, rows=8, spp=2):
     return oracle_lib.algorithmic_bytes(total), total
 
 
-def measured_traffic(args, host, spp):
-    """DRAM bytes (read + write) of one k_trace launch of this exact workload,
-    from the committed ncu summary, or None for another workload."""
-    if args.form != "megakernel" or args.workload != WORKLOAD or (host.width, host.height, spp) != (1920, 1080, 16):
-        return None
-    path = os.path.join(ROOT, "profiles", "k_trace_dram_instanced_spheres_1080p_16spp.md")
+TRAFFIC_PROFILES = {
+    "megakernel": ("k_trace_dram_instanced_spheres_1080p_16spp.md", "traffic_bytes_per_launch:"),
+    "wavefront": ("wavefront_dram_instanced_spheres_1080p_16spp.md", "traffic_bytes_per_step:"),
+}
+
+
+def measured_traffic(form, args, host, spp):
+    """DRAM bytes (read + write) of one step of this exact workload in the
+    given engine, from the committed ncu summary; (None, None) otherwise."""
+    if args.workload != WORKLOAD or (host.width, host.height, spp) != (1920, 1080, 16):
+        return None, None
+    name, key = TRAFFIC_PROFILES[form]
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return int(line.split(":")[1])
+            if line.startswith(key):
+                return int(line.split(":")[1]), "profiles/" + name
     except OSError:
         pass
-    return None
+    return None, None
 
 
 def cpu_baseline(host, spp, seconds):
@@ -306,13 +318,14 @@ def run_b200(args):
     try:
         bpp, traffic = oracle_traffic(host)
         achieved = bpp * paths_per_step / (ms_per_step / 1000.0) / 1e9
-        dram = measured_traffic(args, host, spp)
+        dram, source = measured_traffic(args.form, args, host, spp)
         result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                               "frac": round(achieved / peak, 4), "traffic": dram,
                               "peak_source": peak_kind,
                               "bytes_per_path": round(bpp, 1),
-                              "traffic_source": "profiles/k_trace_dram_instanced_spheres_1080p_16spp.md"
-                              if dram is not None else None}
+                              "kernel": "k_trace (one launch per step)" if args.form == "megakernel" else
+                              "all wavefront kernels of the step (k_wf_extend the largest, ~44 %)",
+                              "traffic_source": source}
     except Exception as exc:  # the oracle library may be absent on a box
         result["roofline"] = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                               "traffic": None, "error": str(exc)[:200]}
@@ -325,6 +338,9 @@ def run_b200(args):
     if not args.no_batch:
         if args.form == "megakernel":
             result["wavefront_same_job"] = same_job_wavefront(dev, acc, spp, paths_per_step, dev_id, flush)
+        else:
+            result["megakernel_same_job"] = same_job_megakernel(args, host, dev, acc, spp, paths_per_step, dev_id,
+                                                                flush)
         del dev, acc, flush
         torch.cuda.empty_cache()
         result["batched"] = mixed_batch(args, dev_id)
@@ -336,7 +352,8 @@ def run_b200(args):
 
 def e2e_context(host, spp, steps):
     """The same job through the public context API with host buffers: commit
-    (host-to-device copy of the bundle), render, read_pixels (device-to-host)."""
+    (host-to-device copy of the bundle), render (which runs the wavefront
+    engine), read_pixels (device-to-host)."""
     from mutracer_b200.context import Context
     ctx = Context()
     b = host.bundle
@@ -357,7 +374,8 @@ def e2e_context(host, spp, steps):
     ctx.destroy()
     return {"value": round(host.width * host.height * spp / dt / 1e6, 3), "unit": "Mpaths/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "ms_per_step": round(dt * 1000, 2), "path": "mt_context_commit_bundle + render + read_pixels"}
+            "ms_per_step": round(dt * 1000, 2),
+            "path": "mt_context_commit_bundle + mt_context_render (wavefront) + mt_context_read_pixels"}
 
 
 def _timed(fn, stream):
@@ -369,6 +387,41 @@ def _timed(fn, stream):
     e.record(stream)
     e.synchronize()
     return s.elapsed_time(e)
+
+
+def same_job_megakernel(args, host, dev, acc, spp, paths, dev_id, flush):
+    """The headline job through the plain drop-in megakernel
+    (mtc_trace_samples), timed like the headline steps, with its own
+    roofline, and checked bit-identical to the wavefront image."""
+    import torch
+    from mutracer_b200 import trace
+    wave = acc.color.clone()
+    mega = trace.Accumulation(host.width, host.height, dev_id)
+    counters = trace.counters_tensor(dev_id)
+    stream = torch.cuda.current_stream()
+    times = []
+    for it in range(4):                   # one warm-up, three timed
+        mega.zero_()
+        flush_l2(flush)
+        ms = _timed(lambda: trace.trace_samples(dev, mega, spp, counters=counters), stream)
+        if it:
+            times.append(ms)
+    ms = sum(times) / len(times)
+    out = {"ms_per_step": round(ms, 2), "mpaths_per_s": round(paths / ms / 1e3, 3),
+           "bit_identical_to_wavefront": bool(torch.equal(mega.color, wave)),
+           "gpu_launches_per_step": 1}
+    peak, kind = load_peaks()
+    try:
+        bpp, _ = oracle_traffic(host)
+        achieved = bpp * paths / (ms / 1000.0) / 1e9
+        dram, source = measured_traffic("megakernel", args, host, spp)
+        out["roofline"] = {"bound": "hbm", "kernel": "k_trace", "achieved": round(achieved, 2), "peak": peak,
+                           "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": dram,
+                           "traffic_source": source, "peak_source": kind}
+    except Exception as exc:
+        out["roofline"] = {"error": str(exc)[:200]}
+    del mega
+    return out
 
 
 def same_job_wavefront(dev, acc, spp, paths, dev_id, flush):

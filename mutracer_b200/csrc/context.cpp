@@ -61,6 +61,7 @@ struct SceneResources {
   DeviceBuffer bvh, ins, attr, mats, env, envDist, lightData, lut, lights;
   DeviceBuffer color, normal, albedo, catcher;
   DeviceBuffer average, flag;  // read_pixels staging: averaged image, non-finite flag
+  DeviceBuffer stream;         // wavefront state of blocking renders (mtc_stream_run)
   mtc_scene_view view{};
   uint32_t width = 0, height = 0;
 };
@@ -142,6 +143,36 @@ void applySettings(Context &c, const mt_render_settings &s) {
 int32_t launch(Context &c, uint32_t samples) {
   mtc_outputs out{c.scene->color.ptr, c.scene->normal.ptr, c.scene->albedo.ptr, c.scene->catcher.ptr};
   return mtc_trace_samples(&c.scene->view, &c.camera, &c.uniform, &out, samples, nullptr, c.stream);
+}
+
+// Blocking renders run the same samples through the wavefront engine
+// (mtc_stream_run: queued traversal and material-regrouped shading), which
+// writes the same bits as mtc_trace_samples at about twice the throughput.
+// Path slots scale with the image, up to 2^20; the state buffer is kept with
+// the scene.  When it cannot be allocated the megakernel renders instead.
+int32_t renderBlocking(Context &c, uint32_t samples) {
+  SceneResources &r = *c.scene;
+  size_t px = size_t(r.width) * r.height;
+  mtc_stream_config cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.struct_size = sizeof(cfg);
+  cfg.slots = uint32_t(std::max<size_t>(1024, std::min<size_t>(px, size_t(1) << 20)));
+  size_t bytes = mtc_stream_state_bytes(1, &cfg);
+  if (bytes == 0 || r.stream.reserve(bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return launch(c, samples);
+  }
+  mtc_job_desc job;
+  std::memset(&job, 0, sizeof(job));
+  job.scene = r.view;
+  job.camera = c.camera;
+  job.uniform = c.uniform;
+  job.out = mtc_outputs{r.color.ptr, r.normal.ptr, r.albedo.ptr, r.catcher.ptr};
+  job.samples = samples;
+  std::vector<char> table(mtc_batch_table_bytes(1));
+  int32_t st = mtc_batch_prepare(&job, 1, nullptr, table.data(), nullptr);
+  if (st != MT_OK) return st;
+  return mtc_stream_run(table.data(), 1, &cfg, r.stream.ptr, nullptr, c.stream);
 }
 
 }  // namespace
@@ -293,7 +324,7 @@ int32_t mt_context_render(mt_context handle, uint32_t additional, char *error, s
     return MT_ERROR_INVALID_ARGUMENT;
   }
   expireJob(*c);
-  int32_t st = launch(*c, additional);
+  int32_t st = renderBlocking(*c, additional);
   if (st != MT_OK) { setError(error, capacity, "launch rejected"); return st; }
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return failContext(*c, e, error, capacity);
