@@ -505,7 +505,8 @@ def mixed_batch(args, dev_id):
         "paths": int(paths), "scene_build_s": round(build_s, 1), "autotune_s": round(tune_s, 1),
         "wavefront_config": {"slots": scfg.slots, "refill_lanes": scfg.refill_lanes,
                              "regroup_interval": scfg.regroup_interval, "sort_rays": scfg.sort_rays,
-                             "steps_per_check": scfg.steps_per_check},
+                             "steps_per_check": scfg.steps_per_check,
+                             "traversal_ctas_per_sm": scfg.traversal_ctas_per_sm},
         "autotune_probe_ms": {k: round(v, 2) for k, v in timings.items()},
         "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["wavefront"]["ms"], 3),
         "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["wavefront"]["ms"], 3),

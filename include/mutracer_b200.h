@@ -337,6 +337,9 @@ typedef struct mtc_stream_config {
                                      octant) before traversal (default 0) */
   uint32_t steps_per_check;       /* traversal steps between refill checks, 1..64
                                      (default 8) */
+  uint32_t traversal_ctas_per_sm; /* resident CTAs of the persistent traversal
+                                     kernels, 1..8 (default 8: full occupancy) */
+  uint32_t _pad[3];
 } mtc_stream_config;
 #define MTC_REGROUP_OFF 0xffffffffu
 size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config);

@@ -126,16 +126,17 @@ class BatchConfig(C.Structure):
 class StreamConfig(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("slots", C.c_uint32), ("iterations_per_check", C.c_uint32),
                 ("max_iterations", C.c_uint32), ("refill_lanes", C.c_uint32), ("regroup_interval", C.c_uint32),
-                ("sort_rays", C.c_uint32), ("steps_per_check", C.c_uint32)]
+                ("sort_rays", C.c_uint32), ("steps_per_check", C.c_uint32),
+                ("traversal_ctas_per_sm", C.c_uint32), ("_pad", C.c_uint32 * 3)]
 
     @classmethod
     def make(cls, slots=0, iterations_per_check=0, max_iterations=0, refill_lanes=0, regroup_interval=0,
-             sort_rays=0, steps_per_check=0):
+             sort_rays=0, steps_per_check=0, traversal_ctas_per_sm=0):
         c = cls()
         c.struct_size = C.sizeof(cls)
         c.slots, c.iterations_per_check, c.max_iterations = slots, iterations_per_check, max_iterations
         c.refill_lanes, c.regroup_interval, c.sort_rays = refill_lanes, regroup_interval, sort_rays
-        c.steps_per_check = steps_per_check
+        c.steps_per_check, c.traversal_ctas_per_sm = steps_per_check, traversal_ctas_per_sm
         return c
 
 

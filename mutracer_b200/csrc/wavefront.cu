@@ -515,11 +515,12 @@ StreamLayout layout(uint32_t capacity, uint32_t slots) {
 }
 
 struct StreamShape {
-  uint32_t slots, iterationsPerCheck, maxIterations, refillLanes, regroupInterval, sortRays, stepsPerCheck;
+  uint32_t slots, iterationsPerCheck, maxIterations, refillLanes, regroupInterval, sortRays, stepsPerCheck,
+      traversalCtasPerSm;
 };
 
 bool streamShape(const mtc_stream_config *c, StreamShape &out) {
-  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u, 0u, 8u};
+  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u, 0u, 8u, 0u};
   if (!c) return true;
   if (c->struct_size != sizeof(mtc_stream_config)) return false;
   if (c->slots) {
@@ -543,6 +544,8 @@ bool streamShape(const mtc_stream_config *c, StreamShape &out) {
     if (c->steps_per_check > 64u) return false;
     out.stepsPerCheck = c->steps_per_check;
   }
+  if (c->traversal_ctas_per_sm > 8u) return false;
+  out.traversalCtasPerSm = c->traversal_ctas_per_sm;
   if (c->refill_lanes) {
     if (c->refill_lanes > 32u) return false;
     out.refillLanes = c->refill_lanes;
@@ -655,6 +658,15 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
       (e = gridFor((const void *)k_wf_regroup, gRegroup)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_sort_rays, gSort)) != cudaSuccess)
     return toStatus(e);
+  if (shape.traversalCtasPerSm) {
+    // Fewer resident traversal warps: a smaller local-memory footprint per SM.
+    int device = 0, sms = 0;
+    if ((e = cudaGetDevice(&device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+      return toStatus(e);
+    gExtend = std::min(gExtend, uint32_t(sms) * shape.traversalCtasPerSm);
+    gShadow = std::min(gShadow, uint32_t(sms) * shape.traversalCtasPerSm);
+  }
   uint32_t *pinned = nullptr;
   if ((e = pinnedWords(&pinned)) != cudaSuccess) return toStatus(e);
   int device = 0;
