@@ -309,6 +309,18 @@ def run_b200(args):
               "mrays_per_s": round(rays_per_step / (ms_per_step / 1000.0) / 1e6, 2),
               "gpu_launches": int(cnt[3]),
               "clocks": clocks.summary()}
+    # End to end through the context API on every rank (its own replica); the
+    # slowest rank sets the step time of the whole job.
+    e2e = None
+    if not args.no_e2e:
+        if world > 1:
+            torch.distributed.barrier()
+        e2e = e2e_context(host, spp, max(1, min(args.steps, 3)))
+        if world > 1:
+            t = torch.tensor([e2e["ms_per_step"]], device=dev_id)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e["ms_per_step"] = round(float(t.item()), 2)
+            e2e["value"] = round(world * paths_per_step / (float(t.item()) / 1000.0) / 1e6, 3)
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -329,13 +341,15 @@ def run_b200(args):
     except Exception as exc:  # the oracle library may be absent on a box
         result["roofline"] = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                               "traffic": None, "error": str(exc)[:200]}
-    try:
-        result["cpu_baseline"] = cpu_baseline(host, spp, args.cpu_seconds)
-    except Exception as exc:
-        result["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
-    if not args.no_e2e:
-        result["e2e"] = e2e_context(host, spp, max(1, min(args.steps, 3)))
-    if not args.no_batch:
+    if e2e is not None:
+        result["e2e"] = e2e
+    # The CPU baseline and the single-GPU batched and served forms run at N=1.
+    if world == 1:
+        try:
+            result["cpu_baseline"] = cpu_baseline(host, spp, args.cpu_seconds)
+        except Exception as exc:
+            result["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    if not args.no_batch and world == 1:
         if args.form == "megakernel":
             result["wavefront_same_job"] = same_job_wavefront(dev, acc, spp, paths_per_step, dev_id, flush)
         else:
