@@ -59,6 +59,9 @@ def parse():
     p.add_argument("--mixed-jobs", type=int, default=64)
     p.add_argument("--mixed-spp-divisor", type=int, default=16,
                    help="scale the mixed jobs' spp (log-uniform 4-256) down by this factor")
+    p.add_argument("--deep-jobs", type=int, default=16)
+    p.add_argument("--deep-spp-divisor", type=int, default=64,
+                   help="scale the deep-transport jobs' 256 spp down by this factor")
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-scenes", type=int, default=8)
@@ -359,6 +362,7 @@ def run_b200(args):
         torch.cuda.empty_cache()
         result["batched"] = mixed_batch(args, dev_id)
         result["served"] = served_stream(args, dev_id)
+        result["deep_transport"] = deep_transport(args, dev_id)
     print(json.dumps(result), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -526,6 +530,46 @@ def mixed_batch(args, dev_id):
         "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["wavefront"]["ms"], 3),
     })
     del jobs
+    torch.cuda.empty_cache()
+    return res
+
+
+def deep_transport(args, dev_id):
+    """Deep transport: concurrent spectral glass-sphere jobs (32 dispersive
+    spheres with scattering interiors, IOR 1.5, Abbe 40, 1 sphere light,
+    bounces 32 -> the reference's 20-event cap, 1280x720), plain per-sample
+    megakernel vs one wavefront pass; images bit-identical."""
+    import torch
+    from mutracer_b200 import batch, scene
+    stream = torch.cuda.current_stream()
+    spp = max(1, 256 // args.deep_spp_divisor)
+    jobs = []
+    for j in range(args.deep_jobs):
+        host = scene.SceneHost("glass_spheres", 1280, 720, j + 1, (32,))
+        jobs.append(batch.RenderJob(scene.DeviceScene(host, dev_id), spp, device=dev_id, job_id=j))
+    paths = batch.total_paths(jobs)
+    sb = batch.StreamBatch(len(jobs), None, None, dev_id)
+    sb.set_jobs(jobs)
+    res = {}
+    ref = None
+    for name, fn in (("plain_per_sample", lambda: batch.run_plain(jobs, per_sample=True)), ("wavefront", sb.run)):
+        ms = []
+        for it in range(2):               # one warm-up, one timed
+            for j in jobs:
+                j.acc.zero_()
+            ms.append(_timed(fn, stream))
+        res[name] = {"ms": round(ms[-1], 2), "mpaths_per_s": round(paths / ms[-1] / 1e3, 3)}
+        imgs = [j.acc.color.clone() for j in jobs]
+        if ref is None:
+            ref = imgs
+        res[name]["bit_identical_to_plain"] = all(torch.equal(a, b) for a, b in zip(imgs, ref))
+    res.update({
+        "workload": f"{len(jobs)} spectral glass jobs (32 dispersive spheres with homogeneous interiors, seeds "
+                    f"1-{len(jobs)}), 1280x720, {spp} spp (256 / {args.deep_spp_divisor}), bounces 32 (20-event cap)",
+        "paths": int(paths),
+        "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["wavefront"]["ms"], 3),
+    })
+    del sb, jobs
     torch.cuda.empty_cache()
     return res
 
