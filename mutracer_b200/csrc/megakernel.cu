@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "dev_shade.cuh"
+#include "js_minmax.h"
 
 using namespace mt;
 
@@ -162,7 +163,7 @@ __device__ void instanceBoundsD(const double *m, const float *local, float *out)
       p[k] = __double2float_rn(__ddiv_rn(v, w));
     }
     if (!isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2])) continue;
-    for (int k = 0; k < 3; k++) { mn[k] = fminf(mn[k], p[k]); mx[k] = fmaxf(mx[k], p[k]); }
+    for (int k = 0; k < 3; k++) { mn[k] = jsMin(mn[k], p[k]); mx[k] = jsMax(mx[k], p[k]); }
   }
   for (int k = 0; k < 3; k++) { out[k] = mn[k]; out[3 + k] = mx[k]; }
 }
@@ -217,7 +218,7 @@ __global__ void k_refit_leaves(float4 *tlas, uint32_t nodeVec4, float *records, 
     const double *m = transforms + size_t(source) * 16;
     float b[6];
     instanceBoundsD(m, localBounds + size_t(source) * 6, b);
-    for (int k = 0; k < 3; k++) { mn[k] = fminf(mn[k], b[k]); mx[k] = fmaxf(mx[k], b[3 + k]); }
+    for (int k = 0; k < 3; k++) { mn[k] = jsMin(mn[k], b[k]); mx[k] = jsMax(mx[k], b[3 + k]); }
     float *rec = records + size_t(target) * 40;
     uint32_t encoded = uint32_t(blasOffsets[source]) | (uint32_t(blasLayouts[source]) << 30);
     rec[0] = __int_as_float(int32_t(encoded));
@@ -245,8 +246,8 @@ __global__ void k_refit_level(float4 *tlas, const int32_t *nodes, uint32_t count
   float4 a = tlas[node], b = tlas[node + 1];
   int32_t right = __float_as_int(a.w);
   float4 l0 = tlas[node + 2], l1 = tlas[node + 3], r0 = tlas[right], r1 = tlas[right + 1];
-  tlas[node] = make_float4(fminf(l0.x, r0.x), fminf(l0.y, r0.y), fminf(l0.z, r0.z), a.w);
-  tlas[node + 1] = make_float4(fmaxf(l1.x, r1.x), fmaxf(l1.y, r1.y), fmaxf(l1.z, r1.z), b.w);
+  tlas[node] = make_float4(jsMin(l0.x, r0.x), jsMin(l0.y, r0.y), jsMin(l0.z, r0.z), a.w);
+  tlas[node + 1] = make_float4(jsMax(l1.x, r1.x), jsMax(l1.y, r1.y), jsMax(l1.z, r1.z), b.w);
 }
 
 // -------------------------------------------------------------- host glue

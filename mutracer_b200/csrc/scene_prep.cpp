@@ -1,5 +1,6 @@
 // Host-side producers of the megakernel's input buffers; see scene_prep.h.
 #include "scene_prep.h"
+#include "js_minmax.h"
 
 #include <algorithm>
 #include <cmath>
@@ -95,12 +96,12 @@ BinnedBvh buildBinnedSahBvh(const float *aabbs, uint32_t count, int bins) {
         binCount[bx]++; binCount[by]++; binCount[bz]++;
         for (int bin : {bx, by, bz}) {
           size_t o = size_t(bin) * 3;
-          binMin[o] = std::min(binMin[o], double(b[0]));
-          binMin[o + 1] = std::min(binMin[o + 1], double(b[1]));
-          binMin[o + 2] = std::min(binMin[o + 2], double(b[2]));
-          binMax[o] = std::max(binMax[o], double(b[3]));
-          binMax[o + 1] = std::max(binMax[o + 1], double(b[4]));
-          binMax[o + 2] = std::max(binMax[o + 2], double(b[5]));
+          binMin[o] = jsMin(binMin[o], double(b[0]));
+          binMin[o + 1] = jsMin(binMin[o + 1], double(b[1]));
+          binMin[o + 2] = jsMin(binMin[o + 2], double(b[2]));
+          binMax[o] = jsMax(binMax[o], double(b[3]));
+          binMax[o + 1] = jsMax(binMax[o + 1], double(b[4]));
+          binMax[o + 2] = jsMax(binMax[o + 2], double(b[5]));
         }
       }
       double splitCost = FAR;
@@ -114,10 +115,10 @@ BinnedBvh buildBinnedSahBvh(const float *aabbs, uint32_t count, int bins) {
           size_t l = (size_t(axis) * BINS + i) * 3;
           size_t rr = (size_t(axis) * BINS + BINS - 1 - i) * 3;
           for (int k = 0; k < 3; k++) {
-            lMin[k] = std::min(lMin[k], binMin[l + k]);
-            lMax[k] = std::max(lMax[k], binMax[l + k]);
-            rMin[k] = std::min(rMin[k], binMin[rr + k]);
-            rMax[k] = std::max(rMax[k], binMax[rr + k]);
+            lMin[k] = jsMin(lMin[k], binMin[l + k]);
+            lMax[k] = jsMax(lMax[k], binMax[l + k]);
+            rMin[k] = jsMin(rMin[k], binMin[rr + k]);
+            rMax[k] = jsMax(rMax[k], binMax[rr + k]);
           }
           leftN += binCount[axis * BINS + i];
           rightN += binCount[axis * BINS + BINS - 1 - i];
@@ -202,24 +203,27 @@ Blas buildBlas(const std::vector<float> &positions, const std::vector<uint32_t> 
   std::vector<float> aabbs(size_t(triCount) * 6);
   std::vector<uint32_t> tris(triCount);
   uint32_t count = 0;
-  float lb[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
   for (uint32_t t = 0; t < triCount; t++) {
+    // triangleBounds (bvhAccel.ts:134-175): Math.min/max over the corners; a
+    // NaN coordinate, or an index past the vertex array (undefined in JS),
+    // makes the box non-finite and the triangle is skipped.
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int c = 0; c < 3; c++) {
-      const float *p = &positions[size_t(indices[t * 3 + c]) * 3];
-      for (int k = 0; k < 3; k++) { mn[k] = std::min(mn[k], p[k]); mx[k] = std::max(mx[k], p[k]); }
+      uint32_t v = indices[t * 3 + c];
+      for (int k = 0; k < 3; k++) {
+        float x = v < b.vertexCount ? positions[size_t(v) * 3 + k] : NAN;
+        mn[k] = jsMin(mn[k], x); mx[k] = jsMax(mx[k], x);
+      }
     }
     bool finite = true;
     for (int k = 0; k < 3; k++) finite = finite && std::isfinite(mn[k]) && std::isfinite(mx[k]);
     if (!finite) continue;
     float *o = &aabbs[size_t(count) * 6];
-    for (int k = 0; k < 3; k++) {
-      o[k] = mn[k]; o[3 + k] = mx[k];
-      lb[k] = std::min(lb[k], mn[k]); lb[3 + k] = std::max(lb[3 + k], mx[k]);
-    }
+    for (int k = 0; k < 3; k++) { o[k] = mn[k]; o[3 + k] = mx[k]; }
     tris[count++] = t;
   }
-  std::memcpy(b.localBounds, lb, sizeof(lb));
+  const float noBounds[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  std::memcpy(b.localBounds, noBounds, sizeof(noBounds));
   if (!count) return b;
   BinnedBvh bvh = buildBinnedSahBvh(aabbs.data(), count, bins);
   Bvh2Layout L = layoutBvh2(bvh);
@@ -243,6 +247,9 @@ Blas buildBlas(const std::vector<float> &positions, const std::vector<uint32_t> 
     }
   }
   b.maxDepth = L.maxDepth;
+  // getBvhBounds (geometryBvhBounds.ts:74-77): a bvh2 BLAS is bounded by its
+  // root node's box.
+  for (int k = 0; k < 3; k++) { b.localBounds[k] = f[k]; b.localBounds[3 + k] = f[4 + k]; }
   return b;
 }
 
@@ -386,7 +393,7 @@ void computeInstanceBounds(const Instance &ins, const float local[6], float out[
                   float((m[1] * x + m[5] * y + m[9] * z + m[13]) / w),
                   float((m[2] * x + m[6] * y + m[10] * z + m[14]) / w)};
     if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) continue;
-    for (int k = 0; k < 3; k++) { mn[k] = std::min(mn[k], p[k]); mx[k] = std::max(mx[k], p[k]); }
+    for (int k = 0; k < 3; k++) { mn[k] = jsMin(mn[k], p[k]); mx[k] = jsMax(mx[k], p[k]); }
   }
   for (int k = 0; k < 3; k++) { out[k] = mn[k]; out[3 + k] = mx[k]; }
 }
@@ -458,8 +465,8 @@ void refitTlasHost(float *tlas, float *records, const std::vector<Instance> &ins
       refitNode(child);
       size_t left = base + 8, right = size_t(child) * 4;
       for (int k = 0; k < 3; k++) {
-        tlas[base + k] = std::min(tlas[left + k], tlas[right + k]);
-        tlas[base + 4 + k] = std::max(tlas[left + 4 + k], tlas[right + 4 + k]);
+        tlas[base + k] = jsMin(tlas[left + k], tlas[right + k]);
+        tlas[base + 4 + k] = jsMax(tlas[left + 4 + k], tlas[right + 4 + k]);
       }
       return;
     }
@@ -470,7 +477,7 @@ void refitTlasHost(float *tlas, float *records, const std::vector<Instance> &ins
       const Instance &ins = instances[source];
       float b[6];
       computeInstanceBounds(ins, blases[ins.blasIndex].localBounds, b);
-      for (int k = 0; k < 3; k++) { mn[k] = std::min(mn[k], b[k]); mx[k] = std::max(mx[k], b[3 + k]); }
+      for (int k = 0; k < 3; k++) { mn[k] = jsMin(mn[k], b[k]); mx[k] = jsMax(mx[k], b[3 + k]); }
       int32_t target = asInt(tlas[record]);
       writeInstanceRecord(records + size_t(target) * 40, ins, blasOffsets[ins.blasIndex], vertexOffsets[ins.blasIndex],
                           blasLayout);

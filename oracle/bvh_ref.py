@@ -4,8 +4,11 @@ producer in mutracer_b200/csrc/scene_prep.cpp bit for bit on small inputs.
 
 Follows src/renderer/binnedSahBvh.ts:70-236 (buildBinnedSahBvh) and :252-275
 (layoutBvh2): float64 arithmetic on values stored as float32 (the JS
-Float32Array bounds/centers and Float64Array bins).
+Float32Array bounds/centers and Float64Array bins), with JavaScript's
+Math.min / Math.max (js_min / js_max) where the reference calls them.
 """
+import math
+
 import numpy as np
 
 FAR = 1e30
@@ -13,6 +16,24 @@ FAR = 1e30
 
 def _f32(x):
     return float(np.float32(x))
+
+
+def js_min(a, b):
+    """JavaScript Math.min: NaN if either is NaN; -0 below +0."""
+    if a != a or b != b:
+        return float("nan")
+    if a == b:
+        return a if math.copysign(1.0, a) < 0 else b
+    return b if b < a else a
+
+
+def js_max(a, b):
+    """JavaScript Math.max: NaN if either is NaN; +0 above -0."""
+    if a != a or b != b:
+        return float("nan")
+    if a == b:
+        return b if math.copysign(1.0, a) < 0 else a
+    return b if b > a else a
 
 
 def _to_int32(v):
@@ -43,8 +64,8 @@ def build_binned_sah(aabbs, bins=8):
     for i in range(count):
         for k in range(3):
             centers[i, k] = _f32((a[i, k] + a[i, 3 + k]) * 0.5)
-            root_min[k] = min(root_min[k], a[i, k]) if a[i, k] < root_min[k] else root_min[k]
-            root_max[k] = a[i, 3 + k] if a[i, 3 + k] > root_max[k] else root_max[k]
+            root_min[k] = float(a[i, k]) if a[i, k] < root_min[k] else root_min[k]
+            root_max[k] = float(a[i, 3 + k]) if a[i, 3 + k] > root_max[k] else root_max[k]
         prim[i] = i
     bounds[0, :3] = root_min
     bounds[0, 3:] = root_max
@@ -79,8 +100,8 @@ def build_binned_sah(aabbs, bins=8):
                     b = axis * bins + bin_of(float(centers[p, axis]), nmin[axis], scale[axis])
                     bcnt[b] += 1
                     for k in range(3):
-                        bmin[b][k] = min(bmin[b][k], a[p, k])
-                        bmax[b][k] = max(bmax[b][k], a[p, 3 + k])
+                        bmin[b][k] = js_min(bmin[b][k], float(a[p, k]))
+                        bmax[b][k] = js_max(bmax[b][k], float(a[p, 3 + k]))
             split_cost, best_axis, best_pos = FAR, 0, 0
             for axis in range(3):
                 if not extent[axis] > min_dim[axis]:
@@ -92,8 +113,8 @@ def build_binned_sah(aabbs, bins=8):
                 for i in range(bins - 1):
                     l, r = axis * bins + i, axis * bins + bins - 1 - i
                     for k in range(3):
-                        lmin[k] = min(lmin[k], bmin[l][k]); lmax[k] = max(lmax[k], bmax[l][k])
-                        rmin[k] = min(rmin[k], bmin[r][k]); rmax[k] = max(rmax[k], bmax[r][k])
+                        lmin[k] = js_min(lmin[k], bmin[l][k]); lmax[k] = js_max(lmax[k], bmax[l][k])
+                        rmin[k] = js_min(rmin[k], bmin[r][k]); rmax[k] = js_max(rmax[k], bmax[r][k])
                     ln += bcnt[l]
                     rn += bcnt[r]
                     lx, ly, lz = lmax[0] - lmin[0], lmax[1] - lmin[1], lmax[2] - lmin[2]

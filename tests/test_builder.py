@@ -3,6 +3,7 @@ Python restatement in oracle/bvh_ref.py (bit-exact), plus the structural
 invariants of the reference's tests/unit/binnedSahBvh.test.ts:71-260 and
 tests/unit/bvhAccel.test.ts:27-260."""
 import ctypes as C
+import math
 
 import numpy as np
 import pytest
@@ -151,3 +152,49 @@ def test_instance_record_and_refit_host():
     before = host.bvh.copy()
     host.refit_host()  # unchanged transforms: refit reproduces the build exactly
     assert np.array_equal(host.bvh.view(np.uint32), before.view(np.uint32))
+
+
+def test_js_min_max_rules():
+    nz = -0.0
+    assert math.copysign(1, bvh_ref.js_min(0.0, nz)) < 0 and math.copysign(1, bvh_ref.js_min(nz, 0.0)) < 0
+    assert math.copysign(1, bvh_ref.js_max(0.0, nz)) > 0 and math.copysign(1, bvh_ref.js_max(nz, 0.0)) > 0
+    assert math.isnan(bvh_ref.js_min(1.0, float("nan"))) and math.isnan(bvh_ref.js_max(float("nan"), 1.0))
+    assert bvh_ref.js_min(2.0, 1.0) == 1.0 and bvh_ref.js_max(2.0, 1.0) == 2.0
+
+
+def test_signed_zero_bounds_follow_math_min():
+    """Bins merge with Math.min / Math.max (-0 below +0 in any order); the
+    root box keeps the first strictly smaller value (`<`)."""
+    nz = np.float32(-0.0)
+    boxes = np.array([[0, 0, 0, 1, 1, 1], [nz, nz, 0, 1, 1, 1], [100, 0, 0, 101, 1, 1], [100, 0, 0, 101, 1, 1]],
+                     np.float32)
+    got = cpp_build(boxes, 8)
+    m, bounds, lf, pc, pi = bvh_ref.build_binned_sah(boxes, 8)
+    assert got[0] == m == 3
+    assert np.array_equal(got[1].view(np.uint32), bounds[:m].view(np.uint32))
+    assert np.array_equal(got[4], pi)
+    left = int(lf[0])
+    assert np.signbit(bounds[left, 0]) and np.signbit(bounds[left, 1])   # Math.min(+0, -0) = -0
+    assert not np.signbit(bounds[0, 0]) and not np.signbit(bounds[0, 1])  # root: first of equal values
+
+
+def test_blas_skips_nan_and_out_of_range_triangles():
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [np.nan, 0, 0], [5, 5, 5], [6, 5, 5], [5, 6, 5]], np.float32)
+    idx = np.array([[0, 1, 2], [0, 3, 2], [4, 5, 6], [0, 1, 99]], np.uint32)
+    L = abi.lib()
+    vec4, depth = C.c_uint64(), C.c_uint32()
+    assert L.mtp_build_blas(pos.ctypes.data, len(pos), idx.ctypes.data, len(idx), 8, None, 0, C.byref(vec4),
+                            C.byref(depth)) == 0
+    buf = np.zeros(vec4.value * 4, np.float32)
+    assert L.mtp_build_blas(pos.ctypes.data, len(pos), idx.ctypes.data, len(idx), 8, buf.ctypes.data, vec4.value,
+                            C.byref(vec4), C.byref(depth)) == 0
+    words = buf.view(np.int32).reshape(-1, 4)
+    leaves = []
+    stack = [0]
+    while stack:
+        o = stack.pop()
+        if words[o, 3] >= 0:
+            stack += [o + 2, int(words[o, 3])]
+        else:
+            leaves += [tuple(words[o + 2 + i, :3]) for i in range(-words[o, 3])]
+    assert sorted(leaves) == [(0, 1, 2), (4, 5, 6)]
