@@ -251,6 +251,51 @@ mt_status mtc_refit_tlas(void *tlas, uint64_t tlas_vec4_count, void *instances,
 mt_status mtc_average_output(const void *accum, uint32_t pixels, uint32_t samples,
                              void *out, uint32_t *nonfinite_flag, void *stream);
 
+/* ------------------------------------------------ BLAS build on the device */
+/* buildBLAS (src/renderer/bvhAccel.ts:200-286, without displacement) on the
+ * GPU: the per-triangle boxes of triangleBounds (bvhAccel.ts:134-175; a
+ * triangle whose box is not finite, or that indexes past the vertex array, is
+ * skipped), the binned-SAH build of src/renderer/binnedSahBvh.ts:70-236
+ * (float64 binning and costs, JavaScript Math.min/max, the same in-place
+ * partition order) and the depth-first BVH2 layout of binnedSahBvh.ts:252-275
+ * (BLAS layout code 0), written to `out_bvh`.  The buffer is bit-identical to
+ * the reference producer's for the same positions, indices and bins. */
+typedef struct mtc_blas_build_input {
+  uint32_t struct_size;
+  uint32_t bins;                   /* SAH bins, 1..64 (buildBLAS uses 8) */
+  const float *positions;          /* device: xyz f32 per vertex */
+  const uint32_t *indices;         /* device: 3 u32 per triangle */
+  uint32_t vertex_count;
+  uint32_t triangle_count;
+} mtc_blas_build_input;
+
+typedef struct mtc_blas_build_result {
+  uint32_t struct_size;
+  uint32_t vec4_count;             /* length of the BVH2 buffer written */
+  uint32_t max_depth;              /* layoutBvh2 maxDepth (traversal stack bound) */
+  uint32_t max_leaf_primitives;
+  uint32_t node_count;
+  uint32_t primitive_count;        /* triangles with a finite box */
+  float local_bounds[6];           /* root box, getBvhBounds (geometryBvhBounds.ts:74-77) */
+  uint32_t host_syncs;             /* stream synchronisations the build made */
+  uint32_t _pad[3];
+} mtc_blas_build_result;
+
+/* Device scratch bytes mtc_build_blas needs for `triangle_count` triangles. */
+uint64_t mtc_blas_build_scratch_bytes(uint32_t triangle_count, uint32_t bins);
+/* Upper bound of the BVH2 length (vec4 units) for `triangle_count` triangles:
+ * 2 per node (at most 2n - 1 nodes) plus one per triangle. */
+uint64_t mtc_blas_build_max_vec4(uint32_t triangle_count);
+/* No reference counterpart as an entry point: it replaces the host-side
+ * buildBLAS call above.  Runs on `stream` and returns once `out_bvh` is
+ * complete (the top of the tree is built level by level, reading one counter
+ * back per level).  result->struct_size must be set by the caller.
+ * MT_ERROR_BUFFER_TOO_SMALL if the layout needs more than out_capacity_vec4
+ * (result->vec4_count then holds the length needed). */
+mt_status mtc_build_blas(const mtc_blas_build_input *input, void *scratch, uint64_t scratch_bytes,
+                         float *out_bvh, uint64_t out_capacity_vec4, mtc_blas_build_result *result,
+                         void *stream);
+
 /* ------------------------------------------------------ batched form */
 /* One render job of a batched launch: its own scene view, camera, uniform
  * and outputs.  All jobs of a batch run in one persistent kernel that pulls

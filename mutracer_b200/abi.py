@@ -140,6 +140,17 @@ class StreamConfig(C.Structure):
         return c
 
 
+class BlasBuildInput(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("bins", C.c_uint32), ("positions", C.c_void_p),
+                ("indices", C.c_void_p), ("vertex_count", C.c_uint32), ("triangle_count", C.c_uint32)]
+
+
+class BlasBuildResult(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("vec4_count", C.c_uint32), ("max_depth", C.c_uint32),
+                ("max_leaf_primitives", C.c_uint32), ("node_count", C.c_uint32), ("primitive_count", C.c_uint32),
+                ("local_bounds", C.c_float * 6), ("host_syncs", C.c_uint32), ("_pad", C.c_uint32 * 3)]
+
+
 class SceneBundle(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("flags", C.c_uint32),
@@ -185,7 +196,8 @@ class SceneInfo(C.Structure):
 
 
 STRUCT_ORDER = [TraceUniform, CameraUniform, SceneView, Outputs, Hit, Counters, JobDesc, BatchConfig,
-                SceneBundle, RenderSettings, ContextSnapshot, JobSnapshot, SceneInfo, StreamConfig]
+                SceneBundle, RenderSettings, ContextSnapshot, JobSnapshot, SceneInfo, StreamConfig, BlasBuildInput,
+                BlasBuildResult]
 
 _lib = None
 
@@ -209,6 +221,10 @@ def _declare(lib):
         "mtc_batch_launch": (C.c_int32, [P, C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
         "mtc_trace_batch_noalloc": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P]),
         "mtc_refit_tlas": (C.c_int32, [P, C.c_uint64, P, C.c_uint32, P, P, P, P, P, P, P, P]),
+        "mtc_blas_build_scratch_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32]),
+        "mtc_blas_build_max_vec4": (C.c_uint64, [C.c_uint32]),
+        "mtc_build_blas": (C.c_int32, [C.POINTER(BlasBuildInput), P, C.c_uint64, P, C.c_uint64,
+                                        C.POINTER(BlasBuildResult), P]),
         "mtp_scene_make": (P, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), C.c_uint32]),
         "mtp_scene_free": (None, [P]),
         "mtp_scene_bundle": (C.c_int, [P, C.POINTER(SceneBundle)]),
@@ -218,6 +234,7 @@ def _declare(lib):
         "mtp_scene_set_transforms": (C.c_int, [P, P, C.c_uint32]),
         "mtp_scene_refit_host": (C.c_int, [P]),
         "mtp_scene_set_blas_layout": (C.c_int, [P, C.c_uint32]),
+        "mtp_scene_mesh": (C.c_int, [P, C.c_uint32, P, P, P, P, P, P, P]),
         "mtp_build_binned_sah": (C.c_int, [P, C.c_uint32, C.c_int, P, P, P, P, P]),
         "mtp_build_blas": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.c_int, P, C.c_uint64, P, P]),
         "mtp_energy_lut": (C.c_int, [P]),

@@ -179,6 +179,23 @@ int mtp_build_blas(const float *positions, uint32_t vertexCount, const uint32_t 
   return MT_OK;
 }
 
+int mtp_scene_mesh(void *scene, uint32_t mesh, float *positions, uint32_t *indices, uint32_t *vertexCount,
+                   uint32_t *triangleCount, uint32_t *blasOffset, uint32_t *blasVec4, uint32_t *bins) {
+  if (!scene) return MT_ERROR_INVALID_ARGUMENT;
+  SceneHost &s = *static_cast<SceneHost *>(scene);
+  if (mesh >= s.sourceIndices.size()) return MT_ERROR_INVALID_ARGUMENT;
+  const std::vector<float> &p = s.sourcePositions[mesh];
+  const std::vector<uint32_t> &ix = s.sourceIndices[mesh];
+  if (vertexCount) *vertexCount = uint32_t(p.size() / 3);
+  if (triangleCount) *triangleCount = uint32_t(ix.size() / 3);
+  if (blasOffset) *blasOffset = s.tlasVec4 + s.blasOffsets[mesh];
+  if (blasVec4) *blasVec4 = uint32_t(s.blases[mesh].buffer.size() / 4);
+  if (bins) *bins = s.blasBins;
+  if (positions) std::memcpy(positions, p.data(), p.size() * 4);
+  if (indices) std::memcpy(indices, ix.data(), ix.size() * 4);
+  return MT_OK;
+}
+
 int mtp_energy_lut(float *out) {
   if (!out) return MT_ERROR_INVALID_ARGUMENT;
   std::vector<float> lut;

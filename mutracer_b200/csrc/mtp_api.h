@@ -29,6 +29,11 @@ int mtp_scene_set_transforms(void *scene, const double *transforms, uint32_t cou
 int mtp_scene_refit_host(void *scene);
 /* Re-encodes the scene's BLASes in layout code 0 (BVH2) or 2 (BVH_GPU). */
 int mtp_scene_set_blas_layout(void *scene, uint32_t layout);
+// Source mesh `mesh` of the scene (the input of its BLAS) and where that BLAS
+// lies in the scene's bvh buffer (vec4 units).  NULL positions/indices query
+// the counts only.
+int mtp_scene_mesh(void *scene, uint32_t mesh, float *positions, uint32_t *indices, uint32_t *vertexCount,
+                   uint32_t *triangleCount, uint32_t *blasOffset, uint32_t *blasVec4, uint32_t *bins);
 int mtp_build_binned_sah(const float *aabbs, uint32_t count, int bins, uint32_t *nodeCount, float *bounds,
                          uint32_t *leftFirst, uint32_t *primCount, uint32_t *primIndices);
 int mtp_build_blas(const float *positions, uint32_t vertexCount, const uint32_t *indices, uint32_t triCount, int bins,

@@ -902,6 +902,13 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   for (const Instance &ins : instances) s.triangleCount += meshes[ins.blasIndex].indices.size() / 3;
   Tlas tlas = buildTlas(instances, s.blases, s.blasOffsets, s.vertexOffsets, tlasBins);
   s.sourceInstances = instances;
+  s.sourcePositions.clear();
+  s.sourceIndices.clear();
+  for (const MeshData &md : meshes) {
+    s.sourcePositions.push_back(md.positions);
+    s.sourceIndices.push_back(md.indices);
+  }
+  s.blasBins = uint32_t(blasBins);
   s.tlasVec4 = uint32_t(tlas.buffer.size() / 4);
   s.bvh = tlas.buffer;
   for (const Blas &b : s.blases) s.bvh.insert(s.bvh.end(), b.buffer.begin(), b.buffer.end());

@@ -122,6 +122,9 @@ struct SceneHost {
   std::vector<Blas> blases;
   std::vector<Instance> sourceInstances;
   std::vector<uint32_t> blasOffsets, vertexOffsets;
+  std::vector<std::vector<float>> sourcePositions;     // per BLAS: xyz f32 per vertex
+  std::vector<std::vector<uint32_t>> sourceIndices;    // per BLAS: 3 per triangle
+  uint32_t blasBins = 8;
   uint32_t blasLayout = 0;  // BLAS layout code of every instance (0 BVH2, 2 BVH_GPU)
   uint64_t triangleCount = 0, uniqueTriangleCount = 0;
   std::string name;

@@ -129,6 +129,18 @@ class SceneHost:
         abi.check(abi.lib().mtp_scene_set_blas_layout(self._handle, layout))
         self.refresh()
 
+    def mesh(self, m):
+        """Source mesh `m` (the input of BLAS m): (positions (V, 3) f32,
+        indices (T, 3) u32, BLAS offset in bvh (vec4), BLAS length (vec4),
+        SAH bins)."""
+        L = abi.lib()
+        u = [C.c_uint32() for _ in range(5)]
+        abi.check(L.mtp_scene_mesh(self._handle, m, None, None, *[C.byref(x) for x in u]))
+        pos = np.zeros((u[0].value, 3), np.float32)
+        idx = np.zeros((u[1].value, 3), np.uint32)
+        abi.check(L.mtp_scene_mesh(self._handle, m, pos.ctypes.data, idx.ctypes.data, *[C.byref(x) for x in u]))
+        return pos, idx, u[2].value, u[3].value, u[4].value
+
     def refit_host(self):
         abi.check(abi.lib().mtp_scene_refit_host(self._handle))
 
