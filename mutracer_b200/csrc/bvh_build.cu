@@ -41,7 +41,7 @@
 
 namespace {
 
-constexpr uint32_t kSmallLimit = 1024;  // subtree roots this small are finished by one CTA
+constexpr uint32_t kSmallLimit = 256;   // subtree roots this small are finished by one warp
 constexpr uint32_t kChunk = 2048;       // primitives per CTA in the level-synchronous phase
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
@@ -55,6 +55,7 @@ constexpr uint32_t kMaxIdentity = 0u;
 struct Globals {
   uint32_t nodeAlloc, activeNext, smallCount, maxDepth;
   uint32_t totalChunks, primCount, maxLeaf, error;  // error: a rank fell outside its node (never expected)
+  uint32_t holes, pad;                                 // node ids reserved by subtree warps and left unused
   double minDim[3];
   unsigned long long rootKey[6];
 };
@@ -66,7 +67,7 @@ struct LargeNode {
   double nMin[3], scale[3];
   float childBounds[12];
   uint32_t node, first, count, depth;
-  uint32_t chunkBegin, chunkCount, leftN, state;
+  uint32_t leftN, state;
   int32_t axis, pos;
 };
 
@@ -77,7 +78,7 @@ struct Scratch {
   float *nodeBounds;
   uint32_t *nodeFirst, *nodeCount, *nodeDepth, *nodeSize, *nodeOffset, *byDepth, *depthCursor;
   int32_t *nodeChild;
-  uint32_t *activeA, *activeB, *smallQ, *chunkR, *bins;
+  uint32_t *activeA, *activeB, *smallQ, *chunkR, *chunkStart, *bins;
   LargeNode *large;
   uint32_t maxActive, maxChunks, nodeCap, binWords;
 };
@@ -119,6 +120,7 @@ size_t carve(Scratch &s, char *base, uint32_t n, uint32_t bins) {
   s.activeB = take<uint32_t>(base, off, s.maxActive);
   s.smallQ = take<uint32_t>(base, off, s.nodeCap);
   s.chunkR = take<uint32_t>(base, off, s.maxChunks);
+  s.chunkStart = take<uint32_t>(base, off, size_t(s.maxActive) + 1);
   s.bins = take<uint32_t>(base, off, size_t(s.maxActive) * s.binWords);
   s.large = take<LargeNode>(base, off, s.maxActive);
   return off;
@@ -143,8 +145,8 @@ __device__ __forceinline__ uint32_t collapsedKey(float f) { return f == 0.0f ? 0
 
 // JavaScript `v | 0` (ToInt32).
 __device__ __forceinline__ int32_t jsInt32(double v) {
+  if (fabs(v) < 2147483648.0) return __double2int_rz(v);  // NaN fails the test
   if (!(v == v) || isinf(v)) return 0;
-  if (fabs(v) < 2147483648.0) return __double2int_rz(v);
   double m = fmod(trunc(v), 4294967296.0);
   if (m < 0) m += 4294967296.0;
   return int32_t(uint32_t(m));
@@ -205,101 +207,133 @@ __device__ uint32_t blockExclusiveSum(uint32_t v, uint32_t &total) {
 }
 
 // --------------------------------------------------- split decision (SAH)
+// Surface-area term of binnedSahBvh.ts:177-178 for bounds given as ordered
+// keys: the reference's running bounds start at FAR / -FAR, hence the clamps.
+// Math.min(FAR, v) / Math.max(-FAR, v) for a finite f32 v (never equal to FAR).
+__device__ __forceinline__ double farMin(float v) { return double(v) < kFar ? double(v) : kFar; }
+__device__ __forceinline__ double farMax(float v) { return double(v) > -kFar ? double(v) : -kFar; }
+__device__ __forceinline__ double keyArea(uint32_t lo0, uint32_t lo1, uint32_t lo2, uint32_t hi0, uint32_t hi1,
+                                          uint32_t hi2) {
+  double x = DA(farMax(keyValue(hi0)), -farMin(keyValue(lo0)));
+  double y = DA(farMax(keyValue(hi1)), -farMin(keyValue(lo1)));
+  double z = DA(farMax(keyValue(hi2)), -farMin(keyValue(lo2)));
+  return areaOf(x, y, z);
+}
+
 struct Decision {
   uint32_t state, leftN;
   int32_t axis, pos;
-  float childBounds[12];
+  float laneBound;  // lane j < 12: component j of the child boxes (left min xyz, max xyz, then right)
 };
 
 // The bins of one node: counts[3B], min keys[3B*3], max keys[3B*3].
 struct BinView {
   const uint32_t *w;
   int B;
-  __device__ double mn(int bin, int k) const {
-    return w[bin] ? jsMin(kFar, double(keyValue(w[3 * B + bin * 3 + k]))) : kFar;
-  }
-  __device__ double mx(int bin, int k) const {
-    return w[bin] ? jsMax(-kFar, double(keyValue(w[12 * B + bin * 3 + k]))) : -kFar;
-  }
 };
 
 // binnedSahBvh.ts:154-183 (sweep), :184-187 (leaf test) and :211-225 (child
-// boxes).  Lanes 0-2 sweep one axis each (cost rows in `cost`, 6 * (B - 1)
-// doubles of this warp); lane 0 combines them in axis order and returns the
-// decision (valid on lane 0 only).
-__device__ Decision decideSplit(const BinView &bins, const float nb[6], uint32_t count, const double minDim[3],
-                                double *cost) {
-  const int B = bins.B, lane = threadIdx.x & 31;
-  double nMin[3], ext[3];
+// boxes), one warp per node.  The reference sweeps each axis keeping running
+// bounds; Math.min/max are exact, so each split candidate (axis, position) is
+// evaluated on its own lane from its bins directly (the side bounds as min/max
+// of ordered keys, then the same float64 operations on the same values), and
+// the warp keeps the first candidate in the reference's (axis, position) order
+// among the cheapest, as its strict `<` does.  The child boxes are 12 lanes, each folding its side's bins in bin
+// order with the reference's strict comparison against the f32-stored box.
+// Every lane returns the decision.
+__device__ Decision decideSplit(const BinView &bins, const float nb[6], uint32_t count, const double minDim[3]) {
+  const int B = bins.B, lane = threadIdx.x & 31, candidates = 3 * (B - 1);
+  double ext[3];
+  uint32_t splittable = 0;  // axes with extent > minDim (binnedSahBvh.ts:159)
   for (int k = 0; k < 3; k++) {
-    nMin[k] = nb[k];
-    ext[k] = DA(double(nb[3 + k]), -nMin[k]);
+    ext[k] = DA(double(nb[3 + k]), -double(nb[k]));
+    splittable |= uint32_t(ext[k] > minDim[k]) << k;
   }
-  double best = kFar;
-  int bestPos = 0;
-  if (lane < 3 && ext[lane] > minDim[lane]) {
-    const int axis = lane;
-    double *leftCost = cost + axis * 2 * (B - 1), *rightCost = leftCost + (B - 1);
-    double lMin[3] = {kFar, kFar, kFar}, lMax[3] = {-kFar, -kFar, -kFar};
-    double rMin[3] = {kFar, kFar, kFar}, rMax[3] = {-kFar, -kFar, -kFar};
-    uint32_t leftN = 0, rightN = 0;
-    for (int i = 0; i < B - 1; i++) {
-      int l = axis * B + i, r = axis * B + B - 1 - i;
-      for (int k = 0; k < 3; k++) {
-        lMin[k] = jsMin(lMin[k], bins.mn(l, k));
-        lMax[k] = jsMax(lMax[k], bins.mx(l, k));
-        rMin[k] = jsMin(rMin[k], bins.mn(r, k));
-        rMax[k] = jsMax(rMax[k], bins.mx(r, k));
-      }
-      leftN += bins.w[l];
-      rightN += bins.w[r];
-      double la = areaOf(DA(lMax[0], -lMin[0]), DA(lMax[1], -lMin[1]), DA(lMax[2], -lMin[2]));
-      double ra = areaOf(DA(rMax[0], -rMin[0]), DA(rMax[1], -rMin[1]), DA(rMax[2], -rMin[2]));
-      leftCost[i] = leftN == 0 ? kFar : DM(la, double(leftN));
-      rightCost[B - 2 - i] = rightN == 0 ? kFar : DM(ra, double(rightN));
-    }
-    for (int i = 0; i < B - 1; i++) {
-      double c = DA(leftCost[i], rightCost[i]);
-      if (c < best) {
-        best = c;
-        bestPos = i;
+  double bestCost = INFINITY;
+  int bestKey = candidates;
+  for (int c = lane; c < candidates; c += 32) {
+    const int axis = c / (B - 1), pos = c - axis * (B - 1);
+    if (!(splittable >> axis & 1u)) continue;
+    // Bounds of each side as ordered keys (their min/max are Math.min/max
+    // of the values); an empty side costs FAR whatever its bounds.
+    uint32_t lLo0 = kMinIdentity, lLo1 = kMinIdentity, lLo2 = kMinIdentity;
+    uint32_t lHi0 = kMaxIdentity, lHi1 = kMaxIdentity, lHi2 = kMaxIdentity;
+    uint32_t rLo0 = kMinIdentity, rLo1 = kMinIdentity, rLo2 = kMinIdentity;
+    uint32_t rHi0 = kMaxIdentity, rHi1 = kMaxIdentity, rHi2 = kMaxIdentity;
+    uint32_t nLeft = 0, nRight = 0;
+    for (int i = 0; i < B; i++) {
+      const int bin = axis * B + i;
+      const uint32_t *lo = bins.w + 3 * B + bin * 3, *hi = bins.w + 12 * B + bin * 3;
+      if (i <= pos) {
+        nLeft += bins.w[bin];
+        lLo0 = min(lLo0, lo[0]); lLo1 = min(lLo1, lo[1]); lLo2 = min(lLo2, lo[2]);
+        lHi0 = max(lHi0, hi[0]); lHi1 = max(lHi1, hi[1]); lHi2 = max(lHi2, hi[2]);
+      } else {
+        nRight += bins.w[bin];
+        rLo0 = min(rLo0, lo[0]); rLo1 = min(rLo1, lo[1]); rLo2 = min(rLo2, lo[2]);
+        rHi0 = max(rHi0, hi[0]); rHi1 = max(rHi1, hi[1]); rHi2 = max(rHi2, hi[2]);
       }
     }
+    double sideCost[2] = {kFar, kFar};
+    if (nLeft) sideCost[0] = DM(keyArea(lLo0, lLo1, lLo2, lHi0, lHi1, lHi2), double(nLeft));
+    if (nRight) sideCost[1] = DM(keyArea(rLo0, rLo1, rLo2, rHi0, rHi1, rHi2), double(nRight));
+    double cost = DA(sideCost[0], sideCost[1]);
+    if (cost < bestCost) {  // candidates of a lane come in increasing order
+      bestCost = cost;
+      bestKey = c;
+    }
   }
-  double best1 = __shfl_sync(0xffffffffu, best, 1), best2 = __shfl_sync(0xffffffffu, best, 2);
-  int pos1 = __shfl_sync(0xffffffffu, bestPos, 1), pos2 = __shfl_sync(0xffffffffu, bestPos, 2);
+  for (int o = 16; o; o >>= 1) {
+    double oc = __shfl_xor_sync(0xffffffffu, bestCost, o);
+    int ok = __shfl_xor_sync(0xffffffffu, bestKey, o);
+    if (oc < bestCost || (oc == bestCost && ok < bestKey)) {
+      bestCost = oc;
+      bestKey = ok;
+    }
+  }
   Decision d;
   d.state = kLeaf;
   d.leftN = 0;
   d.axis = 0;
   d.pos = 0;
-  if (lane != 0) return d;
   double split = kFar;
-  if (best < split) { split = best; d.axis = 0; d.pos = bestPos; }
-  if (best1 < split) { split = best1; d.axis = 1; d.pos = pos1; }
-  if (best2 < split) { split = best2; d.axis = 2; d.pos = pos2; }
-  double area = areaOf(ext[0], ext[1], ext[2]);
-  split = DA(1.0, __ddiv_rn(split, area));  // C_TRAV + C_INT * cost / area
+  if (bestCost < kFar) {
+    split = bestCost;
+    d.axis = bestKey / (B - 1);
+    d.pos = bestKey - d.axis * (B - 1);
+  }
+  split = DA(1.0, __ddiv_rn(split, areaOf(ext[0], ext[1], ext[2])));  // C_TRAV + C_INT * cost / area
   if (!(split < double(count))) return d;
   uint32_t leftN = 0;
   for (int i = 0; i <= d.pos; i++) leftN += bins.w[d.axis * B + i];
   d.leftN = leftN;
   d.state = (leftN == 0 || leftN == count) ? kPartitionLeaf : kSplit;
-  const float farF = float(kFar);
-  for (int c = 0; c < 2; c++)
-    for (int k = 0; k < 3; k++) {
-      d.childBounds[c * 6 + k] = farF;
-      d.childBounds[c * 6 + 3 + k] = -farF;
-    }
-  for (int i = 0; i < B; i++) {
-    int bin = d.axis * B + i;
-    float *base = d.childBounds + (i <= d.pos ? 0 : 6);
-    for (int k = 0; k < 3; k++) {
-      double lo = bins.mn(bin, k), hi = bins.mx(bin, k);
-      if (lo < double(base[k])) base[k] = __double2float_rn(lo);
-      if (hi > double(base[3 + k])) base[3 + k] = __double2float_rn(hi);
+  // Child boxes (binnedSahBvh.ts:215-224): the box starts at f32(FAR) and
+  // takes a bin's bound when strictly smaller.  An empty bin's FAR, or a
+  // bound at or beyond FAR, stores f32(FAR) again, so only the non-empty
+  // bins' f32 values matter, clamped to f32(FAR); the first of equal values
+  // stays.
+  float v = 0.0f;
+  if (lane < 12) {
+    const int side = lane / 6, comp = lane % 6, k = comp % 3;
+    const bool isMax = comp >= 3;
+    const float far = float(kFar);
+    v = isMax ? -far : far;
+    const uint32_t *keys = bins.w + (isMax ? 12 * B : 3 * B) + k;
+    for (int i = side ? d.pos + 1 : 0; i < (side ? B : d.pos + 1); i++) {
+      const int bin = d.axis * B + i;
+      if (!bins.w[bin]) continue;
+      float x = keyValue(keys[bin * 3]);
+      if (isMax) {
+        x = x > -far ? x : -far;
+        if (x > v) v = x;
+      } else {
+        x = x < far ? x : far;
+        if (x < v) v = x;
+      }
     }
   }
+  d.laneBound = v;
   return d;
 }
 
@@ -352,6 +386,7 @@ __global__ void k_init(Globals *g) {
   g->primCount = 0;
   g->maxLeaf = 0;
   g->error = 0;
+  g->holes = 0;
   for (int k = 0; k < 3; k++) {
     g->rootKey[k] = ~0ull;
     g->rootKey[3 + k] = 0ull;
@@ -476,54 +511,43 @@ __global__ void k_root_finalize(Scratch s) {
 }
 
 // ------------------------------------------- level-synchronous phase
-__global__ void __launch_bounds__(1024) k_large_setup(Scratch s, const uint32_t *active, uint32_t activeCount,
-                                                      int B) {
-  uint32_t running = 0;
-  for (uint32_t base = 0; base < activeCount; base += 1024) {
-    uint32_t a = base + threadIdx.x, chunks = 0;
-    if (a < activeCount) {
-      LargeNode &L = s.large[a];
-      uint32_t node = active[a];
-      const float *nb = s.nodeBounds + size_t(node) * 6;
-      double ext[3];
-      for (int k = 0; k < 3; k++) {
-        L.nMin[k] = nb[k];
-        ext[k] = DA(double(nb[3 + k]), -L.nMin[k]);
-        L.scale[k] = ext[k] > s.g->minDim[k] ? __ddiv_rn(double(B), ext[k]) : 0.0;
-      }
-      L.node = node;
-      L.first = s.nodeFirst[node];
-      L.count = s.nodeCount[node];
-      L.depth = s.nodeDepth[node];
-      if (areaOf(ext[0], ext[1], ext[2]) == 0.0) {
-        L.state = kLeaf;
-      } else {
-        L.state = kBinned;
-        chunks = (L.count + kChunk - 1) / kChunk;
-      }
-      initBins(s.bins + size_t(a) * s.binWords, B, 0, 1);
-    }
-    uint32_t total;
-    uint32_t ex = blockExclusiveSum<1024>(chunks, total);
-    if (a < activeCount) {
-      s.large[a].chunkBegin = running + ex;
-      s.large[a].chunkCount = chunks;
-    }
-    running += total;
+// Per active node: split parameters, a fresh set of bins, and its chunk count
+// (chunkStart, scanned into each node's first chunk afterwards).
+__global__ void __launch_bounds__(kThreads) k_large_setup(Scratch s, const uint32_t *active, uint32_t activeCount,
+                                                          int B) {
+  uint32_t a = blockIdx.x * kThreads + threadIdx.x;
+  if (a == 0) s.g->activeNext = 0;
+  if (a >= activeCount) return;
+  LargeNode &L = s.large[a];
+  uint32_t node = active[a], chunks = 0;
+  const float *nb = s.nodeBounds + size_t(node) * 6;
+  double ext[3];
+  for (int k = 0; k < 3; k++) {
+    L.nMin[k] = nb[k];
+    ext[k] = DA(double(nb[3 + k]), -L.nMin[k]);
+    L.scale[k] = ext[k] > s.g->minDim[k] ? __ddiv_rn(double(B), ext[k]) : 0.0;
   }
-  if (threadIdx.x == 0) {
-    s.g->totalChunks = running;
-    s.g->activeNext = 0;
+  L.node = node;
+  L.first = s.nodeFirst[node];
+  L.count = s.nodeCount[node];
+  L.depth = s.nodeDepth[node];
+  if (areaOf(ext[0], ext[1], ext[2]) == 0.0) {
+    L.state = kLeaf;
+  } else {
+    L.state = kBinned;
+    chunks = (L.count + kChunk - 1) / kChunk;
   }
+  s.chunkStart[a] = chunks;
+  initBins(s.bins + size_t(a) * s.binWords, B, 0, 1);
 }
 
 // Node of chunk c: the last node whose first chunk is <= c (nodes without
-// chunks share their chunkBegin with the next node).
+// chunks share their first chunk with the next node).
 __device__ uint32_t chunkNode(const Scratch &s, uint32_t activeCount, uint32_t c) {
   uint32_t lo = 0, hi = activeCount;
   while (hi - lo > 1) {
     uint32_t mid = (lo + hi) / 2;
-    if (s.large[mid].chunkBegin <= c) lo = mid;
+    if (s.chunkStart[mid] <= c) lo = mid;
     else hi = mid;
   }
   return lo;
@@ -533,7 +557,8 @@ __global__ void __launch_bounds__(kThreads) k_large_bin(Scratch s, uint32_t acti
   extern __shared__ uint32_t sBins[];
   uint32_t c = blockIdx.x;
   if (c >= s.g->totalChunks) return;
-  const LargeNode &L = s.large[chunkNode(s, activeCount, c)];
+  const uint32_t a = chunkNode(s, activeCount, c), cb = s.chunkStart[a];
+  const LargeNode &L = s.large[a];
   double nMin[3], scale[3];
   for (int k = 0; k < 3; k++) {
     nMin[k] = L.nMin[k];
@@ -541,13 +566,13 @@ __global__ void __launch_bounds__(kThreads) k_large_bin(Scratch s, uint32_t acti
   }
   initBins(sBins, B, threadIdx.x, kThreads);
   __syncthreads();
-  uint32_t begin = (c - L.chunkBegin) * kChunk, end = min(begin + kChunk, L.count);
+  uint32_t begin = (c - cb) * kChunk, end = min(begin + kChunk, L.count);
   for (uint32_t i = begin + threadIdx.x; i < end; i += kThreads) {
     uint32_t p = s.prim[L.first + i];
     addToBins(sBins, B, s.center + size_t(p) * 3, s.aabb + size_t(p) * 6, nMin, scale);
   }
   __syncthreads();
-  uint32_t *G = s.bins + size_t(&L - s.large) * s.binWords;
+  uint32_t *G = s.bins + size_t(a) * s.binWords;
   for (int e = threadIdx.x; e < 21 * B; e += kThreads) {
     uint32_t v = sBins[e];
     if (e < 3 * B) {
@@ -561,7 +586,6 @@ __global__ void __launch_bounds__(kThreads) k_large_bin(Scratch s, uint32_t acti
 }
 
 __global__ void __launch_bounds__(kThreads) k_large_sah(Scratch s, uint32_t activeCount, int B) {
-  __shared__ double sCost[kWarps][6 * (kMaxBins - 1)];
   const int warp = threadIdx.x >> 5;
   uint32_t a = blockIdx.x * kWarps + warp;
   if (a >= activeCount) return;
@@ -569,13 +593,13 @@ __global__ void __launch_bounds__(kThreads) k_large_sah(Scratch s, uint32_t acti
   if (L.state != kBinned) return;
   BinView bins{s.bins + size_t(a) * s.binWords, B};
   double minDim[3] = {s.g->minDim[0], s.g->minDim[1], s.g->minDim[2]};
-  Decision d = decideSplit(bins, s.nodeBounds + size_t(L.node) * 6, L.count, minDim, sCost[warp]);
+  Decision d = decideSplit(bins, s.nodeBounds + size_t(L.node) * 6, L.count, minDim);
+  if ((threadIdx.x & 31) < 12) L.childBounds[threadIdx.x & 31] = d.laneBound;
   if ((threadIdx.x & 31) == 0) {
     L.state = d.state;
     L.axis = d.axis;
     L.pos = d.pos;
     L.leftN = d.leftN;
-    for (int k = 0; k < 12; k++) L.childBounds[k] = d.childBounds[k];
   }
 }
 
@@ -589,10 +613,11 @@ __device__ __forceinline__ bool goesRight(const Scratch &s, const LargeNode &L, 
 __global__ void __launch_bounds__(kThreads) k_large_classify(Scratch s, uint32_t activeCount, int B) {
   uint32_t c = blockIdx.x;
   if (c >= s.g->totalChunks) return;
-  const LargeNode &L = s.large[chunkNode(s, activeCount, c)];
+  const uint32_t a = chunkNode(s, activeCount, c), cb = s.chunkStart[a];
+  const LargeNode &L = s.large[a];
   uint32_t cnt = 0;
   if (partitions(L.state)) {
-    uint32_t begin = (c - L.chunkBegin) * kChunk, end = min(begin + kChunk, L.count);
+    uint32_t begin = (c - cb) * kChunk, end = min(begin + kChunk, L.count);
     for (uint32_t i = begin + threadIdx.x; i < end; i += kThreads) cnt += goesRight(s, L, i, B);
   }
   uint32_t total;
@@ -604,9 +629,10 @@ __global__ void __launch_bounds__(kThreads) k_large_classify(Scratch s, uint32_t
 __global__ void __launch_bounds__(kThreads) k_large_rank(Scratch s, uint32_t activeCount, int B) {
   uint32_t c = blockIdx.x;
   if (c >= s.g->totalChunks) return;
-  const LargeNode &L = s.large[chunkNode(s, activeCount, c)];
+  const uint32_t a = chunkNode(s, activeCount, c), cb = s.chunkStart[a];
+  const LargeNode &L = s.large[a];
   if (!partitions(L.state)) return;
-  uint32_t begin = (c - L.chunkBegin) * kChunk, end = min(begin + kChunk, L.count);
+  uint32_t begin = (c - cb) * kChunk, end = min(begin + kChunk, L.count);
   uint32_t i0 = begin + threadIdx.x * kPerThread, bits = 0, cnt = 0;
   for (int j = 0; j < kPerThread; j++) {
     uint32_t i = i0 + j;
@@ -616,7 +642,7 @@ __global__ void __launch_bounds__(kThreads) k_large_rank(Scratch s, uint32_t act
     }
   }
   uint32_t total;
-  uint32_t prefR = s.chunkR[c] - s.chunkR[L.chunkBegin] + blockExclusiveSum<kThreads>(cnt, total);
+  uint32_t prefR = s.chunkR[c] - s.chunkR[cb] + blockExclusiveSum<kThreads>(cnt, total);
   for (int j = 0; j < kPerThread; j++) {
     uint32_t i = i0 + j;
     if (i >= end) break;
@@ -637,9 +663,10 @@ __global__ void __launch_bounds__(kThreads) k_large_rank(Scratch s, uint32_t act
 __global__ void __launch_bounds__(kThreads) k_large_scatter(Scratch s, uint32_t activeCount) {
   uint32_t c = blockIdx.x;
   if (c >= s.g->totalChunks) return;
-  const LargeNode &L = s.large[chunkNode(s, activeCount, c)];
+  const uint32_t a = chunkNode(s, activeCount, c), cb = s.chunkStart[a];
+  const LargeNode &L = s.large[a];
   if (!partitions(L.state)) return;
-  uint32_t begin = (c - L.chunkBegin) * kChunk, end = min(begin + kChunk, L.count);
+  uint32_t begin = (c - cb) * kChunk, end = min(begin + kChunk, L.count);
   for (uint32_t i = begin + threadIdx.x; i < end; i += kThreads) {
     uint32_t r = s.rank[L.first + i];
     uint32_t dest = partitionDest(i, r >> 31, r & 0x7fffffffu, L.count, L.leftN, s.rf + L.first, s.lb + L.first);
@@ -651,9 +678,10 @@ __global__ void __launch_bounds__(kThreads) k_large_scatter(Scratch s, uint32_t 
 __global__ void __launch_bounds__(kThreads) k_large_copy(Scratch s, uint32_t activeCount) {
   uint32_t c = blockIdx.x;
   if (c >= s.g->totalChunks) return;
-  const LargeNode &L = s.large[chunkNode(s, activeCount, c)];
+  const uint32_t a = chunkNode(s, activeCount, c), cb = s.chunkStart[a];
+  const LargeNode &L = s.large[a];
   if (!partitions(L.state)) return;
-  uint32_t begin = (c - L.chunkBegin) * kChunk, end = min(begin + kChunk, L.count);
+  uint32_t begin = (c - cb) * kChunk, end = min(begin + kChunk, L.count);
   for (uint32_t i = begin + threadIdx.x; i < end; i += kThreads) s.prim[L.first + i] = s.tmp[L.first + i];
 }
 
@@ -682,164 +710,195 @@ __global__ void __launch_bounds__(kThreads) k_large_children(Scratch s, uint32_t
   atomicMax(&s.g->maxDepth, L.depth + 1);
 }
 
-// ------------------------------------------------ per-CTA subtree phase
-struct SmallShared {
-  float *aabb, *center;
-  uint32_t *global, *perm, *tmp, *rf, *lb, *bins;
-  uint4 *front[2];
-  double *cost;
-  Decision *dec;
-  uint32_t *frontCount;
+// ------------------------------------------------ per-warp subtree phase
+constexpr int kSubtreeWarps = 4;  // warps (independent subtrees) per CTA
+
+// Shared memory of one warp: centroids, the subtree's primitive ids, its
+// working permutation, the partition scratch (tmp, and rf | lb side by side),
+// the DFS stack and the bins.
+struct WarpShared {
+  float *center, *stackBounds;
+  uint32_t *global, *perm, *tmp, *ranks, *bins;
+  uint4 *stack;
 };
 
-size_t smallSharedBytes(int B) {
-  size_t bytes = size_t(kSmallLimit) * (6 + 3) * 4 + size_t(kSmallLimit) * 5 * 4;
-  bytes += 2 * size_t(kSmallLimit / 2) * sizeof(uint4);
-  bytes += size_t(kWarps) * 21 * B * 4;
-  bytes = (bytes + 7) / 8 * 8;
-  bytes += size_t(kWarps) * 6 * std::max(B - 1, 1) * sizeof(double);
-  bytes += size_t(kWarps) * sizeof(Decision);
-  bytes += 2 * sizeof(uint32_t);
-  return bytes;
+// Pending nodes hold at least two primitives each, in disjoint ranges.
+constexpr uint32_t kStackDepth = kSmallLimit / 2 + 1;
+
+__host__ __device__ inline size_t warpSharedBytes(int B) {
+  return (size_t(kStackDepth) * (sizeof(uint4) + 6 * 4) + size_t(kSmallLimit) * (3 * 4 + 4 * 4) + size_t(21) * B * 4 +
+          15) / 16 * 16;
 }
 
-__device__ SmallShared carveShared(unsigned char *base, int B) {
-  SmallShared S;
-  size_t off = 0;
-  auto grab = [&](size_t bytes) { unsigned char *p = base + off; off += bytes; return p; };
-  S.aabb = (float *)grab(size_t(kSmallLimit) * 6 * 4);
-  S.center = (float *)grab(size_t(kSmallLimit) * 3 * 4);
-  S.global = (uint32_t *)grab(kSmallLimit * 4);
-  S.perm = (uint32_t *)grab(kSmallLimit * 4);
-  S.tmp = (uint32_t *)grab(kSmallLimit * 4);
-  S.rf = (uint32_t *)grab(kSmallLimit * 4);
-  S.lb = (uint32_t *)grab(kSmallLimit * 4);
-  S.front[0] = (uint4 *)grab((kSmallLimit / 2) * sizeof(uint4));
-  S.front[1] = (uint4 *)grab((kSmallLimit / 2) * sizeof(uint4));
-  S.bins = (uint32_t *)grab(size_t(kWarps) * 21 * B * 4);
-  off = (off + 7) / 8 * 8;
-  S.cost = (double *)grab(size_t(kWarps) * 6 * (B > 1 ? B - 1 : 1) * sizeof(double));
-  S.dec = (Decision *)grab(kWarps * sizeof(Decision));
-  S.frontCount = (uint32_t *)grab(2 * sizeof(uint32_t));
+__device__ WarpShared carveWarp(unsigned char *base, int B) {
+  WarpShared S;
+  S.stack = reinterpret_cast<uint4 *>(base);
+  S.stackBounds = reinterpret_cast<float *>(base + kStackDepth * sizeof(uint4));
+  S.center = S.stackBounds + kStackDepth * 6;
+  S.global = reinterpret_cast<uint32_t *>(S.center + kSmallLimit * 3);
+  S.perm = S.global + kSmallLimit;
+  S.tmp = S.perm + kSmallLimit;
+  S.ranks = S.tmp + kSmallLimit;
+  S.bins = S.ranks + kSmallLimit;
   return S;
 }
 
-// One warp splits one node of a CTA-resident subtree (entry: node id, first
-// in the CTA's range, count, depth) and appends its children to `next`.
-__device__ void splitNodeWarp(const Scratch &s, const SmallShared &S, uint4 entry, uint32_t rootFirst, int B,
-                              const double minDim[3], int nextSlot) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t id = entry.x, lf = entry.y, cnt = entry.z, depth = entry.w;
-  float nb[6];
-  for (int k = 0; k < 6; k++) nb[k] = s.nodeBounds[size_t(id) * 6 + k];
-  double nMin[3], ext[3], scale[3];
-  for (int k = 0; k < 3; k++) {
-    nMin[k] = nb[k];
-    ext[k] = DA(double(nb[3 + k]), -nMin[k]);
-    scale[k] = ext[k] > minDim[k] ? __ddiv_rn(double(B), ext[k]) : 0.0;
-  }
-  if (areaOf(ext[0], ext[1], ext[2]) == 0.0 || cnt == 1) return;
-  uint32_t *w = S.bins + size_t(warp) * 21 * B;
-  initBins(w, B, lane, 32);
-  __syncwarp();
-  for (uint32_t i = lane; i < cnt; i += 32) {
-    uint32_t li = S.perm[lf + i];
-    addToBins(w, B, S.center + li * 3, S.aabb + li * 6, nMin, scale);
-  }
-  __syncwarp();
-  Decision d = decideSplit(BinView{w, B}, nb, cnt, minDim, S.cost + size_t(warp) * 6 * (B > 1 ? B - 1 : 1));
-  if (lane == 0) S.dec[warp] = d;
-  __syncwarp();
-  d = S.dec[warp];
-  if (d.state == kLeaf) return;
-  const int axis = d.axis;
-  const uint32_t nL = d.leftN;
-  // Pass 1: ranks and the rf / lb tables.
-  uint32_t prefix = 0;
-  for (uint32_t base = 0; base < cnt; base += 32) {
-    uint32_t i = base + lane;
-    bool right = i < cnt && binOf(S.center[S.perm[lf + i] * 3 + axis], nMin[axis], scale[axis], B) > d.pos;
-    uint32_t ballot = __ballot_sync(0xffffffffu, right);
-    uint32_t prefR = prefix + __popc(ballot & ((1u << lane) - 1));
-    if (i < cnt) {
-      uint32_t slot = right ? prefR : nL - (i - prefR) - 1;
-      if (slot >= (right ? cnt - nL : nL)) s.g->error = 1;
-      else if (right) S.rf[lf + slot] = i;
-      else S.lb[lf + slot] = i;
-    }
-    prefix += __popc(ballot);
-  }
-  __syncwarp();
-  // Pass 2: the permutation, into tmp.
-  prefix = 0;
-  for (uint32_t base = 0; base < cnt; base += 32) {
-    uint32_t i = base + lane;
-    bool right = i < cnt && binOf(S.center[S.perm[lf + i] * 3 + axis], nMin[axis], scale[axis], B) > d.pos;
-    uint32_t ballot = __ballot_sync(0xffffffffu, right);
-    uint32_t prefR = prefix + __popc(ballot & ((1u << lane) - 1));
-    if (i < cnt) {
-      uint32_t dest = partitionDest(i, right, prefR, cnt, nL, S.rf + lf, S.lb + lf);
-      if (dest < cnt) S.tmp[lf + dest] = S.perm[lf + i];
-      else s.g->error = 1;
-    }
-    prefix += __popc(ballot);
-  }
-  __syncwarp();
-  for (uint32_t i = lane; i < cnt; i += 32) S.perm[lf + i] = S.tmp[lf + i];
-  __syncwarp();
-  if (d.state != kSplit || lane != 0) return;
-  uint32_t child = atomicAdd(&s.g->nodeAlloc, 2u);
-  for (int c = 0; c < 2; c++) {
-    uint32_t ccnt = c ? cnt - nL : nL, clf = lf + (c ? nL : 0);
-    writeChild(s, child + c, d.childBounds + 6 * c, rootFirst + clf, ccnt, depth + 1);
-    if (ccnt >= 2) S.front[nextSlot][atomicAdd(&S.frontCount[nextSlot], 1u)] = make_uint4(child + c, clf, ccnt, depth + 1);
-  }
-  s.nodeChild[id] = int32_t(child);
-  atomicMax(&s.g->maxDepth, depth + 1);
-}
-
-__global__ void __launch_bounds__(kThreads) k_small(Scratch s, int B) {
+// One warp builds the whole subtree under a node of at most kSmallLimit
+// primitives, depth first (children are pushed right then left, so the stack
+// holds at most one pending node per level).  Node ids come from a block of
+// 2n - 2 reserved up front; ids left unused are marked depth 0 (holes the
+// layout skips).
+__global__ void __launch_bounds__(kSubtreeWarps * 32) k_subtree(Scratch s, uint32_t rootCount, int B) {
   extern __shared__ __align__(16) unsigned char smem[];
-  SmallShared S = carveShared(smem, B);
-  const uint32_t root = s.smallQ[blockIdx.x];
-  const uint32_t rootFirst = s.nodeFirst[root], n = s.nodeCount[root];
-  for (uint32_t i = threadIdx.x; i < n; i += kThreads) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t task = blockIdx.x * kSubtreeWarps + warp;
+  if (task >= rootCount) return;
+  WarpShared S = carveWarp(smem + size_t(warp) * warpSharedBytes(B), B);
+  const uint32_t root = s.smallQ[task], rootFirst = s.nodeFirst[root], n = s.nodeCount[root];
+  for (uint32_t i = lane; i < n; i += 32) {
     uint32_t p = s.prim[rootFirst + i];
     S.global[i] = p;
     S.perm[i] = i;
-    for (int k = 0; k < 6; k++) S.aabb[i * 6 + k] = s.aabb[size_t(p) * 6 + k];
     for (int k = 0; k < 3; k++) S.center[i * 3 + k] = s.center[size_t(p) * 3 + k];
   }
-  double minDim[3] = {s.g->minDim[0], s.g->minDim[1], s.g->minDim[2]};
-  if (threadIdx.x == 0) {
-    S.front[0][0] = make_uint4(root, 0, n, s.nodeDepth[root]);
-    S.frontCount[0] = 1;
+  const double minDim[3] = {s.g->minDim[0], s.g->minDim[1], s.g->minDim[2]};
+  uint32_t idBase = 0;
+  if (lane == 0) idBase = atomicAdd(&s.g->nodeAlloc, 2 * n - 2);
+  idBase = __shfl_sync(0xffffffffu, idBase, 0);
+  uint32_t used = 0, top = 0, maxDepth = 0;
+  if (lane == 0) S.stack[0] = make_uint4(root, 0, n, s.nodeDepth[root]);
+  if (lane < 6) S.stackBounds[lane] = s.nodeBounds[size_t(root) * 6 + lane];
+  top = 1;
+  __syncwarp();
+  while (top) {
+    const uint4 e = S.stack[--top];
+    float nb[6];
+    for (int k = 0; k < 6; k++) nb[k] = S.stackBounds[top * 6 + k];
+    __syncwarp();
+    const uint32_t id = e.x, lf = e.y, cnt = e.z, depth = e.w;
+    double nMin[3], ext[3], scale[3];
+    for (int k = 0; k < 3; k++) {
+      nMin[k] = nb[k];
+      ext[k] = DA(double(nb[3 + k]), -nMin[k]);
+      scale[k] = ext[k] > minDim[k] ? __ddiv_rn(double(B), ext[k]) : 0.0;
+    }
+    if (areaOf(ext[0], ext[1], ext[2]) == 0.0) continue;
+    initBins(S.bins, B, lane, 32);
+    __syncwarp();
+    for (uint32_t i = lane; i < cnt; i += 32) {
+      uint32_t li = S.perm[lf + i];
+      addToBins(S.bins, B, S.center + li * 3, s.aabb + size_t(S.global[li]) * 6, nMin, scale);
+    }
+    __syncwarp();
+    const Decision d = decideSplit(BinView{S.bins, B}, nb, cnt, minDim);
+    if (d.state == kLeaf) continue;
+    const int axis = d.axis;
+    const double axisMin = axis == 0 ? nMin[0] : (axis == 1 ? nMin[1] : nMin[2]);
+    const double axisScale = axis == 0 ? scale[0] : (axis == 1 ? scale[1] : scale[2]);
+    const uint32_t nL = d.leftN, nR = cnt - nL;
+    uint32_t *rf = S.ranks + lf, *lb = S.ranks + lf + nR;
+    // Pass 1: sides (kept as ballots), ranks and the rf / lb tables.
+    uint32_t ballots[kSmallLimit / 32];
+    uint32_t prefix = 0;
+#pragma unroll
+    for (int j = 0; j < int(kSmallLimit / 32); j++) {
+      const uint32_t i = j * 32 + lane;
+      if (j * 32u >= cnt) break;
+      bool right = i < cnt && binOf(S.center[S.perm[lf + i] * 3 + axis], axisMin, axisScale, B) > d.pos;
+      ballots[j] = __ballot_sync(0xffffffffu, right);
+      uint32_t prefR = prefix + __popc(ballots[j] & ((1u << lane) - 1));
+      if (i < cnt) {
+        uint32_t slot = right ? prefR : nL - (i - prefR) - 1;
+        if (slot >= (right ? nR : nL)) s.g->error = 1;
+        else if (right) rf[slot] = i;
+        else lb[slot] = i;
+      }
+      prefix += __popc(ballots[j]);
+    }
+    __syncwarp();
+    // Pass 2: the permutation, into tmp; then back.
+    prefix = 0;
+#pragma unroll
+    for (int j = 0; j < int(kSmallLimit / 32); j++) {
+      const uint32_t i = j * 32 + lane;
+      if (j * 32u >= cnt) break;
+      const bool right = ballots[j] >> lane & 1u;
+      uint32_t prefR = prefix + __popc(ballots[j] & ((1u << lane) - 1));
+      if (i < cnt) {
+        uint32_t dest = partitionDest(i, right, prefR, cnt, nL, rf, lb);
+        if (dest < cnt) S.tmp[lf + dest] = S.perm[lf + i];
+        else s.g->error = 1;
+      }
+      prefix += __popc(ballots[j]);
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < cnt; i += 32) S.perm[lf + i] = S.tmp[lf + i];
+    __syncwarp();
+    if (d.state != kSplit) continue;
+    const uint32_t child = idBase + used;
+    used += 2;
+    if (lane < 12) s.nodeBounds[size_t(child) * 6 + lane] = d.laneBound;
+    if (lane < 2) {
+      const uint32_t c = child + lane;
+      s.nodeFirst[c] = rootFirst + lf + (lane ? nL : 0);
+      s.nodeCount[c] = lane ? nR : nL;
+      s.nodeDepth[c] = depth + 1;
+      s.nodeChild[c] = -1;
+    }
+    if (lane == 0) {
+      s.nodeChild[id] = int32_t(child);
+      if (nR >= 2) S.stack[top] = make_uint4(child + 1, lf + nL, nR, depth + 1);
+      if (nL >= 2) S.stack[top + (nR >= 2)] = make_uint4(child, lf, nL, depth + 1);
+    }
+    if (lane < 6 && nL >= 2) S.stackBounds[(top + (nR >= 2)) * 6 + lane] = d.laneBound;
+    if (lane >= 6 && lane < 12 && nR >= 2) S.stackBounds[top * 6 + lane - 6] = d.laneBound;
+    top += (nR >= 2) + (nL >= 2);
+    maxDepth = max(maxDepth, depth + 1);
+    __syncwarp();
   }
-  __syncthreads();
-  int cur = 0;
-  uint32_t fcount = 1;
-  while (fcount) {
-    if (threadIdx.x == 0) S.frontCount[cur ^ 1] = 0;
-    __syncthreads();
-    for (uint32_t f = threadIdx.x >> 5; f < fcount; f += kWarps)
-      splitNodeWarp(s, S, S.front[cur][f], rootFirst, B, minDim, cur ^ 1);
-    __syncthreads();
-    cur ^= 1;
-    fcount = S.frontCount[cur];
+  for (uint32_t i = lane; i < n; i += 32) s.prim[rootFirst + i] = S.global[S.perm[i]];
+  for (uint32_t i = used + lane; i < 2 * n - 2; i += 32) s.nodeDepth[idBase + i] = 0;
+  if (lane == 0) {
+    if (maxDepth) atomicMax(&s.g->maxDepth, maxDepth);
+    if (used < 2 * n - 2) atomicAdd(&s.g->holes, 2 * n - 2 - used);
   }
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n; i += kThreads) s.prim[rootFirst + i] = S.global[S.perm[i]];
 }
 
 // ------------------------------------------------------------ layout
-__global__ void k_depth_hist(Scratch s, uint32_t nodeCount) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nodeCount) atomicAdd(&s.depthCursor[s.nodeDepth[i]], 1u);
+// Nodes by depth: per-CTA counts in shared memory (depths <= depthCount),
+// then one global reservation per (CTA, depth).
+constexpr uint32_t kDepthNodes = 2048;  // nodes per CTA
+constexpr uint32_t kMaxSharedDepths = 8192;
+
+__global__ void __launch_bounds__(kThreads) k_depth_hist(Scratch s, uint32_t nodeCount, uint32_t depthCount) {
+  extern __shared__ uint32_t hist[];
+  for (uint32_t d = threadIdx.x; d < depthCount; d += kThreads) hist[d] = 0;
+  __syncthreads();
+  uint32_t end = min(nodeCount, (blockIdx.x + 1) * kDepthNodes);
+  for (uint32_t i = blockIdx.x * kDepthNodes + threadIdx.x; i < end; i += kThreads) atomicAdd(&hist[s.nodeDepth[i]], 1u);
+  __syncthreads();
+  for (uint32_t d = threadIdx.x; d < depthCount; d += kThreads)
+    if (hist[d]) atomicAdd(&s.depthCursor[d], hist[d]);
 }
 
-__global__ void k_depth_scatter(Scratch s, uint32_t nodeCount) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nodeCount) s.byDepth[atomicAdd(&s.depthCursor[s.nodeDepth[i]], 1u)] = i;
+__global__ void __launch_bounds__(kThreads) k_depth_scatter(Scratch s, uint32_t nodeCount, uint32_t depthCount) {
+  extern __shared__ uint32_t hist[];
+  for (uint32_t d = threadIdx.x; d < depthCount; d += kThreads) hist[d] = 0;
+  __syncthreads();
+  const uint32_t begin = blockIdx.x * kDepthNodes, end = min(nodeCount, begin + kDepthNodes);
+  uint32_t rank[kDepthNodes / kThreads];
+  for (int j = 0; j < int(kDepthNodes / kThreads); j++) {
+    uint32_t i = begin + j * kThreads + threadIdx.x;
+    if (i < end) rank[j] = atomicAdd(&hist[s.nodeDepth[i]], 1u);
+  }
+  __syncthreads();
+  for (uint32_t d = threadIdx.x; d < depthCount; d += kThreads)
+    if (hist[d]) hist[d] = atomicAdd(&s.depthCursor[d], hist[d]);
+  __syncthreads();
+  for (int j = 0; j < int(kDepthNodes / kThreads); j++) {
+    uint32_t i = begin + j * kThreads + threadIdx.x;
+    if (i < end) s.byDepth[hist[s.nodeDepth[i]] + rank[j]] = i;
+  }
 }
 
 // Subtree length in vec4 (2 per node plus one per leaf primitive), one depth.
@@ -966,7 +1025,8 @@ mt_status mtc_build_blas(const mtc_blas_build_input *input, void *scratch, uint6
   uint32_t active = g.activeNext, *cur = s.activeA, *next = s.activeB;
   while (active) {
     uint32_t grid = n / kChunk + 1 + active;
-    k_large_setup<<<1, 1024, 0, st>>>(s, cur, active, int(B));
+    k_large_setup<<<(active + kThreads - 1) / kThreads, kThreads, 0, st>>>(s, cur, active, int(B));
+    k_scan<<<1, 1024, 0, st>>>(s.chunkStart, nullptr, active, &s.g->totalChunks);
     k_large_bin<<<grid, kThreads, binSmem, st>>>(s, active, int(B));
     k_large_sah<<<(active + kWarps - 1) / kWarps, kThreads, 0, st>>>(s, active, int(B));
     k_large_classify<<<grid, kThreads, 0, st>>>(s, active, int(B));
@@ -981,11 +1041,12 @@ mt_status mtc_build_blas(const mtc_blas_build_input *input, void *scratch, uint6
     std::swap(cur, next);
   }
 
-  // Subtrees of at most kSmallLimit primitives, one CTA each.
+  // Subtrees of at most kSmallLimit primitives, one warp each.
   if (g.smallCount) {
-    size_t smem = smallSharedBytes(int(B));
-    MT_TRY(cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k_small<<<g.smallCount, kThreads, smem, st>>>(s, int(B));
+    size_t smem = warpSharedBytes(int(B)) * kSubtreeWarps;
+    MT_TRY(cudaFuncSetAttribute(k_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_subtree<<<(g.smallCount + kSubtreeWarps - 1) / kSubtreeWarps, kSubtreeWarps * 32, smem, st>>>(s, g.smallCount,
+                                                                                                  int(B));
     MT_LAUNCHED();
   }
   MT_TRY(hs.read(&g, s.g));
@@ -996,9 +1057,14 @@ mt_status mtc_build_blas(const mtc_blas_build_input *input, void *scratch, uint6
   const uint32_t nodes = g.nodeAlloc, maxDepth = g.maxDepth;
 
   // Nodes by depth, then sizes bottom up and offsets top down.
-  MT_TRY(cudaMemsetAsync(s.depthCursor, 0, sizeof(uint32_t) * (maxDepth + 2), st));
-  const uint32_t nodeBlocks = (nodes + 255) / 256;
-  k_depth_hist<<<nodeBlocks, 256, 0, st>>>(s, nodes);
+  const uint32_t depthCount = maxDepth + 2;
+  if (depthCount > kMaxSharedDepths) return MT_ERROR_UNAVAILABLE;  // a BVH this deep has no traversal stack anyway
+  MT_TRY(cudaMemsetAsync(s.depthCursor, 0, sizeof(uint32_t) * depthCount, st));
+  const uint32_t nodeBlocks = (nodes + kDepthNodes - 1) / kDepthNodes;
+  const size_t depthSmem = sizeof(uint32_t) * depthCount;
+  MT_TRY(cudaFuncSetAttribute(k_depth_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, int(depthSmem)));
+  MT_TRY(cudaFuncSetAttribute(k_depth_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(depthSmem)));
+  k_depth_hist<<<nodeBlocks, kThreads, depthSmem, st>>>(s, nodes, depthCount);
   MT_LAUNCHED();
   std::vector<uint32_t> hist(maxDepth + 2), base(maxDepth + 2);
   MT_TRY(hs.read(hist.data(), s.depthCursor, maxDepth + 2));
@@ -1008,7 +1074,7 @@ mt_status mtc_build_blas(const mtc_blas_build_input *input, void *scratch, uint6
     running += hist[d];
   }
   MT_TRY(cudaMemcpyAsync(s.depthCursor, base.data(), sizeof(uint32_t) * (maxDepth + 2), cudaMemcpyHostToDevice, st));
-  k_depth_scatter<<<nodeBlocks, 256, 0, st>>>(s, nodes);
+  k_depth_scatter<<<nodeBlocks, kThreads, depthSmem, st>>>(s, nodes, depthCount);
   for (uint32_t d = maxDepth; d >= 1; d--)
     if (hist[d]) k_size_level<<<(hist[d] + 255) / 256, 256, 0, st>>>(s, s.byDepth + base[d], hist[d]);
   MT_LAUNCHED();
@@ -1020,7 +1086,7 @@ mt_status mtc_build_blas(const mtc_blas_build_input *input, void *scratch, uint6
   result->vec4_count = rootSize;
   result->max_depth = maxDepth;
   result->max_leaf_primitives = g.maxLeaf;
-  result->node_count = nodes;
+  result->node_count = nodes - g.holes;
   result->primitive_count = g.primCount;
   for (int k = 0; k < 6; k++) result->local_bounds[k] = rootBox[k];
   if (!out_bvh || rootSize > out_capacity_vec4) {
