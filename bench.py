@@ -363,6 +363,7 @@ def run_b200(args):
         result["batched"] = mixed_batch(args, dev_id)
         result["served"] = served_stream(args, dev_id)
         result["deep_transport"] = deep_transport(args, dev_id)
+        result["blas_build"] = blas_build(args, dev_id)
     print(json.dumps(result), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -571,6 +572,45 @@ def deep_transport(args, dev_id):
     })
     del sb, jobs
     torch.cuda.empty_cache()
+    return res
+
+
+def blas_build(args, dev_id):
+    """BLAS build on the device (mtc_build_blas) against the host producer
+    (the C++ restatement of buildBLAS, one core) on the same seeded terrain
+    meshes; the buffers must be byte-identical.  The host build runs on the
+    smaller mesh only (about 7 s); the device build on both."""
+    import torch
+    from mutracer_b200 import blas
+    res = {}
+    for side in (1000, 2000):
+        pos, idx = blas.terrain_mesh(side, side, seed=3)
+        n = len(idx)
+        pos_t = torch.from_numpy(pos).to(dev_id)
+        idx_t = torch.from_numpy(idx.view(np.int32)).to(dev_id)
+        builder = blas.BlasBuilder(n, 8, dev_id)
+        out = torch.empty(blas.max_vec4(n) * 4, dtype=torch.float32, device=dev_id)
+        builder.build(pos_t, idx_t, out)
+        ms = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            buf, info = builder.build(pos_t, idx_t, out)   # returns once the buffer is complete
+            ms.append((time.perf_counter() - t0) * 1e3)
+        entry = {"triangles": n, "device_ms": round(float(np.median(ms)), 2), "nodes": int(info.node_count),
+                 "max_depth": int(info.max_depth), "host_syncs": int(info.host_syncs),
+                 "mtris_per_s": round(n / float(np.median(ms)) / 1e3, 1)}
+        if side == 1000:
+            t0 = time.perf_counter()
+            want, _ = blas.host_build(pos, idx, 8)
+            entry["host_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+            entry["speedup_vs_host"] = round(entry["host_ms"] / entry["device_ms"], 1)
+            entry["byte_identical"] = buf.cpu().numpy().view(np.uint32).tobytes() == want.view(np.uint32).tobytes()
+        res[f"terrain_{n}"] = entry
+        del builder, out, buf, pos_t, idx_t
+        torch.cuda.empty_cache()
+    res["workload"] = ("seeded terrain meshes (1000^2 and 2000^2 cells, 2 triangles each, shuffled), bins 8; host "
+                       "producer = C++ restatement of buildBLAS on one core")
     return res
 
 

@@ -3,6 +3,8 @@
 memory, producing the same BVH2 buffer as the host producer."""
 import ctypes as C
 
+import numpy as np
+
 from . import abi
 
 
@@ -56,3 +58,61 @@ class BlasBuilder:
                                            C.c_void_p(out.data_ptr()), out.numel() // 4, C.byref(res),
                                            C.c_void_p(st.cuda_stream)))
         return out[: res.vec4_count * 4], res
+
+
+def terrain_mesh(w, h, seed=0, amplitude=0.3):
+    """Seeded height-field mesh over the unit square: (w+1) x (h+1) vertices,
+    2 w h triangles in a shuffled order (positions f32 (V, 3), indices u32
+    (T, 3))."""
+    rng = np.random.default_rng(seed)
+    ys, xs = np.mgrid[0:h + 1, 0:w + 1].astype(np.float32)
+    z = amplitude * rng.standard_normal(xs.shape).astype(np.float32)
+    pos = np.stack([xs / w, z, ys / h], -1).reshape(-1, 3)
+    v = (np.arange(h)[:, None] * (w + 1) + np.arange(w)[None, :]).reshape(-1)
+    a, b, c, d = v, v + 1, v + w + 1, v + w + 2
+    idx = np.concatenate([np.stack([a, b, d], 1), np.stack([a, d, c], 1)]).astype(np.uint32)
+    return pos, idx[rng.permutation(len(idx))]
+
+
+def host_build(positions, indices, bins=8):
+    """The host producer (the C++ restatement of buildBLAS): (buffer f32,
+    max depth)."""
+    pos = np.ascontiguousarray(positions, np.float32)
+    idx = np.ascontiguousarray(indices, np.uint32)
+    nt = idx.size // 3
+    buf = np.zeros(max(5 * nt, 1) * 4, np.float32)
+    vec4, depth = C.c_uint64(), C.c_uint32()
+    abi.check(abi.lib().mtp_build_blas(pos.ctypes.data, pos.size // 3, idx.ctypes.data, nt, int(bins),
+                                       buf.ctypes.data, buf.size // 4, C.byref(vec4), C.byref(depth)))
+    return buf[: vec4.value * 4], depth.value
+
+
+def main(argv=None):
+    """Builds a seeded terrain mesh on the device (one warm-up build, then
+    timed builds) and prints one JSON line per timed build."""
+    import argparse
+    import json
+    import time
+
+    import torch
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--side", type=int, default=2000, help="cells per side (2 side^2 triangles)")
+    p.add_argument("--bins", type=int, default=8)
+    p.add_argument("--repeat", type=int, default=1)
+    a = p.parse_args(argv)
+    pos, idx = terrain_mesh(a.side, a.side, seed=3)
+    pos_t, idx_t = torch.from_numpy(pos).cuda(), torch.from_numpy(idx.view(np.int32)).cuda()
+    builder = BlasBuilder(len(idx), a.bins)
+    out = torch.empty(max_vec4(len(idx)) * 4, dtype=torch.float32, device="cuda")
+    builder.build(pos_t, idx_t, out)
+    for _ in range(a.repeat):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, res = builder.build(pos_t, idx_t, out)
+        ms = (time.perf_counter() - t0) * 1e3
+        print(json.dumps({"triangles": len(idx), "ms": round(ms, 3), "nodes": res.node_count,
+                          "max_depth": res.max_depth, "host_syncs": res.host_syncs}), flush=True)
+
+
+if __name__ == "__main__":
+    main()

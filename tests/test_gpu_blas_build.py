@@ -15,14 +15,8 @@ torch = pytest.importorskip("torch")
 
 
 def host_blas(pos, idx, bins):
-    pos = np.ascontiguousarray(pos, np.float32)
-    idx = np.ascontiguousarray(idx, np.uint32)
-    nt = idx.size // 3
-    buf = np.zeros(max(5 * nt, 1) * 4, np.float32)
-    vec4, depth = C.c_uint64(), C.c_uint32()
-    assert abi.lib().mtp_build_blas(pos.ctypes.data, pos.size // 3, idx.ctypes.data, nt, bins, buf.ctypes.data,
-                                    buf.size // 4, C.byref(vec4), C.byref(depth)) == abi.MT_OK
-    return buf[: vec4.value * 4], depth.value
+    from mutracer_b200 import blas
+    return blas.host_build(pos, idx, bins)
 
 
 def device_blas(pos, idx, bins):
@@ -36,14 +30,8 @@ def device_blas(pos, idx, bins):
 
 
 def grid_mesh(w, h, seed=0, amplitude=0.3):
-    rng = np.random.default_rng(seed)
-    ys, xs = np.mgrid[0:h + 1, 0:w + 1].astype(np.float32)
-    z = amplitude * rng.standard_normal(xs.shape).astype(np.float32)
-    pos = np.stack([xs / w, z, ys / h], -1).reshape(-1, 3)
-    v = (np.arange(h)[:, None] * (w + 1) + np.arange(w)[None, :]).reshape(-1)
-    a, b, c, d = v, v + 1, v + w + 1, v + w + 2
-    idx = np.concatenate([np.stack([a, b, d], 1), np.stack([a, d, c], 1)]).astype(np.uint32)
-    return pos, idx[rng.permutation(len(idx))]
+    from mutracer_b200 import blas
+    return blas.terrain_mesh(w, h, seed, amplitude)
 
 
 def soup(n, seed=0, spread=10.0, size=0.3):
