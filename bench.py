@@ -576,10 +576,11 @@ def deep_transport(args, dev_id):
 
 
 def blas_build(args, dev_id):
-    """BLAS build on the device (mtc_build_blas) against the host producer
-    (the C++ restatement of buildBLAS, one core) on the same seeded terrain
-    meshes; the buffers must be byte-identical.  The host build runs on the
-    smaller mesh only (about 7 s); the device build on both."""
+    """BLAS build and refit on the device (mtc_build_blas, mtc_refit_blas)
+    against the host producer (the C++ restatements of buildBLAS and
+    refitBLAS, one core) on the same seeded terrain meshes; the buffers must
+    be byte-identical.  The host build runs on the smaller mesh only (about
+    7 s); the device build on both."""
     import torch
     from mutracer_b200 import blas
     res = {}
@@ -600,17 +601,40 @@ def blas_build(args, dev_id):
         entry = {"triangles": n, "device_ms": round(float(np.median(ms)), 2), "nodes": int(info.node_count),
                  "max_depth": int(info.max_depth), "host_syncs": int(info.host_syncs),
                  "mtris_per_s": round(n / float(np.median(ms)) / 1e3, 1)}
+        # refitBLAS after a deformation (x1.5): plan once, then one launch per depth.
+        bvh = buf.clone()
+        t0 = time.perf_counter()
+        refit = blas.BlasRefit(bvh)
+        entry["refit_plan_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+        moved_t = pos_t * 1.5
+        refit.refit(moved_t)
+        rms = []
+        for _ in range(5):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record()
+            refit.refit(moved_t, area=False)
+            ev[1].record()
+            torch.cuda.synchronize()
+            rms.append(ev[0].elapsed_time(ev[1]))
+        entry["refit_device_ms"] = round(float(np.median(rms)), 3)
         if side == 1000:
             t0 = time.perf_counter()
             want, _ = blas.host_build(pos, idx, 8)
             entry["host_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
             entry["speedup_vs_host"] = round(entry["host_ms"] / entry["device_ms"], 1)
             entry["byte_identical"] = buf.cpu().numpy().view(np.uint32).tobytes() == want.view(np.uint32).tobytes()
+            moved = moved_t.cpu().numpy()
+            t0 = time.perf_counter()
+            want_refit, _ = blas.host_refit(want, moved)
+            entry["refit_host_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+            entry["refit_byte_identical"] = \
+                bvh.cpu().numpy().view(np.uint32).tobytes() == want_refit.view(np.uint32).tobytes()
         res[f"terrain_{n}"] = entry
-        del builder, out, buf, pos_t, idx_t
+        del builder, out, buf, pos_t, idx_t, bvh, refit
         torch.cuda.empty_cache()
     res["workload"] = ("seeded terrain meshes (1000^2 and 2000^2 cells, 2 triangles each, shuffled), bins 8; host "
-                       "producer = C++ restatement of buildBLAS on one core")
+                       "producer = C++ restatement of buildBLAS / refitBLAS on one core; refit after scaling the "
+                       "positions by 1.5")
     return res
 
 

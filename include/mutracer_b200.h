@@ -296,6 +296,33 @@ mt_status mtc_build_blas(const mtc_blas_build_input *input, void *scratch, uint6
                          float *out_bvh, uint64_t out_capacity_vec4, mtc_blas_build_result *result,
                          void *stream);
 
+/* ------------------------------------------------ BLAS refit on the device */
+/* refitBLAS (src/renderer/bvhAccel.ts:800-870, BVH2 layout, no displacement)
+ * after vertex deformation: every node box of a layout-0 BLAS rewritten in
+ * place, leaves from their finite vertices, interior nodes from their
+ * children (Math.min/max), the boxes bit-identical to the reference's.
+ * mtc_blas_refit_prepare walks the BLAS once and stores its nodes by depth
+ * in `plan` (device memory of mtc_blas_refit_plan_bytes bytes, 256-byte
+ * aligned), like the reference's cached getBlasRefitData (bvhAccel.ts:
+ * 758-796); it synchronises `stream` once per depth and rejects a buffer
+ * whose offsets leave it or do not follow the depth-first order.  A plan
+ * stays valid while the BLAS topology does. */
+typedef struct mtc_blas_refit_plan_info {
+  uint32_t struct_size;
+  uint32_t node_count;
+  uint32_t levels;                 /* pass to mtc_refit_blas */
+  uint32_t _pad[5];
+} mtc_blas_refit_plan_info;
+uint64_t mtc_blas_refit_plan_bytes(uint64_t bvh_vec4_count);
+mt_status mtc_blas_refit_prepare(const void *bvh, uint64_t bvh_vec4_count, void *plan, uint64_t plan_bytes,
+                                 mtc_blas_refit_plan_info *info, void *stream);
+/* Asynchronous on `stream` (levels + 1 launches; capturable in a graph).
+ * positions: xyz f32 per vertex (device).  surface_area (device, may be
+ * NULL) receives the sum of 2(xz + xy + zy) over the refitted nodes, the
+ * reference's rebuild hint, summed in a fixed tree order. */
+mt_status mtc_refit_blas(void *bvh, uint64_t bvh_vec4_count, const void *plan, uint32_t levels,
+                         const float *positions, uint32_t vertex_count, double *surface_area, void *stream);
+
 /* ------------------------------------------------------ batched form */
 /* One render job of a batched launch: its own scene view, camera, uniform
  * and outputs.  All jobs of a batch run in one persistent kernel that pulls

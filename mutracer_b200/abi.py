@@ -151,6 +151,11 @@ class BlasBuildResult(C.Structure):
                 ("local_bounds", C.c_float * 6), ("host_syncs", C.c_uint32), ("_pad", C.c_uint32 * 3)]
 
 
+class BlasRefitPlanInfo(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("node_count", C.c_uint32), ("levels", C.c_uint32),
+                ("_pad", C.c_uint32 * 5)]
+
+
 class SceneBundle(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("flags", C.c_uint32),
@@ -197,7 +202,7 @@ class SceneInfo(C.Structure):
 
 STRUCT_ORDER = [TraceUniform, CameraUniform, SceneView, Outputs, Hit, Counters, JobDesc, BatchConfig,
                 SceneBundle, RenderSettings, ContextSnapshot, JobSnapshot, SceneInfo, StreamConfig, BlasBuildInput,
-                BlasBuildResult]
+                BlasBuildResult, BlasRefitPlanInfo]
 
 _lib = None
 
@@ -238,6 +243,10 @@ def _declare(lib):
         "mtp_build_binned_sah": (C.c_int, [P, C.c_uint32, C.c_int, P, P, P, P, P]),
         "mtp_build_blas": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.c_int, P, C.c_uint64, P, P]),
         "mtp_energy_lut": (C.c_int, [P]),
+        "mtp_refit_blas": (C.c_int, [P, C.c_uint64, P, C.c_uint32, C.POINTER(C.c_double)]),
+        "mtc_blas_refit_plan_bytes": (C.c_uint64, [C.c_uint64]),
+        "mtc_blas_refit_prepare": (C.c_int32, [P, C.c_uint64, P, C.c_uint64, C.POINTER(BlasRefitPlanInfo), P]),
+        "mtc_refit_blas": (C.c_int32, [P, C.c_uint64, P, C.c_uint32, P, C.c_uint32, P, P]),
         "mtp_camera_look_at": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                          C.POINTER(C.c_double), C.c_double, C.POINTER(CameraUniform)]),
         "mtp_env_distribution": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P]),

@@ -60,6 +60,51 @@ class BlasBuilder:
         return out[: res.vec4_count * 4], res
 
 
+class BlasRefit:
+    """refitBLAS on the device for one layout-0 BLAS (a device tensor view of
+    its vec4 words): the plan is made once (mtc_blas_refit_prepare); refit()
+    rewrites every node box from new positions (mtc_refit_blas,
+    asynchronous, capturable)."""
+
+    def __init__(self, bvh, stream=None):
+        import torch
+        self.bvh = bvh
+        self.vec4 = bvh.numel() // 4
+        self.plan = torch.empty(int(abi.lib().mtc_blas_refit_plan_bytes(self.vec4)), dtype=torch.uint8,
+                                device=bvh.device)
+        self.area = torch.zeros(1, dtype=torch.float64, device=bvh.device)
+        info = abi.BlasRefitPlanInfo()
+        info.struct_size = C.sizeof(info)
+        st = stream if stream is not None else torch.cuda.current_stream(bvh.device)
+        abi.check(abi.lib().mtc_blas_refit_prepare(C.c_void_p(bvh.data_ptr()), self.vec4,
+                                                   C.c_void_p(self.plan.data_ptr()), self.plan.numel(),
+                                                   C.byref(info), C.c_void_p(st.cuda_stream)))
+        self.levels, self.nodes = info.levels, info.node_count
+
+    def refit(self, positions, stream=None, area=True):
+        """positions: (V, 3) float32 on the device.  Returns the device
+        float64 tensor receiving the summed surface area (when area)."""
+        import torch
+        st = stream if stream is not None else torch.cuda.current_stream(self.bvh.device)
+        abi.check(abi.lib().mtc_refit_blas(C.c_void_p(self.bvh.data_ptr()), self.vec4,
+                                           C.c_void_p(self.plan.data_ptr()), self.levels,
+                                           C.c_void_p(positions.data_ptr()) if positions.numel() else None,
+                                           positions.numel() // 3,
+                                           C.c_void_p(self.area.data_ptr()) if area else None,
+                                           C.c_void_p(st.cuda_stream)))
+        return self.area
+
+
+def host_refit(buffer, positions):
+    """The host refitBLAS (C++ restatement) on a copy: (buffer f32, area)."""
+    out = np.array(buffer, np.float32)
+    pos = np.ascontiguousarray(positions, np.float32)
+    area = C.c_double()
+    abi.check(abi.lib().mtp_refit_blas(out.ctypes.data, out.size // 4, pos.ctypes.data if pos.size else None,
+                                       len(pos), C.byref(area)))
+    return out, area.value
+
+
 def terrain_mesh(w, h, seed=0, amplitude=0.3):
     """Seeded height-field mesh over the unit square: (w+1) x (h+1) vertices,
     2 w h triangles in a shuffled order (positions f32 (V, 3), indices u32
@@ -99,6 +144,7 @@ def main(argv=None):
     p.add_argument("--side", type=int, default=2000, help="cells per side (2 side^2 triangles)")
     p.add_argument("--bins", type=int, default=8)
     p.add_argument("--repeat", type=int, default=1)
+    p.add_argument("--refit", action="store_true", help="also time the refit plan and device refits")
     a = p.parse_args(argv)
     pos, idx = terrain_mesh(a.side, a.side, seed=3)
     pos_t, idx_t = torch.from_numpy(pos).cuda(), torch.from_numpy(idx.view(np.int32)).cuda()
@@ -112,6 +158,21 @@ def main(argv=None):
         ms = (time.perf_counter() - t0) * 1e3
         print(json.dumps({"triangles": len(idx), "ms": round(ms, 3), "nodes": res.node_count,
                           "max_depth": res.max_depth, "host_syncs": res.host_syncs}), flush=True)
+    if a.refit:
+        bvh = out[: res.vec4_count * 4]
+        t0 = time.perf_counter()
+        r = BlasRefit(bvh)
+        plan_ms = (time.perf_counter() - t0) * 1e3
+        moved = pos_t * 1.5
+        r.refit(moved)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for _ in range(a.repeat):
+            ev[0].record()
+            r.refit(moved, area=False)
+            ev[1].record()
+            torch.cuda.synchronize()
+            print(json.dumps({"refit_triangles": len(idx), "plan_ms": round(plan_ms, 3), "levels": r.levels,
+                              "refit_ms": round(ev[0].elapsed_time(ev[1]), 3)}), flush=True)
 
 
 if __name__ == "__main__":

@@ -196,6 +196,17 @@ int mtp_scene_mesh(void *scene, uint32_t mesh, float *positions, uint32_t *indic
   return MT_OK;
 }
 
+int mtp_refit_blas(float *bvh, uint64_t vec4Count, const float *positions, uint32_t vertexCount, double *area) {
+  if (!bvh || vec4Count < 2 || (vertexCount && !positions)) return MT_ERROR_INVALID_ARGUMENT;
+  try {
+    double a = refitBlasHost(bvh, size_t(vec4Count), positions, vertexCount);
+    if (area) *area = a;
+  } catch (const std::exception &) {
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  return MT_OK;
+}
+
 int mtp_energy_lut(float *out) {
   if (!out) return MT_ERROR_INVALID_ARGUMENT;
   std::vector<float> lut;

@@ -38,6 +38,8 @@ int mtp_build_binned_sah(const float *aabbs, uint32_t count, int bins, uint32_t 
                          uint32_t *leftFirst, uint32_t *primCount, uint32_t *primIndices);
 int mtp_build_blas(const float *positions, uint32_t vertexCount, const uint32_t *indices, uint32_t triCount, int bins,
                    float *out, uint64_t capacity, uint64_t *vec4Count, uint32_t *maxDepth);
+// Host refitBLAS (bvhAccel.ts:800-870) of a layout-0 BLAS buffer in place.
+int mtp_refit_blas(float *bvh, uint64_t vec4Count, const float *positions, uint32_t vertexCount, double *area);
 int mtp_energy_lut(float *out);
 /* CameraUniform of a perspective look-at camera for a width x height image
  * (the generators' own camera construction). */

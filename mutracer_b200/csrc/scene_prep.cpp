@@ -253,6 +253,56 @@ Blas buildBlas(const std::vector<float> &positions, const std::vector<uint32_t> 
   return b;
 }
 
+// bvhAccel.ts:800-870 refitBLAS (BVH2, no displacement): node boxes rewritten
+// in post order (descendants first; in the depth-first layout that is
+// descending offset order), leaves from their vertices with three finite
+// coordinates (an index past the position array is skipped), interior nodes
+// from their children, all with Math.min/max.  Returns the summed surface
+// area 2(xz + xy + zy) in that order (the rebuild hint's numerator).
+double refitBlasHost(float *f, size_t vec4, const float *positions, uint32_t vertexCount) {
+  std::vector<uint32_t> preorder;
+  std::vector<uint32_t> stack = {0};
+  while (!stack.empty()) {
+    uint32_t o = stack.back();
+    stack.pop_back();
+    if (size_t(o) + 2 > vec4) throw std::runtime_error("BLAS node offset outside the buffer");
+    preorder.push_back(o);
+    int32_t w = asInt(f[size_t(o) * 4 + 3]);
+    if (w >= 0) {
+      if (size_t(w) + 2 > vec4 || uint32_t(w) <= o + 2) throw std::runtime_error("BLAS child offset out of order");
+      stack.push_back(uint32_t(w));
+      stack.push_back(o + 2);
+    } else if (size_t(o) + 2 + size_t(-int64_t(w)) > vec4) {
+      throw std::runtime_error("BLAS leaf outside the buffer");
+    }
+  }
+  double area = 0.0;
+  for (size_t k = preorder.size(); k-- > 0;) {
+    float *n = f + size_t(preorder[k]) * 4;
+    int32_t w = asInt(n[3]);
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (w >= 0) {
+      const float *l = n + 8, *r = f + size_t(w) * 4;
+      for (int c = 0; c < 3; c++) { mn[c] = jsMin(l[c], r[c]); mx[c] = jsMax(l[4 + c], r[4 + c]); }
+    } else {
+      for (int32_t t = 0; t < -w; t++) {
+        const float *rec = n + 8 + size_t(t) * 4;
+        for (int c = 0; c < 3; c++) {
+          uint32_t v = uint32_t(asInt(rec[c]));
+          if (v >= vertexCount) continue;
+          const float *p = positions + size_t(v) * 3;
+          if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) continue;
+          for (int k2 = 0; k2 < 3; k2++) { mn[k2] = jsMin(mn[k2], p[k2]); mx[k2] = jsMax(mx[k2], p[k2]); }
+        }
+      }
+    }
+    double x = double(mx[0]) - double(mn[0]), y = double(mx[1]) - double(mn[1]), z = double(mx[2]) - double(mn[2]);
+    area += 2 * (x * z + x * y + z * y);
+    for (int c = 0; c < 3; c++) { n[c] = mn[c]; n[4 + c] = mx[c]; }
+  }
+  return area;
+}
+
 std::vector<float> blasToGpuLayout(const std::vector<float> &f) {
   if (f.empty()) return {};
   auto ptr = [&](uint32_t off) { return asInt(f[size_t(off) * 4 + 3]); };

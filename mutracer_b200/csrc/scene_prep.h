@@ -141,6 +141,10 @@ void setBlasLayout(SceneHost &s, uint32_t layout);
 // index) (right min, leaf count) (right max, first record), node k at vec4
 // 4k, leaf primitive records after the nodes.
 std::vector<float> blasToGpuLayout(const std::vector<float> &bvh2);
+// refitBLAS (bvhAccel.ts:800-870) on a layout-0 BLAS in place; returns the
+// summed node surface area in post order.  Throws on offsets that leave the
+// buffer or break the depth-first order.
+double refitBlasHost(float *bvh, size_t vec4, const float *positions, uint32_t vertexCount);
 
 struct CameraDesc {
   double eye[3], target[3], up[3];

@@ -13,7 +13,8 @@ extern "C" int mtc_struct_sizes(uint32_t *out, uint32_t capacity) {
       uint32_t(sizeof(mtc_job_desc)),      uint32_t(sizeof(mtc_batch_config)),   uint32_t(sizeof(mt_scene_bundle)),
       uint32_t(sizeof(mt_render_settings)), uint32_t(sizeof(mt_context_snapshot)), uint32_t(sizeof(mt_job_snapshot)),
       uint32_t(sizeof(mtp_scene_info_t)), uint32_t(sizeof(mtc_stream_config)),
-      uint32_t(sizeof(mtc_blas_build_input)), uint32_t(sizeof(mtc_blas_build_result))};
+      uint32_t(sizeof(mtc_blas_build_input)), uint32_t(sizeof(mtc_blas_build_result)),
+      uint32_t(sizeof(mtc_blas_refit_plan_info))};
   uint32_t n = sizeof(sizes) / sizeof(sizes[0]);
   for (uint32_t i = 0; i < n && i < capacity; i++) out[i] = sizes[i];
   return int(n);

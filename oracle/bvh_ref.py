@@ -186,3 +186,46 @@ def layout_bvh2(node_count, left_first, prim_count):
         if not prims:
             stack += [int(left_first[node]) + 1, depth + 1, int(left_first[node]), depth + 1]
     return order, offsets, vec4, max_depth
+
+
+def refit_blas(buffer, positions):
+    """bvhAccel.ts:800-870 refitBLAS (BVH2, no displacement) on a copy of a
+    layout-0 BLAS buffer: post order (descendants before ancestors), leaves
+    from the finite vertices of their triangles (indices past the position
+    array skipped), interior nodes from their children, Math.min/max.
+    Returns (buffer f32, summed surface area in post order)."""
+    f = np.array(buffer, dtype=np.float32).reshape(-1, 4)
+    ints = f.view(np.int32)
+    pos = np.asarray(positions, dtype=np.float32).reshape(-1, 3)
+    preorder, stack = [], [0]
+    while stack:
+        o = stack.pop()
+        preorder.append(o)
+        w = int(ints[o, 3])
+        if w >= 0:
+            stack += [w, o + 2]
+    area = 0.0
+    for o in reversed(preorder):
+        w = int(ints[o, 3])
+        mn, mx = [math.inf] * 3, [-math.inf] * 3
+        if w >= 0:
+            for c in range(3):
+                mn[c] = js_min(float(f[o + 2, c]), float(f[w, c]))
+                mx[c] = js_max(float(f[o + 3, c]), float(f[w + 1, c]))
+        else:
+            for t in range(-w):
+                for c in range(3):
+                    v = int(np.uint32(ints[o + 2 + t, c]))
+                    if v >= len(pos):
+                        continue
+                    p = [float(x) for x in pos[v]]
+                    if not all(math.isfinite(x) for x in p):
+                        continue
+                    for k in range(3):
+                        mn[k] = js_min(mn[k], p[k])
+                        mx[k] = js_max(mx[k], p[k])
+        x, y, z = mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]
+        area += 2 * (x * z + x * y + z * y)
+        f[o, :3] = mn
+        f[o + 1, :3] = mx
+    return f.reshape(-1), area
