@@ -243,6 +243,8 @@ def _declare(lib):
         "mtp_build_binned_sah": (C.c_int, [P, C.c_uint32, C.c_int, P, P, P, P, P]),
         "mtp_build_blas": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.c_int, P, C.c_uint64, P, P]),
         "mtp_energy_lut": (C.c_int, [P]),
+        "mtp_light_alias_table": (C.c_int, [P, C.c_uint32, P, P, C.POINTER(C.c_double)]),
+        "mtp_light_power": (C.c_double, [C.c_int, P, C.c_float, C.c_float, C.c_float]),
         "mtp_refit_blas": (C.c_int, [P, C.c_uint64, P, C.c_uint32, C.POINTER(C.c_double)]),
         "mtc_blas_refit_plan_bytes": (C.c_uint64, [C.c_uint64]),
         "mtc_blas_refit_prepare": (C.c_int32, [P, C.c_uint64, P, C.c_uint64, C.POINTER(BlasRefitPlanInfo), P]),

@@ -207,6 +207,27 @@ int mtp_refit_blas(float *bvh, uint64_t vec4Count, const float *positions, uint3
   return MT_OK;
 }
 
+int mtp_light_alias_table(const double *weights, uint32_t n, uint32_t *words, float *pmfs, double *total) {
+  if (!weights || !words || !n) return MT_ERROR_INVALID_ARGUMENT;
+  std::vector<int> types(n, MTC_CHOICE_ANALYTIC), indices(n);
+  for (uint32_t i = 0; i < n; i++) indices[i] = int(i);
+  AliasTable t = buildAlias(types, indices, std::vector<double>(weights, weights + n));
+  std::memcpy(words, t.words.data(), std::min<size_t>(t.words.size(), size_t(n) * 4) * 4);
+  if (pmfs) for (uint32_t i = 0; i < n && i < t.pmfs.size(); i++) pmfs[i] = t.pmfs[i];
+  if (total) *total = t.total;
+  return MT_OK;
+}
+
+double mtp_light_power(int type, const float *color, float intensity, float area, float radius) {
+  LightDesc L;
+  L.type = type;
+  for (int c = 0; c < 3; c++) L.color[c] = color ? color[c] : 1.0f;
+  L.intensity = intensity;
+  L.area = area;
+  L.radius = radius;
+  return lightPower(L);
+}
+
 int mtp_energy_lut(float *out) {
   if (!out) return MT_ERROR_INVALID_ARGUMENT;
   std::vector<float> lut;

@@ -41,6 +41,11 @@ int mtp_build_blas(const float *positions, uint32_t vertexCount, const uint32_t 
 // Host refitBLAS (bvhAccel.ts:800-870) of a layout-0 BLAS buffer in place.
 int mtp_refit_blas(float *bvh, uint64_t vec4Count, const float *positions, uint32_t vertexCount, double *area);
 int mtp_energy_lut(float *out);
+// Light-selection table of `n` weighted choices (source type 2 = analytic,
+// source index = position): 4 words per choice, the PMFs and the total.
+int mtp_light_alias_table(const double *weights, uint32_t n, uint32_t *words, float *pmfs, double *total);
+// Sampling power of one analytic light (type MTC_LIGHT_*).
+double mtp_light_power(int type, const float *color, float intensity, float area, float radius);
 /* CameraUniform of a perspective look-at camera for a width x height image
  * (the generators' own camera construction). */
 int mtp_camera_look_at(uint32_t width, uint32_t height, const double *eye, const double *target, const double *up,

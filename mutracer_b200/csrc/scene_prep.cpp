@@ -802,7 +802,7 @@ void buildEnergyLut(std::vector<float> &lut) {
 }
 
 // ---------------------------------------------------------------- lights
-static double lightPower(const LightDesc &L) {
+double lightPower(const LightDesc &L) {
   double lum = luminanceD(L.color[0], L.color[1], L.color[2]) * L.intensity;
   if (!(lum > 0)) return 0.0;
   switch (L.type) {
@@ -815,13 +815,9 @@ static double lightPower(const LightDesc &L) {
   }
 }
 
-struct AliasTable {
-  std::vector<uint32_t> words;  // 4 per choice
-  std::vector<float> pmfs;
-  double total = 0.0;
-};
+
 // lightSampling.ts:172-212 buildLightAliasTable
-static AliasTable buildAlias(const std::vector<int> &types, const std::vector<int> &indices, const std::vector<double> &weights) {
+AliasTable buildAlias(const std::vector<int> &types, const std::vector<int> &indices, const std::vector<double> &weights) {
   AliasTable t;
   size_t count = weights.size();
   for (double w : weights) t.total += w;

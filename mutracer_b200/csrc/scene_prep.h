@@ -91,6 +91,18 @@ struct LightDesc {
   float frameX[3] = {1, 0, 0};
 };
 
+// estimateAnalyticLightPower (lightSampling.ts): luminance x intensity x
+// emitting area x pi (4 pi for delta emitters).
+double lightPower(const LightDesc &L);
+// buildLightAliasTable (lightSampling.ts:172-212): 16-byte texels
+// (probability f32, alias i32, source type, source index), f32 PMFs, total.
+struct AliasTable {
+  std::vector<uint32_t> words;  // 4 per choice
+  std::vector<float> pmfs;
+  double total = 0.0;
+};
+AliasTable buildAlias(const std::vector<int> &types, const std::vector<int> &indices, const std::vector<double> &weights);
+
 // Environment: RGBA32F image + RG32F distribution + power estimate.
 struct Environment {
   uint32_t width = 0, height = 0;

@@ -1290,6 +1290,19 @@ int oracle_spectrum_cdf(float *out, unsigned capacity) {
 float oracle_spectrum_camera_wavelength(unsigned channel, float u) {
   return oracle::spectrumCameraWavelength(channel, u);
 }
+// spectrum.ts:79-93 spectrumSample on the f32 table (distribution 0-2: RGB
+// camera channels, 3: photons): the wavelength, and its pdf in *pdf.
+float oracle_spectrum_sample(unsigned distribution, float u, float *pdf) {
+  const float *cdf = oracle::spectrumTables().cdf + distribution * 61u;
+  unsigned low = 0, high = 60;
+  while (high - low > 1u) {
+    unsigned middle = (low + high) / 2u;
+    if (cdf[middle] <= u) low = middle; else high = middle;
+  }
+  float mass = cdf[low + 1] - cdf[low];
+  if (pdf) *pdf = mass / 5.0f;
+  return 400.0f + 5.0f * (float(low) + (u - cdf[low]) / mass);
+}
 
 // envMapPdf(uv) and sampleEnvmap(rnd) over a scene's environment:
 // out = {envMapPdf(u, v), sampled pdf, envMapPdf(sampled uv), |direction|}
