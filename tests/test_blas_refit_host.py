@@ -82,3 +82,49 @@ def test_device_entry_points_validate_on_host():
         abi.MT_ERROR_INVALID_ARGUMENT
     assert L.mtc_refit_blas(C.c_void_p(256), 100, C.c_void_p((1 << 20) + 8), 3, None, 0, None, None) == \
         abi.MT_ERROR_INVALID_ARGUMENT
+
+
+def test_refit_moves_parent_bounds():
+    """bvhAccel.test.ts:181-197: moving one vertex to x = 8 moves the root's
+    max x to 8."""
+    pos = np.array([0, 0, 0, 1, 0, 0, 0, 1, 0, 2, 0, 0, 3, 0, 0, 2, 1, 0], np.float32).reshape(-1, 3)
+    idx = np.array([[0, 1, 2], [3, 4, 5]], np.uint32)
+    buf, _ = blas.host_build(pos, idx)
+    moved = pos.copy()
+    moved[4, 0] = 8
+    st, got, _ = host_refit(buf, moved)
+    assert st == abi.MT_OK and got[4] == 8
+
+
+def uv_sphere(width_segments, height_segments, radius=1.0):
+    pos = []
+    for y in range(height_segments + 1):
+        v = y / height_segments
+        for x in range(width_segments + 1):
+            u = x / width_segments
+            pos.append([-radius * np.cos(u * 2 * np.pi) * np.sin(v * np.pi), radius * np.cos(v * np.pi),
+                        radius * np.sin(u * 2 * np.pi) * np.sin(v * np.pi)])
+    idx = []
+    w = width_segments + 1
+    for y in range(height_segments):
+        for x in range(width_segments):
+            a, b, c, d = y * w + x + 1, y * w + x, (y + 1) * w + x, (y + 1) * w + x + 1
+            if y != 0:
+                idx.append([a, b, d])
+            if y != height_segments - 1:
+                idx.append([b, c, d])
+    return np.array(pos, np.float32), np.array(idx, np.uint32)
+
+
+def test_rebuild_hint_after_area_doubles():
+    """binnedSahBvh.test.ts:196-207: refits at scale 0.99 and 1.3 keep the
+    BLAS; at 1.6 the node area exceeds twice the build's (rebuild)."""
+    pos, idx = uv_sphere(16, 8)
+    buf, _ = blas.host_build(pos, idx)
+    _, _, build_area = host_refit(buf, pos)
+    for scale, keep in ((0.99, True), (1.3, True), (1.6, False)):
+        st, got, area = host_refit(buf, (pos * np.float32(scale)).astype(np.float32))
+        assert st == abi.MT_OK and (not (area > build_area * 2)) == keep
+        f = got.reshape(-1, 4)
+        assert np.allclose(f[0, :3], (pos * np.float32(scale)).min(0)) and \
+            np.allclose(f[1, :3], (pos * np.float32(scale)).max(0))

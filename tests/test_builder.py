@@ -198,3 +198,25 @@ def test_blas_skips_nan_and_out_of_range_triangles():
         else:
             leaves += [tuple(words[o + 2 + i, :3]) for i in range(-words[o, 3])]
     assert sorted(leaves) == [(0, 1, 2), (4, 5, 6)]
+
+
+def test_bin_edge_probe_stays_inside_its_ancestors():
+    """binnedSahBvh.test.ts:106-131: a centroid on the boundary between two
+    root bins is partitioned to the side whose bounds contain it."""
+    f = lambda x: float(np.float32(x))
+    lo, hi, c = -1000.0, f(1000.3), f(0.14999441802501678)
+    boxes = [lo, 0, 0, lo + 0.01, 1, 1, hi - 0.01, 0, 0, hi, 1, 1, c, 0, 0, c, 1, 1]
+    for b in range(8):
+        x = lo + ((b + 0.5) * (hi - lo)) / 8
+        boxes += [x - 0.01, 0, 0, x + 0.01, 1, 1]
+    aabbs = np.array(boxes, np.float32).reshape(-1, 6)
+    m, bounds, lf, pc, pi = cpp_build(aabbs, 8)
+    ref = bvh_ref.build_binned_sah(aabbs, 8)
+    assert m == ref[0] and np.array_equal(bounds.view(np.uint32), ref[1][:m].view(np.uint32))
+
+    def contains(node):
+        prims = list(pi[lf[node]: lf[node] + pc[node]]) if pc[node] else contains(lf[node]) + contains(lf[node] + 1)
+        for p in prims:
+            assert (aabbs[p, :3] >= bounds[node, :3]).all() and (aabbs[p, 3:] <= bounds[node, 3:]).all()
+        return prims
+    assert len(contains(0)) == len(aabbs)

@@ -130,3 +130,18 @@ def test_scene_blases_rebuilt_on_device(kind, params):
         assert res.vec4_count == length
         want = host.bvh[offset * 4: (offset + length) * 4]
         assert got.view(np.uint32).tobytes() == want.view(np.uint32).tobytes()
+
+
+@pytest.mark.gpu
+def test_bin_edge_probe_as_triangles():
+    """The bin-edge probe of binnedSahBvh.test.ts:106-131, each box given as
+    a triangle spanning its corners (the triangle's box is the box)."""
+    f = lambda x: float(np.float32(x))
+    lo, hi, c = -1000.0, f(1000.3), f(0.14999441802501678)
+    boxes = [[lo, 0, 0, lo + 0.01, 1, 1], [hi - 0.01, 0, 0, hi, 1, 1], [c, 0, 0, c, 1, 1]]
+    for b in range(8):
+        x = lo + ((b + 0.5) * (hi - lo)) / 8
+        boxes.append([x - 0.01, 0, 0, x + 0.01, 1, 1])
+    b = np.array(boxes, np.float32)
+    pos = np.stack([b[:, :3], b[:, 3:], np.concatenate([b[:, :1], b[:, 4:5], b[:, 2:3]], 1)], 1).reshape(-1, 3)
+    check_same(pos, np.arange(len(pos), dtype=np.uint32).reshape(-1, 3))

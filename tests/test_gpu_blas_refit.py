@@ -76,3 +76,21 @@ def test_refit_after_device_build_and_malformed():
     bad.view(torch.int32)[3] = bad.numel() // 4 + 10   # root's right child past the end
     with pytest.raises(abi.MtError):
         blas.BlasRefit(bad)
+
+
+@pytest.mark.gpu
+def test_device_rebuild_hint():
+    """binnedSahBvh.test.ts:196-207 through the device refit's area."""
+    from tests.test_blas_refit_host import uv_sphere
+    pos, idx = uv_sphere(16, 8)
+    buf, _ = blas.host_build(pos, idx)
+    dev = torch.from_numpy(buf.copy()).cuda()
+    r = blas.BlasRefit(dev)
+    build_area = r.refit(torch.from_numpy(pos).cuda()).item()
+    for scale, keep in ((0.99, True), (1.3, True), (1.6, False)):
+        moved = (pos * np.float32(scale)).astype(np.float32)
+        area = r.refit(torch.from_numpy(moved).cuda()).item()
+        assert (not (area > build_area * 2)) == keep
+        want, want_area = blas.host_refit(buf, moved)
+        assert dev.cpu().numpy().view(np.uint32).tobytes() == want.view(np.uint32).tobytes()
+        assert abs(area - want_area) <= 1e-12 * want_area
