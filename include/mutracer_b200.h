@@ -15,8 +15,9 @@
  *
  *  2. mt_context_* / mt_job_* — the persistent host API of
  *     native/include/mutracer-context.h:57-187 with the status codes of
- *     native/include/mutracer-status.h:15-45.  commit takes the flattened
- *     buffer bundle (mt_scene_bundle) instead of the scene descriptor v8.
+ *     native/include/mutracer-status.h:15-45.  commit / commit_with_settings
+ *     take the scene descriptor v8 (the features this build renders; others
+ *     are refused by name); commit_bundle takes the flattened buffers.
  *
  * All entry points return an mt_status (0 = MT_OK).  Functions that take
  * `char *error, size_t capacity` write a truncated NUL-terminated message.
@@ -503,6 +504,19 @@ int32_t mt_render_settings_default(mt_render_settings *output);
 int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *bundle,
                                  const mt_render_settings *settings, char *error,
                                  size_t capacity);
+/* mutracer-context.h:94 and :132-133: commit a scene descriptor v8 (the
+ * byte layout of native/docs/scene-format.md).  A malformed descriptor returns
+ * MT_ERROR_INVALID_ARGUMENT with a message naming the problem; a valid one
+ * that uses a feature this build does not render (texture maps, material
+ * graphs, IES profiles, background maps, vertex colors, multi-material
+ * meshes, emissive meshes, partial opacity, bevel) returns
+ * MT_ERROR_UNAVAILABLE naming the feature.  Either way the previously
+ * committed scene stays.  commit uses mt_render_settings_default. */
+int32_t mt_context_commit(mt_context handle, const uint8_t *input, size_t length, char *error,
+                          size_t capacity);
+int32_t mt_context_commit_with_settings(mt_context handle, const uint8_t *input, size_t length,
+                                        const mt_render_settings *settings, char *error,
+                                        size_t capacity);
 /* mutracer-context.h:104 */
 int32_t mt_context_render(mt_context handle, uint32_t additional_samples, char *error,
                           size_t capacity);

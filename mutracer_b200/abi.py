@@ -257,6 +257,10 @@ def _declare(lib):
         "mt_context_destroy": (C.c_int32, [C.c_uint64, C.c_char_p, C.c_size_t]),
         "mt_context_commit_bundle": (C.c_int32, [C.c_uint64, C.POINTER(SceneBundle), C.POINTER(RenderSettings),
                                                  C.c_char_p, C.c_size_t]),
+        "mt_context_commit": (C.c_int32, [C.c_uint64, P, C.c_size_t, C.c_char_p, C.c_size_t]),
+        "mt_context_commit_with_settings": (C.c_int32, [C.c_uint64, P, C.c_size_t, C.POINTER(RenderSettings),
+                                                        C.c_char_p, C.c_size_t]),
+        "mtp_descriptor_decode": (P, [P, C.c_size_t, C.POINTER(C.c_int32), C.c_char_p, C.c_size_t]),
         "mt_context_render": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_char_p, C.c_size_t]),
         "mt_context_reset": (C.c_int32, [C.c_uint64, C.c_char_p, C.c_size_t]),
         "mt_context_wait": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_char_p, C.c_size_t]),

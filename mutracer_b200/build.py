@@ -15,7 +15,7 @@ LIB = os.path.join(OUT, "libmutracer_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU = ["megakernel.cu", "batch_noalloc.cu", "wavefront.cu", "bvh_build.cu", "blas_refit.cu"]
-CPP = ["scene_prep.cpp", "host_api.cpp", "context.cpp", "sizes.cpp"]
+CPP = ["scene_prep.cpp", "host_api.cpp", "context.cpp", "sizes.cpp", "descriptor.cpp"]
 
 
 def _deps():

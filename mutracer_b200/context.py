@@ -31,6 +31,18 @@ class Context:
         abi.check(abi.lib().mt_context_commit_bundle(self.handle, C.byref(host_scene.bundle),
                                                      C.byref(settings) if settings is not None else None, e, _ERR), e)
 
+    def commit_descriptor(self, data, settings=None):
+        """mt_context_commit / mt_context_commit_with_settings on a scene
+        descriptor v8 (bytes, e.g. mutracer_b200.descriptor.Descriptor)."""
+        e = _err()
+        buf = np.frombuffer(bytes(data), np.uint8)
+        ptr = C.c_void_p(buf.ctypes.data) if buf.size else None
+        if settings is None:
+            abi.check(abi.lib().mt_context_commit(self.handle, ptr, buf.size, e, _ERR), e)
+        else:
+            abi.check(abi.lib().mt_context_commit_with_settings(self.handle, ptr, buf.size, C.byref(settings), e,
+                                                                _ERR), e)
+
     def render(self, samples):
         e = _err()
         abi.check(abi.lib().mt_context_render(self.handle, samples, e, _ERR), e)

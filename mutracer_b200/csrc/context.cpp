@@ -18,6 +18,8 @@
 #include <vector>
 
 #include "../../include/mutracer_b200.h"
+#include "mtp_api.h"
+#include "scene_prep.h"
 
 namespace {
 
@@ -310,6 +312,37 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   c->failed = false;
   c->lastCommit = MT_COMMIT_FULL;
   return MT_OK;
+}
+
+// mutracer-context.h:94 / :132-133: the scene descriptor v8 decoded (and
+// validated) on the host, then committed like a buffer bundle.  A rejected
+// descriptor leaves the previous scene committed.
+int32_t mt_context_commit_with_settings(mt_context handle, const uint8_t *input, size_t length,
+                                        const mt_render_settings *settings, char *error, size_t capacity) {
+  if (!findContext(handle)) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  if (settings && settings->struct_size != sizeof(mt_render_settings)) {
+    setError(error, capacity, "settings struct_size");
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  mtp::SceneHost scene;
+  std::string message;
+  int32_t st = mtp::decodeSceneDescriptor(input, length, scene, message);
+  if (st != MT_OK) {
+    setError(error, capacity, message);
+    return st;
+  }
+  mt_render_settings defaults;
+  if (!settings) {
+    mt_render_settings_default(&defaults);
+    settings = &defaults;
+  }
+  mt_scene_bundle bundle;
+  mtp_scene_bundle(&scene, &bundle);
+  return mt_context_commit_bundle(handle, &bundle, settings, error, capacity);
+}
+
+int32_t mt_context_commit(mt_context handle, const uint8_t *input, size_t length, char *error, size_t capacity) {
+  return mt_context_commit_with_settings(handle, input, length, nullptr, error, capacity);
 }
 
 int32_t mt_context_render(mt_context handle, uint32_t additional, char *error, size_t capacity) {

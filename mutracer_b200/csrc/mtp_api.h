@@ -50,6 +50,10 @@ double mtp_light_power(int type, const float *color, float intensity, float area
  * (the generators' own camera construction). */
 int mtp_camera_look_at(uint32_t width, uint32_t height, const double *eye, const double *target, const double *up,
                        double fov_y_deg, mtc_camera_uniform *out);
+/* Decodes a scene descriptor v8 (the input of mt_context_commit) into a host
+ * scene (free with mtp_scene_free); NULL with *status and a message when the
+ * descriptor is rejected.  The same decoding mt_context_commit runs. */
+void *mtp_descriptor_decode(const uint8_t *bytes, size_t length, int32_t *status, char *error, size_t capacity);
 int mtp_env_distribution(const float *image, uint32_t width, uint32_t height, float *distribution, double *power);
 
 #ifdef __cplusplus

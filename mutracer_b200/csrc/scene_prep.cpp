@@ -1001,7 +1001,8 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
     types.push_back(type); idx.push_back(index); weights.push_back(w);
   };
   push(MTC_CHOICE_ENVIRONMENT, 0, s.env.image.empty() ? 0.0 : s.env.power);
-  for (size_t i = 0; i < lights.size(); i++) push(MTC_CHOICE_ANALYTIC, int(i), lightPower(lights[i]));
+  for (size_t i = 0; i < lights.size(); i++)
+    push(MTC_CHOICE_ANALYTIC, int(i), lights[i].packed ? lights[i].power : lightPower(lights[i]));
   AliasTable alias = buildAlias(types, idx, weights);
   std::vector<float> analyticPmf(lights.size(), 0.0f);
   float envPmf = 0.0f;
@@ -1020,6 +1021,11 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   for (size_t i = 0; i < lights.size(); i++) {
     const LightDesc &L = lights[i];
     float *d = &s.lights[i * 24];
+    if (L.packed) {
+      std::memcpy(d, L.rows, sizeof(L.rows));
+      d[16] = analyticPmf[i];
+      continue;
+    }
     d[0] = L.position[0]; d[1] = L.position[1]; d[2] = L.position[2]; d[3] = float(L.type);
     d[4] = L.color[0] * L.intensity; d[5] = L.color[1] * L.intensity; d[6] = L.color[2] * L.intensity;
     d[15] = -1.0f;

@@ -89,6 +89,11 @@ struct LightDesc {
   float u[3] = {1, 0, 0}, v[3] = {0, 0, 1};  // rect: full edge vectors; disk: frame * radius
   float radius = 0.0f, spread = 1.0f, area = 1.0f;
   float frameX[3] = {1, 0, 0};
+  // Rows packed by the caller (every analytic type, wgpuSceneUniform.ts:70-152)
+  // and their selection power; assembleScene then only writes the PMF word.
+  bool packed = false;
+  float rows[24] = {};
+  double power = 0.0;
 };
 
 // estimateAnalyticLightPower (lightSampling.ts): luminance x intensity x
@@ -174,6 +179,10 @@ struct MeshData {
 void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std::vector<Instance> &instances,
                    const std::vector<MaterialDesc> &materials, const std::vector<LightDesc> &lights, int blasBins,
                    int tlasBins, bool normalFloat);
+
+// Scene descriptor v8 (mt_context_commit's input) decoded into `s`: MT_OK,
+// or the status of a rejected descriptor with `message` naming the problem.
+int32_t decodeSceneDescriptor(const uint8_t *bytes, size_t length, SceneHost &s, std::string &message);
 
 // Synthetic workloads.
 void makeCornell(SceneHost &s, uint32_t width, uint32_t height, uint64_t seed);

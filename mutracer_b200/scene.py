@@ -45,6 +45,15 @@ class SceneHost:
         self.kind = kind
         self.refresh()
 
+    @classmethod
+    def from_handle(cls, handle, kind="descriptor"):
+        """Wraps a host scene made elsewhere (mtp_descriptor_decode)."""
+        self = cls.__new__(cls)
+        self._handle = handle
+        self.kind = kind
+        self.refresh()
+        return self
+
     def refresh(self):
         L = abi.lib()
         self.bundle = abi.SceneBundle()
