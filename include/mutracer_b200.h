@@ -509,7 +509,7 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *bundl
  * MT_ERROR_INVALID_ARGUMENT with a message naming the problem; a valid one
  * that uses a feature this build does not render (texture maps, material
  * graphs, IES profiles, background maps, vertex colors, multi-material
- * meshes, emissive meshes, partial opacity, bevel) returns
+ * meshes, partial opacity, bevel) returns
  * MT_ERROR_UNAVAILABLE naming the feature.  Either way the previously
  * committed scene stays.  commit uses mt_render_settings_default. */
 int32_t mt_context_commit(mt_context handle, const uint8_t *input, size_t length, char *error,

@@ -22,8 +22,8 @@
 // message naming the problem, as the reference's validator does.  Valid
 // descriptors that use what this build does not render (texture maps,
 // material graphs, IES profiles, rect-light textures, background maps,
-// vertex colors, meshes whose triangles use several materials, emissive
-// meshes, partial opacity, bevel, shadow catchers, unlit materials, most
+// vertex colors, meshes whose triangles use several materials, partial
+// opacity, bevel, shadow catchers, unlit materials, most
 // material extensions beyond OpenPBR scalars and colors) are refused with
 // MT_ERROR_UNAVAILABLE and a message naming the feature.
 #include <algorithm>
@@ -301,6 +301,7 @@ LightDesc decodeLight(const Words &d, uint32_t o, uint32_t version, uint32_t ind
 struct DecodedMaterial {
   MaterialDesc desc;
   float emissionColor[3], emissionLuminance, coatColor[3], opacity;
+  double emission[3];  // materialEmission in float64, before the f32 row store
 };
 
 void setColor(float *dst, const float *src) { for (int c = 0; c < 3; c++) dst[c] = src[c]; }
@@ -413,6 +414,7 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
       const double w = std::min(double(md.coatWeight), 1.0);
       e = e * (1 + w * (std::sqrt(std::max(double(m.coatColor[c]), 0.0)) - 1));
     }
+    m.emission[c] = e;
     md.emission[c] = float(e);
   }
   return m;
@@ -440,6 +442,38 @@ std::vector<float> generateNormals(const std::vector<float> &p, const std::vecto
     n[i] = float(x * len); n[i + 1] = float(y * len); n[i + 2] = float(z * len);
   }
   return n;
+}
+
+// collectEmissiveTriangles (lightSampling.ts:237-321) for one instance: world
+// corners through vec3.transformMat4 (f32 results), area 0.5 |e0 x e1| from
+// f32 edges and cross product, triangles below 1e-10 area skipped.
+void collectEmissive(const MeshData &md, const double *m, uint32_t material, double luminanceValue, SceneHost &s) {
+  for (size_t t = 0; t + 2 < md.indices.size(); t += 3) {
+    EmissiveTriangle tri;
+    for (int c = 0; c < 3; c++) {
+      const float *p = &md.positions[size_t(md.indices[t + c]) * 3];
+      const double x = p[0], y = p[1], z = p[2];
+      double w = m[3] * x + m[7] * y + m[11] * z + m[15];
+      if (w == 0) w = 1.0;
+      tri.p[c * 3] = float((m[0] * x + m[4] * y + m[8] * z + m[12]) / w);
+      tri.p[c * 3 + 1] = float((m[1] * x + m[5] * y + m[9] * z + m[13]) / w);
+      tri.p[c * 3 + 2] = float((m[2] * x + m[6] * y + m[10] * z + m[14]) / w);
+    }
+    float e0[3], e1[3], cr[3];
+    for (int k = 0; k < 3; k++) {
+      e0[k] = float(double(tri.p[3 + k]) - tri.p[k]);
+      e1[k] = float(double(tri.p[6 + k]) - tri.p[k]);
+    }
+    cr[0] = float(double(e0[1]) * e1[2] - double(e0[2]) * e1[1]);
+    cr[1] = float(double(e0[2]) * e1[0] - double(e0[0]) * e1[2]);
+    cr[2] = float(double(e0[0]) * e1[1] - double(e0[1]) * e1[0]);
+    const double area = 0.5 * std::sqrt(double(cr[0]) * cr[0] + double(cr[1]) * cr[1] + double(cr[2]) * cr[2]);
+    if (!(area > 1e-10) || !std::isfinite(area)) continue;
+    tri.area = area;
+    tri.luminance = luminanceValue;
+    tri.material = int32_t(material);
+    s.emissive.push_back(tri);
+  }
 }
 
 void decodeScene(const Words &d, SceneHost &s) {
@@ -515,12 +549,12 @@ void decodeScene(const Words &d, SceneHost &s) {
   }
   // Materials.
   std::vector<MaterialDesc> mats(materials);
-  std::vector<bool> emissive(materials);
+  std::vector<double> samplingLuminance(materials);
   for (uint32_t i = 0; i < materials; i++) {
     DecodedMaterial m = decodeMaterial(d, u[11] + i * kMaterialWords, version, i);
     mats[i] = m.desc;
-    // Emissive-triangle light sources (scenePreparation.ts:153).
-    emissive[i] = luminance(m.emissionColor) * m.emissionLuminance > 1e-8;
+    // colorLuminance(materialEmission(material)) (lightSampling.ts:255-256).
+    samplingLuminance[i] = std::max(m.emission[0] * 0.2126 + m.emission[1] * 0.7152 + m.emission[2] * 0.0722, 0.0);
   }
   // Geometries.
   std::vector<MeshData> meshData(geometries);
@@ -591,7 +625,6 @@ void decodeScene(const Words &d, SceneHost &s) {
     if (material >= materials) reject(at("mesh", i) + ": material index out of range");
     if (flags & 1) continue;                        // hidden mesh or batch
     if (meshData[g].indices.empty()) continue;      // nothing to intersect
-    if (emissive[material]) unsupported("emissive meshes (emissive-triangle light sampling)");
     auto push = [&](const double *m, const float *color) {
       Instance ins;
       ins.blasIndex = g;
@@ -599,6 +632,7 @@ void decodeScene(const Words &d, SceneHost &s) {
       ins.material = int32_t(255 + (material << 8));
       if (color) setColor(ins.color, color);
       instances.push_back(ins);
+      if (samplingLuminance[material] > 1e-8) collectEmissive(meshData[g], m, material, samplingLuminance[material], s);
     };
     if (!u[23]) {
       push(world, nullptr);
@@ -617,8 +651,7 @@ void decodeScene(const Words &d, SceneHost &s) {
     for (uint32_t k = 0; k < count; k++) {
       double local[16], composed[16];
       d.matrix(u[bo + 1] + uint64_t(k) * 16, "batch instance", local);
-      mul4(world, local, composed);  // the mesh world matrix outside each local matrix
-      for (double &v : composed) v = double(float(v));
+      mul4(world, local, composed);  // the mesh world matrix outside each local matrix (float64)
       float c[3] = {1, 1, 1};
       if (colors)
         for (int j = 0; j < 3; j++) c[j] = d.finite(u[bo + 2] + uint64_t(k) * 3 + j, "batch color");

@@ -1003,19 +1003,33 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   push(MTC_CHOICE_ENVIRONMENT, 0, s.env.image.empty() ? 0.0 : s.env.power);
   for (size_t i = 0; i < lights.size(); i++)
     push(MTC_CHOICE_ANALYTIC, int(i), lights[i].packed ? lights[i].power : lightPower(lights[i]));
+  for (size_t i = 0; i < s.emissive.size(); i++)
+    push(MTC_CHOICE_EMISSIVE_TRIANGLE, int(i), s.emissive[i].area * s.emissive[i].luminance);
   AliasTable alias = buildAlias(types, idx, weights);
-  std::vector<float> analyticPmf(lights.size(), 0.0f);
+  std::vector<float> analyticPmf(lights.size(), 0.0f), emissivePmf(s.emissive.size(), 0.0f);
   float envPmf = 0.0f;
   for (size_t i = 0; i < types.size(); i++) {
     if (types[i] == MTC_CHOICE_ENVIRONMENT) envPmf = alias.pmfs[i];
-    else analyticPmf[idx[i]] = alias.pmfs[i];
+    else if (types[i] == MTC_CHOICE_ANALYTIC) analyticPmf[idx[i]] = alias.pmfs[i];
+    else emissivePmf[idx[i]] = alias.pmfs[i];
   }
+  // Texture: 6 texels per emissive triangle, then the choices (4096 texels
+  // per side at most).
+  const uint32_t emissiveTexels = uint32_t(s.emissive.size()) * 6;
   uint32_t choiceTexels = std::max<uint32_t>(uint32_t(types.size()), 1u);
-  uint32_t totalTexels = std::max(choiceTexels, 1u);
-  uint32_t width = std::min(8192u, std::max(16u, uint32_t(std::ceil(std::sqrt(double(totalTexels)) / 16.0) * 16)));
+  uint32_t totalTexels = std::max(emissiveTexels + choiceTexels, 1u);
+  uint32_t width = std::min(4096u, std::max(16u, uint32_t(std::ceil(std::sqrt(double(totalTexels)) / 16.0) * 16)));
   uint32_t height = (totalTexels + width - 1) / width;
+  if (height > 4096) throw std::runtime_error("Too many emissive triangles for the light sampling texture.");
   s.lightSampling.assign(size_t(width) * height * 4, 0.0f);
-  std::memcpy(s.lightSampling.data(), alias.words.data(), alias.words.size() * 4);
+  for (size_t i = 0; i < s.emissive.size(); i++) {
+    const EmissiveTriangle &t = s.emissive[i];
+    float *d = &s.lightSampling[i * 24];
+    d[0] = t.p[0]; d[1] = t.p[1]; d[2] = t.p[2]; d[3] = emissivePmf[i];
+    d[4] = t.p[3]; d[5] = t.p[4]; d[6] = t.p[5]; d[7] = float(t.area);
+    d[8] = t.p[6]; d[9] = t.p[7]; d[10] = t.p[8]; d[11] = float(t.material);
+  }
+  std::memcpy(s.lightSampling.data() + size_t(emissiveTexels) * 4, alias.words.data(), alias.words.size() * 4);
   // Analytic light records (wgpuSceneUniform.ts:70-152).
   s.lights.assign(lights.size() * 24, 0.0f);
   for (size_t i = 0; i < lights.size(); i++) {
@@ -1059,7 +1073,7 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   u.light_choice_count = int32_t(types.size());
   u.light_weight_total = float(alias.total);
   u.light_sampling_texture_width = int32_t(width);
-  u.light_choice_texel_offset = 0;
+  u.light_choice_texel_offset = int32_t(emissiveTexels);
   u.scene_feature_flags = features;
 }
 

@@ -121,8 +121,20 @@ void makeAnalyticSky(Environment &env, uint32_t width, uint32_t height, uint64_t
 // decodeOpenPbrEnergyLut.ts, tabulated by this build's own quadrature.
 void buildEnergyLut(std::vector<float> &lut);
 
+// One emissive triangle of the light-sampling table (lightSampling.ts
+// collectEmissiveTriangles :237-321, packEmissiveTriangles :329-348): world
+// corners (f32), area and sampling luminance (float64), material index.
+struct EmissiveTriangle {
+  float p[9];
+  double area = 0.0, luminance = 0.0;
+  int32_t material = 0;
+};
+
 struct SceneHost {
   uint32_t width = 0, height = 0, flags = 0;
+  // Emissive triangles sampled by next-event estimation; assembleScene packs
+  // them ahead of the light choices (sceneAssembly.ts:42-84).
+  std::vector<EmissiveTriangle> emissive;
   std::vector<float> bvh;            // TLAS then BLASes
   std::vector<float> instances;      // 40 floats per record
   std::vector<uint32_t> attributes;  // compact vertex words

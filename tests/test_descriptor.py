@@ -357,7 +357,6 @@ def test_spot_and_triangle_material_rules():
 @pytest.mark.parametrize("name,build", [
     ("texture map", lambda d: d.add_material(textures=(0, D.NO_TEXTURE, D.NO_TEXTURE, D.NO_TEXTURE))),
     ("opacity", lambda d: d.add_material(opacity=0.5)),
-    ("emissive mesh", lambda d: d.add_mesh(0, d.add_material(emission_luminance=3.0))),
     ("vertex colors", lambda d: d.add_geometry(QUAD, QUAD_IDX, colors=np.ones((4, 3), F))),
     ("extension", lambda d: d.add_material(extensions=[(53, (0.1,))])),
     ("unlit", lambda d: d.add_material(extensions=[(52, 1)])),
@@ -383,3 +382,42 @@ def test_multi_material_mesh_is_unsupported_but_uniform_table_is_fine():
     a, b = d.add_material(), d.add_material()
     d.add_mesh(g, a, material_table=[a, b])
     assert "several materials" in rejected(d, abi.MT_ERROR_UNAVAILABLE)
+
+
+def test_emissive_meshes_enter_the_light_table():
+    """collectEmissiveTriangles / packEmissiveTriangles / prepareSceneLightSampling:
+    world-space corners, areas, material index and selection pmf per triangle,
+    then the choice table; weights are area x luminance(materialEmission)."""
+    d = base()
+    g = d.add_geometry(QUAD * F(0.5), QUAD_IDX)
+    lamp = d.add_material(emission_color=(1.0, 0.8, 0.6), emission_luminance=4.0, coat_weight=0.5,
+                          extensions=[(26, (0.25, 0.5, 1.0))])
+    world = D.translate([0.5, 1.0, -0.25], 2.0)
+    d.add_mesh(g, lamp, transform=world)
+    h = decoded(d)
+    u = h.uniform
+    assert u.light_choice_texel_offset == 12 and u.light_choice_count == 1 + 2   # rect light + 2 triangles
+    tex = h.light_sampling.reshape(-1, 4)
+    pos = (QUAD * F(0.5)).astype(np.float64)
+    wm = np.array(world, np.float64).reshape(4, 4).T
+    wpos = ((wm[:3, :3] @ pos.T).T + wm[:3, 3]).astype(F)
+    emission = np.array([1.0, 0.8, 0.6]) * 4.0
+    emission *= 1 + 0.5 * (np.sqrt(np.array([0.25, 0.5, 1.0])) - 1)
+    lum = max(float(emission @ [0.2126, 0.7152, 0.0722]), 0.0)
+    pmfs = []
+    for t in range(2):
+        tri = wpos[QUAD_IDX[t * 3: t * 3 + 3]]
+        rows = tex[t * 6: t * 6 + 6]
+        assert np.array_equal(rows[0, :3], tri[0]) and np.array_equal(rows[1, :3], tri[1])
+        assert np.array_equal(rows[2, :3], tri[2]) and rows[2, 3] == lamp
+        e0, e1 = (tri[1] - tri[0]).astype(F), (tri[2] - tri[0]).astype(F)
+        cr = np.cross(e0.astype(np.float64), e1.astype(np.float64)).astype(F).astype(np.float64)
+        area = 0.5 * math.sqrt(float(cr @ cr))
+        assert rows[1, 3] == F(area)
+        pmfs.append(rows[0, 3])
+    rect_power = 5 * math.pi * 0.25                      # intensity 5, 0.5 x 0.5 rect, white
+    total = rect_power + 2 * area * lum
+    assert abs(u.light_weight_total - total) < 1e-4 * total
+    assert all(abs(p - area * lum / total) < 1e-6 for p in pmfs)
+    mat_rows = h.materials.reshape(-1, 26, 4)
+    assert np.allclose(mat_rows[lamp, 3, :3], emission.astype(F))

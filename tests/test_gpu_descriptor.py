@@ -1,8 +1,8 @@
 """mt_context_commit on a scene descriptor v8, on a B200: the image equals
 the same decoded scene committed as a buffer bundle and traced through the
 device-buffer entry point; image parity against the CPU oracle on a scene
-using every analytic light type, instancing, generated normals and an
-environment map with yaw; a rejected descriptor leaves the committed scene."""
+using every analytic light type, an emissive mesh, instancing, generated
+normals and an environment map with yaw; a rejected descriptor leaves the committed scene."""
 import numpy as np
 import pytest
 
@@ -40,6 +40,9 @@ def room(width=96, height=72):
     colors = np.array([[1, 1, 1], [1, .5, .5], [.5, 1, .5], [.5, .5, 1]], F)
     d.add_mesh(box, coated, batch=(transforms, colors))
     d.add_mesh(box, white, hidden=True)
+    panel = d.add_geometry(np.array([[-.5, 0, -.3], [.5, 0, -.3], [.5, 0, .3], [-.5, 0, .3]], F), [0, 1, 2, 0, 2, 3])
+    lamp = d.add_material(emission_color=(1.0, 0.85, 0.7), emission_luminance=3.0)
+    d.add_mesh(panel, lamp, transform=[1, 0, 0, 0, 0, -1, 0, 0, 0, 0, -1, 0, -1.5, 2.6, -0.5, 1])  # facing down
     d.add_light(D.LIGHT_RECT, intensity=6, size=1.0, height_or_inner=0.6, transform=D.look_at([0, 2.8, 0.4], [0, 0, 0]))
     d.add_light(D.LIGHT_SPOT, color=(1, .8, .6), intensity=40, size=0.05, height_or_inner=15, spread_or_outer=35,
                 transform=D.look_at([2, 2.5, 2], [0, 0, 0]))
