@@ -131,13 +131,14 @@ typedef struct mtc_camera_uniform {
 
 /* Compact vertex layout of attrBuffers (src/renderer/compactVertices.ts:7-28):
  * u32 words, position f32x3 at word 0, normal at normal_offset (oct-encoded
- * u32, or f32x3 when normal_float != 0).  UV/color/tangent words may be present
- * in the stride; this build's synthetic scenes carry none. */
+ * u32, or f32x3 when normal_float != 0), the primary UV set (f32x2) at
+ * uv_offset when nonzero (UV_OFF; 0 = no UVs).  Color/tangent words may be
+ * present in the stride and are not read. */
 typedef struct mtc_vertex_layout {
   uint32_t stride;
   uint32_t normal_offset;
   uint32_t normal_float;
-  uint32_t _pad;
+  uint32_t uv_offset;
 } mtc_vertex_layout;
 
 /* Device-side view of the bind groups (all pointers are device pointers). */
@@ -166,7 +167,23 @@ typedef struct mtc_scene_view {
   const void *analytic_lights;     /* binding 2: vec4f[6 * lights_count] */
   uint32_t tlas_stack_size;        /* TLAS_STACK_SIZE (1..64) */
   uint32_t blas_stack_size;        /* BLAS_STACK_SIZE (1..64) */
+  /* Material maps (the map / mapInfo bindings of materialBuffer.wgsl.ts
+   * :258-335 with independent textures): MTC_MAP_VEC4_ROWS vec4 per map
+   * (see mtc_map_record below), texels as RGBA f32 vec4, row 0 at v = 0. */
+  const void *maps;
+  const void *map_texels;
+  uint32_t map_count;
+  uint32_t map_texel_count;        /* texels in map_texels (a map reaching past it samples zero) */
 } mtc_scene_view;
+/* One material map, 3 vec4 (f32 words; integers as their bit patterns):
+ *   [0] width (u32), height (u32), first texel (u32), 0
+ *   [1] UV scale xy, UV offset xy (mapTransform)
+ *   [2] UV set (0 / 1), color linear (1: data or float map, no sRGB decode),
+ *       wrap S, wrap T (0 repeat, 1 clamp to edge, 2 mirrored repeat)
+ * Texels are the decoded RGBA of the stored image (RGBA8 / 255, or the
+ * float image rounded to f16 as the reference's RGBA16F storage keeps it),
+ * rows flipped when the texture is. */
+#define MTC_MAP_VEC4_ROWS 3
 /* flags: shader specialisation constants that are not in the uniform
  * (HAS_MEDIUM, SPECTRAL and SAMPLING_PATTERN of wgpuMaterialConstants.ts:40-70).
  * The sampling pattern (MT_SAMPLING_*) occupies bits 4..5.  BLAS_GPU_LAYOUT is
@@ -228,6 +245,16 @@ mt_status mtc_trace_samples(const mtc_scene_view *scene,
  * querySceneSoftware, intersect.wgsl.ts:660-684 (bounces 0, single-sided). */
 mt_status mtc_query_first_hit(const mtc_scene_view *scene, const float *rays,
                               uint32_t count, mtc_hit *hits, void *stream);
+
+/* Raw material-map lookups: texels[i] (RGBA, 4 floats) = the bilinear
+ * sampleMap of map indices[i] at uvs[2i..2i+1] (materialBuffer.wgsl.ts:
+ * 335-378: the map's UV transform and wrap modes applied, no color decoding);
+ * zero for an index outside the scene's maps.  All arrays in device memory.
+ * No reference counterpart: a diagnostic that exposes the shading code's
+ * texture filter for bit-exact checks. */
+mt_status mtc_sample_maps(const mtc_scene_view *scene, const int32_t *indices,
+                          const float *uvs, uint32_t count, float *texels,
+                          void *stream);
 
 /* Full TLAS refit on the device: rewrites the instance records (inverse
  * transform, transform, BLAS placement) and every TLAS node box from the
@@ -466,6 +493,8 @@ typedef struct mt_scene_bundle {
   uint32_t tlas_stack_size, blas_stack_size;
   mtc_camera_uniform camera;
   mtc_trace_uniform uniform;       /* settings fields are overwritten by mt_render_settings */
+  const float *maps; uint32_t map_count;       /* MTC_MAP_VEC4_ROWS vec4 per map */
+  const float *map_texels; uint64_t map_texel_count;
 } mt_scene_bundle;
 
 /* mutracer-context.h:86-100 */

@@ -33,6 +33,7 @@ MTC_SCENE_BLAS_GPU_LAYOUT = 0x100
 MTC_FEATURE_USE_ENVMAP = 1
 MTC_INSTANCE_VEC4_STRIDE = 10
 MTC_MATERIAL_VEC4_ROWS = 26
+MTC_MAP_VEC4_ROWS = 3
 MTC_LIGHT_VEC4_ROWS = 6
 MTC_ENERGY_LUT_WIDTH = 32
 MTC_ENERGY_LUT_HEIGHT = 2177
@@ -73,7 +74,7 @@ class CameraUniform(C.Structure):
 
 class VertexLayout(C.Structure):
     _fields_ = [("stride", C.c_uint32), ("normal_offset", C.c_uint32), ("normal_float", C.c_uint32),
-                ("_pad", C.c_uint32)]
+                ("uv_offset", C.c_uint32)]
 
 
 class SceneView(C.Structure):
@@ -87,6 +88,7 @@ class SceneView(C.Structure):
         ("env_height", C.c_uint32), ("light_sampling", C.c_void_p), ("light_sampling_texels", C.c_uint32),
         ("blas_offset", C.c_int32), ("energy_lut", C.c_void_p), ("analytic_lights", C.c_void_p),
         ("tlas_stack_size", C.c_uint32), ("blas_stack_size", C.c_uint32),
+        ("maps", C.c_void_p), ("map_texels", C.c_void_p), ("map_count", C.c_uint32), ("map_texel_count", C.c_uint32),
     ]
 
 
@@ -170,6 +172,8 @@ class SceneBundle(C.Structure):
         ("analytic_lights", C.POINTER(C.c_float)),
         ("tlas_stack_size", C.c_uint32), ("blas_stack_size", C.c_uint32),
         ("camera", CameraUniform), ("uniform", TraceUniform),
+        ("maps", C.POINTER(C.c_float)), ("map_count", C.c_uint32),
+        ("map_texels", C.POINTER(C.c_float)), ("map_texel_count", C.c_uint64),
     ]
 
 
@@ -215,6 +219,7 @@ def _declare(lib):
         "mtc_trace_samples": (C.c_int32, [C.POINTER(SceneView), C.POINTER(CameraUniform), C.POINTER(TraceUniform),
                                           C.POINTER(Outputs), C.c_uint32, P, P]),
         "mtc_query_first_hit": (C.c_int32, [C.POINTER(SceneView), P, C.c_uint32, P, P]),
+        "mtc_sample_maps": (C.c_int32, [C.POINTER(SceneView), P, P, C.c_uint32, P, P]),
         "mtc_batch_scratch_bytes": (C.c_size_t, [C.c_uint32]),
         "mtc_trace_batch": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P, P, P, P]),
         "mtc_batch_table_bytes": (C.c_size_t, [C.c_uint32]),

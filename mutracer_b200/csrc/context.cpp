@@ -60,7 +60,7 @@ struct DeviceBuffer {
 };
 
 struct SceneResources {
-  DeviceBuffer bvh, ins, attr, mats, env, envDist, lightData, lut, lights;
+  DeviceBuffer bvh, ins, attr, mats, env, envDist, lightData, lut, lights, maps, mapTexels;
   DeviceBuffer color, normal, albedo, catcher;
   DeviceBuffer average, flag;  // read_pixels staging: averaged image, non-finite flag
   DeviceBuffer stream;         // wavefront state of blocking renders (mtc_stream_run)
@@ -239,7 +239,10 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   if (settings && settings->struct_size != sizeof(mt_render_settings)) { setError(error, capacity, "settings struct_size"); return MT_ERROR_INVALID_ARGUMENT; }
   if (b->width == 0 || b->height == 0 || b->width > 16384 || b->height > 16384 || !b->bvh || !b->instances ||
       !b->attributes || !b->materials || !b->energy_lut || !b->light_sampling || b->vertex_layout.stride < 4 ||
-      (b->env_map && !b->env_distribution) || (b->lights_count && !b->analytic_lights)) {
+      (b->env_map && !b->env_distribution) || (b->lights_count && !b->analytic_lights) ||
+      (b->vertex_layout.uv_offset && (b->vertex_layout.uv_offset < 3 ||
+                                      b->vertex_layout.uv_offset + 2 > b->vertex_layout.stride)) ||
+      (b->map_count && !b->maps) || (b->map_texel_count && !b->map_texels) || b->map_texel_count > UINT32_MAX) {
     setError(error, capacity, "invalid buffer bundle");
     return MT_ERROR_INVALID_ARGUMENT;
   }
@@ -267,6 +270,8 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   up(r->lightData, b->light_sampling, size_t(b->light_sampling_texels) * 16);
   up(r->lut, b->energy_lut, size_t(MTC_ENERGY_LUT_WIDTH) * MTC_ENERGY_LUT_HEIGHT * 4);
   up(r->lights, b->analytic_lights, b->lights_count ? size_t(b->lights_count) * MTC_LIGHT_VEC4_ROWS * 16 : 0);
+  up(r->maps, b->maps, size_t(b->map_count) * MTC_MAP_VEC4_ROWS * 16);
+  up(r->mapTexels, b->map_texels, size_t(b->map_texel_count) * 16);
   for (DeviceBuffer *d : {&r->color, &r->normal, &r->albedo, &r->catcher}) {
     size_t bytes = px * 16 * (d == &r->catcher ? 3 : 1);
     if (e == cudaSuccess) e = d->reserve(bytes);
@@ -296,6 +301,9 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   v.energy_lut = r->lut.data();
   v.analytic_lights = r->lights.data();
   v.tlas_stack_size = b->tlas_stack_size; v.blas_stack_size = b->blas_stack_size;
+  v.maps = b->map_count ? r->maps.data() : nullptr; v.map_count = b->map_count;
+  v.map_texels = b->map_texel_count ? r->mapTexels.data() : nullptr;
+  v.map_texel_count = uint32_t(b->map_texel_count);
   r->width = b->width; r->height = b->height;
   // Publish: accumulation restarts.
   c->scene = std::move(r);

@@ -20,16 +20,30 @@
 //
 // Malformed descriptors are rejected with MT_ERROR_INVALID_ARGUMENT and a
 // message naming the problem, as the reference's validator does.  Valid
-// descriptors that use what this build does not render (texture maps,
-// material graphs, IES profiles, rect-light textures, background maps,
-// vertex colors, meshes whose triangles use several materials, partial
-// opacity, bevel, shadow catchers, unlit materials, most
+// descriptors that use what this build does not render (texture slots other
+// than base color, normal and metallic-roughness, UDIM sets, second UV sets,
+// textures the atlas would downscale, material graphs, IES profiles,
+// rect-light textures, background maps, vertex colors, meshes whose
+// triangles use several materials, partial opacity and base-color alpha
+// blending, UV projections, bevel, shadow catchers, unlit materials, most
 // material extensions beyond OpenPBR scalars and colors) are refused with
 // MT_ERROR_UNAVAILABLE and a message naming the feature.
+//
+// Material textures (scene-records.ts:22-39 decodeTexture, MaterialData.ts
+// :19-56, textureAtlas.ts:134-283, textureAtlasPixels.ts:9-66) become this
+// library's map table: the maps in mergeTexturesFromMaterials order (slot
+// by slot, material by material, one entry per texture), texels as RGBA f32
+// at full size (the atlas keeps full size whenever its shelf packing fits;
+// otherwise the descriptor is refused), rows flipped at packing for flip_y,
+// RGBA8 as byte / 255 or, when any material texture is RGBA32F, every texel
+// rounded to half precision as RGBA16F storage holds it.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <set>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "mtp_api.h"
@@ -302,15 +316,24 @@ struct DecodedMaterial {
   MaterialDesc desc;
   float emissionColor[3], emissionLuminance, coatColor[3], opacity;
   double emission[3];  // materialEmission in float64, before the f32 row store
+  // Descriptor texture indices of the slots this build samples.
+  uint32_t map = NONE, normalMap = NONE, metallicRoughnessMap = NONE;
 };
 
 void setColor(float *dst, const float *src) { for (int c = 0; c < 3; c++) dst[c] = src[c]; }
 
-DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uint32_t index) {
+DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uint32_t index, uint32_t textures) {
   DecodedMaterial m;
   MaterialDesc &md = m.desc;
   float v[14];
   for (int i = 0; i < 14; i++) v[i] = d.finite(o + i, "material value");
+  // Value ranges (scene.rs material validation): unit-interval factors,
+  // IOR >= 1, nonnegative colors and luminance.
+  for (int k : {3, 4, 5, 11, 12, 13})
+    if (!(v[k] >= 0.0f && v[k] <= 1.0f)) reject(at("material", index) + ": values out of range");
+  for (int k : {0, 1, 2, 7, 8, 9, 10})
+    if (v[k] < 0.0f) reject(at("material", index) + ": values out of range");
+  if (v[6] < 1.0f) reject(at("material", index) + ": values out of range");
   setColor(md.baseColor, v);
   md.specularRoughness = v[3];
   md.baseMetalness = v[4];
@@ -324,7 +347,11 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
   if (d.u[o + 14] > 1) reject(at("material", index) + ": thin_walled is 0 or 1");
   md.thin = d.u[o + 14] != 0;
   for (int k = 15; k < 19; k++)
-    if (d.u[o + k] != NONE) unsupported("a material texture map");
+    if (d.u[o + k] != NONE && d.u[o + k] >= textures) reject(at("material", index) + ": texture reference out of range");
+  m.map = d.u[o + 15];
+  m.normalMap = d.u[o + 16];
+  m.metallicRoughnessMap = d.u[o + 17];
+  uint32_t emissiveMap = d.u[o + 18], alphaMode = 0, mapAlphaUsage = 0;
   if (d.u[o + 21]) {
     if (version < 8) reject(at("material", index) + ": graph_offset must be 0 before version 8");
     unsupported("a material graph");
@@ -355,6 +382,21 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
     auto flag = [&](bool &dst) {
       if (u0 > 1 || d.u[w + 2] || d.u[w + 3]) reject(at("material", index) + ": malformed bool extension");
       dst = u0 != 0;
+    };
+    auto pair = [&](float *dst) {
+      if (!std::isfinite(f[0]) || !std::isfinite(f[1]) || d.u[w + 3])
+        reject(at("material", index) + ": malformed vec2 extension");
+      dst[0] = f[0];
+      dst[1] = f[1];
+    };
+    auto choice = [&](uint32_t variants) {
+      if (u0 >= variants || d.u[w + 2] || d.u[w + 3]) reject(at("material", index) + ": invalid material enum");
+      return u0;
+    };
+    auto texture = [&]() {
+      if (d.u[w + 2] || d.u[w + 3]) reject(at("material", index) + ": malformed texture extension");
+      if (u0 != NONE && u0 >= textures) reject(at("material", index) + ": texture reference out of range");
+      return u0;
     };
     switch (id) {
       case 1: scalar(md.baseWeight); break;
@@ -388,15 +430,25 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
       case 36: scalar(m.opacity); break;
       case 37: flag(md.thin); break;
       case 38: flag(md.doubleSided); break;
-      // Texture slots left empty change nothing.
-      case 39: case 40: case 43: case 44: case 46: case 47: case 48: case 49: case 50: case 59: case 64: case 65:
+      case 39: m.map = texture(); break;
+      case 43: emissiveMap = texture(); break;
+      case 44: m.normalMap = texture(); break;
+      case 46: m.metallicRoughnessMap = texture(); break;
+      // Other texture slots left empty change nothing.
+      case 40: case 47: case 48: case 49: case 50: case 59: case 64: case 65:
       case 66: case 67: case 68: case 69: case 70: case 74:
-        if (u0 != NONE) unsupported("a material texture map");
+        if (texture() != NONE) unsupported("material texture slot " + std::to_string(id));
         break;
       case 41:  // alpha mode: auto or opaque keep a fully opaque material opaque
-        if (u0 > 3) reject(at("material", index) + ": alpha mode out of range");
-        if (u0 > 1) unsupported("alpha mask / blend modes");
+        alphaMode = choice(4);
+        if (alphaMode > 1) unsupported("alpha mask / blend modes");
         break;
+      case 45: pair(md.normalScale); break;
+      case 54: mapAlphaUsage = choice(3); break;  // opaque, alpha, transmission
+      case 55:
+        if (choice(4) != 0) unsupported("UV projections");
+        break;
+      case 56: pair(md.uvScale); break;  // uvProjectionScale scales the UVs of every map
       case 51: case 52: {
         bool on = false;
         flag(on);
@@ -407,6 +459,11 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
     }
   }
   if (m.opacity != 1.0f) unsupported("material opacity below 1");
+  if (emissiveMap != NONE) unsupported("an emissive map");
+  // resolveMaterialAlphaMode (MaterialState.ts:251-264): auto with the base
+  // color's alpha as opacity blends, which needs any-hit traversal.
+  if (mapAlphaUsage == 1 && alphaMode == 0 && m.map != NONE) unsupported("base color alpha as opacity");
+  md.mapAlphaUsage = mapAlphaUsage == 1 ? 2 : mapAlphaUsage == 2 ? 3 : 0;  // mapAlphaUsageConstants
   // materialEmission (materialEmission.ts:10-22): emission crosses the coat once.
   for (int c = 0; c < 3; c++) {
     double e = double(m.emissionColor[c]) * m.emissionLuminance;
@@ -447,6 +504,143 @@ std::vector<float> generateNormals(const std::vector<float> &p, const std::vecto
 // collectEmissiveTriangles (lightSampling.ts:237-321) for one instance: world
 // corners through vec3.transformMat4 (f32 results), area 0.5 |e0 x e1| from
 // f32 edges and cross product, triangles below 1e-10 area skipped.
+// ------------------------------------------------------------ textures
+constexpr uint64_t kTextureBudgetBytes = 3ull << 30;  // scene-configuration.ts:8 textureBudgetBytes
+
+struct TextureRecord {
+  uint32_t width, height, storage, pixels, flipY, uvChannel, wrapS, wrapT, udim;
+  float transform[4];  // uv scale xy, uv offset xy
+  std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t> source() const {
+    return {pixels, width, height, storage, flipY};
+  }
+};
+
+// float16Bits (float16.ts:1-16): nearest, ties to even, as RGBA16F storage
+// holds the value; returned widened to f32.
+float halfStored(double value) {
+  auto roundEven = [](double v) {
+    const double integer = std::floor(v), fraction = v - integer;
+    return integer + ((fraction > 0.5 || (fraction == 0.5 && std::fmod(integer, 2.0) == 1.0)) ? 1.0 : 0.0);
+  };
+  const bool negative = value < 0 || (value == 0 && std::signbit(value));
+  const double absolute = std::fabs(value);
+  uint32_t bits;
+  if (std::isnan(absolute)) bits = 0x7e00;
+  else if (absolute >= 65520) bits = 0x7c00;
+  else if (absolute < std::ldexp(1.0, -14)) bits = uint32_t(roundEven(absolute * std::ldexp(1.0, 24)));
+  else {
+    const int exponent = int(std::floor(std::log2(absolute)));
+    bits = uint32_t((exponent + 14) * 1024 + roundEven(absolute / std::ldexp(1.0, exponent - 10)));
+  }
+  const int e = int(bits >> 10) & 31, mantissa = int(bits & 1023);
+  float f;
+  if (e == 31) f = mantissa ? NAN : INFINITY;
+  else if (e == 0) f = float(std::ldexp(double(mantissa), -24));
+  else f = float(std::ldexp(double(1024 + mantissa), e - 25));
+  return negative ? -f : f;
+}
+
+// planTextureAtlas at full size (textureAtlas.ts:196-248 with packTextureAtlas
+// :65-130): true when the shelf packing of the distinct pixel sources fits the
+// atlas's page budget without scaling.
+bool atlasKeepsFullSize(const std::vector<TextureRecord> &sources, uint32_t bytesPerPixel) {
+  const double budget = double(kTextureBudgetBytes);
+  uint32_t maxDimension = 1;
+  for (const TextureRecord &t : sources) maxDimension = std::max({maxDimension, t.width, t.height});
+  const double fromBudget = std::max(1.0, std::floor(std::sqrt(budget / bytesPerPixel)));
+  const uint64_t pageSize = uint64_t(std::max(1.0, std::floor(std::min({double(maxDimension), 16384.0, fromBudget}))));
+  const double pageBytes = double(pageSize) * double(pageSize) * bytesPerPixel;
+  const size_t maxPages = size_t(std::max(1.0, std::min(256.0, std::floor(budget / pageBytes))));
+  if (pageSize < maxDimension) return false;
+  std::vector<size_t> order(sources.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    return sources[a].height != sources[b].height ? sources[a].height > sources[b].height
+                                                   : sources[a].width > sources[b].width;
+  });
+  struct Shelf { uint64_t height, x; };
+  struct Page { uint64_t nextY; std::vector<Shelf> shelves; };
+  std::vector<Page> pages;
+  for (size_t i : order) {
+    const uint64_t w = sources[i].width, h = sources[i].height;
+    bool placed = false;
+    for (size_t layer = 0; layer < pages.size() && !placed; layer++) {
+      Page &page = pages[layer];
+      for (Shelf &shelf : page.shelves)
+        if (h <= shelf.height && shelf.x + w <= pageSize) {
+          shelf.x += w;
+          placed = true;
+          break;
+        }
+      if (!placed && page.nextY + h <= pageSize) {
+        page.shelves.push_back({h, w});
+        page.nextY += h;
+        placed = true;
+      }
+    }
+    if (!placed) pages.push_back({h, {{h, w}}});
+  }
+  return pages.size() <= maxPages;
+}
+
+// The map table of `maps` (descriptor texture indices in MaterialData order):
+// one record of MTC_MAP_VEC4_ROWS vec4 per map and the texels of each
+// distinct pixel source (writeRawAtlasPlacement at unit scale).
+void packMaterialMaps(const Words &d, const std::vector<TextureRecord> &records, const std::vector<uint32_t> &maps,
+                      bool geometryHasUv1, SceneHost &s) {
+  bool floatStorage = false;
+  std::vector<TextureRecord> sources;
+  std::set<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>> seen;
+  for (uint32_t t : maps) {
+    const TextureRecord &r = records[t];
+    if (r.udim) unsupported("UDIM texture sets");
+    if (r.uvChannel == 1 && geometryHasUv1) unsupported("textures on a second UV set");
+    floatStorage |= r.storage == 1;
+    if (seen.insert(r.source()).second) sources.push_back(r);
+  }
+  if (!atlasKeepsFullSize(sources, floatStorage ? 8 : 4)) unsupported("material textures that the atlas would downscale");
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>, uint32_t> firstTexel;
+  s.maps.assign(maps.size() * MTC_MAP_VEC4_ROWS * 4, 0.0f);
+  for (size_t i = 0; i < maps.size(); i++) {
+    const TextureRecord &r = records[maps[i]];
+    auto found = firstTexel.find(r.source());
+    uint32_t first;
+    if (found != firstTexel.end()) {
+      first = found->second;
+    } else {
+      first = uint32_t(s.mapTexels.size() / 4);
+      firstTexel[r.source()] = first;
+      s.mapTexels.resize(s.mapTexels.size() + size_t(r.width) * r.height * 4);
+      float *out = &s.mapTexels[size_t(first) * 4];
+      for (uint32_t y = 0; y < r.height; y++) {
+        const uint32_t sy = r.flipY ? r.height - 1 - y : y;
+        for (uint32_t x = 0; x < r.width; x++) {
+          const uint64_t texel = uint64_t(sy) * r.width + x;
+          for (int c = 0; c < 4; c++) {
+            float v;
+            if (r.storage == 0) {
+              const uint32_t byte = (d.u[r.pixels + texel] >> (8 * c)) & 255u;
+              v = floatStorage ? halfStored(double(byte) / 255.0) : float(byte) / 255.0f;
+            } else {
+              v = halfStored(double(d.f[r.pixels + texel * 4 + c]));
+            }
+            *out++ = v;
+          }
+        }
+      }
+    }
+    float *row = &s.maps[i * MTC_MAP_VEC4_ROWS * 4];
+    uint32_t head[3] = {r.width, r.height, first};
+    std::memcpy(row, head, sizeof(head));
+    for (int k = 0; k < 4; k++) row[4 + k] = r.transform[k];
+    // uv channel, color linear (float sources), wrap S, wrap T (0 repeat, 1 clamp, 2 mirror)
+    row[8] = float(r.uvChannel);
+    row[9] = r.storage == 1 ? 1.0f : 0.0f;
+    row[10] = float(r.wrapS);
+    row[11] = float(r.wrapT);
+  }
+}
+
 void collectEmissive(const MeshData &md, const double *m, uint32_t material, double luminanceValue, SceneHost &s) {
   for (size_t t = 0; t + 2 < md.indices.size(); t += 3) {
     EmissiveTriangle tri;
@@ -527,9 +721,32 @@ void decodeScene(const Words &d, SceneHost &s) {
     unsupported("a grounded background projection");
   }
 
+  // Texture records (the reference validator's raw-texture rules).
+  std::vector<TextureRecord> textureRecords(textures);
+  {
+    std::set<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>> spans;
+    uint64_t pixels = 0;
+    for (uint32_t i = 0; i < textures; i++) {
+      const uint32_t o = u[13] + i * textureWords;
+      TextureRecord &t = textureRecords[i];
+      t = {u[o], u[o + 1], u[o + 2], u[o + 3], u[o + 4], u[o + 5], u[o + 10], u[o + 11], version >= 7 ? u[o + 12] : 0u,
+           {0, 0, 0, 0}};
+      if (t.width == 0 || t.height == 0 || t.width > 16384 || t.height > 16384 || t.storage > 1 || t.flipY > 1 ||
+          t.uvChannel > 1 || t.wrapS > 2 || t.wrapT > 2 || t.udim > 1 || (t.udim && (t.width % 10 || t.height % 10)))
+        reject(at("texture", i) + ": invalid raw texture record");
+      if (spans.insert(t.source()).second) pixels += uint64_t(t.width) * t.height;
+      if (pixels > kTextureBudgetBytes / 4 + 4194304u) reject("textures exceed the material plus environment input budget");
+      const uint64_t count = uint64_t(t.width) * t.height * (t.storage ? 4 : 1);
+      if (!d.array("texture pixels", t.pixels, count)) reject(at("texture", i) + " has no pixels");
+      if (t.storage)
+        for (uint64_t k = 0; k < count; k++) d.finite(t.pixels + k, "texture pixel");
+      for (int k = 0; k < 4; k++) t.transform[k] = d.finite(o + 6 + k, "texture UV transform");
+    }
+  }
+
   s.width = width;
   s.height = height;
-  // Textures: only the environment map is read (linear RGBA32F).
+  // The environment map (linear RGBA32F).
   if (envPlusOne) {
     const uint32_t o = u[13] + (envPlusOne - 1) * textureWords;
     const uint32_t w = u[o], h = u[o + 1];
@@ -550,15 +767,20 @@ void decodeScene(const Words &d, SceneHost &s) {
   // Materials.
   std::vector<MaterialDesc> mats(materials);
   std::vector<double> samplingLuminance(materials);
+  std::vector<uint32_t> slotTextures[3];  // map, normalMap, metallicRoughnessMap per material
   for (uint32_t i = 0; i < materials; i++) {
-    DecodedMaterial m = decodeMaterial(d, u[11] + i * kMaterialWords, version, i);
+    DecodedMaterial m = decodeMaterial(d, u[11] + i * kMaterialWords, version, i, textures);
     mats[i] = m.desc;
+    slotTextures[0].push_back(m.map);
+    slotTextures[1].push_back(m.normalMap);
+    slotTextures[2].push_back(m.metallicRoughnessMap);
     // colorLuminance(materialEmission(material)) (lightSampling.ts:255-256).
     samplingLuminance[i] = std::max(m.emission[0] * 0.2126 + m.emission[1] * 0.7152 + m.emission[2] * 0.0722, 0.0);
   }
   // Geometries.
   std::vector<MeshData> meshData(geometries);
   std::vector<std::vector<uint32_t>> vertexMaterial(geometries);
+  bool geometryHasUv1 = false, tangentFrames = false;
   for (uint32_t g = 0; g < geometries; g++) {
     const uint32_t o = u[9] + g * kGeometryWords;
     const uint32_t vc = u[o], ic = u[o + 1];
@@ -579,10 +801,13 @@ void decodeScene(const Words &d, SceneHost &s) {
     } else {
       md.normals = generateNormals(md.positions, md.indices, vc);
     }
-    d.array("uvs", u[o + 5], uint64_t(vc) * 2);      // only texture maps read UVs
-    d.array("uv1s", u[o + 6], uint64_t(vc) * 2);
+    if (d.array("uvs", u[o + 5], uint64_t(vc) * 2)) {
+      md.uvs.assign(d.f + u[o + 5], d.f + u[o + 5] + size_t(vc) * 2);
+      tangentFrames = true;  // decodeGeometry generates tangents from UVs
+    }
+    geometryHasUv1 |= d.array("uv1s", u[o + 6], uint64_t(vc) * 2);
     if (d.array("vertex colors", u[o + 7], uint64_t(vc) * 3)) unsupported("vertex colors");
-    d.array("tangents", u[o + 8], uint64_t(vc) * 4);  // only anisotropy reads tangents
+    tangentFrames |= d.array("tangents", u[o + 8], uint64_t(vc) * 4);
     if (d.array("material indices", u[o + 9], vc)) {
       vertexMaterial[g].assign(u + u[o + 9], u + u[o + 9] + vc);
       const std::vector<uint32_t> &vm = vertexMaterial[g];
@@ -624,6 +849,10 @@ void decodeScene(const Words &d, SceneHost &s) {
     }
     if (material >= materials) reject(at("mesh", i) + ": material index out of range");
     if (flags & 1) continue;                        // hidden mesh or batch
+    // Vertex tangents orient anisotropic lobes (openpbr_make_basis); this
+    // build shades them in the normal's own frame.
+    if (tangentFrames && mats[material].specularAnisotropy > 0)
+      unsupported("anisotropic materials in a scene with vertex tangents or UVs");
     if (meshData[g].indices.empty()) continue;      // nothing to intersect
     auto push = [&](const double *m, const float *color) {
       Instance ins;
@@ -657,6 +886,29 @@ void decodeScene(const Words &d, SceneHost &s) {
         for (int j = 0; j < 3; j++) c[j] = d.finite(u[bo + 2] + uint64_t(k) * 3 + j, "batch color");
       push(composed, c);
     }
+  }
+  // Material maps: MaterialData's texture list (mergeTexturesFromMaterials
+  // over the slots map, normalMap, metallicRoughnessMap in that order, each
+  // over the materials in order, one entry per texture).
+  std::vector<uint32_t> mapTextures;
+  std::vector<int32_t> mapOf(textures, -1);
+  for (int slot = 0; slot < 3; slot++)
+    for (uint32_t i = 0; i < materials; i++) {
+      const uint32_t t = slotTextures[slot][i];
+      int32_t index = -1;
+      if (t != NONE) {
+        if (mapOf[t] < 0) {
+          mapOf[t] = int32_t(mapTextures.size());
+          mapTextures.push_back(t);
+        }
+        index = mapOf[t];
+      }
+      (slot == 0 ? mats[i].diffuseMap : slot == 1 ? mats[i].normalMap : mats[i].metallicRoughnessMap) = index;
+    }
+  if (mapTextures.empty()) {
+    for (MeshData &md : meshData) md.uvs.clear();  // nothing samples them
+  } else {
+    packMaterialMaps(d, textureRecords, mapTextures, geometryHasUv1, s);
   }
   // Lights.
   std::vector<LightDesc> lightList;

@@ -458,9 +458,83 @@ MTD void sampleLightChoiceTable(const JobData &J, V3 p, V3 rnd, LightSample &ls)
   }
 }
 
+// ------------------------------------------------------------ material maps
+// materialBuffer.wgsl.ts:316-378 wrapMapCoordinate / sampleMap / loadMapTexel
+// with independent textures.  The shader filters footprints inside the image
+// in hardware and repeat footprints that cross its edge by hand; both are the
+// bilinear mix of the four texels around wrapped * size - 0.5 with clamped
+// (repeat: modular) texel coordinates, evaluated here in software for every
+// footprint.  Rounded operations throughout (no contraction), so a lookup is
+// bit-identical to the CPU restatement.
+MTD float wrapMapCoordinate(float v, float mode) {
+  if (mode < 0.5f) return __fsub_rn(v, floorf(v));
+  if (mode < 1.5f) return clampf(v, 0.0f, 1.0f);
+  const float m = __fsub_rn(v, __fmul_rn(2.0f, floorf(__fmul_rn(v, 0.5f))));
+  return __fsub_rn(1.0f, fabsf(__fsub_rn(1.0f, m)));
+}
+static __device__ __noinline__ float4 sampleMap(const DevScene &s, int idx, V2 uv) {
+  if (idx < 0 || uint32_t(idx) >= s.mapCount) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4 *mi = s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS;
+  const float4 a = ld4(mi), t = ld4(mi + 1), modes = ld4(mi + 2);
+  const int w = asi(a.x), h = asi(a.y);
+  const uint32_t first = asu(a.z);
+  if (w < 1 || h < 1 || uint64_t(first) + uint64_t(w) * uint64_t(h) > s.mapTexelCount)
+    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float tx = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.x, t.x), t.z), modes.z), float(w)), 0.5f);
+  const float ty = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.y, t.y), t.w), modes.w), float(h)), 0.5f);
+  const float fx = floorf(tx), fy = floorf(ty), wx = __fsub_rn(tx, fx), wy = __fsub_rn(ty, fy);
+  // Finite coordinates wrap into [-1, size - 1]; the clamp only pins NaN.
+  const int bx = int(fminf(fmaxf(fx, -1.0f), float(w))), by = int(fminf(fmaxf(fy, -1.0f), float(h)));
+  auto load = [&](int x, int y) {
+    int px = modes.z < 0.5f ? ((x % w) + w) % w : min(max(x, 0), w - 1);
+    int py = modes.w < 0.5f ? ((y % h) + h) % h : min(max(y, 0), h - 1);
+    return ld4(s.mapTexels + first + size_t(py) * size_t(w) + size_t(px));
+  };
+  const float4 t00 = load(bx, by), t10 = load(bx + 1, by), t01 = load(bx, by + 1), t11 = load(bx + 1, by + 1);
+  auto mix1 = [](float p, float q, float k) { return __fadd_rn(__fmul_rn(p, __fsub_rn(1.0f, k)), __fmul_rn(q, k)); };
+  auto mix4 = [&](float4 p, float4 q, float k) {
+    return make_float4(mix1(p.x, q.x, k), mix1(p.y, q.y, k), mix1(p.z, q.z, k), mix1(p.w, q.w, k));
+  };
+  return mix4(mix4(t00, t10, wx), mix4(t01, t11, wx), wy);
+}
+// sRGBToLinear / decodeMapColor (materialBuffer.wgsl.ts:258-265).
+MTD float srgbToLinear(float c) {
+  return c < 0.04045f ? c * 0.0773993808f : powf(c * 0.9478672986f + 0.0521327014f, 2.4f);
+}
+MTD V3 decodeMapColor(const DevScene &s, int idx, V3 c) {
+  const float linear = ld4(s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS + 2).y;
+  if (int(rintf(linear)) % 2 == 1) return c;
+  return {srgbToLinear(c.x), srgbToLinear(c.y), srgbToLinear(c.z)};
+}
+
+struct Material;
+// The texture part of getMaterial (materialBuffer.wgsl.ts:80-125): base color
+// (sRGB-decoded, its alpha to transmission or alpha per mapAlphaUsage) and
+// metallic-roughness (b scales metalness, g roughness).  Out of line: only
+// materials with maps call it.
+static __device__ __noinline__ void applyMaterialMaps(const DevScene &s, float4 r2, float mapAlphaUsage, V2 uv,
+                                                      V3 &baseColor, float &transmission, float &alpha,
+                                                      float &metalness, float &roughness) {
+  const int diffuse = int(r2.z), mrt = int(r2.w);
+  if (diffuse >= 0) {
+    float4 t = sampleMap(s, diffuse, uv);
+    V3 c = decodeMapColor(s, diffuse, {t.x, t.y, t.z});
+    baseColor = {baseColor.x * c.x, baseColor.y * c.y, baseColor.z * c.z};
+    // mapAlphaUsageConstants (materialConstants.ts:2): 3 transmission, 2 alpha
+    if (mapAlphaUsage == 3.0f) transmission = 1.0f - t.w;
+    else if (mapAlphaUsage == 2.0f) alpha *= t.w;
+  }
+  if (mrt >= 0) {
+    float4 t = sampleMap(s, mrt, uv);
+    metalness *= t.z;
+    roughness *= t.y;
+  }
+}
+
 // --------------------------------------------------------------- material
-// materialBuffer.wgsl.ts:170-257 getMaterial (no texture maps)
-MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, Material &m) {
+// materialBuffer.wgsl.ts:170-257 getMaterial (maps: base color and
+// metallic-roughness)
+MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 uv, Material &m) {
   // A miss keeps the previous hit's indices (zero before the first hit);
   // clamp so an empty or single-material scene never reads past its buffers.
   if (materialIndex < 0 || uint32_t(materialIndex) >= J.s.matCount) materialIndex = 0;
@@ -508,6 +582,9 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, Mat
   m.coatAnisotropy = clampf(r17.y, 0.0f, 1.0f);
   m.coatIor = fmaxf(r17.z, 1.0f);
   m.coatDarkening = clampf(r17.w, 0.0f, 1.0f);
+  if (r2.z >= 0.0f || r2.w >= 0.0f)
+    applyMaterialMaps(J.s, r2, r5.w, uv, m.baseColor, m.transmissionWeight, m.alpha, m.baseMetalness,
+                      m.specularRoughness);
   if (m.alphaMode == 0) m.alpha = 1.0f;
   else if (m.alphaMode == 1) m.alpha = m.alpha >= r22.w ? 1.0f : 0.0f;
   m.anisotropyDirection = {1.0f, 0.0f};
@@ -551,14 +628,42 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, Mat
 // ------------------------------------------------------------- surface hit
 struct SurfaceInteraction {
   V3 position; bool albedoSampled;
+  V2 uv;  // primary UV times the material's uvScale (0 without UVs)
   V3 normal, vertexNormal, shadowOffset, faceNormal; bool hit;
   int32_t triangleIndex, instanceIndex, materialIndex;
   float wavelength; int32_t spectralChannel;
   int32_t mediumType; V3 mediumExtinction, mediumScattering; float mediumAnisotropy;
 };
 
+// getMatNormal (materialBuffer.wgsl.ts:377-418): the tangent frame from the
+// triangle's position and UV differences (co-tangent construction), or a
+// fixed-axis frame when the UVs have no gradient; the map's xy scaled by the
+// material's normalMapScale.  Local space.  Out of line: only materials with
+// a normal map call it.
+static __device__ __noinline__ V3 applyNormalMap(const DevScene &s, int idx, float2 scale, V2 uv, V3 normal, V3 dp1,
+                                                 V3 dp2, V2 duv1, V2 duv2) {
+  V3 dp2perp = cross(dp2, normal), dp1perp = cross(normal, dp1);
+  V3 dpdu = dp2perp * duv1.x + dp1perp * duv2.x;
+  V3 dpdv = dp2perp * duv1.y + dp1perp * duv2.y;
+  float g2 = fmaxf(dot(dpdu, dpdu), dot(dpdv, dpdv));
+  if (g2 > 1e-12f) {
+    float invmax = rsqrtf(g2);
+    dpdu = dpdu * invmax;
+    dpdv = dpdv * invmax;
+  } else {
+    V3 axis = fabsf(normal.z) < 0.999f ? V3{0.0f, 0.0f, 1.0f} : V3{0.0f, 1.0f, 0.0f};
+    dpdu = normalize(cross(axis, normal));
+    dpdv = cross(normal, dpdu);
+  }
+  float4 t = sampleMap(s, idx, uv);
+  V3 n = {2.0f * t.x - 1.0f, 2.0f * t.y - 1.0f, 2.0f * t.z - 1.0f};
+  n = normalize(V3{n.x * scale.x, n.y * scale.y, n.z});
+  return normalize(dpdu * n.x + dpdv * n.y + normal * n.z);
+}
+
 // fetchAttributes + completeSurfaceInteraction (intersect.wgsl.ts:1233-1419,
-// 1539-1601) for compact vertices without UV/tangent words.
+// 1539-1601) for compact vertices with an optional primary UV pair (no
+// tangent words, no UV projection).
 MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, const TraversalHit &h, V3 rayO, V3 rayD) {
   const DevScene &s = J.s;
   const float4 *insv = s.ins + size_t(h.insIdx) * MTC_INSTANCE_VEC4_STRIDE;
@@ -603,10 +708,29 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
     hh = fminf(-fminf(fminf(h0, h1), h2), hh * 0.5f);
   }
   V3 shadowOffset = smoothNormal * hh;
+  // UVs (intersect.wgsl.ts:1274-1319, 1408-1418): interpolated, times the
+  // instance material's uvScale; a normal map bends the shading normal.
+  V2 uv0 = {0.0f, 0.0f}, uv1 = uv0, uv2 = uv0;
+  if (s.vuvOff) {
+    auto vuv = [&](int32_t i) {
+      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vuvOff;
+      return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
+    };
+    uv0 = vuv(i0); uv1 = vuv(i1); uv2 = vuv(i2);
+  }
+  const float4 *md = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  const float4 r7 = ld4(md + 7);
+  si.uv = {(bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x) * r7.z,
+           (bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y) * r7.w};
+  V3 mapped = normal;
+  const float4 r1 = ld4(md + 1);
+  if (r1.y >= 0.0f)
+    mapped = applyNormalMap(s, int(r1.y), make_float2(r1.z, r1.w), si.uv, normal, p0 - p2, p1 - p2,
+                            V2{uv0.x - uv2.x, uv0.y - uv2.y}, V2{uv1.x - uv2.x, uv1.y - uv2.y});
   auto nt = [&](V3 v) { return V3{dot(xyz(w0), v), dot(xyz(w1), v), dot(xyz(w2), v)}; };
   si.faceNormal = normalize(nt(h.hitNormal));
-  si.normal = normalize(nt(normal));
-  si.vertexNormal = si.normal;
+  si.vertexNormal = normalize(nt(normal));
+  si.normal = r1.y >= 0.0f ? normalize(nt(mapped)) : si.vertexNormal;
   si.shadowOffset = mat4v(l0, l1, l2, l3, shadowOffset, 0.0f);
   si.position = mat4v(l0, l1, l2, l3, position, 1.0f);
 }
@@ -1139,6 +1263,7 @@ static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, 
   si.wavelength = 0.0f; si.spectralChannel = 0; si.mediumType = 0; si.mediumExtinction = v3(0.0f);
   si.mediumScattering = v3(0.0f); si.mediumAnisotropy = 0.0f;
   si.position = v3(0.0f); si.normal = v3(0.0f); si.vertexNormal = v3(0.0f); si.shadowOffset = v3(0.0f);
+  si.uv = v2(0.0f, 0.0f);
   si.faceNormal = v3(0.0f);
   Path &path = ps.path;
   path.scatteringMediumEntered = false;
@@ -1207,7 +1332,7 @@ static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const Trav
     completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
   }
   Material ma;
-  getMaterial(c.J, si.materialIndex, si.instanceIndex, ma);
+  getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
   if (event == 0) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
       ps.aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
@@ -1248,10 +1373,10 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
       si.triangleIndex = h.triangleIndex;
       completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
     }
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
   } else {
     // The primary material is a pure function of the primary vertex.
-    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, ma);
+    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, sp.primarySi.uv, ma);
   }
   if (event == 0) {
     if (!sp.primaryReady) {

@@ -21,6 +21,10 @@ struct DevScene {
   uint32_t vstride, vnormalOff, vnormalFloat;
   uint32_t flags;
   uint32_t insCount, matCount;
+  const float4 *maps;       // MTC_MAP_VEC4_ROWS per material map
+  const float4 *mapTexels;  // RGBA per texel
+  uint32_t mapCount, mapTexelCount;
+  uint32_t vuvOff;          // word offset of the f32 UV pair (0: no UVs)
 };
 
 // One render job: scene, uniforms, outputs (the plain kernel takes one as a

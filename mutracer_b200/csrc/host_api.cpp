@@ -86,6 +86,10 @@ int mtp_scene_bundle(void *scene, mt_scene_bundle *b) {
   b->blas_stack_size = s.blasStack;
   b->camera = s.camera;
   b->uniform = s.uniform;
+  b->maps = s.maps.empty() ? nullptr : s.maps.data();
+  b->map_count = uint32_t(s.maps.size() / (MTC_MAP_VEC4_ROWS * 4));
+  b->map_texels = s.mapTexels.empty() ? nullptr : s.mapTexels.data();
+  b->map_texel_count = s.mapTexels.size() / 4;
   return MT_OK;
 }
 

@@ -7,6 +7,7 @@
 //                  and runs every sample of its tile in order, so a job's
 //                  image is bit-identical alone and in a batch;
 //  - k_first_hit:  querySceneSoftware (intersect.wgsl.ts:660-684);
+//  - k_sample_maps: raw material-map lookups (sampleMap) for parity checks;
 //  - k_refit_*:    TLAS refit (bvhAccel.ts:579-740) on the device.
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -102,6 +103,14 @@ __global__ void __launch_bounds__(128)
     }
   }
   flushCounters(cnt, paths, counters);
+}
+
+__global__ void k_sample_maps(const __grid_constant__ DevScene s, const int32_t *indices, const float2 *uvs,
+                              uint32_t count, float4 *out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float2 uv = uvs[i];
+  out[i] = sampleMap(s, indices[i], V2{uv.x, uv.y});
 }
 
 template <bool kGpuLayout>
@@ -262,7 +271,9 @@ bool validScene(const mtc_scene_view *s) {
   return s && s->struct_size == sizeof(mtc_scene_view) && s->bvh && s->instances && s->attributes && s->materials &&
          s->material_count > 0 && s->energy_lut && s->light_sampling &&
          s->vertex_layout.stride >= 4 && s->vertex_layout.normal_offset + (s->vertex_layout.normal_float ? 3u : 1u) <=
-                                             s->vertex_layout.stride;
+                                             s->vertex_layout.stride &&
+         (s->vertex_layout.uv_offset == 0 || (s->vertex_layout.uv_offset >= 3 &&
+                                              s->vertex_layout.uv_offset + 2 <= s->vertex_layout.stride));
 }
 
 DevScene toDev(const mtc_scene_view *v) {
@@ -284,6 +295,11 @@ DevScene toDev(const mtc_scene_view *v) {
   s.flags = v->flags;
   s.insCount = v->instance_count;
   s.matCount = v->material_count;
+  s.maps = (const float4 *)v->maps;
+  s.mapTexels = (const float4 *)v->map_texels;
+  s.mapCount = v->maps && v->map_texels ? v->map_count : 0;
+  s.mapTexelCount = v->map_texel_count;
+  s.vuvOff = v->vertex_layout.uv_offset;
   return s;
 }
 
@@ -375,6 +391,15 @@ mt_status mtc_query_first_hit(const mtc_scene_view *scene, const float *rays, ui
   else
     k_first_hit<false><<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
         toDev(scene), blasBase, scene->instance_count == 0, (const float4 *)rays, count, hits);
+  return cudaStatus(cudaGetLastError());
+}
+
+mt_status mtc_sample_maps(const mtc_scene_view *scene, const int32_t *indices, const float *uvs, uint32_t count,
+                          float *texels, void *stream) {
+  if (!validScene(scene) || (count && (!indices || !uvs || !texels))) return MT_ERROR_INVALID_ARGUMENT;
+  if (count == 0) return MT_OK;
+  k_sample_maps<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(toDev(scene), indices, (const float2 *)uvs,
+                                                                      count, (float4 *)texels);
   return cudaStatus(cudaGetLastError());
 }
 

@@ -544,13 +544,15 @@ void packMaterial(const MaterialDesc &m, float *r) {
   auto row = [&](int i) { return r + i * 4; };
   auto set3 = [](float *d, const float *s) { d[0] = s[0]; d[1] = s[1]; d[2] = s[2]; };
   set3(row(0), m.baseColor); row(0)[3] = float(m.type);
-  row(1)[0] = m.specularRoughness; row(1)[1] = -1.0f; row(1)[2] = 1.0f; row(1)[3] = 1.0f;
-  row(2)[0] = m.baseMetalness; row(2)[1] = m.specularAnisotropy; row(2)[2] = -1.0f; row(2)[3] = -1.0f;
+  row(1)[0] = m.specularRoughness; row(1)[1] = float(m.normalMap);
+  row(1)[2] = m.normalScale[0]; row(1)[3] = m.normalScale[1];
+  row(2)[0] = m.baseMetalness; row(2)[1] = m.specularAnisotropy;
+  row(2)[2] = float(m.diffuseMap); row(2)[3] = float(m.metallicRoughnessMap);
   set3(row(3), m.emission); row(3)[3] = -1.0f;
   row(4)[0] = m.specularIor; row(4)[1] = m.transmissionWeight; row(4)[2] = 0.0f; row(4)[3] = m.thin ? 1.0f : 0.0f;
-  row(5)[0] = 0.0f; row(5)[1] = m.dispersionScale; row(5)[2] = m.thinFilmThickness; row(5)[3] = 0.0f;
+  row(5)[0] = 0.0f; row(5)[1] = m.dispersionScale; row(5)[2] = m.thinFilmThickness; row(5)[3] = float(m.mapAlphaUsage);
   row(6)[0] = -1.0f; row(6)[1] = -1.0f; row(6)[2] = -1.0f; row(6)[3] = -1.0f;
-  row(7)[0] = 0.0f; row(7)[1] = -1.0f; row(7)[2] = 1.0f; row(7)[3] = 1.0f;
+  row(7)[0] = 0.0f; row(7)[1] = -1.0f; row(7)[2] = m.uvScale[0]; row(7)[3] = m.uvScale[1];
   row(9)[0] = 1.0f; row(9)[1] = -1.0f; row(9)[2] = m.thinFilmIor; row(9)[3] = -1.0f;
   row(10)[0] = m.baseWeight; row(10)[1] = m.diffuseRoughness; row(10)[2] = m.specularWeight; row(10)[3] = m.subsurfaceWeight;
   set3(row(11), m.specularColor); row(11)[3] = m.fuzzWeight;
@@ -961,9 +963,13 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   s.instances = tlas.instances;
   s.tlasStack = std::min(64u, std::max(1u, tlas.maxDepth));
   s.blasStack = std::min(64u, blasDepth);
-  // Compact vertices: position f32x3 + oct normal (or f32x3 normal).
-  uint32_t stride = normalFloat ? 6 : 4;
-  s.layout = {stride, 3, normalFloat ? 1u : 0u, 0};
+  // Compact vertices (compactVertices.ts:7-27, 67-90): position f32x3 + oct
+  // normal (or f32x3 normal), then an f32 UV pair when any mesh has UVs.
+  bool hasUv = false;
+  for (const MeshData &md : meshes) hasUv |= !md.uvs.empty();
+  const uint32_t uvOffset = hasUv ? (normalFloat ? 6u : 4u) : 0u;
+  uint32_t stride = (normalFloat ? 6 : 4) + (hasUv ? 2 : 0);
+  s.layout = {stride, 3, normalFloat ? 1u : 0u, uvOffset};
   s.attributes.assign(size_t(vertexOffset) * stride, 0);
   for (size_t m = 0; m < meshes.size(); m++) {
     const MeshData &md = meshes[m];
@@ -973,6 +979,7 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
       std::memcpy(w, &md.positions[size_t(v) * 3], 12);
       if (normalFloat) std::memcpy(w + 3, &md.normals[size_t(v) * 3], 12);
       else w[3] = octEncode(md.normals[v * 3], md.normals[v * 3 + 1], md.normals[v * 3 + 2]);
+      if (uvOffset && !md.uvs.empty()) std::memcpy(w + uvOffset, &md.uvs[size_t(v) * 2], 8);
     }
   }
   // Materials.

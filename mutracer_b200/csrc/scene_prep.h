@@ -78,6 +78,12 @@ struct MaterialDesc {
   float mediumExtinction[3] = {0, 0, 0}, mediumScattering[3] = {0, 0, 0}, mediumAnisotropy = 0.0f;
   bool thin = false, doubleSided = false;
   int type = 0;
+  // Material maps (indices into SceneHost::maps, -1 none): base color,
+  // metallic-roughness (b metalness, g roughness), tangent-space normal.
+  int diffuseMap = -1, metallicRoughnessMap = -1, normalMap = -1;
+  float normalScale[2] = {1, 1};
+  float uvScale[2] = {1, 1};     // uvProjectionScale: multiplies the interpolated UV
+  int mapAlphaUsage = 0;         // mapAlphaUsageConstants: 0 opaque, 2 alpha, 3 transmission
 };
 void packMaterial(const MaterialDesc &m, float rows[MTC_MATERIAL_VEC4_ROWS * 4]);
 
@@ -141,6 +147,8 @@ struct SceneHost {
   mtc_vertex_layout layout{4, 3, 0, 0};
   std::vector<float> materials;
   std::vector<float> lights;         // 24 floats per light
+  std::vector<float> maps;           // MTC_MAP_VEC4_ROWS * 4 floats per map
+  std::vector<float> mapTexels;      // RGBA f32 per texel, maps back to back
   std::vector<float> lightSampling;  // RGBA32F texels
   std::vector<float> lut;
   Environment env;
@@ -187,6 +195,7 @@ void defaultUniform(SceneHost &s, uint32_t bounces, uint32_t candidates, uint32_
 struct MeshData {
   std::vector<float> positions, normals;
   std::vector<uint32_t> indices;
+  std::vector<float> uvs;  // 2 per vertex, or empty (zero UVs when another mesh has some)
 };
 void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std::vector<Instance> &instances,
                    const std::vector<MaterialDesc> &materials, const std::vector<LightDesc> &lights, int blasBins,

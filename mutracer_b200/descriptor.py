@@ -66,12 +66,14 @@ class Descriptor:
         return int(np.array([x], np.float32).view(np.uint32)[0])
 
     # ------------------------------------------------------------ records
-    def add_geometry(self, positions, indices, normals=None, material_indices=None, uvs=None, colors=None):
+    def add_geometry(self, positions, indices, normals=None, material_indices=None, uvs=None, colors=None,
+                     uv1s=None):
         pos = np.asarray(positions, np.float32).reshape(-1, 3)
         idx = np.asarray(indices, np.uint32).reshape(-1)
         rec = [len(pos), len(idx), self.append(pos), self.append(idx, np.uint32),
                self.append(normals) if normals is not None else 0,
-               self.append(uvs) if uvs is not None else 0, 0,
+               self.append(uvs) if uvs is not None else 0,
+               self.append(uv1s) if uv1s is not None else 0,
                self.append(colors) if colors is not None else 0, 0,
                self.append(material_indices, np.uint32) if material_indices is not None else 0, 0, 0]
         self.geometries.append(rec)
@@ -80,8 +82,9 @@ class Descriptor:
     def add_material(self, base_color=(0.8, 0.8, 0.8), roughness=0.3, metalness=0.0, transmission=0.0, ior=1.5,
                      emission_color=(1, 1, 1), emission_luminance=0.0, coat_weight=0.0, coat_roughness=0.0,
                      opacity=1.0, thin_walled=False, textures=(NO_TEXTURE,) * 4, extensions=()):
-        """extensions: (id, (x, y, z)) floats, or (id, int) for bool / enum /
-        texture ids."""
+        """textures: (map, normal map, metallic-roughness map, emissive map)
+        texture indices or NO_TEXTURE.  extensions: (id, (x, y, z)) floats,
+        or (id, int) for bool / enum / texture ids."""
         ext_off = 0
         if extensions:
             words = []
@@ -130,13 +133,30 @@ class Descriptor:
         self.lights.append(rec)
         return len(self.lights) - 1
 
-    def add_texture_rgba32f(self, width, height, pixels):
-        off = self.append(np.asarray(pixels, np.float32).reshape(-1))
-        rec = [width, height, 1, off, 0, 0, self._f(1), self._f(1), 0, 0, 0, 0]
+    def add_texture_rgba32f(self, width, height, pixels, **kw):
+        return self.add_texture(width, height, np.asarray(pixels, np.float32), storage=1, **kw)
+
+    def add_texture(self, width, height, pixels, storage=0, flip_y=False, uv_channel=0, uv_scale=(1, 1),
+                    uv_offset=(0, 0), wrap_s=0, wrap_t=0, udim=0, pixels_offset=None):
+        """storage 0: RGBA8, `pixels` (h, w, 4) uint8 packed one word per
+        texel (R in the low byte); storage 1: RGBA32F floats.  `pixels_offset`
+        reuses the pixel words of an earlier texture (shared source)."""
+        if pixels_offset is not None:
+            off = pixels_offset
+        elif storage == 0:
+            off = self.append(np.ascontiguousarray(pixels, np.uint8).reshape(-1).view(np.uint32), np.uint32)
+        else:
+            off = self.append(np.asarray(pixels, np.float32).reshape(-1))
+        f = self._f
+        rec = [width, height, storage, off, int(flip_y), uv_channel, f(uv_scale[0]), f(uv_scale[1]),
+               f(uv_offset[0]), f(uv_offset[1]), wrap_s, wrap_t]
         if self.version >= 7:
-            rec.append(0)
+            rec.append(udim)
         self.textures.append(rec)
         return len(self.textures) - 1
+
+    def texture_pixels_offset(self, texture):
+        return self.textures[texture][3]
 
     def camera_record(self, projection=0, fov=45.0, near=0.1, far=1000.0, left=-1.0, right=1.0, bottom=-1.0,
                       top=1.0, zoom=1.0, f_stop=0.0, focus_distance=10.0, sensor_height=24.0, meters_per_unit=1.0,

@@ -72,6 +72,10 @@ class SceneHost:
         self.light_sampling = _np(b.light_sampling, b.light_sampling_texels * 4, np.float32)
         self.energy_lut = _np(b.energy_lut, abi.MTC_ENERGY_LUT_WIDTH * abi.MTC_ENERGY_LUT_HEIGHT, np.float32)
         self.lights = _np(b.analytic_lights, b.lights_count * abi.MTC_LIGHT_VEC4_ROWS * 4, np.float32)
+        self.maps = _np(b.maps, b.map_count * abi.MTC_MAP_VEC4_ROWS * 4, np.float32) if b.map_count \
+            else np.zeros(0, np.float32)
+        self.map_texels = _np(b.map_texels, b.map_texel_count * 4, np.float32) if b.map_texel_count \
+            else np.zeros(0, np.float32)
 
     @property
     def uniform(self):
@@ -115,6 +119,9 @@ class SceneHost:
         v.energy_lut = C.cast(b.energy_lut, C.c_void_p)
         v.analytic_lights = C.cast(b.analytic_lights, C.c_void_p) if b.lights_count else None
         v.tlas_stack_size, v.blas_stack_size = b.tlas_stack_size, b.blas_stack_size
+        v.maps = C.cast(b.maps, C.c_void_p) if b.map_count else None
+        v.map_texels = C.cast(b.map_texels, C.c_void_p) if b.map_texel_count else None
+        v.map_count, v.map_texel_count = b.map_count, b.map_texel_count
         return v
 
     def refit_inputs(self):
@@ -193,6 +200,8 @@ class DeviceScene:
         self.light_sampling = up(host.light_sampling)
         self.energy_lut = up(host.energy_lut)
         self.lights = up(host.lights)
+        self.maps = up(host.maps)
+        self.map_texels = up(host.map_texels)
         b = host.bundle
         v = abi.SceneView()
         v.struct_size = C.sizeof(abi.SceneView)
@@ -219,6 +228,8 @@ class DeviceScene:
         v.energy_lut = ptr(self.energy_lut)
         v.analytic_lights = ptr(self.lights)
         v.tlas_stack_size, v.blas_stack_size = b.tlas_stack_size, b.blas_stack_size
+        v.maps, v.map_texels = ptr(self.maps), ptr(self.map_texels)
+        v.map_count, v.map_texel_count = b.map_count, b.map_texel_count
         self.view = v
         self.uniform = abi.TraceUniform.from_buffer_copy(b.uniform)
         self.camera = abi.CameraUniform.from_buffer_copy(b.camera)
@@ -228,4 +239,4 @@ class DeviceScene:
     def device_bytes(self):
         return sum(t.numel() * t.element_size() for t in (self.bvh, self.instances, self.attributes,
                    self.materials, self.env_map, self.env_distribution, self.light_sampling, self.energy_lut,
-                   self.lights) if t is not None)
+                   self.lights, self.maps, self.map_texels) if t is not None)

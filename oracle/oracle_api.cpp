@@ -24,6 +24,10 @@ static Scene makeScene(const mtc_scene_view *sv, const mtc_trace_uniform *u, con
   s.lut = (const float *)sv->energy_lut;
   s.lights = (const V4 *)sv->analytic_lights;
   s.vl = sv->vertex_layout;
+  s.maps = (const V4 *)sv->maps;
+  s.mapTexels = (const V4 *)sv->map_texels;
+  s.mapCount = sv->maps && sv->map_texels ? sv->map_count : 0;
+  s.mapTexelCount = sv->map_texel_count;
   s.flags = sv->flags;
   s.tlasStack = sv->tlas_stack_size;
   s.blasStack = sv->blas_stack_size;
@@ -107,6 +111,17 @@ int oracle_trace_samples(const mtc_scene_view *sv, const mtc_camera_uniform *cam
     traffic_out[6] = total.extension_rays; traffic_out[7] = total.shadow_rays;
   }
   return 0;
+}
+
+// Raw sampleMap lookups (materialBuffer.wgsl.ts:335-378) over a scene's maps:
+// out[4i..4i+3] for map indices[i] at uvs[2i..2i+1].
+void oracle_sample_maps(const mtc_scene_view *sv, const int32_t *indices, const float *uvs, uint32_t count,
+                        float *out) {
+  Scene s = makeScene(sv, nullptr, nullptr);
+  for (uint32_t i = 0; i < count; i++) {
+    V4 t = sampleMap(s, indices[i], {uvs[2 * i], uvs[2 * i + 1]});
+    out[4 * i] = t.x; out[4 * i + 1] = t.y; out[4 * i + 2] = t.z; out[4 * i + 3] = t.w;
+  }
 }
 
 // Sampler primitives for the golden tests (sobol.wgsl.ts).

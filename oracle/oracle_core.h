@@ -34,6 +34,9 @@ struct Scene {
   const V4 *lightData = nullptr;
   const float *lut = nullptr;
   const V4 *lights = nullptr;
+  // Material maps: MTC_MAP_VEC4_ROWS vec4 per map, texels RGBA f32.
+  const V4 *maps = nullptr, *mapTexels = nullptr;
+  u32 mapCount = 0, mapTexelCount = 0;
   mtc_vertex_layout vl{};
   u32 flags = 0;
   u32 tlasStack = 64, blasStack = 64;
@@ -81,6 +84,13 @@ u32 owen(u32 x, u32 seed);
 u32 sobolD1(u32 v);
 u32 zSobolIndex(u32 morton, u32 dim, u32 logSPP);
 u32 morton2(u32 x, u32 y);
+
+// sampleMap (materialBuffer.wgsl.ts:335-367): bilinear footprint of texel
+// wrapped(uv * scale + offset) * size - 0.5 with repeat or clamped texel
+// coordinates; zero for an index or texel range outside the scene's maps.
+V4 sampleMap(const Scene &s, i32 idx, V2 uv);
+// decodeMapColor (materialBuffer.wgsl.ts:270-278).
+V3 decodeMapColor(const Scene &s, i32 idx, V3 c);
 
 // Traversal (intersect.wgsl.ts:213-629, 660-684, 696-740, 829-879).
 FirstHit querySceneSoftware(const Scene &s, const Ray &r, Traffic *tr);

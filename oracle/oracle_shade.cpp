@@ -548,8 +548,9 @@ static void sampleLightChoiceTable(const Scene &s, V3 p, V3 rnd, LightSample &ls
 }
 
 // --------------------------------------------------------------- material
-// materialBuffer.wgsl.ts:170-257 getMaterial (no texture maps)
-Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex) {
+// materialBuffer.wgsl.ts:170-257 getMaterial with the base color and
+// metallic-roughness maps of its texture block (:79-120)
+Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv) {
   const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   Material m;
   m.baseColor = xyz(d[0]);
@@ -590,9 +591,23 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex) {
   m.coatAnisotropy = clampf(d[17].y, 0.0f, 1.0f);
   m.coatIor = fmaxf(d[17].z, 1.0f);
   m.coatDarkening = clampf(d[17].w, 0.0f, 1.0f);
+  const i32 diffuseMapIndex = i32(d[2].z);
+  if (diffuseMapIndex >= 0) {
+    V4 t = sampleMap(s, diffuseMapIndex, uv);
+    m.baseColor = m.baseColor * decodeMapColor(s, diffuseMapIndex, {t.x, t.y, t.z});
+    // mapAlphaUsageConstants (materialConstants.ts:2): 3 transmission, 2 alpha
+    if (d[5].w == 3.0f) m.transmissionWeight = 1.0f - t.w;
+    else if (d[5].w == 2.0f) m.alpha *= t.w;
+  }
   // alpha mode resolution (materialBuffer.wgsl.ts:65-73)
   if (m.alphaMode == 0) m.alpha = 1.0f;
   else if (m.alphaMode == 1) m.alpha = m.alpha >= d[22].w ? 1.0f : 0.0f;
+  const i32 mrtMapIndex = i32(d[2].w);
+  if (mrtMapIndex >= 0) {
+    V4 t = sampleMap(s, mrtMapIndex, uv);
+    m.baseMetalness *= t.z;
+    m.specularRoughness *= t.y;
+  }
   m.anisotropyDirection = {1.0f, 0.0f};
   m.anisotropyDirectionEnabled = d[24].y != 0.0f;
   m.coatAnisotropyRotation = d[25].x;
@@ -1076,7 +1091,7 @@ static V4 integrateRgb(Ctx &c, V2 uv, const Ray &ray, Aux &aux) {
   bool sampleIgnored = false;
   for (int event = 0; event <= eventLimit; event++) {
     intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-    ma = getMaterial(c.s, si.materialIndex, si.instanceIndex);
+    ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv);
     if (c.tr) c.tr->material_fetches++;
     if (event == 0) {
       if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
@@ -1129,7 +1144,7 @@ static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
   for (int step = 0; step < stepLimit; step++) {
     if (!primaryReady || (event != 0 && !path.abort)) {
       intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex);
+      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv);
       if (c.tr) c.tr->material_fetches++;
     }
     if (event == 0) {
@@ -1340,7 +1355,7 @@ int oracle_bsdf(const float *rows, uint32_t features, const float *view, const f
   s.mats = (const om::V4 *)rows;
   s.ins = (const om::V4 *)ins;
   s.u = &u;
-  oracle::Material m = oracle::getMaterial(s, 0, 0);
+  oracle::Material m = oracle::getMaterial(s, 0, 0, {0.0f, 0.0f});
   om::V3 v = om::normalize({view[0], view[1], view[2]});
   om::V3 n = {0.0f, 0.0f, 1.0f};
   float ndv = om::dot(v, n);

@@ -193,6 +193,84 @@ static inline TriHit intersectTriangle(V3 o, V3 p0, V3 p1, V3 p2, int maxDim, V3
   return ti;
 }
 
+// ------------------------------------------------------------ material maps
+// wrapMapCoordinate (materialBuffer.wgsl.ts:316-320): 0 repeat, 1 clamp,
+// 2 mirrored repeat.
+static float wrapMapCoordinate(float v, float mode) {
+  if (mode < 0.5f) return v - std::floor(v);
+  if (mode < 1.5f) return clampf(v, 0.0f, 1.0f);
+  return 1.0f - std::fabs(1.0f - (v - 2.0f * std::floor(v * 0.5f)));
+}
+
+// sampleMap + loadMapTexel (materialBuffer.wgsl.ts:335-378).  The shader
+// filters footprints that stay inside the image in hardware and the repeat
+// footprints that cross its edge by hand; both are the bilinear mix of the
+// four texels around wrapped * size - 0.5 with clamped (or, for repeat,
+// modular) texel coordinates, which is what this evaluates everywhere.
+V4 sampleMap(const Scene &s, i32 idx, V2 uv) {
+  if (idx < 0 || u32(idx) >= s.mapCount) return {0, 0, 0, 0};
+  const V4 *mi = s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS;
+  const i32 w = asi(mi[0].x), h = asi(mi[0].y);
+  const u32 first = asu(mi[0].z);
+  if (w < 1 || h < 1 || uint64_t(first) + uint64_t(w) * uint64_t(h) > s.mapTexelCount) return {0, 0, 0, 0};
+  const V4 t = mi[1], modes = mi[2];
+  const float tx = wrapMapCoordinate(uv.x * t.x + t.z, modes.z) * float(w) - 0.5f;
+  const float ty = wrapMapCoordinate(uv.y * t.y + t.w, modes.w) * float(h) - 0.5f;
+  const float fx = std::floor(tx), fy = std::floor(ty), wx = tx - fx, wy = ty - fy;
+  // Finite coordinates wrap into [-1, size - 1]; the clamp only pins NaN.
+  const i32 bx = i32(fminf(fmaxf(fx, -1.0f), float(w))), by = i32(fminf(fmaxf(fy, -1.0f), float(h)));
+  auto load = [&](i32 x, i32 y) {
+    i32 px = std::min(std::max(x, 0), w - 1), py = std::min(std::max(y, 0), h - 1);
+    if (modes.z < 0.5f) px = ((x % w) + w) % w;
+    if (modes.w < 0.5f) py = ((y % h) + h) % h;
+    return s.mapTexels[first + size_t(py) * size_t(w) + size_t(px)];
+  };
+  auto mix = [](V4 a, V4 b, float k) {
+    return V4{a.x * (1.0f - k) + b.x * k, a.y * (1.0f - k) + b.y * k, a.z * (1.0f - k) + b.z * k,
+              a.w * (1.0f - k) + b.w * k};
+  };
+  return mix(mix(load(bx, by), load(bx + 1, by), wx), mix(load(bx, by + 1), load(bx + 1, by + 1), wx), wy);
+}
+
+// sRGBToLinear / decodeMapColor (materialBuffer.wgsl.ts:266-278).
+static float srgbToLinear(float c) {
+  return c < 0.04045f ? c * 0.0773993808f : std::pow(c * 0.9478672986f + 0.0521327014f, 2.4f);
+}
+V3 decodeMapColor(const Scene &s, i32 idx, V3 c) {
+  if (i32(std::nearbyint(s.maps[size_t(idx) * MTC_MAP_VEC4_ROWS + 2].y)) % 2 == 1) return c;
+  return {srgbToLinear(c.x), srgbToLinear(c.y), srgbToLinear(c.z)};
+}
+
+// getMatNormal (materialBuffer.wgsl.ts:377-418), local space.
+static V3 getMatNormal(const Scene &s, i32 materialIndex, V2 uv, V3 normal, V3 dp1, V3 dp2, V2 duv1, V2 duv2) {
+  const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  const i32 idx = i32(d[1].y);
+  if (idx < 0) return normal;
+  V3 dp2perp = cross(dp2, normal), dp1perp = cross(normal, dp1);
+  V3 dpdu = dp2perp * duv1.x + dp1perp * duv2.x;
+  V3 dpdv = dp2perp * duv1.y + dp1perp * duv2.y;
+  float g2 = fmaxf(dot(dpdu, dpdu), dot(dpdv, dpdv));
+  if (g2 > 1e-12f) {
+    float invmax = 1.0f / std::sqrt(g2);
+    dpdu = dpdu * invmax;
+    dpdv = dpdv * invmax;
+  } else {
+    V3 axis = std::fabs(normal.z) < 0.999f ? V3{0, 0, 1} : V3{0, 1, 0};
+    dpdu = normalize(cross(axis, normal));
+    dpdv = cross(normal, dpdu);
+  }
+  V4 t = sampleMap(s, idx, uv);
+  V3 n = {2.0f * t.x - 1.0f, 2.0f * t.y - 1.0f, 2.0f * t.z - 1.0f};
+  n = normalize(V3{n.x * d[1].z, n.y * d[1].w, n.z});
+  return normalize(dpdu * n.x + dpdv * n.y + normal * n.z);
+}
+
+static inline V2 vertexUv(const Scene &s, i32 i) {
+  if (!s.vl.uv_offset) return {0, 0};
+  const u32 *w = s.attr + size_t(i) * s.vl.stride + s.vl.uv_offset;
+  return {asf(w[0]), asf(w[1])};
+}
+
 static inline V3 vertexPosition(const Scene &s, i32 i) {
   const u32 *w = s.attr + size_t(i) * s.vl.stride;
   return {asf(w[0]), asf(w[1]), asf(w[2])};
@@ -419,14 +497,16 @@ static void completeSurfaceInteraction(const Scene &s, SurfaceInteraction &si, c
   V3 bary = h.hitBary;
   V3 n0 = vertexNormal(s, h.idx[0]), n1 = vertexNormal(s, h.idx[1]), n2 = vertexNormal(s, h.idx[2]);
   V3 normal = normalize(n0 * bary.x + n1 * bary.y + n2 * bary.z);
-  si.uv = {0, 0};
-  si.uv1 = {0, 0};
+  const V2 uv0 = vertexUv(s, h.idx[0]), uv1 = vertexUv(s, h.idx[1]), uv2 = vertexUv(s, h.idx[2]);
   const V4 *dm = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
+  uv = {uv.x * dm[7].z, uv.y * dm[7].w};
+  const V2 duv1 = {uv0.x - uv2.x, uv0.y - uv2.y}, duv2 = {uv1.x - uv2.x, uv1.y - uv2.y};
   if (dm[24].x >= 0.0f || dm[24].y != 0.0f || dm[25].x != 0.0f) {
     V3 dp1 = h.tri[0] - h.tri[2];
     V3 dp2 = h.tri[1] - h.tri[2];
     V3 gt, gb;
-    anisotropyAxes(normal, dp1, dp2, {0, 0}, {0, 0}, {0, 0, 0, 0}, gt, gb);
+    anisotropyAxes(normal, dp1, dp2, duv1, duv2, {0, 0, 0, 0}, gt, gb);
     si.geometryTangent = gt; si.geometryBitangent = gb;
     si.directionTangent = gt; si.directionBitangent = gb;
   }
@@ -460,6 +540,9 @@ static void completeSurfaceInteraction(const Scene &s, SurfaceInteraction &si, c
     }
     si.shadowOffset = smoothNormal * hh;
   }
+  si.uv = uv;
+  si.uv1 = uv;  // no secondary UV set: vertexUv1 aliases the primary one
+  si.normal = getMatNormal(s, si.materialIndex, uv, normal, h.tri[0] - h.tri[2], h.tri[1] - h.tri[2], duv1, duv2);
   const V4 *w2l = insv + 1;
   const V4 *l2w = insv + 5;
   auto nt = [&](V3 v) { return V3{dot(xyz(w2l[0]), v), dot(xyz(w2l[1]), v), dot(xyz(w2l[2]), v)}; };

@@ -39,6 +39,7 @@ def lib():
         L.oracle_morton2.argtypes = [C.c_uint32, C.c_uint32]
         L.oracle_morton2.restype = C.c_uint32
         L.oracle_structured_sample.argtypes = [C.c_uint32] * 6 + [C.c_int, C.c_uint32, P]
+        L.oracle_sample_maps.argtypes = [C.POINTER(abi.SceneView), P, P, C.c_uint32, P]
         _lib = L
     return _lib
 
@@ -55,6 +56,17 @@ def first_hits(host_scene, rays):
     lib().oracle_query_first_hit(C.byref(v), C.byref(host_scene.uniform), rays.ctypes.data, rays.shape[0],
                                  hits.ctypes.data, threads())
     return hits
+
+
+def sample_maps(host_scene, indices, uvs):
+    """sampleMap on the CPU: (n, 4) float32 texels for map `indices` (n,) at
+    `uvs` (n, 2)."""
+    indices = np.ascontiguousarray(indices, dtype=np.int32)
+    uvs = np.ascontiguousarray(uvs, dtype=np.float32)
+    out = np.zeros((indices.shape[0], 4), np.float32)
+    v = host_scene.host_view()
+    lib().oracle_sample_maps(C.byref(v), indices.ctypes.data, uvs.ctypes.data, indices.shape[0], out.ctypes.data)
+    return out
 
 
 class Accum:

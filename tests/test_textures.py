@@ -1,0 +1,296 @@
+"""Material textures on the host: descriptor texture records decoded into the
+map table (scene-records.ts decodeTexture, MaterialData.ts, textureAtlas.ts,
+textureAtlasPixels.ts, float16.ts), the texture rules of the reference's
+validator, and the CPU restatement of sampleMap (materialBuffer.wgsl.ts
+:316-378) against an independent float32 NumPy evaluation.
+
+Pinned to the reference's own vectors in tests/unit/rawMaterialTextures.test.ts:
+the half-float table (:93-97), HDR data kept in RGBA16F storage with one map
+per texture (:35-47), and flip_y / byte sources in float storage (:49-66)."""
+import numpy as np
+import pytest
+
+from mutracer_b200 import abi
+from mutracer_b200 import descriptor as D
+from tests import oracle_lib
+from tests.test_descriptor import QUAD, QUAD_IDX, base, decoded, rejected
+
+F = np.float32
+NONE = D.NO_TEXTURE
+QUAD_UV = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], F)
+
+
+def half_bits(values):
+    with np.errstate(over="ignore"):  # 65520 is stored as infinity
+        return np.asarray(values, F).astype(np.float16).view(np.uint16)
+
+
+def maps_of(host):
+    rows = host.maps.reshape(-1, abi.MTC_MAP_VEC4_ROWS, 4)
+    heads = rows[:, 0, :3].copy().view(np.uint32)
+    return rows, heads
+
+
+def texels_of(host, index):
+    rows, heads = maps_of(host)
+    w, h, first = (int(x) for x in heads[index])
+    return host.map_texels.reshape(-1, 4)[first:first + w * h].reshape(h, w, 4).copy()
+
+
+def textured(pixels, storage=0, slot=0, **kw):
+    """base() with one textured material on a UV quad; `slot` 0 map, 1 normal,
+    2 metallic-roughness."""
+    d = base()
+    h, w = np.asarray(pixels).shape[:2]
+    t = d.add_texture(w, h, pixels, storage=storage, **kw)
+    g = d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV)
+    slots = [NONE] * 4
+    slots[slot] = t
+    m = d.add_material(textures=tuple(slots))
+    d.add_mesh(g, m, transform=D.translate([0, 0.5, 0]))
+    return d, m
+
+
+# ----------------------------------------------------------- storage
+def test_half_float_table_matches_reference_vectors():
+    # rawMaterialTextures.test.ts:93-97 (the finite entries)
+    values = [0.0, -0.0, 1.0, -2.0, 65504.0, 65520.0, 2.0 ** -24, 2.0 ** -25, 3 * 2.0 ** -25, 2.0 ** -14,
+              1 + 2.0 ** -11, 1 + 3 * 2.0 ** -11]
+    bits = [0, 0x8000, 0x3c00, 0xc000, 0x7bff, 0x7c00, 1, 0, 2, 0x400, 0x3c00, 0x3c02]
+    pixels = np.array(values, F).reshape(1, 3, 4)
+    d, _ = textured(pixels, storage=1)
+    h = decoded(d)  # keeps the decoded scene alive while its arrays are read
+    got = texels_of(h, 0).reshape(-1)
+    assert half_bits(got).tolist() == bits
+    assert np.signbit(got[1])
+
+
+def test_hdr_data_kept_in_half_float_and_one_map_per_texture():
+    # rawMaterialTextures.test.ts:35-47: one texture in three slots is one map.
+    d = base()
+    t = d.add_texture_rgba32f(1, 1, [2, .5, .25, .75])
+    g = d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV)
+    m = d.add_material(textures=(t, t, t, NONE))
+    d.add_mesh(g, m)
+    h = decoded(d)
+    rows, heads = maps_of(h)
+    assert len(rows) == 1 and rows[0, 2, 1] == 1.0                       # color linear
+    assert half_bits(texels_of(h, 0).reshape(-1)).tolist() == [0x4000, 0x3800, 0x3400, 0x3a00]
+    mat = h.materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)[m]
+    assert mat[2, 2] == 0 and mat[1, 1] == 0 and mat[2, 3] == 0          # map, normal, metallic-roughness
+
+
+def test_flip_y_and_byte_sources_in_float_storage():
+    # rawMaterialTextures.test.ts:49-66: a byte texture beside a float one is
+    # stored as half floats of byte / 255; flip_y reverses the rows.
+    d = base()
+    byte = d.add_texture(1, 2, np.array([[[255, 128, 0, 255]], [[0, 0, 0, 0]]], np.uint8))
+    raw = d.add_texture_rgba32f(1, 2, [2, .5, 0, .75, 4, 1, 0, .25], flip_y=True, uv_channel=1)
+    g = d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV)
+    d.add_mesh(g, d.add_material(textures=(byte, NONE, NONE, NONE)))
+    d.add_mesh(g, d.add_material(textures=(raw, NONE, NONE, NONE)), transform=D.translate([0, 1, 0]))
+    h = decoded(d)
+    rows, _ = maps_of(h)
+    assert rows[:, 2, 1].tolist() == [0, 1] and rows[:, 2, 0].tolist() == [0, 1]
+    expect_byte = [0x3c00, int(half_bits([np.float64(128) / 255])[0]), 0, 0x3c00, 0, 0, 0, 0]
+    assert half_bits(texels_of(h, 0).reshape(-1)).tolist() == expect_byte
+    assert half_bits(texels_of(h, 1).reshape(-1)).tolist() == [0x4400, 0x3c00, 0, 0x3400, 0x4000, 0x3800, 0, 0x3a00]
+
+
+def test_rgba8_texels_are_bytes_over_255_with_rows_flipped():
+    rng = np.random.default_rng(3)
+    pixels = rng.integers(0, 256, (3, 5, 4), dtype=np.uint8)
+    d, m = textured(pixels, flip_y=True, uv_scale=(2, -1), uv_offset=(0.25, 0.5), wrap_s=2, wrap_t=1)
+    h = decoded(d)
+    want = pixels[::-1].astype(F) / F(255)
+    assert np.array_equal(texels_of(h, 0), want)
+    rows, heads = maps_of(h)
+    assert heads[0].tolist() == [5, 3, 0]
+    assert rows[0, 1].tolist() == [2, -1, 0.25, 0.5]
+    assert rows[0, 2].tolist() == [0, 0, 2, 1]                            # uv set, sRGB, mirror, clamp
+
+
+def test_material_rows_and_map_order():
+    """MaterialData order: all base-color maps, then normal maps, then
+    metallic-roughness maps; a shared pixel source is stored once."""
+    d = base()
+    px = np.full((2, 2, 4), 200, np.uint8)
+    a = d.add_texture(2, 2, px)
+    b = d.add_texture(2, 2, None, pixels_offset=d.texture_pixels_offset(a), wrap_s=1)  # same pixels
+    n = d.add_texture(2, 2, np.full((2, 2, 4), 128, np.uint8))
+    g = d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV)
+    m0 = d.add_material(textures=(NONE, n, b, NONE), extensions=[(45, (0.5, -2.0)), (56, (3.0, 4.0)), (54, 2)])
+    m1 = d.add_material(textures=(a, NONE, NONE, NONE))
+    d.add_mesh(g, m0)
+    d.add_mesh(g, m1)
+    h = decoded(d)
+    rows, heads = maps_of(h)
+    assert len(rows) == 3                                                # a (map), n (normal), b (mr)
+    assert heads[0, 2] == heads[2, 2] and heads[1, 2] != heads[0, 2]     # b reuses a's texels
+    assert rows[2, 2, 2] == 1 and rows[0, 2, 2] == 0
+    mats = h.materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)
+    assert mats[m0, 1, 1:].tolist() == [1, 0.5, -2.0]
+    assert mats[m0, 2, 2:].tolist() == [-1, 2] and mats[m1, 2, 2:].tolist() == [0, -1]
+    assert mats[m0, 5, 3] == 3 and mats[m1, 5, 3] == 0                  # transmission, opaque
+    assert mats[m0, 7, 2:].tolist() == [3, 4] and mats[m1, 7, 2:].tolist() == [1, 1]
+
+
+def test_vertex_layout_carries_uvs_only_when_maps_sample_them():
+    d, _ = textured(np.zeros((1, 1, 4), np.uint8))
+    h = decoded(d)
+    lay = h.bundle.vertex_layout
+    assert (lay.stride, lay.uv_offset) == (6, 4)
+    words = h.attributes.reshape(-1, 6)
+    assert np.array_equal(words[-4:, 4:6].view(F), QUAD_UV)             # the textured quad's vertices
+    assert not words[:4, 4:6].any()                                      # base quad: no UVs -> zero
+    d = base()
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV), 0)
+    lay = decoded(d).bundle.vertex_layout
+    assert (lay.stride, lay.uv_offset) == (4, 0)
+
+
+# ---------------------------------------------------------- validation
+def _texture_word(d, k, value):
+    def edit(words):
+        o = int(words[13]) + k
+        words[o] = value
+    return edit
+
+
+@pytest.mark.parametrize("k,value", [(0, 0), (1, 16385), (2, 2), (4, 2), (5, 2), (10, 3), (11, 3), (12, 2),
+                                     (3, 0x7fffffff), (6, 0x7fc00000)])
+def test_invalid_texture_records_are_rejected(k, value):
+    d, _ = textured(np.zeros((1, 1, 4), np.uint8))
+    w = np.frombuffer(d.to_bytes(), np.uint32).copy()
+    _texture_word(d, k, value)(w)
+    rejected(d, data=w.tobytes())
+
+
+def test_texture_rejections_of_pixels_udim_and_references():
+    d, _ = textured(np.array([[[1, 2, np.nan, 4]]], F), storage=1)
+    assert "finite" in rejected(d)
+    d, _ = textured(np.zeros((3, 15, 4), np.uint8), udim=1)               # udim needs multiples of ten
+    rejected(d)
+    d = base()
+    d.add_material(textures=(3, NONE, NONE, NONE))
+    assert "out of range" in rejected(d)
+    d = base()
+    d.add_material(extensions=[(44, 7)])
+    assert "out of range" in rejected(d)
+    d = base()
+    d.add_material(extensions=[(54, 3)])
+    rejected(d)
+    d = base()
+    d.add_material(extensions=[(45, (1.0, float("inf")))])
+    rejected(d)
+
+
+@pytest.mark.parametrize("name", ["emissive", "emissive ext", "alpha map", "udim", "uv1", "alpha blend",
+                                  "projection", "anisotropy"])
+def test_unsupported_texture_features_are_named(name):
+    px = np.zeros((10, 10, 4), np.uint8)
+    d = base()
+    t = d.add_texture(10, 10, px, udim=int(name == "udim"), uv_channel=int(name == "uv1"))
+    g = d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV, **({"uv1s": QUAD_UV} if name == "uv1" else {}))
+    slots, ext = [t, NONE, NONE, NONE], []
+    if name == "emissive":
+        slots = [NONE, NONE, NONE, t]
+    elif name == "emissive ext":
+        ext = [(43, t)]
+    elif name == "alpha map":
+        ext = [(40, t)]
+    elif name == "alpha blend":
+        ext = [(54, 1)]
+    elif name == "projection":
+        ext = [(55, 1)]
+    elif name == "anisotropy":
+        ext = [(9, (0.5,))]
+    d.add_mesh(g, d.add_material(textures=tuple(slots), extensions=ext))
+    assert "not supported" in rejected(d, abi.MT_ERROR_UNAVAILABLE)
+
+
+def test_supported_neighbours_of_unsupported_cases():
+    px = np.zeros((1, 1, 4), np.uint8)
+    # base-color alpha as opacity under an opaque alpha mode stays opaque
+    d = base()
+    t = d.add_texture(1, 1, px)
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV),
+               d.add_material(textures=(t, NONE, NONE, NONE), extensions=[(54, 1), (41, 1)]))
+    h = decoded(d)
+    assert h.materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)[-1, 5, 3] == 2
+    # uv channel 1 without any UV1 coordinates samples the primary set
+    d = base()
+    t = d.add_texture(1, 1, px, uv_channel=1)
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV), d.add_material(textures=(t, NONE, NONE, NONE)))
+    decoded(d)
+    # anisotropy without UVs or tangents anywhere
+    d = base()
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX), d.add_material(extensions=[(9, (0.5,))]))
+    decoded(d)
+    # the emissive slot empty in an extension clears the record's emissive map
+    d = base()
+    t = d.add_texture(1, 1, px)
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX), d.add_material(textures=(NONE, NONE, NONE, t), extensions=[(43, NONE)]))
+    decoded(d)
+
+
+# ------------------------------------------------------------ sampling
+def np_sample(texels, rec, idx_uv):
+    """sampleMap in float32 NumPy, operation by operation (WGSL mix =
+    a * (1 - t) + b * t)."""
+    w, h = int(rec[0, :1].view(np.int32)[0]), int(rec[0, 1:2].view(np.int32)[0])
+    sx, sy, ox, oy = (F(x) for x in rec[1])
+    ms, mt = rec[2, 2], rec[2, 3]
+
+    def wrap(v, mode):
+        if mode < 0.5:
+            return F(v - F(np.floor(v)))
+        if mode < 1.5:
+            return F(min(max(v, F(0)), F(1)))
+        m = F(v - F(F(2) * F(np.floor(F(v * F(0.5))))))
+        return F(F(1) - F(abs(F(F(1) - m))))
+
+    out = []
+    for u, v in idx_uv:
+        tx = F(F(wrap(F(F(F(u) * sx) + ox), ms) * F(w)) - F(0.5))
+        ty = F(F(wrap(F(F(F(v) * sy) + oy), mt) * F(h)) - F(0.5))
+        fx, fy = F(np.floor(tx)), F(np.floor(ty))
+        wx, wy = F(tx - fx), F(ty - fy)
+        bx, by = int(fx), int(fy)
+
+        def load(x, y):
+            px = x % w if ms < 0.5 else min(max(x, 0), w - 1)
+            py = y % h if mt < 0.5 else min(max(y, 0), h - 1)
+            return texels[py, px].astype(F)
+
+        def mix(p, q, k):
+            return (p * (F(1) - k)).astype(F) + (q * k).astype(F)
+
+        out.append(mix(mix(load(bx, by), load(bx + 1, by), wx), mix(load(bx, by + 1), load(bx + 1, by + 1), wx), wy))
+    return np.array(out, F)
+
+
+def uv_grid():
+    # the lookup grid of the reference's filter check (tests/gpu/bindlessTextureSampling.ts:38-40)
+    c = np.arange(257)
+    return np.stack([(c % 17) / 8.0 - 0.5, (c // 17) / 7.0 - 0.5], 1).astype(F)
+
+
+@pytest.mark.parametrize("wrap", [(0, 0), (1, 1), (2, 2), (0, 2), (1, 0)])
+def test_oracle_sample_map_matches_numpy(wrap):
+    rng = np.random.default_rng(11)
+    pixels = rng.integers(0, 256, (3, 4, 4), dtype=np.uint8)
+    d, _ = textured(pixels, wrap_s=wrap[0], wrap_t=wrap[1], uv_scale=(1.5, -0.75), uv_offset=(0.1, 0.3))
+    h = decoded(d)
+    rows, _ = maps_of(h)
+    uvs = uv_grid()
+    got = oracle_lib.sample_maps(h, np.zeros(len(uvs), np.int32), uvs)
+    want = np_sample(texels_of(h, 0), rows[0], uvs)
+    assert np.array_equal(got, want)
+
+
+def test_oracle_sample_map_index_guards():
+    d, _ = textured(np.full((1, 1, 4), 255, np.uint8))
+    h = decoded(d)
+    got = oracle_lib.sample_maps(h, np.array([-1, 1, 0], np.int32), np.zeros((3, 2), F))
+    assert np.array_equal(got[:2], np.zeros((2, 4), F)) and np.array_equal(got[2], np.ones(4, F))
