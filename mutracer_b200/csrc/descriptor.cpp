@@ -316,8 +316,8 @@ struct DecodedMaterial {
   MaterialDesc desc;
   float emissionColor[3], emissionLuminance, coatColor[3], opacity;
   double emission[3];  // materialEmission in float64, before the f32 row store
-  // Descriptor texture indices of the slots this build samples.
-  uint32_t map = NONE, normalMap = NONE, metallicRoughnessMap = NONE;
+  // Descriptor texture index per texture slot (MapSlot order), NONE for none.
+  uint32_t slots[kMapSlots];
 };
 
 void setColor(float *dst, const float *src) { for (int c = 0; c < 3; c++) dst[c] = src[c]; }
@@ -348,10 +348,12 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
   md.thin = d.u[o + 14] != 0;
   for (int k = 15; k < 19; k++)
     if (d.u[o + k] != NONE && d.u[o + k] >= textures) reject(at("material", index) + ": texture reference out of range");
-  m.map = d.u[o + 15];
-  m.normalMap = d.u[o + 16];
-  m.metallicRoughnessMap = d.u[o + 17];
-  uint32_t emissiveMap = d.u[o + 18], alphaMode = 0, mapAlphaUsage = 0;
+  std::fill(m.slots, m.slots + kMapSlots, NONE);
+  m.slots[kMapBase] = d.u[o + 15];
+  m.slots[kMapNormal] = d.u[o + 16];
+  m.slots[kMapMetallicRoughness] = d.u[o + 17];
+  m.slots[kMapEmissive] = d.u[o + 18];
+  uint32_t alphaMode = 0, mapAlphaUsage = 0;
   if (d.u[o + 21]) {
     if (version < 8) reject(at("material", index) + ": graph_offset must be 0 before version 8");
     unsupported("a material graph");
@@ -430,15 +432,27 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
       case 36: scalar(m.opacity); break;
       case 37: flag(md.thin); break;
       case 38: flag(md.doubleSided); break;
-      case 39: m.map = texture(); break;
-      case 43: emissiveMap = texture(); break;
-      case 44: m.normalMap = texture(); break;
-      case 46: m.metallicRoughnessMap = texture(); break;
-      // Other texture slots left empty change nothing.
-      case 40: case 47: case 48: case 49: case 50: case 59: case 64: case 65:
-      case 66: case 67: case 68: case 69: case 70: case 74:
-        if (texture() != NONE) unsupported("material texture slot " + std::to_string(id));
-        break;
+      // Texture slots (material-properties.ts ids 39-74).
+      case 39: m.slots[kMapBase] = texture(); break;
+      case 40: m.slots[kMapAlpha] = texture(); break;
+      case 43: m.slots[kMapEmissive] = texture(); break;
+      case 44: m.slots[kMapNormal] = texture(); break;
+      case 46: m.slots[kMapMetallicRoughness] = texture(); break;
+      case 47: m.slots[kMapRoughness] = texture(); break;
+      case 48: m.slots[kMapMetalness] = texture(); break;
+      case 49: m.slots[kMapTransmission] = texture(); break;
+      case 50: m.slots[kMapThinFilm] = texture(); break;
+      case 59: m.slots[kMapDisplacement] = texture(); break;
+      case 64: m.slots[kMapCoatWeight] = texture(); break;
+      case 65: m.slots[kMapCoatRoughness] = texture(); break;
+      case 66: m.slots[kMapFuzzColor] = texture(); break;
+      case 67: m.slots[kMapFuzzRoughness] = texture(); break;
+      case 68: m.slots[kMapSpecularWeight] = texture(); break;
+      case 69: m.slots[kMapSpecularColor] = texture(); break;
+      case 70: m.slots[kMapAnisotropy] = texture(); break;
+      case 74: m.slots[kMapCoatNormal] = texture(); break;
+      case 62: scalar(md.thinFilmThicknessMinimum); break;
+      case 63: md.thinFilmMapChannel = int(choice(4)); break;
       case 41:  // alpha mode: auto or opaque keep a fully opaque material opaque
         alphaMode = choice(4);
         if (alphaMode > 1) unsupported("alpha mask / blend modes");
@@ -459,15 +473,20 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
     }
   }
   if (m.opacity != 1.0f) unsupported("material opacity below 1");
-  if (emissiveMap != NONE) unsupported("an emissive map");
+  if (m.slots[kMapDisplacement] != NONE) unsupported("displacement maps");
+  if (m.slots[kMapAnisotropy] != NONE) unsupported("anisotropy maps");
+  if (m.slots[kMapCoatNormal] != NONE) unsupported("coat normal maps");
   // resolveMaterialAlphaMode (MaterialState.ts:251-264): auto with the base
-  // color's alpha as opacity blends, which needs any-hit traversal.
-  if (mapAlphaUsage == 1 && alphaMode == 0 && m.map != NONE) unsupported("base color alpha as opacity");
+  // color's alpha as opacity, or with an alpha map, blends, which needs
+  // any-hit traversal.
+  if (alphaMode == 0 && ((mapAlphaUsage == 1 && m.slots[kMapBase] != NONE) || m.slots[kMapAlpha] != NONE))
+    unsupported("texture alpha as opacity");
   md.mapAlphaUsage = mapAlphaUsage == 1 ? 2 : mapAlphaUsage == 2 ? 3 : 0;  // mapAlphaUsageConstants
-  // materialEmission (materialEmission.ts:10-22): emission crosses the coat once.
+  // materialEmission (materialEmission.ts:10-22): emission crosses the coat
+  // once; with a coat weight map the shader applies that passage instead.
   for (int c = 0; c < 3; c++) {
     double e = double(m.emissionColor[c]) * m.emissionLuminance;
-    if (md.coatWeight > 0) {
+    if (md.coatWeight > 0 && m.slots[kMapCoatWeight] == NONE) {
       const double w = std::min(double(md.coatWeight), 1.0);
       e = e * (1 + w * (std::sqrt(std::max(double(m.coatColor[c]), 0.0)) - 1));
     }
@@ -663,6 +682,11 @@ void collectEmissive(const MeshData &md, const double *m, uint32_t material, dou
     cr[2] = float(double(e0[0]) * e1[1] - double(e0[1]) * e1[0]);
     const double area = 0.5 * std::sqrt(double(cr[0]) * cr[0] + double(cr[1]) * cr[1] + double(cr[2]) * cr[2]);
     if (!(area > 1e-10) || !std::isfinite(area)) continue;
+    if (!md.uvs.empty())
+      for (int c = 0; c < 3; c++) {
+        tri.uv[c * 2] = md.uvs[size_t(md.indices[t + c]) * 2];
+        tri.uv[c * 2 + 1] = md.uvs[size_t(md.indices[t + c]) * 2 + 1];
+      }
     tri.area = area;
     tri.luminance = luminanceValue;
     tri.material = int32_t(material);
@@ -767,13 +791,11 @@ void decodeScene(const Words &d, SceneHost &s) {
   // Materials.
   std::vector<MaterialDesc> mats(materials);
   std::vector<double> samplingLuminance(materials);
-  std::vector<uint32_t> slotTextures[3];  // map, normalMap, metallicRoughnessMap per material
+  std::vector<DecodedMaterial> decodedMaterials;
   for (uint32_t i = 0; i < materials; i++) {
     DecodedMaterial m = decodeMaterial(d, u[11] + i * kMaterialWords, version, i, textures);
     mats[i] = m.desc;
-    slotTextures[0].push_back(m.map);
-    slotTextures[1].push_back(m.normalMap);
-    slotTextures[2].push_back(m.metallicRoughnessMap);
+    decodedMaterials.push_back(m);
     // colorLuminance(materialEmission(material)) (lightSampling.ts:255-256).
     samplingLuminance[i] = std::max(m.emission[0] * 0.2126 + m.emission[1] * 0.7152 + m.emission[2] * 0.0722, 0.0);
   }
@@ -888,13 +910,13 @@ void decodeScene(const Words &d, SceneHost &s) {
     }
   }
   // Material maps: MaterialData's texture list (mergeTexturesFromMaterials
-  // over the slots map, normalMap, metallicRoughnessMap in that order, each
-  // over the materials in order, one entry per texture).
+  // over MATERIAL_TEXTURE_NAMES slot by slot, each over the materials in
+  // order, one entry per texture).
   std::vector<uint32_t> mapTextures;
   std::vector<int32_t> mapOf(textures, -1);
-  for (int slot = 0; slot < 3; slot++)
+  for (int slot = 0; slot < kMapSlots; slot++)
     for (uint32_t i = 0; i < materials; i++) {
-      const uint32_t t = slotTextures[slot][i];
+      const uint32_t t = decodedMaterials[i].slots[slot];
       int32_t index = -1;
       if (t != NONE) {
         if (mapOf[t] < 0) {
@@ -903,7 +925,7 @@ void decodeScene(const Words &d, SceneHost &s) {
         }
         index = mapOf[t];
       }
-      (slot == 0 ? mats[i].diffuseMap : slot == 1 ? mats[i].normalMap : mats[i].metallicRoughnessMap) = index;
+      mats[i].maps[slot] = index;
     }
   if (mapTextures.empty()) {
     for (MeshData &md : meshData) md.uvs.clear();  // nothing samples them

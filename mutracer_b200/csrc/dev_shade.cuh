@@ -132,6 +132,137 @@ MTD float spectrumCameraWavelength(uint32_t channel, float u) {
   return 500.0f - 25.0f * (1.0f - expf((wavelength - 500.0f) / 25.0f));
 }
 
+// ------------------------------------------------------------ material maps
+// materialBuffer.wgsl.ts:316-378 wrapMapCoordinate / sampleMap / loadMapTexel
+// with independent textures.  The shader filters footprints inside the image
+// in hardware and repeat footprints that cross its edge by hand; both are the
+// bilinear mix of the four texels around wrapped * size - 0.5 with clamped
+// (repeat: modular) texel coordinates, evaluated here in software for every
+// footprint.  Rounded operations throughout (no contraction), so a lookup is
+// bit-identical to the CPU restatement.
+MTD float wrapMapCoordinate(float v, float mode) {
+  if (mode < 0.5f) return __fsub_rn(v, floorf(v));
+  if (mode < 1.5f) return clampf(v, 0.0f, 1.0f);
+  const float m = __fsub_rn(v, __fmul_rn(2.0f, floorf(__fmul_rn(v, 0.5f))));
+  return __fsub_rn(1.0f, fabsf(__fsub_rn(1.0f, m)));
+}
+static __device__ __noinline__ float4 sampleMap(const DevScene &s, int idx, V2 uv) {
+  if (idx < 0 || uint32_t(idx) >= s.mapCount) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4 *mi = s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS;
+  const float4 a = ld4(mi), t = ld4(mi + 1), modes = ld4(mi + 2);
+  const int w = asi(a.x), h = asi(a.y);
+  const uint32_t first = asu(a.z);
+  if (w < 1 || h < 1 || uint64_t(first) + uint64_t(w) * uint64_t(h) > s.mapTexelCount)
+    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float tx = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.x, t.x), t.z), modes.z), float(w)), 0.5f);
+  const float ty = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.y, t.y), t.w), modes.w), float(h)), 0.5f);
+  const float fx = floorf(tx), fy = floorf(ty), wx = __fsub_rn(tx, fx), wy = __fsub_rn(ty, fy);
+  // Finite coordinates wrap into [-1, size - 1]; the clamp only pins NaN.
+  const int bx = int(fminf(fmaxf(fx, -1.0f), float(w))), by = int(fminf(fmaxf(fy, -1.0f), float(h)));
+  auto load = [&](int x, int y) {
+    int px = modes.z < 0.5f ? ((x % w) + w) % w : min(max(x, 0), w - 1);
+    int py = modes.w < 0.5f ? ((y % h) + h) % h : min(max(y, 0), h - 1);
+    return ld4(s.mapTexels + first + size_t(py) * size_t(w) + size_t(px));
+  };
+  const float4 t00 = load(bx, by), t10 = load(bx + 1, by), t01 = load(bx, by + 1), t11 = load(bx + 1, by + 1);
+  auto mix1 = [](float p, float q, float k) { return __fadd_rn(__fmul_rn(p, __fsub_rn(1.0f, k)), __fmul_rn(q, k)); };
+  auto mix4 = [&](float4 p, float4 q, float k) {
+    return make_float4(mix1(p.x, q.x, k), mix1(p.y, q.y, k), mix1(p.z, q.z, k), mix1(p.w, q.w, k));
+  };
+  return mix4(mix4(t00, t10, wx), mix4(t01, t11, wx), wy);
+}
+// sRGBToLinear / decodeMapColor (materialBuffer.wgsl.ts:258-265).
+MTD float srgbToLinear(float c) {
+  return c < 0.04045f ? c * 0.0773993808f : powf(c * 0.9478672986f + 0.0521327014f, 2.4f);
+}
+MTD V3 decodeMapColor(const DevScene &s, int idx, V3 c) {
+  if (idx < 0 || uint32_t(idx) >= s.mapCount) return c;
+  const float linear = ld4(s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS + 2).y;
+  if (int(rintf(linear)) % 2 == 1) return c;
+  return {srgbToLinear(c.x), srgbToLinear(c.y), srgbToLinear(c.z)};
+}
+
+MTD V3 mulv(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+// A material's map index names a map of this scene (an index past the map
+// table, like -1, means no map).
+MTD bool mapValid(const DevScene &s, float index) { return index >= 0.0f && index < float(s.mapCount); }
+
+// getMaterialEmission (materialBuffer.wgsl.ts:381-403): the packed emission
+// times the sRGB-decoded emissive map and, for standard materials, the coat
+// weight map's single coat passage.  `uv` is the caller's (the surface's
+// scaled UV, or a light sample's unscaled one).
+static __device__ __noinline__ V3 materialEmission(const DevScene &s, const float4 *d, V2 uv) {
+  const float4 r3 = ld4(d + 3);
+  V3 emission = xyz(r3);
+  const int emissive = int(r3.w), coatWeightMap = int(ld4(d + 6).x);
+  if (mapValid(s, r3.w)) {
+    const float4 t = sampleMap(s, emissive, uv);
+    emission = mulv(emission, decodeMapColor(s, emissive, {t.x, t.y, t.z}));
+  }
+  if (mapValid(s, ld4(d + 6).x) && ld4(d).w == 0.0f) {
+    const float4 r16 = ld4(d + 16);
+    const float w = clampf(r16.w, 0.0f, 1.0f) * sampleMap(s, coatWeightMap, uv).x;
+    const V3 c = {sqrtf(fmaxf(r16.x, 0.0f)), sqrtf(fmaxf(r16.y, 0.0f)), sqrtf(fmaxf(r16.z, 0.0f))};
+    emission = mulv(emission, V3{(1.0f - w) + c.x * w, (1.0f - w) + c.y * w, (1.0f - w) + c.z * w});
+  }
+  return emission;
+}
+// Any texture slot getMaterial samples (emissive, base color, alpha,
+// transmission, metallic-roughness, roughness, metalness, thin film, coat
+// weight, coat roughness, fuzz color, fuzz roughness, specular weight,
+// specular color).
+MTD bool materialHasMaps(float4 r2, float4 r3, float4 r6, float4 r9, float4 r18, float4 r19, float4 r21,
+                         float4 r22) {
+  return fmaxf(fmaxf(fmaxf(r2.z, r2.w), fmaxf(r3.w, r6.x)), fmaxf(fmaxf(r6.y, r6.w), fmaxf(r9.y, r9.w))) >= 0.0f ||
+         fmaxf(fmaxf(r18.w, r19.w), fmaxf(fmaxf(r21.w, r22.x), fmaxf(r22.y, r22.z))) >= 0.0f;
+}
+// The texture block of getMaterial (materialBuffer.wgsl.ts:79-139, slots of
+// materialTextureSlots.ts), in the reference's order; the alpha-mode
+// resolution that sits between the alpha and transmission maps touches only
+// alpha, so the caller resolves it after this.  Out of line: only materials
+// with maps call it.
+static __device__ __noinline__ void applyMaterialMaps(const DevScene &s, const float4 *d, V2 uv, Material &m) {
+  m.emission = materialEmission(s, d, uv);
+  const float4 r2 = ld4(d + 2), r5 = ld4(d + 5), r6 = ld4(d + 6), r9 = ld4(d + 9), r22 = ld4(d + 22);
+  auto slot = [&](float index, float4 &t) {
+    if (!mapValid(s, index)) return false;
+    t = sampleMap(s, int(index), uv);
+    return true;
+  };
+  float4 t;
+  if (slot(r2.z, t)) {
+    m.baseColor = mulv(m.baseColor, decodeMapColor(s, int(r2.z), {t.x, t.y, t.z}));
+    // mapAlphaUsageConstants (materialConstants.ts:2): 3 transmission, 2 alpha
+    if (r5.w == 3.0f) m.transmissionWeight = 1.0f - t.w;
+    else if (r5.w == 2.0f) m.alpha *= t.w;
+  }
+  if (slot(r22.z, t)) m.alpha *= t.y;
+  if (slot(r9.w, t)) m.transmissionWeight *= t.x;
+  if (slot(r2.w, t)) {
+    m.baseMetalness *= t.z;
+    m.specularRoughness *= t.y;
+  }
+  if (slot(r22.x, t)) m.specularRoughness *= t.y;
+  if (slot(r22.y, t)) m.baseMetalness *= t.z;
+  if (slot(r9.y, t)) {
+    // thinFilmTextureSample (materialTextureSlots.ts:214-228)
+    const float4 r25 = ld4(d + 25);
+    if (r25.z == 0.0f && r25.w == 0.0f) {
+      m.thinFilmThickness *= t.x;
+    } else {
+      const int channel = int(r25.w);
+      const float k = channel == 0 ? t.x : channel == 1 ? t.y : channel == 2 ? t.z : t.w;
+      m.thinFilmThickness = (r25.z * (1.0f - k) + r5.z * k) * 1000.0f;
+    }
+  }
+  if (slot(r6.x, t)) m.coatWeight *= t.x;
+  if (slot(r6.y, t)) m.coatRoughness *= t.y;
+  if (slot(r6.w, t)) m.fuzzColor = mulv(m.fuzzColor, decodeMapColor(s, int(r6.w), {t.x, t.y, t.z}));
+  if (slot(ld4(d + 18).w, t)) m.fuzzRoughness *= t.w;
+  if (slot(ld4(d + 19).w, t)) m.specularWeight *= t.w;
+  if (slot(ld4(d + 21).w, t)) m.specularColor = mulv(m.specularColor, decodeMapColor(s, int(ld4(d + 21).w), {t.x, t.y, t.z}));
+}
+
 // ------------------------------------------------------------------ lights
 struct Light {
   V3 position; float litType; V3 emission; float area; V3 u; float radiusOrSpread; V3 v; float textureIndex;
@@ -420,7 +551,16 @@ MTD void sampleEmissiveTriangle(const JobData &J, int index, V3 p, V2 rnd, Light
   ls.normal = normal;
   float cl = dot(normal, -ls.direction);
   if (cl <= 0.0f) { ls.emission = v3(0.0f); ls.pdf = 0.0f; return; }
-  ls.emission = xyz(ld4(J.s.mats + size_t(int(c.w)) * MTC_MATERIAL_VEC4_ROWS + 3));
+  // getMaterialEmission at the sampled point's unscaled UV (sampleLight.wgsl.ts:356-358)
+  const float4 *md = J.s.mats + size_t(int(c.w)) * MTC_MATERIAL_VEC4_ROWS;
+  const float4 r3 = ld4(md + 3);
+  if (mapValid(J.s, r3.w) || mapValid(J.s, ld4(md + 6).x)) {
+    const float4 uv01 = ld4(t + 3), uv2 = ld4(t + 4);
+    ls.emission = materialEmission(J.s, md, V2{bc.x * uv01.x + bc.y * uv01.z + bc.z * uv2.x,
+                                               bc.x * uv01.y + bc.y * uv01.w + bc.z * uv2.y});
+  } else {
+    ls.emission = xyz(r3);
+  }
   ls.selectionPmf = a.w;
   ls.pdf = a.w * (ls.dist * ls.dist) / fmaxf(b.w * cl, 1e-8f);
 }
@@ -458,82 +598,8 @@ MTD void sampleLightChoiceTable(const JobData &J, V3 p, V3 rnd, LightSample &ls)
   }
 }
 
-// ------------------------------------------------------------ material maps
-// materialBuffer.wgsl.ts:316-378 wrapMapCoordinate / sampleMap / loadMapTexel
-// with independent textures.  The shader filters footprints inside the image
-// in hardware and repeat footprints that cross its edge by hand; both are the
-// bilinear mix of the four texels around wrapped * size - 0.5 with clamped
-// (repeat: modular) texel coordinates, evaluated here in software for every
-// footprint.  Rounded operations throughout (no contraction), so a lookup is
-// bit-identical to the CPU restatement.
-MTD float wrapMapCoordinate(float v, float mode) {
-  if (mode < 0.5f) return __fsub_rn(v, floorf(v));
-  if (mode < 1.5f) return clampf(v, 0.0f, 1.0f);
-  const float m = __fsub_rn(v, __fmul_rn(2.0f, floorf(__fmul_rn(v, 0.5f))));
-  return __fsub_rn(1.0f, fabsf(__fsub_rn(1.0f, m)));
-}
-static __device__ __noinline__ float4 sampleMap(const DevScene &s, int idx, V2 uv) {
-  if (idx < 0 || uint32_t(idx) >= s.mapCount) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const float4 *mi = s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS;
-  const float4 a = ld4(mi), t = ld4(mi + 1), modes = ld4(mi + 2);
-  const int w = asi(a.x), h = asi(a.y);
-  const uint32_t first = asu(a.z);
-  if (w < 1 || h < 1 || uint64_t(first) + uint64_t(w) * uint64_t(h) > s.mapTexelCount)
-    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const float tx = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.x, t.x), t.z), modes.z), float(w)), 0.5f);
-  const float ty = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.y, t.y), t.w), modes.w), float(h)), 0.5f);
-  const float fx = floorf(tx), fy = floorf(ty), wx = __fsub_rn(tx, fx), wy = __fsub_rn(ty, fy);
-  // Finite coordinates wrap into [-1, size - 1]; the clamp only pins NaN.
-  const int bx = int(fminf(fmaxf(fx, -1.0f), float(w))), by = int(fminf(fmaxf(fy, -1.0f), float(h)));
-  auto load = [&](int x, int y) {
-    int px = modes.z < 0.5f ? ((x % w) + w) % w : min(max(x, 0), w - 1);
-    int py = modes.w < 0.5f ? ((y % h) + h) % h : min(max(y, 0), h - 1);
-    return ld4(s.mapTexels + first + size_t(py) * size_t(w) + size_t(px));
-  };
-  const float4 t00 = load(bx, by), t10 = load(bx + 1, by), t01 = load(bx, by + 1), t11 = load(bx + 1, by + 1);
-  auto mix1 = [](float p, float q, float k) { return __fadd_rn(__fmul_rn(p, __fsub_rn(1.0f, k)), __fmul_rn(q, k)); };
-  auto mix4 = [&](float4 p, float4 q, float k) {
-    return make_float4(mix1(p.x, q.x, k), mix1(p.y, q.y, k), mix1(p.z, q.z, k), mix1(p.w, q.w, k));
-  };
-  return mix4(mix4(t00, t10, wx), mix4(t01, t11, wx), wy);
-}
-// sRGBToLinear / decodeMapColor (materialBuffer.wgsl.ts:258-265).
-MTD float srgbToLinear(float c) {
-  return c < 0.04045f ? c * 0.0773993808f : powf(c * 0.9478672986f + 0.0521327014f, 2.4f);
-}
-MTD V3 decodeMapColor(const DevScene &s, int idx, V3 c) {
-  const float linear = ld4(s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS + 2).y;
-  if (int(rintf(linear)) % 2 == 1) return c;
-  return {srgbToLinear(c.x), srgbToLinear(c.y), srgbToLinear(c.z)};
-}
-
-struct Material;
-// The texture part of getMaterial (materialBuffer.wgsl.ts:80-125): base color
-// (sRGB-decoded, its alpha to transmission or alpha per mapAlphaUsage) and
-// metallic-roughness (b scales metalness, g roughness).  Out of line: only
-// materials with maps call it.
-static __device__ __noinline__ void applyMaterialMaps(const DevScene &s, float4 r2, float mapAlphaUsage, V2 uv,
-                                                      V3 &baseColor, float &transmission, float &alpha,
-                                                      float &metalness, float &roughness) {
-  const int diffuse = int(r2.z), mrt = int(r2.w);
-  if (diffuse >= 0) {
-    float4 t = sampleMap(s, diffuse, uv);
-    V3 c = decodeMapColor(s, diffuse, {t.x, t.y, t.z});
-    baseColor = {baseColor.x * c.x, baseColor.y * c.y, baseColor.z * c.z};
-    // mapAlphaUsageConstants (materialConstants.ts:2): 3 transmission, 2 alpha
-    if (mapAlphaUsage == 3.0f) transmission = 1.0f - t.w;
-    else if (mapAlphaUsage == 2.0f) alpha *= t.w;
-  }
-  if (mrt >= 0) {
-    float4 t = sampleMap(s, mrt, uv);
-    metalness *= t.z;
-    roughness *= t.y;
-  }
-}
-
 // --------------------------------------------------------------- material
-// materialBuffer.wgsl.ts:170-257 getMaterial (maps: base color and
-// metallic-roughness)
+// materialBuffer.wgsl.ts:170-257 getMaterial with its texture block
 MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 uv, Material &m) {
   // A miss keeps the previous hit's indices (zero before the first hit);
   // clamp so an empty or single-material scene never reads past its buffers.
@@ -544,6 +610,7 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 
   float4 r9 = ld4(d + 9), r10 = ld4(d + 10), r11 = ld4(d + 11), r12 = ld4(d + 12), r14 = ld4(d + 14);
   float4 r15 = ld4(d + 15), r16 = ld4(d + 16), r17 = ld4(d + 17), r18 = ld4(d + 18), r20 = ld4(d + 20);
   float4 r21 = ld4(d + 21), r22 = ld4(d + 22), r23 = ld4(d + 23), r24 = ld4(d + 24), r25 = ld4(d + 25);
+  float4 r6 = ld4(d + 6), r19 = ld4(d + 19);
   m.baseColor = xyz(r0);
   m.materialType = int(r0.w);
   m.specularRoughness = r1.x;
@@ -582,9 +649,7 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 
   m.coatAnisotropy = clampf(r17.y, 0.0f, 1.0f);
   m.coatIor = fmaxf(r17.z, 1.0f);
   m.coatDarkening = clampf(r17.w, 0.0f, 1.0f);
-  if (r2.z >= 0.0f || r2.w >= 0.0f)
-    applyMaterialMaps(J.s, r2, r5.w, uv, m.baseColor, m.transmissionWeight, m.alpha, m.baseMetalness,
-                      m.specularRoughness);
+  if (materialHasMaps(r2, r3, r6, r9, r18, r19, r21, r22)) applyMaterialMaps(J.s, d, uv, m);
   if (m.alphaMode == 0) m.alpha = 1.0f;
   else if (m.alphaMode == 1) m.alpha = m.alpha >= r22.w ? 1.0f : 0.0f;
   m.anisotropyDirection = {1.0f, 0.0f};
@@ -724,13 +789,14 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
            (bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y) * r7.w};
   V3 mapped = normal;
   const float4 r1 = ld4(md + 1);
-  if (r1.y >= 0.0f)
+  const bool normalMapped = mapValid(s, r1.y);
+  if (normalMapped)
     mapped = applyNormalMap(s, int(r1.y), make_float2(r1.z, r1.w), si.uv, normal, p0 - p2, p1 - p2,
                             V2{uv0.x - uv2.x, uv0.y - uv2.y}, V2{uv1.x - uv2.x, uv1.y - uv2.y});
   auto nt = [&](V3 v) { return V3{dot(xyz(w0), v), dot(xyz(w1), v), dot(xyz(w2), v)}; };
   si.faceNormal = normalize(nt(h.hitNormal));
   si.vertexNormal = normalize(nt(normal));
-  si.normal = r1.y >= 0.0f ? normalize(nt(mapped)) : si.vertexNormal;
+  si.normal = normalMapped ? normalize(nt(mapped)) : si.vertexNormal;
   si.shadowOffset = mat4v(l0, l1, l2, l3, shadowOffset, 0.0f);
   si.position = mat4v(l0, l1, l2, l3, position, 1.0f);
 }

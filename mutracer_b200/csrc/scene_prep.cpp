@@ -544,16 +544,20 @@ void packMaterial(const MaterialDesc &m, float *r) {
   auto row = [&](int i) { return r + i * 4; };
   auto set3 = [](float *d, const float *s) { d[0] = s[0]; d[1] = s[1]; d[2] = s[2]; };
   set3(row(0), m.baseColor); row(0)[3] = float(m.type);
-  row(1)[0] = m.specularRoughness; row(1)[1] = float(m.normalMap);
+  row(1)[0] = m.specularRoughness; row(1)[1] = float(m.maps[kMapNormal]);
   row(1)[2] = m.normalScale[0]; row(1)[3] = m.normalScale[1];
   row(2)[0] = m.baseMetalness; row(2)[1] = m.specularAnisotropy;
-  row(2)[2] = float(m.diffuseMap); row(2)[3] = float(m.metallicRoughnessMap);
-  set3(row(3), m.emission); row(3)[3] = -1.0f;
+  row(2)[2] = float(m.maps[kMapBase]); row(2)[3] = float(m.maps[kMapMetallicRoughness]);
+  set3(row(3), m.emission); row(3)[3] = float(m.maps[kMapEmissive]);
   row(4)[0] = m.specularIor; row(4)[1] = m.transmissionWeight; row(4)[2] = 0.0f; row(4)[3] = m.thin ? 1.0f : 0.0f;
-  row(5)[0] = 0.0f; row(5)[1] = m.dispersionScale; row(5)[2] = m.thinFilmThickness; row(5)[3] = float(m.mapAlphaUsage);
-  row(6)[0] = -1.0f; row(6)[1] = -1.0f; row(6)[2] = -1.0f; row(6)[3] = -1.0f;
-  row(7)[0] = 0.0f; row(7)[1] = -1.0f; row(7)[2] = m.uvScale[0]; row(7)[3] = m.uvScale[1];
-  row(9)[0] = 1.0f; row(9)[1] = -1.0f; row(9)[2] = m.thinFilmIor; row(9)[3] = -1.0f;
+  // finiteFilmThickness (thinFilmParameters.ts:9-11): negative thickness packs as 0
+  row(5)[0] = 0.0f; row(5)[1] = m.dispersionScale; row(5)[2] = std::max(0.0f, m.thinFilmThickness);
+  row(5)[3] = float(m.mapAlphaUsage);
+  row(6)[0] = float(m.maps[kMapCoatWeight]); row(6)[1] = float(m.maps[kMapCoatRoughness]);
+  row(6)[2] = float(m.maps[kMapCoatNormal]); row(6)[3] = float(m.maps[kMapFuzzColor]);
+  row(7)[0] = 0.0f; row(7)[1] = float(m.maps[kMapDisplacement]); row(7)[2] = m.uvScale[0]; row(7)[3] = m.uvScale[1];
+  row(9)[0] = m.opacity; row(9)[1] = float(m.maps[kMapThinFilm]); row(9)[2] = m.thinFilmIor;
+  row(9)[3] = float(m.maps[kMapTransmission]);
   row(10)[0] = m.baseWeight; row(10)[1] = m.diffuseRoughness; row(10)[2] = m.specularWeight; row(10)[3] = m.subsurfaceWeight;
   set3(row(11), m.specularColor); row(11)[3] = m.fuzzWeight;
   set3(row(12), m.transmissionColor); row(12)[3] = 0.0f;
@@ -561,13 +565,15 @@ void packMaterial(const MaterialDesc &m, float *r) {
   set3(row(15), m.fuzzColor); row(15)[3] = m.fuzzRoughness;
   set3(row(16), m.coatColor); row(16)[3] = m.coatWeight;
   row(17)[0] = m.coatRoughness; row(17)[1] = 0.0f; row(17)[2] = m.coatIor; row(17)[3] = m.coatDarkening;
-  row(18)[0] = m.thinFilmWeight; row(18)[1] = m.abbe; row(18)[2] = 0.0f; row(18)[3] = -1.0f;
-  row(19)[3] = -1.0f;
+  row(18)[0] = m.thinFilmWeight; row(18)[1] = m.abbe; row(18)[2] = 0.0f; row(18)[3] = float(m.maps[kMapFuzzRoughness]);
+  row(19)[3] = float(m.maps[kMapSpecularWeight]);
   set3(row(20), m.mediumExtinction); row(20)[3] = m.mediumAnisotropy;
-  set3(row(21), m.mediumScattering); row(21)[3] = -1.0f;
-  row(22)[0] = -1.0f; row(22)[1] = -1.0f; row(22)[2] = -1.0f; row(22)[3] = 0.5f;
-  row(23)[2] = m.doubleSided ? 1.0f : 0.0f; row(23)[3] = 0.0f;
-  row(24)[0] = -1.0f; row(24)[1] = 0.0f; row(24)[2] = 1.0f; row(24)[3] = 1.0f;
+  set3(row(21), m.mediumScattering); row(21)[3] = float(m.maps[kMapSpecularColor]);
+  row(22)[0] = float(m.maps[kMapRoughness]); row(22)[1] = float(m.maps[kMapMetalness]);
+  row(22)[2] = float(m.maps[kMapAlpha]); row(22)[3] = std::max(0.0f, m.alphaCutoff);
+  row(23)[2] = m.doubleSided ? 1.0f : 0.0f; row(23)[3] = float(m.alphaMode);
+  row(24)[0] = float(m.maps[kMapAnisotropy]); row(24)[1] = 0.0f; row(24)[2] = 1.0f; row(24)[3] = 1.0f;
+  row(25)[2] = std::max(0.0f, m.thinFilmThicknessMinimum); row(25)[3] = float(m.thinFilmMapChannel);
 }
 
 // ---------------------------------------------------------- environment
@@ -1035,6 +1041,7 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
     d[0] = t.p[0]; d[1] = t.p[1]; d[2] = t.p[2]; d[3] = emissivePmf[i];
     d[4] = t.p[3]; d[5] = t.p[4]; d[6] = t.p[5]; d[7] = float(t.area);
     d[8] = t.p[6]; d[9] = t.p[7]; d[10] = t.p[8]; d[11] = float(t.material);
+    for (int k = 0; k < 6; k++) d[12 + k] = d[18 + k] = t.uv[k];
   }
   std::memcpy(s.lightSampling.data() + size_t(emissiveTexels) * 4, alias.words.data(), alias.words.size() * 4);
   // Analytic light records (wgpuSceneUniform.ts:70-152).

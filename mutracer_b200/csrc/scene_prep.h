@@ -63,6 +63,13 @@ void refitTlasHost(float *tlas, float *records, const std::vector<Instance> &ins
                    const std::vector<Blas> &blases, const std::vector<uint32_t> &blasOffsets,
                    const std::vector<uint32_t> &vertexOffsets, uint32_t blasLayout = 0);
 
+// Texture slots of a material (MATERIAL_TEXTURE_NAMES, materialTextureNames.ts:3-8).
+enum MapSlot {
+  kMapBase, kMapAlpha, kMapNormal, kMapEmissive, kMapMetallicRoughness, kMapRoughness, kMapMetalness,
+  kMapTransmission, kMapThinFilm, kMapDisplacement, kMapCoatWeight, kMapCoatRoughness, kMapFuzzColor,
+  kMapFuzzRoughness, kMapSpecularWeight, kMapSpecularColor, kMapAnisotropy, kMapCoatNormal, kMapSlots
+};
+
 struct MaterialDesc {
   float baseColor[3] = {0.8f, 0.8f, 0.8f};
   float baseWeight = 1.0f, baseMetalness = 0.0f, diffuseRoughness = 0.0f;
@@ -78,12 +85,16 @@ struct MaterialDesc {
   float mediumExtinction[3] = {0, 0, 0}, mediumScattering[3] = {0, 0, 0}, mediumAnisotropy = 0.0f;
   bool thin = false, doubleSided = false;
   int type = 0;
-  // Material maps (indices into SceneHost::maps, -1 none): base color,
-  // metallic-roughness (b metalness, g roughness), tangent-space normal.
-  int diffuseMap = -1, metallicRoughnessMap = -1, normalMap = -1;
+  // Material maps: indices into SceneHost::maps (-1 none) per slot, in the
+  // reference's slot order (materialTextureNames.ts).
+  int maps[kMapSlots] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
   float normalScale[2] = {1, 1};
   float uvScale[2] = {1, 1};     // uvProjectionScale: multiplies the interpolated UV
   int mapAlphaUsage = 0;         // mapAlphaUsageConstants: 0 opaque, 2 alpha, 3 transmission
+  float thinFilmThicknessMinimum = 0.0f;
+  int thinFilmMapChannel = 0;    // r, g, b, a
+  float opacity = 1.0f, alphaCutoff = 0.0f;
+  int alphaMode = 0;             // materialAlphaModeConstants: 0 opaque, 1 mask, 2 blend
 };
 void packMaterial(const MaterialDesc &m, float rows[MTC_MATERIAL_VEC4_ROWS * 4]);
 
@@ -132,6 +143,7 @@ void buildEnergyLut(std::vector<float> &lut);
 // corners (f32), area and sampling luminance (float64), material index.
 struct EmissiveTriangle {
   float p[9];
+  float uv[6] = {0, 0, 0, 0, 0, 0};  // corner UVs (the secondary set repeats them)
   double area = 0.0, luminance = 0.0;
   int32_t material = 0;
 };

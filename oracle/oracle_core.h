@@ -89,6 +89,9 @@ u32 morton2(u32 x, u32 y);
 // wrapped(uv * scale + offset) * size - 0.5 with repeat or clamped texel
 // coordinates; zero for an index or texel range outside the scene's maps.
 V4 sampleMap(const Scene &s, i32 idx, V2 uv);
+// A material's map index names a map of this scene (an index past the map
+// table, like -1, means no map).
+bool mapValid(const Scene &s, float index);
 // decodeMapColor (materialBuffer.wgsl.ts:270-278).
 V3 decodeMapColor(const Scene &s, i32 idx, V3 c);
 

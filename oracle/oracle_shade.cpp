@@ -493,6 +493,27 @@ static void sampleAnalyticLight(const Light &L, V3 p, V2 rnd, LightSample &ls) {
   if (type == MTC_LIGHT_CYLINDER) lightSampleCylinder(L, p, rnd, ls);
 }
 // sampleLight.wgsl.ts:319-357 (material emission without maps)
+// getMaterialEmission (materialBuffer.wgsl.ts:381-403).
+V3 getMaterialEmission(const Scene &s, i32 materialIndex, V2 uv) {
+  const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  V3 emission = xyz(d[3]);
+  const i32 emissiveMapIndex = i32(d[3].w);
+  if (mapValid(s, d[3].w)) {
+    V4 t = sampleMap(s, emissiveMapIndex, uv);
+    emission = emission * decodeMapColor(s, emissiveMapIndex, {t.x, t.y, t.z});
+  }
+  if (d[0].w == 0.0f) {
+    const i32 coatWeightMapIndex = i32(d[6].x);
+    if (mapValid(s, d[6].x)) {
+      const float coatWeight = clampf(d[16].w, 0.0f, 1.0f) * sampleMap(s, coatWeightMapIndex, uv).x;
+      const V3 c = {std::sqrt(fmaxf(d[16].x, 0.0f)), std::sqrt(fmaxf(d[16].y, 0.0f)), std::sqrt(fmaxf(d[16].z, 0.0f))};
+      emission = emission * V3{1.0f * (1.0f - coatWeight) + c.x * coatWeight, 1.0f * (1.0f - coatWeight) + c.y * coatWeight,
+                               1.0f * (1.0f - coatWeight) + c.z * coatWeight};
+    }
+  }
+  return emission;
+}
+
 static void sampleEmissiveTriangle(const Scene &s, i32 index, V3 p, V2 rnd, LightSample &ls) {
   const V4 *t = s.lightData + size_t(index) * 6;
   V3 p0 = xyz(t[0]), p1 = xyz(t[1]), p2 = xyz(t[2]);
@@ -509,7 +530,9 @@ static void sampleEmissiveTriangle(const Scene &s, i32 index, V3 p, V2 rnd, Ligh
   ls.normal = normal;
   float cl = dot(normal, -ls.direction);
   if (cl <= 0.0f) { ls.emission = v3(0.0f); ls.pdf = 0.0f; return; }
-  ls.emission = xyz(s.mats[size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS + 3]);
+  // getMaterialEmission at the unscaled barycentric UV (sampleLight.wgsl.ts:331-358)
+  V2 uv = {b.x * t[3].x + b.y * t[3].z + b.z * t[4].x, b.x * t[3].y + b.y * t[3].w + b.z * t[4].y};
+  ls.emission = getMaterialEmission(s, materialIndex, uv);
   ls.selectionPmf = selectionPmf;
   ls.pdf = selectionPmf * (ls.dist * ls.dist) / fmaxf(area * cl, 1e-8f);
 }
@@ -548,8 +571,8 @@ static void sampleLightChoiceTable(const Scene &s, V3 p, V3 rnd, LightSample &ls
 }
 
 // --------------------------------------------------------------- material
-// materialBuffer.wgsl.ts:170-257 getMaterial with the base color and
-// metallic-roughness maps of its texture block (:79-120)
+// materialBuffer.wgsl.ts:170-257 getMaterial with its texture block
+// (:79-139 and the slots of materialTextureSlots.ts)
 Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv) {
   const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   Material m;
@@ -558,7 +581,7 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   m.specularRoughness = d[1].x;
   m.baseMetalness = d[2].x;
   m.specularAnisotropy = clampf(d[2].y, 0.0f, 1.0f);
-  m.emission = xyz(d[3]);
+  m.emission = getMaterialEmission(s, materialIndex, uv);
   m.inside = false;
   m.specularIor = d[4].x;
   m.transmissionWeight = d[4].y;
@@ -592,21 +615,58 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   m.coatIor = fmaxf(d[17].z, 1.0f);
   m.coatDarkening = clampf(d[17].w, 0.0f, 1.0f);
   const i32 diffuseMapIndex = i32(d[2].z);
-  if (diffuseMapIndex >= 0) {
+  if (mapValid(s, d[2].z)) {
     V4 t = sampleMap(s, diffuseMapIndex, uv);
     m.baseColor = m.baseColor * decodeMapColor(s, diffuseMapIndex, {t.x, t.y, t.z});
     // mapAlphaUsageConstants (materialConstants.ts:2): 3 transmission, 2 alpha
     if (d[5].w == 3.0f) m.transmissionWeight = 1.0f - t.w;
     else if (d[5].w == 2.0f) m.alpha *= t.w;
   }
+  // simpleTextureSample (materialTextureSlots.ts:184-212): factor *= channel
+  auto simple = [&](float index, float &target, int channel) {
+    if (!mapValid(s, index)) return;
+    const i32 idx = i32(index);
+    V4 t = sampleMap(s, idx, uv);
+    target *= channel == 0 ? t.x : channel == 1 ? t.y : channel == 2 ? t.z : t.w;
+  };
+  simple(d[22].z, m.alpha, 1);  // alphaMap: g
   // alpha mode resolution (materialBuffer.wgsl.ts:65-73)
   if (m.alphaMode == 0) m.alpha = 1.0f;
   else if (m.alphaMode == 1) m.alpha = m.alpha >= d[22].w ? 1.0f : 0.0f;
+  simple(d[9].w, m.transmissionWeight, 0);  // transmissionMap: r
   const i32 mrtMapIndex = i32(d[2].w);
-  if (mrtMapIndex >= 0) {
+  if (mapValid(s, d[2].w)) {
     V4 t = sampleMap(s, mrtMapIndex, uv);
     m.baseMetalness *= t.z;
     m.specularRoughness *= t.y;
+  }
+  simple(d[22].x, m.specularRoughness, 1);  // roughnessMap: g
+  simple(d[22].y, m.baseMetalness, 2);      // metalnessMap: b
+  const i32 thinFilmMapIndex = i32(d[9].y);
+  if (mapValid(s, d[9].y)) {
+    // thinFilmTextureSample (materialTextureSlots.ts:214-228)
+    V4 t = sampleMap(s, thinFilmMapIndex, uv);
+    if (d[25].z == 0.0f && d[25].w == 0.0f) {
+      m.thinFilmThickness *= t.x;
+    } else {
+      const i32 channel = i32(d[25].w);
+      const float k = channel == 0 ? t.x : channel == 1 ? t.y : channel == 2 ? t.z : t.w;
+      m.thinFilmThickness = (d[25].z * (1.0f - k) + d[5].z * k) * 1000.0f;
+    }
+  }
+  simple(d[6].x, m.coatWeight, 0);      // coatWeightMap: r
+  simple(d[6].y, m.coatRoughness, 1);   // coatRoughnessMap: g
+  const i32 fuzzColorMapIndex = i32(d[6].w);
+  if (mapValid(s, d[6].w)) {
+    V4 t = sampleMap(s, fuzzColorMapIndex, uv);
+    m.fuzzColor = m.fuzzColor * decodeMapColor(s, fuzzColorMapIndex, {t.x, t.y, t.z});
+  }
+  simple(d[18].w, m.fuzzRoughness, 3);  // fuzzRoughnessMap: a
+  simple(d[19].w, m.specularWeight, 3); // specularWeightMap: a
+  const i32 specularColorMapIndex = i32(d[21].w);
+  if (mapValid(s, d[21].w)) {
+    V4 t = sampleMap(s, specularColorMapIndex, uv);
+    m.specularColor = m.specularColor * decodeMapColor(s, specularColorMapIndex, {t.x, t.y, t.z});
   }
   m.anisotropyDirection = {1.0f, 0.0f};
   m.anisotropyDirectionEnabled = d[24].y != 0.0f;

@@ -232,11 +232,14 @@ V4 sampleMap(const Scene &s, i32 idx, V2 uv) {
   return mix(mix(load(bx, by), load(bx + 1, by), wx), mix(load(bx, by + 1), load(bx + 1, by + 1), wx), wy);
 }
 
+bool mapValid(const Scene &s, float index) { return index >= 0.0f && index < float(s.mapCount); }
+
 // sRGBToLinear / decodeMapColor (materialBuffer.wgsl.ts:266-278).
 static float srgbToLinear(float c) {
   return c < 0.04045f ? c * 0.0773993808f : std::pow(c * 0.9478672986f + 0.0521327014f, 2.4f);
 }
 V3 decodeMapColor(const Scene &s, i32 idx, V3 c) {
+  if (idx < 0 || u32(idx) >= s.mapCount) return c;
   if (i32(std::nearbyint(s.maps[size_t(idx) * MTC_MAP_VEC4_ROWS + 2].y)) % 2 == 1) return c;
   return {srgbToLinear(c.x), srgbToLinear(c.y), srgbToLinear(c.z)};
 }
@@ -244,8 +247,8 @@ V3 decodeMapColor(const Scene &s, i32 idx, V3 c) {
 // getMatNormal (materialBuffer.wgsl.ts:377-418), local space.
 static V3 getMatNormal(const Scene &s, i32 materialIndex, V2 uv, V3 normal, V3 dp1, V3 dp2, V2 duv1, V2 duv2) {
   const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  if (!mapValid(s, d[1].y)) return normal;
   const i32 idx = i32(d[1].y);
-  if (idx < 0) return normal;
   V3 dp2perp = cross(dp2, normal), dp1perp = cross(normal, dp1);
   V3 dpdu = dp2perp * duv1.x + dp1perp * duv2.x;
   V3 dpdv = dp2perp * duv1.y + dp1perp * duv2.y;

@@ -3,7 +3,10 @@ restatement of sampleMap on the reference's lookup grid for every wrap mode,
 byte and half-float storage; a textured scene (sRGB base-color checker,
 normal maps with scaled UVs, a metallic-roughness map, base-color alpha as
 transmission) with image parity against the oracle, and bit-identical through
-the batch entry point, the wavefront engine and mt_context_commit."""
+the batch entry point, the wavefront engine and mt_context_commit; a scene
+using every other supported slot (emissive map sampled by NEE, roughness,
+metalness, specular, coat, fuzz, transmission, thin-film and alpha maps) with
+image parity against the oracle."""
 import ctypes as C
 import math
 
@@ -183,3 +186,60 @@ def test_textured_scene_identical_in_every_engine(cuda):
     finally:
         ctx.destroy()
     assert alone.color[:, :3].mean().item() > 0.01
+
+
+def slots_room(width=96, height=72):
+    """Every supported texture slot on one scene: an emissive-mapped lamp
+    (sampled by NEE at its UVs), roughness / metalness / specular maps,
+    coat weight and coat roughness maps on an emitting coated sphere, fuzz
+    maps, transmission and thin-film maps, an alpha map under the opaque
+    alpha mode."""
+    rng = np.random.default_rng(9)
+    d = D.Descriptor(width, height)
+
+    def noise(w, h):
+        return d.add_texture(w, h, rng.integers(0, 256, (h, w, 4), dtype=np.uint8))
+    yy, xx = np.mgrid[0:8, 0:8]
+    glow = np.zeros((8, 8, 4), np.uint8)
+    glow[(xx + yy) % 2 == 0] = [255, 200, 120, 255]
+    glow[(xx + yy) % 2 == 1] = [60, 120, 255, 255]
+    glow_tex = d.add_texture(8, 8, glow)
+    floor = d.add_geometry(QUAD * F(3), QUAD_IDX, uvs=QUAD_UV)
+    spos, suv, sidx = uv_sphere(24, 12, 0.45)
+    sphere = d.add_geometry(spos, sidx, uvs=suv)
+    panel = d.add_geometry(np.array([[-.5, 0, 0], [.5, 0, 0], [.5, 1.0, 0], [-.5, 1.0, 0]], F), [0, 1, 2, 0, 2, 3],
+                           uvs=QUAD_UV)
+    lamp_geo = d.add_geometry(np.array([[-.6, 0, -.4], [.6, 0, -.4], [.6, 0, .4], [-.6, 0, .4]], F),
+                              [0, 2, 1, 0, 3, 2], uvs=QUAD_UV)
+    floor_mat = d.add_material(base_color=(0.6, 0.6, 0.6), roughness=0.7, extensions=[(40, noise(4, 4)), (41, 1)])
+    lamp = d.add_material(emission_color=(1, 1, 1), emission_luminance=5.0, textures=(NONE, NONE, NONE, glow_tex))
+    spec = d.add_material(base_color=(0.8, 0.5, 0.3), roughness=0.8, metalness=1.0,
+                          extensions=[(47, noise(8, 4)), (48, noise(4, 8)), (68, noise(4, 4)), (69, noise(4, 4))])
+    coated = d.add_material(base_color=(0.3, 0.3, 0.3), roughness=0.5, coat_weight=1.0, coat_roughness=0.4,
+                            emission_color=(1, 0.5, 0.2), emission_luminance=0.3,
+                            extensions=[(26, (0.5, 0.8, 1.0)), (64, noise(8, 8)), (65, noise(8, 8))])
+    fuzzy = d.add_material(base_color=(0.5, 0.2, 0.4), roughness=0.6,
+                           extensions=[(22, (1.0,)), (66, noise(4, 4)), (67, noise(4, 4))])
+    film = d.add_material(base_color=(1, 1, 1), roughness=0.05, transmission=1.0, ior=1.45, thin_walled=True,
+                          extensions=[(31, (1.0,)), (32, (0.6,)), (49, noise(4, 4)), (50, noise(8, 8)),
+                                      (62, (0.1,)), (63, 1)])
+    d.add_mesh(floor, floor_mat)
+    d.add_mesh(lamp_geo, lamp, transform=[1, 0, 0, 0, 0, -1, 0, 0, 0, 0, -1, 0, 0, 2.4, -0.3, 1])  # facing down
+    d.add_mesh(sphere, spec, transform=D.translate([-1.1, 0.45, 0]))
+    d.add_mesh(sphere, coated, transform=D.translate([0, 0.45, -0.4]))
+    d.add_mesh(sphere, fuzzy, transform=D.translate([1.1, 0.45, 0]))
+    d.add_mesh(panel, film, transform=D.translate([0, 0, 0.9]))
+    d.add_light(D.LIGHT_SPHERE, color=(1, 0.95, 0.9), intensity=3, size=0.1, transform=D.translate([1.5, 2.0, 2.0]))
+    d.set_camera(fov=45, transform=D.look_at([0, 1.4, 4.0], [0, 0.6, 0]))
+    return d
+
+
+def test_every_slot_scene_oracle_parity(cuda):
+    st, msg, host = D.decode(slots_room().to_bytes())
+    assert st == abi.MT_OK, msg
+    assert host.bundle.map_count == 12 and host.uniform.light_choice_count >= 3
+    gpu, ref, _, _ = _render_pair(cuda, host, 32)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert np.isfinite(gpu).all()
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma

@@ -74,7 +74,10 @@ def _material(**kw):
     rows[15] = [1, 1, 1, kw.get("fuzz_roughness", 0.5)]
     rows[16] = [*kw.get("coat_color", (1, 1, 1)), kw.get("coat", 0.0)]
     rows[17] = [kw.get("coat_roughness", 0.1), 0, kw.get("coat_ior", 1.6), kw.get("coat_darkening", 1.0)]
+    rows[6] = [-1, -1, -1, -1]                                 # no coat / fuzz maps
     rows[18] = [kw.get("film", 0.0), 20, 0, -1]
+    rows[19] = [0, 0, 0, -1]
+    rows[21] = [0, 0, 0, -1]
     rows[22] = [-1, -1, -1, 0.5]
     rows[24] = [-1, 0, 1, 1]
     return rows

@@ -185,18 +185,20 @@ def test_texture_rejections_of_pixels_udim_and_references():
     rejected(d)
 
 
-@pytest.mark.parametrize("name", ["emissive", "emissive ext", "alpha map", "udim", "uv1", "alpha blend",
-                                  "projection", "anisotropy"])
+@pytest.mark.parametrize("name", ["displacement", "anisotropy map", "coat normal", "alpha map", "udim", "uv1",
+                                  "alpha blend", "projection", "anisotropy"])
 def test_unsupported_texture_features_are_named(name):
     px = np.zeros((10, 10, 4), np.uint8)
     d = base()
     t = d.add_texture(10, 10, px, udim=int(name == "udim"), uv_channel=int(name == "uv1"))
     g = d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV, **({"uv1s": QUAD_UV} if name == "uv1" else {}))
     slots, ext = [t, NONE, NONE, NONE], []
-    if name == "emissive":
-        slots = [NONE, NONE, NONE, t]
-    elif name == "emissive ext":
-        ext = [(43, t)]
+    if name == "displacement":
+        ext = [(59, t)]
+    elif name == "anisotropy map":
+        ext = [(70, t)]
+    elif name == "coat normal":
+        ext = [(74, t)]
     elif name == "alpha map":
         ext = [(40, t)]
     elif name == "alpha blend":
@@ -227,10 +229,11 @@ def test_supported_neighbours_of_unsupported_cases():
     d = base()
     d.add_mesh(d.add_geometry(QUAD, QUAD_IDX), d.add_material(extensions=[(9, (0.5,))]))
     decoded(d)
-    # the emissive slot empty in an extension clears the record's emissive map
+    # an alpha map under the opaque alpha mode changes nothing
     d = base()
     t = d.add_texture(1, 1, px)
-    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX), d.add_material(textures=(NONE, NONE, NONE, t), extensions=[(43, NONE)]))
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV),
+               d.add_material(extensions=[(40, t), (41, 1)]))
     decoded(d)
 
 
@@ -294,3 +297,63 @@ def test_oracle_sample_map_index_guards():
     h = decoded(d)
     got = oracle_lib.sample_maps(h, np.array([-1, 1, 0], np.int32), np.zeros((3, 2), F))
     assert np.array_equal(got[:2], np.zeros((2, 4), F)) and np.array_equal(got[2], np.ones(4, F))
+
+
+# ----------------------------------------------------------- all slots
+SLOT_EXTENSIONS = {  # extension id -> (row, component) of the packed map index (materialLayoutSchema.ts)
+    39: (2, 2), 40: (22, 2), 43: (3, 3), 44: (1, 1), 46: (2, 3), 47: (22, 0), 48: (22, 1), 49: (9, 3),
+    50: (9, 1), 64: (6, 0), 65: (6, 1), 66: (6, 3), 67: (18, 3), 68: (19, 3), 69: (21, 3)}
+
+
+def test_every_supported_slot_packs_its_map_index():
+    """One texture per slot: the map list follows MATERIAL_TEXTURE_NAMES
+    order (map, alphaMap, normalMap, emissiveMap, metallicRoughnessMap,
+    roughnessMap, metalnessMap, transmissionMap, thinFilmMap, coatWeightMap,
+    coatRoughnessMap, fuzzColorMap, fuzzRoughnessMap, specularWeightMap,
+    specularColorMap), each index lands in its packed field."""
+    order = [39, 40, 44, 43, 46, 47, 48, 49, 50, 64, 65, 66, 67, 68, 69]
+    d = base()
+    tex = {eid: d.add_texture(1, 1, np.full((1, 1, 4), 10 + k, np.uint8)) for k, eid in enumerate(order)}
+    ext = [(eid, tex[eid]) for eid in sorted(tex)] + [(41, 1), (62, (-0.5,)), (63, 2)]
+    m = d.add_material(extensions=ext, coat_weight=0.5)
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV), m)
+    h = decoded(d)
+    rows = h.materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)[m]
+    for position, eid in enumerate(order):
+        r, c = SLOT_EXTENSIONS[eid]
+        assert rows[r, c] == position, eid
+    assert rows[25, 2:].tolist() == [0.0, 2.0]            # thin-film minimum clamped at 0, channel b
+    assert rows[23, 3] == 0                                # opaque
+    assert maps_of(h)[0].shape[0] == len(order)
+
+
+def test_coat_weight_map_leaves_emission_raw():
+    # materialEmission.ts:10-22: with a coat weight map the packed emission
+    # carries no coat passage (the shader applies it per texel).
+    d = base()
+    t = d.add_texture(1, 1, np.full((1, 1, 4), 128, np.uint8))
+    a = d.add_material(emission_color=(1, 1, 1), emission_luminance=2.0, coat_weight=1.0,
+                       extensions=[(26, (0.25, 0.25, 0.25))])
+    b = d.add_material(emission_color=(1, 1, 1), emission_luminance=2.0, coat_weight=1.0,
+                       extensions=[(26, (0.25, 0.25, 0.25)), (64, t)])
+    g = d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV)
+    d.add_mesh(g, a)
+    d.add_mesh(g, b, transform=D.translate([0, 1, 0]))
+    rows = decoded(d).materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)
+    assert np.allclose(rows[a, 3, :3], 1.0) and np.allclose(rows[b, 3, :3], 2.0)
+
+
+def test_emissive_triangles_carry_corner_uvs():
+    d = base()
+    t = d.add_texture(2, 2, np.full((2, 2, 4), 200, np.uint8))
+    uvs = np.array([[0.1, 0.2], [0.9, 0.2], [0.9, 0.8], [0.1, 0.8]], F)
+    lamp = d.add_material(emission_color=(1, 1, 1), emission_luminance=3.0, textures=(NONE, NONE, NONE, t))
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=uvs), lamp, transform=D.translate([0, 1, 0]))
+    h = decoded(d)
+    tri = h.light_sampling.reshape(-1, 4)[:12].reshape(2, 6, 4)   # 2 triangles x 6 texels
+    for k in range(2):
+        corners = QUAD_IDX[k * 3:k * 3 + 3]
+        want = uvs[corners].reshape(-1)
+        assert np.array_equal(tri[k, 3:6].reshape(-1)[:6], want)
+        assert np.array_equal(tri[k, 3:6].reshape(-1)[6:], want)      # secondary set repeats the primary
+    assert h.materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)[lamp, 3, 3] == 0
