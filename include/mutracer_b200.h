@@ -185,7 +185,12 @@ typedef struct mtc_scene_view {
  * rows flipped when the texture is. */
 #define MTC_MAP_VEC4_ROWS 3
 /* flags: shader specialisation constants that are not in the uniform
- * (HAS_MEDIUM, SPECTRAL and SAMPLING_PATTERN of wgpuMaterialConstants.ts:40-70).
+ * (HAS_MEDIUM, SPECTRAL, HAS_ALPHA and SAMPLING_PATTERN of
+ * wgpuMaterialConstants.ts:40-70).  HAS_ALPHA (some material's resolved alpha
+ * mode is mask or blend) turns on the shadow rays' alpha test
+ * (intersectionAlpha.wgsl.ts) and the RGB integrator that splits a partly
+ * covered primary hit into a back and a front path (rayTrace.compute.ts
+ * :815-890); spectral scenes keep their integrator.
  * The sampling pattern (MT_SAMPLING_*) occupies bits 4..5.  BLAS_GPU_LAYOUT is
  * bit 2 (layout code 2) of the reference's blasLayoutMask: set it when any
  * instance record carries BLAS layout code 2 (BVH_GPU); without it such
@@ -193,7 +198,7 @@ typedef struct mtc_scene_view {
  * BVH2 (layout code 0) is always traversed. */
 enum { MTC_SCENE_HAS_MEDIUM = 1u, MTC_SCENE_SPECTRAL = 2u,
        MTC_SCENE_PATTERN_SHIFT = 4u, MTC_SCENE_PATTERN_MASK = 0x30u,
-       MTC_SCENE_BLAS_GPU_LAYOUT = 0x100u };
+       MTC_SCENE_BLAS_GPU_LAYOUT = 0x100u, MTC_SCENE_HAS_ALPHA = 0x200u };
 
 /* G3 accumulation outputs (rayTrace.compute.ts:294-299; never overwritten,
  * always accumulated).  shadow_catcher holds 3 vec4 per pixel

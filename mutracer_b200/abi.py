@@ -30,6 +30,7 @@ MTC_SCENE_SPECTRAL = 2
 MTC_SCENE_PATTERN_SHIFT = 4
 MTC_SCENE_PATTERN_MASK = 0x30
 MTC_SCENE_BLAS_GPU_LAYOUT = 0x100
+MTC_SCENE_HAS_ALPHA = 0x200
 MTC_FEATURE_USE_ENVMAP = 1
 MTC_INSTANCE_VEC4_STRIDE = 10
 MTC_MATERIAL_VEC4_ROWS = 26

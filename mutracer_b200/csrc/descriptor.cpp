@@ -453,10 +453,8 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
       case 74: m.slots[kMapCoatNormal] = texture(); break;
       case 62: scalar(md.thinFilmThicknessMinimum); break;
       case 63: md.thinFilmMapChannel = int(choice(4)); break;
-      case 41:  // alpha mode: auto or opaque keep a fully opaque material opaque
-        alphaMode = choice(4);
-        if (alphaMode > 1) unsupported("alpha mask / blend modes");
-        break;
+      case 41: alphaMode = choice(4); break;  // auto, opaque, mask, blend
+      case 42: scalar(md.alphaCutoff); break;
       case 45: pair(md.normalScale); break;
       case 54: mapAlphaUsage = choice(3); break;  // opaque, alpha, transmission
       case 55:
@@ -472,15 +470,20 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
       default: unsupported("material extension " + std::to_string(id));
     }
   }
-  if (m.opacity != 1.0f) unsupported("material opacity below 1");
   if (m.slots[kMapDisplacement] != NONE) unsupported("displacement maps");
   if (m.slots[kMapAnisotropy] != NONE) unsupported("anisotropy maps");
   if (m.slots[kMapCoatNormal] != NONE) unsupported("coat normal maps");
-  // resolveMaterialAlphaMode (MaterialState.ts:251-264): auto with the base
-  // color's alpha as opacity, or with an alpha map, blends, which needs
-  // any-hit traversal.
-  if (alphaMode == 0 && ((mapAlphaUsage == 1 && m.slots[kMapBase] != NONE) || m.slots[kMapAlpha] != NONE))
-    unsupported("texture alpha as opacity");
+  // resolveMaterialAlphaMode (MaterialState.ts:251-264) to
+  // materialAlphaModeConstants: explicit modes stay; auto masks with a
+  // positive cutoff, blends with partial opacity, the base color's alpha as
+  // opacity or an alpha map, and is opaque otherwise.
+  md.opacity = m.opacity;
+  if (alphaMode == 1) md.alphaMode = 0;
+  else if (alphaMode == 2) md.alphaMode = 1;
+  else if (alphaMode == 3) md.alphaMode = 2;
+  else if (md.alphaCutoff > 0) md.alphaMode = 1;
+  else if (m.opacity < 1 || mapAlphaUsage == 1 || m.slots[kMapAlpha] != NONE) md.alphaMode = 2;
+  else md.alphaMode = 0;
   md.mapAlphaUsage = mapAlphaUsage == 1 ? 2 : mapAlphaUsage == 2 ? 3 : 0;  // mapAlphaUsageConstants
   // materialEmission (materialEmission.ts:10-22): emission crosses the coat
   // once; with a coat weight map the shader applies that passage instead.
@@ -936,6 +939,8 @@ void decodeScene(const Words &d, SceneHost &s) {
   std::vector<LightDesc> lightList;
   for (uint32_t i = 0; i < lights; i++) lightList.push_back(decodeLight(d, u[12] + i * lightWords, version, i));
   assembleScene(s, meshData, instances, mats, lightList, 8, 8, false);
+  if ((s.flags & MTC_SCENE_SPECTRAL) && (s.flags & MTC_SCENE_HAS_ALPHA))
+    unsupported("alpha coverage in a dispersive (spectral) scene");
   decodeCamera(d, u[14], width, height, s.camera);
   defaultUniform(s, 6, 2, 12345, 0);
   mtc_trace_uniform &tu = s.uniform;

@@ -132,45 +132,6 @@ MTD float spectrumCameraWavelength(uint32_t channel, float u) {
   return 500.0f - 25.0f * (1.0f - expf((wavelength - 500.0f) / 25.0f));
 }
 
-// ------------------------------------------------------------ material maps
-// materialBuffer.wgsl.ts:316-378 wrapMapCoordinate / sampleMap / loadMapTexel
-// with independent textures.  The shader filters footprints inside the image
-// in hardware and repeat footprints that cross its edge by hand; both are the
-// bilinear mix of the four texels around wrapped * size - 0.5 with clamped
-// (repeat: modular) texel coordinates, evaluated here in software for every
-// footprint.  Rounded operations throughout (no contraction), so a lookup is
-// bit-identical to the CPU restatement.
-MTD float wrapMapCoordinate(float v, float mode) {
-  if (mode < 0.5f) return __fsub_rn(v, floorf(v));
-  if (mode < 1.5f) return clampf(v, 0.0f, 1.0f);
-  const float m = __fsub_rn(v, __fmul_rn(2.0f, floorf(__fmul_rn(v, 0.5f))));
-  return __fsub_rn(1.0f, fabsf(__fsub_rn(1.0f, m)));
-}
-static __device__ __noinline__ float4 sampleMap(const DevScene &s, int idx, V2 uv) {
-  if (idx < 0 || uint32_t(idx) >= s.mapCount) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const float4 *mi = s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS;
-  const float4 a = ld4(mi), t = ld4(mi + 1), modes = ld4(mi + 2);
-  const int w = asi(a.x), h = asi(a.y);
-  const uint32_t first = asu(a.z);
-  if (w < 1 || h < 1 || uint64_t(first) + uint64_t(w) * uint64_t(h) > s.mapTexelCount)
-    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const float tx = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.x, t.x), t.z), modes.z), float(w)), 0.5f);
-  const float ty = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.y, t.y), t.w), modes.w), float(h)), 0.5f);
-  const float fx = floorf(tx), fy = floorf(ty), wx = __fsub_rn(tx, fx), wy = __fsub_rn(ty, fy);
-  // Finite coordinates wrap into [-1, size - 1]; the clamp only pins NaN.
-  const int bx = int(fminf(fmaxf(fx, -1.0f), float(w))), by = int(fminf(fmaxf(fy, -1.0f), float(h)));
-  auto load = [&](int x, int y) {
-    int px = modes.z < 0.5f ? ((x % w) + w) % w : min(max(x, 0), w - 1);
-    int py = modes.w < 0.5f ? ((y % h) + h) % h : min(max(y, 0), h - 1);
-    return ld4(s.mapTexels + first + size_t(py) * size_t(w) + size_t(px));
-  };
-  const float4 t00 = load(bx, by), t10 = load(bx + 1, by), t01 = load(bx, by + 1), t11 = load(bx + 1, by + 1);
-  auto mix1 = [](float p, float q, float k) { return __fadd_rn(__fmul_rn(p, __fsub_rn(1.0f, k)), __fmul_rn(q, k)); };
-  auto mix4 = [&](float4 p, float4 q, float k) {
-    return make_float4(mix1(p.x, q.x, k), mix1(p.y, q.y, k), mix1(p.z, q.z, k), mix1(p.w, q.w, k));
-  };
-  return mix4(mix4(t00, t10, wx), mix4(t01, t11, wx), wy);
-}
 // sRGBToLinear / decodeMapColor (materialBuffer.wgsl.ts:258-265).
 MTD float srgbToLinear(float c) {
   return c < 0.04045f ? c * 0.0773993808f : powf(c * 0.9478672986f + 0.0521327014f, 2.4f);
@@ -183,9 +144,7 @@ MTD V3 decodeMapColor(const DevScene &s, int idx, V3 c) {
 }
 
 MTD V3 mulv(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
-// A material's map index names a map of this scene (an index past the map
-// table, like -1, means no map).
-MTD bool mapValid(const DevScene &s, float index) { return index >= 0.0f && index < float(s.mapCount); }
+
 
 // getMaterialEmission (materialBuffer.wgsl.ts:381-403): the packed emission
 // times the sRGB-decoded emissive map and, for standard materials, the coat
@@ -801,14 +760,17 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
   si.position = mat4v(l0, l1, l2, l3, position, 1.0f);
 }
 
-// intersect.wgsl.ts:829-879
+// intersect.wgsl.ts:829-879; scenes with alpha test each candidate's
+// coverage with the path's sampler.
 template <bool kGpuLayout>
 MTD bool intersectSceneShadow(const JobData &J, const Ray &r, float lightDistance, int32_t tri, int32_t ins,
-                              Counters &cnt) {
+                              Counters &cnt, Sampler &smp) {
   if (J.u.is_empty > 0) return false;
   cnt.shadow++;
   TraversalHit h;
   h.tMax = fminf(fmaxf(lightDistance, 0.0f), RAY_MAX_DISTANCE);
+  if (J.s.flags & MTC_SCENE_HAS_ALPHA)
+    return traverse<true, kGpuLayout, true>(J.s, J.u.blas_offset, r.o, r.d, 1, true, tri, ins, h, &smp);
   return traverse<true, kGpuLayout>(J.s, J.u.blas_offset, r.o, r.d, 1, true, tri, ins, h);
 }
 
@@ -1267,7 +1229,9 @@ struct PathSample {
 
 // Locals of the spectral integrator (rayTrace.compute.ts:947-1057) that live
 // across its three wavelength paths: the primary vertex they share, the
-// sampler state each restarts from, and the running sums.
+// sampler state each restarts from, and the running sums.  The alpha-split
+// RGB integrator (:815-890) keeps its primary vertex, guides and camera ray
+// in the same fields, plus the coverage split and the back path's result.
 struct SpectralState {
   SurfaceInteraction primarySi;
   Aux primaryAux;        // the integrator's outAux: primary-hit guides
@@ -1279,7 +1243,17 @@ struct SpectralState {
   bool primaryReady, dispersivePrimary, allBlank;
   V3 color, guideAlbedo, guideNormal;
   float alpha;
+  // alpha split: coverage of the primary hit, whether it was split, whether
+  // the front path runs (frontPending: its first step reuses the primary
+  // vertex without a query), and the back path's (li, alpha) and guides
+  float coverage;
+  bool split, front, frontPending;
+  float4 back;
+  Aux backAux;
 };
+
+// The alpha-split integrator runs for RGB scenes with a non-opaque material.
+MTD bool alphaSplit(const JobData &J) { return (J.s.flags & MTC_SCENE_HAS_ALPHA) && !isSpectral(J); }
 
 // rayTrace.compute.ts:1157-1208 main up to the integrator call: sampler
 // state for (x, y, outNormal.a + sampleSequenceOffset), Sobol jitter, camera
@@ -1346,6 +1320,14 @@ static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, 
   ps.event = 0;
   ps.sampleIgnored = false;
   ps.isNotTransparent = false;
+  if (alphaSplit(J)) {
+    sp.primaryReady = false;
+    sp.cameraRay = cam;
+    sp.coverage = 1.0f;
+    sp.split = false;
+    sp.front = false;
+    sp.frontPending = false;
+  }
   if (isSpectral(J)) {
     sp.primaryReady = false;
     sp.primaryAux = {v3(0.0f), v3(0.0f), false};
@@ -1414,6 +1396,109 @@ static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const Trav
   shadeVertex(c, ps.coord, path, ps.depth, si, ma, ps.aux, ps.sampleIgnored);
   if (path.abort) return true;
   ps.event = event + 1;
+  return false;
+}
+
+// One iteration of the alpha-split RGB integrator (rayTrace.compute.ts
+// :815-890) once its query (if any) is answered.  The primary hit keeps the
+// guides; if it is a standard or unlit surface with coverage below 1 the
+// sample splits: the back path continues through it first (event 0 again,
+// from just behind the surface), then the front path restarts at the primary
+// vertex with full coverage, and finishAlphaSplit mixes the two by the
+// coverage.  Returns true when the current path has ended.
+static __device__ __noinline__ bool shadeStepAlpha(Ctx &c, PathSample &ps, SpectralState &sp, const TraversalHit &h) {
+  Path &path = ps.path;
+  SurfaceInteraction &si = ps.si;
+  const int bounceLimit = max(c.J.u.bounces, 0);
+  const int eventLimit = min(bounceLimit * 3, 20);
+  const int event = ps.event;
+  Material ma;
+  if (sp.frontPending) {
+    sp.frontPending = false;
+    si = sp.primarySi;
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
+    ma.alpha = 1.0f;
+  } else {
+    si.hit = false;
+    if (h.insIdx >= 0) {
+      si.triangleIndex = h.triangleIndex;
+      completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
+    }
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
+  }
+  if (!sp.primaryReady) {
+    if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
+      ps.aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+      ps.aux.normal = dot(si.normal, si.position - cameraEye(c.J)) > 0.0f ? -si.normal : si.normal;
+      si.albedoSampled = ma.transmissionWeight > 0.5f;
+    }
+    sp.primarySi = si;
+    sp.primaryAux = ps.aux;
+    sp.primaryReady = true;
+    sp.coverage = clampf(ma.alpha, 0.0f, 1.0f);
+    sp.split = si.hit && (ma.materialType == 0 || ma.materialType == 2) && sp.coverage < 1.0f;
+    if (sp.split) {
+      path.ray.o = si.position + sp.cameraRay.d * (EPS * 0.02f);
+      si.albedoSampled = false;
+      return false;
+    }
+  } else if (event == 0 && !sp.front && sp.split) {
+    if (si.hit && ma.materialType == 0) {
+      ps.aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+      ps.aux.normal = dot(si.normal, si.position - cameraEye(c.J)) > 0.0f ? -si.normal : si.normal;
+      si.albedoSampled = ma.transmissionWeight > 0.5f;
+    }
+  }
+  if (event == 0) {
+    ps.isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
+  } else {
+    completeVertex(c, path, ps.depth, si, ma, ps.sampleIgnored);
+  }
+  if (ps.isNotTransparent && event > bounceLimit) path.abort = true;
+  if (!path.abort && event < eventLimit) shadeVertex(c, ps.coord, path, ps.depth, si, ma, ps.aux, ps.sampleIgnored);
+  if (path.abort || event >= eventLimit) return true;
+  ps.event = event + 1;
+  return false;
+}
+
+// End of an alpha-split path, after its last shadow ray (rayTrace.compute.ts
+// :870-888): true when the sample is complete (unsplit, zero coverage, or the
+// front path done: radiance, alpha and guides mixed by the coverage);
+// otherwise the back path's result is kept and the front path starts.
+MTD bool finishAlphaSplit(const JobData &J, PathSample &ps, SpectralState &sp) {
+  if (!sp.split || sp.coverage <= 0.0f) return true;
+  const float k = sp.coverage;
+  auto mix3 = [k](V3 a, V3 b) { return V3{a.x * (1.0f - k) + b.x * k, a.y * (1.0f - k) + b.y * k, a.z * (1.0f - k) + b.z * k}; };
+  if (sp.front) {
+    Aux &a = ps.aux;
+    const Aux &b = sp.backAux;
+    a.albedo = mix3(b.albedo, a.albedo);
+    const V3 n = mix3(b.normal, a.normal);
+    a.normal = dot(n, n) > 1e-12f ? normalize(n) : v3(0.0f);
+    a.isBlank = b.isBlank && a.isBlank;
+    ps.path.li = mix3(xyz(sp.back), ps.path.li);
+    ps.path.alpha = sp.back.w * (1.0f - k) + ps.path.alpha * k;
+    return true;
+  }
+  sp.back = make_float4(ps.path.li.x, ps.path.li.y, ps.path.li.z, ps.path.alpha);
+  sp.backAux = ps.aux;
+  sp.front = true;
+  sp.frontPending = true;
+  ps.event = 0;
+  ps.depth = 0;
+  ps.sampleIgnored = false;
+  ps.aux = sp.primaryAux;
+  Path &path = ps.path;
+  path.scatteringMediumEntered = false;
+  path.ray = sp.cameraRay;
+  path.li = v3(0.0f);
+  path.alpha = J.u.transmissive_output_alpha_min < 1.0f ? 0.0f : 1.0f;
+  path.beta = v3(1.0f);
+  path.fromEye = true;
+  path.abort = false;
+  path.scatteringPdf = 0.0f;
+  path.scatteringIsDelta = false;
+  path.isNextRefraction = false;
   return false;
 }
 
@@ -1539,9 +1624,10 @@ MTD bool stepPath(Ctx &c, PathSample &ps, SpectralState &sp) {
   h.tMax = RAY_MAX_DISTANCE;
   h.triangleIndex = -1;
   h.insIdx = -1;
-  const bool spectral = isSpectral(c.J);
-  if (!spectral || !reusesPrimary(c.J, ps, sp.primaryReady)) traceExtension<kGpuLayout>(c.J, ps, h, c.cnt);
-  return spectral ? shadeStepSpectral(c, ps, sp, h) : shadeStep(c, ps, h);
+  const bool spectral = isSpectral(c.J), split = alphaSplit(c.J);
+  const bool reuse = spectral ? reusesPrimary(c.J, ps, sp.primaryReady) : split && sp.frontPending;
+  if (!reuse) traceExtension<kGpuLayout>(c.J, ps, h, c.cnt);
+  return spectral ? shadeStepSpectral(c, ps, sp, h) : split ? shadeStepAlpha(c, ps, sp, h) : shadeStep(c, ps, h);
 }
 
 // The deferred NEE visibility test of sampleScattering (sampleMaterial.wgsl.ts
@@ -1551,7 +1637,7 @@ MTD void resolveShadow(Ctx &c, PathSample &ps) {
   if (!c.shadow.valid) return;
   c.shadow.valid = false;
   if (!intersectSceneShadow<kGpuLayout>(c.J, c.shadow.ray, c.shadow.maxDistance, c.shadow.triangleIndex,
-                            c.shadow.instanceIndex, c.cnt))
+                                        c.shadow.instanceIndex, c.cnt, c.smp))
     ps.path.li += c.shadow.contribution;
 }
 
@@ -1599,7 +1685,7 @@ static __device__ __noinline__ void tracePixelSamples(const JobData &J, uint32_t
   const uint32_t idx = x + y * J.width;
   PathSample ps;
   SpectralState sp;
-  const bool spectral = isSpectral(J);
+  const bool spectral = isSpectral(J), split = alphaSplit(J);
   uint32_t left = samples;
   bool active = left > 0u;
   if (active) beginSample(c, x, y, ps, sp);
@@ -1610,6 +1696,7 @@ static __device__ __noinline__ void tracePixelSamples(const JobData &J, uint32_t
     bool ended = stepPath<kGpuLayout>(c, ps, sp);
     resolveShadow<kGpuLayout>(c, ps);
     if (ended && spectral) ended = finishWavelength(J, ps, sp);
+    else if (ended && split) ended = finishAlphaSplit(J, ps, sp);
     if (ended) {
       endSample(J, idx, ps);
       if (--left == 0u) active = false;

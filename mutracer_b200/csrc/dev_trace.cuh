@@ -231,6 +231,82 @@ MTD V3 vertexNormal(const DevScene &s, int32_t i) {
   return normalize(v);
 }
 
+// ------------------------------------------------------------ material maps
+// materialBuffer.wgsl.ts:316-378 wrapMapCoordinate / sampleMap / loadMapTexel
+// with independent textures.  The shader filters footprints inside the image
+// in hardware and repeat footprints that cross its edge by hand; both are the
+// bilinear mix of the four texels around wrapped * size - 0.5 with clamped
+// (repeat: modular) texel coordinates, evaluated here in software for every
+// footprint.  Rounded operations throughout (no contraction), so a lookup is
+// bit-identical to the CPU restatement.
+MTD float wrapMapCoordinate(float v, float mode) {
+  if (mode < 0.5f) return __fsub_rn(v, floorf(v));
+  if (mode < 1.5f) return clampf(v, 0.0f, 1.0f);
+  const float m = __fsub_rn(v, __fmul_rn(2.0f, floorf(__fmul_rn(v, 0.5f))));
+  return __fsub_rn(1.0f, fabsf(__fsub_rn(1.0f, m)));
+}
+static __device__ __noinline__ float4 sampleMap(const DevScene &s, int idx, V2 uv) {
+  if (idx < 0 || uint32_t(idx) >= s.mapCount) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4 *mi = s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS;
+  const float4 a = ld4(mi), t = ld4(mi + 1), modes = ld4(mi + 2);
+  const int w = asi(a.x), h = asi(a.y);
+  const uint32_t first = asu(a.z);
+  if (w < 1 || h < 1 || uint64_t(first) + uint64_t(w) * uint64_t(h) > s.mapTexelCount)
+    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float tx = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.x, t.x), t.z), modes.z), float(w)), 0.5f);
+  const float ty = __fsub_rn(__fmul_rn(wrapMapCoordinate(__fadd_rn(__fmul_rn(uv.y, t.y), t.w), modes.w), float(h)), 0.5f);
+  const float fx = floorf(tx), fy = floorf(ty), wx = __fsub_rn(tx, fx), wy = __fsub_rn(ty, fy);
+  // Finite coordinates wrap into [-1, size - 1]; the clamp only pins NaN.
+  const int bx = int(fminf(fmaxf(fx, -1.0f), float(w))), by = int(fminf(fmaxf(fy, -1.0f), float(h)));
+  auto load = [&](int x, int y) {
+    int px = modes.z < 0.5f ? ((x % w) + w) % w : min(max(x, 0), w - 1);
+    int py = modes.w < 0.5f ? ((y % h) + h) % h : min(max(y, 0), h - 1);
+    return ld4(s.mapTexels + first + size_t(py) * size_t(w) + size_t(px));
+  };
+  const float4 t00 = load(bx, by), t10 = load(bx + 1, by), t01 = load(bx, by + 1), t11 = load(bx + 1, by + 1);
+  auto mix1 = [](float p, float q, float k) { return __fadd_rn(__fmul_rn(p, __fsub_rn(1.0f, k)), __fmul_rn(q, k)); };
+  auto mix4 = [&](float4 p, float4 q, float k) {
+    return make_float4(mix1(p.x, q.x, k), mix1(p.y, q.y, k), mix1(p.z, q.z, k), mix1(p.w, q.w, k));
+  };
+  return mix4(mix4(t00, t10, wx), mix4(t01, t11, wx), wy);
+}
+// A material's map index names a map of this scene (an index past the map
+// table, like -1, means no map).
+MTD bool mapValid(const DevScene &s, float index) { return index >= 0.0f && index < float(s.mapCount); }
+
+// intersectionAlphaPasses (intersectionAlpha.wgsl.ts:14-90): whether a shadow
+// ray's candidate hit on a triangle of `material` occludes.  Coverage is the
+// material's alpha times the base color's alpha (map alpha usage "alpha") and
+// the alpha map's g at the hit's UV, then resolved by the alpha mode: opaque
+// occludes, mask compares with the cutoff, blend draws hashedSample(1).
+static __device__ __noinline__ bool alphaPasses(const DevScene &s, int32_t material, int32_t i0, int32_t i1,
+                                                int32_t i2, V3 bary, Sampler &smp) {
+  const float4 *d = s.mats + size_t(material) * MTC_MATERIAL_VEC4_ROWS;
+  const float4 r2 = ld4(d + 2), r5 = ld4(d + 5), r22 = ld4(d + 22);
+  float alpha = ld4(d + 9).x;
+  const bool baseAlpha = r5.w == 2.0f && mapValid(s, r2.z), alphaMap = mapValid(s, r22.z);
+  if (baseAlpha || alphaMap) {
+    V2 uv0 = {0.0f, 0.0f}, uv1 = uv0, uv2 = uv0;
+    if (s.vuvOff) {
+      auto vuv = [&](int32_t i) {
+        const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vuvOff;
+        return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
+      };
+      uv0 = vuv(i0); uv1 = vuv(i1); uv2 = vuv(i2);
+    }
+    const float4 r7 = ld4(d + 7);
+    const V2 uv = {(bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x) * r7.z,
+                   (bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y) * r7.w};
+    if (baseAlpha) alpha *= sampleMap(s, int(r2.z), uv).w;
+    if (alphaMap) alpha *= sampleMap(s, int(r22.z), uv).y;
+  }
+  const int mode = int(ld4(d + 23).w);
+  if (mode == 0) alpha = 1.0f;
+  else if (mode == 1) alpha = alpha >= r22.w ? 1.0f : 0.0f;
+  if (mode == 2) return smp.hashedSample(1u) <= alpha;
+  return alpha >= 1.0f;
+}
+
 struct TraversalHit {
   float tMax;
   V3 hitNormal, hitBary;
@@ -244,9 +320,16 @@ struct TraversalHit {
 // (getBVHTraverseCode's layout branches are compiled only for the layouts a
 // scene uses): without it only BVH2 (layout 0) BLASes are traversed and the
 // BVH_GPU (layout 2) code is not compiled in.
-template <bool shadow, bool kGpuLayout>
+//
+// A shadow query with kAlpha tests each candidate hit's coverage
+// (alphaPasses, drawing from `alphaSmp`): a hit that does not occlude
+// restores the query's tMax and traversal goes on (intersect.wgsl.ts
+// :846-866).  Without kAlpha the test is not compiled in.
+template <bool shadow, bool kGpuLayout, bool kAlpha = false>
 __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 rayO, V3 rayD, int bounces,
-                                      bool doubleSided, int32_t currentTri, int32_t currentIns, TraversalHit &h) {
+                                      bool doubleSided, int32_t currentTri, int32_t currentIns, TraversalHit &h,
+                                      Sampler *alphaSmp = nullptr) {
+  const float tMaxInit = h.tMax;
   int32_t tlasStack[MTC_MAX_STACK];
   int32_t blasStack[MTC_MAX_STACK];
   int tlasTop = -1;
@@ -352,7 +435,14 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
           h.hitNormal = candidateNormal;
           h.tMax = t;
           h.hitBary = bary;
-          if (shadow) return true;
+          if (shadow) {
+            if (kAlpha && !alphaPasses(s, sideMaterial, asi(r3.x) + vertexOffset, asi(r3.y) + vertexOffset,
+                                       asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
+              h.tMax = tMaxInit;
+              continue;
+            }
+            return true;
+          }
           h.triangleIndex = triangleIndex;
           h.insIdx = insIdx;
         }
@@ -371,7 +461,7 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
 // current TLAS leaf.  Visit order, box tests, the `>` tie rule and the
 // self-hit and backface rules are those of traverse(), so the hits are
 // bit-identical to it.
-template <bool shadow, bool kGpuLayout>
+template <bool shadow, bool kGpuLayout, bool kAlpha = false>
 struct RayTraversal {
   const float4 *bvh, *ins, *mats;
   const uint32_t *attr;
@@ -394,6 +484,12 @@ struct RayTraversal {
   uint32_t blasLayout;
   bool found;
   TraversalHit h;
+  // Shadow queries of scenes with alpha: the scene and the path's sampler
+  // for alphaPasses, and the query's tMax to restore after a hit that does
+  // not occlude.  Null otherwise.
+  const DevScene *alphaScene;
+  Sampler *alphaSmp;
+  float tMaxInit;
 
   MTD V3 position(int32_t i) const {
     const uint32_t *w = attr + size_t(i) * vstride;
@@ -408,6 +504,11 @@ struct RayTraversal {
   MTD bool begin(const DevScene &s, int32_t base, V3 ro, V3 rd, int b, bool ds, int32_t ct, int32_t ci, float tMax) {
     bvh = s.bvh; ins = s.ins; mats = s.mats; attr = s.attr; vstride = s.vstride; blasBase = base;
     rayO = ro; rayD = rd; bounces = b; doubleSided = ds; currentTri = ct; currentIns = ci;
+    if (kAlpha) {
+      alphaScene = nullptr;
+      alphaSmp = nullptr;
+      tMaxInit = tMax;
+    }
     h.tMax = tMax;
     h.triangleIndex = -1;
     h.insIdx = -1;
@@ -516,6 +617,12 @@ struct RayTraversal {
       h.tMax = t;
       h.hitBary = bary;
       if (shadow) {
+        if (kAlpha && alphaSmp &&
+            !alphaPasses(*alphaScene, sideMaterial, asi(r3.x) + vertexOffset, asi(r3.y) + vertexOffset,
+                         asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
+          h.tMax = tMaxInit;
+          continue;
+        }
         found = true;
         return true;
       }

@@ -1006,6 +1006,10 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   if (!s.env.image.empty()) features |= MTC_FEATURE_USE_ENVMAP;
   if (hasMedium) s.flags |= MTC_SCENE_HAS_MEDIUM;
   if (spectral) s.flags |= MTC_SCENE_SPECTRAL;
+  // HAS_ALPHA: some material resolves to mask or blend (wgpuMaterialConstants.ts:60-62).
+  s.flags &= ~uint32_t(MTC_SCENE_HAS_ALPHA);
+  for (const MaterialDesc &m : materials)
+    if (m.alphaMode != 0) s.flags |= MTC_SCENE_HAS_ALPHA;
   // Light choices: environment, analytic lights (sceneAssembly.ts:42-82).
   std::vector<int> types, idx;
   std::vector<double> weights;

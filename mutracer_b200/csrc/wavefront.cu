@@ -262,7 +262,8 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
         // traceExtension: an empty scene is a miss without a traversal, and a
         // spectral wavelength path restarting at the shared primary vertex
         // traces nothing.
-        if (J.u.is_empty > 0 || (isSpectral(J) && reusesPrimary(J, sl.ps, v.spectral[s].primaryReady))) {
+        if (J.u.is_empty > 0 || (isSpectral(J) && reusesPrimary(J, sl.ps, v.spectral[s].primaryReady)) ||
+            (alphaSplit(J) && v.spectral[s].frontPending)) {
           TraversalHit none;
           none.tMax = RAY_MAX_DISTANCE;
           none.triangleIndex = -1;
@@ -372,7 +373,9 @@ __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
     c.shadow.valid = false;
     PathSample ps = sl.ps;
     TraversalHit h = v.hits[s];
-    bool ended = isSpectral(J) ? shadeStepSpectral(c, ps, v.spectral[s], h) : shadeStep(c, ps, h);
+    bool ended = isSpectral(J)   ? shadeStepSpectral(c, ps, v.spectral[s], h)
+                 : alphaSplit(J) ? shadeStepAlpha(c, ps, v.spectral[s], h)
+                                 : shadeStep(c, ps, h);
     sl.ps = ps;
     sl.smp = c.smp;
     sl.shadow = c.shadow;
@@ -385,10 +388,10 @@ __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
 
 // NEE visibility of the queued shadow rays (intersectSceneShadow and
 // resolveShadow), persistent like k_wf_extend.
-template <bool kGpuLayout>
+template <bool kGpuLayout, bool kAlpha>
 __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS) k_wf_shadow(StreamView v) {
   const uint32_t n = v.q->shadowCount;
-  RayTraversal<true, kGpuLayout> rt;
+  RayTraversal<true, kGpuLayout, kAlpha> rt;
   uint32_t s = 0, shadowRays = 0;
   bool busy = false, exhausted = false;
   for (;;) {
@@ -412,10 +415,16 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS) k_wf_s
         } else {
           shadowRays++;
           float tMax = fminf(fmaxf(q.maxDistance, 0.0f), RAY_MAX_DISTANCE);
-          if (rt.begin(J.s, J.u.blas_offset, q.ray.o, q.ray.d, 1, true, q.triangleIndex, q.instanceIndex, tMax))
+          if (rt.begin(J.s, J.u.blas_offset, q.ray.o, q.ray.d, 1, true, q.triangleIndex, q.instanceIndex, tMax)) {
             busy = true;
-          else
+            // Coverage draws advance the path's own sampler, in place.
+            if (kAlpha && (J.s.flags & MTC_SCENE_HAS_ALPHA)) {
+              rt.alphaScene = &J.s;
+              rt.alphaSmp = &v.slots[s].smp;
+            }
+          } else {
             done = true;
+          }
         }
       }
     }
@@ -449,8 +458,10 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
     Slot &sl = v.slots[s];
     const JobData &J = v.jobs[sl.job];
     PathSample ps = sl.ps;
-    if (isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) {
-      // The next wavelength path of this sample starts at event 0.
+    if ((isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) ||
+        (alphaSplit(J) && !finishAlphaSplit(J, ps, v.spectral[s]))) {
+      // The next wavelength path, or the front path, of this sample starts
+      // at event 0.
       sl.ps = ps;
       enqueueRay(v, cur ^ 1u, s);
       continue;
@@ -653,7 +664,7 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
   if ((e = gridFor((const void *)k_wf_seed, gSeed)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_extend<false>, gExtend)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_shade, gShade)) != cudaSuccess ||
-      (e = gridFor((const void *)k_wf_shadow<false>, gShadow)) != cudaSuccess ||
+      (e = gridFor((const void *)k_wf_shadow<false, false>, gShadow)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_finish, gFinish)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_regroup, gRegroup)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_sort_rays, gSort)) != cudaSuccess)
@@ -681,6 +692,7 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
 
   // The BLAS-layout specialisation (blasLayoutMask) of the traversal kernels.
   const bool gpuLayout = (hdr.flagsUnion & MTC_SCENE_BLAS_GPU_LAYOUT) != 0u;
+  const bool alpha = (hdr.flagsUnion & MTC_SCENE_HAS_ALPHA) != 0u;  // shadow rays test coverage
   k_wf_seed<<<gSeed, kStreamThreads, 0, st>>>(v);
   e = cudaGetLastError();
   uint32_t cur = 0, iterations = 0, chunk = 0;
@@ -693,8 +705,13 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
       else k_wf_extend<false><<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
       if (regroup) k_wf_regroup<<<gRegroup, kStreamThreads, 0, st>>>(v, cur);
       k_wf_shade<<<gShade, kStreamThreads, 0, st>>>(v, cur, regroup);
-      if (gpuLayout) k_wf_shadow<true><<<gShadow, kStreamThreads, 0, st>>>(v);
-      else k_wf_shadow<false><<<gShadow, kStreamThreads, 0, st>>>(v);
+      if (alpha) {
+        if (gpuLayout) k_wf_shadow<true, true><<<gShadow, kStreamThreads, 0, st>>>(v);
+        else k_wf_shadow<false, true><<<gShadow, kStreamThreads, 0, st>>>(v);
+      } else {
+        if (gpuLayout) k_wf_shadow<true, false><<<gShadow, kStreamThreads, 0, st>>>(v);
+        else k_wf_shadow<false, false><<<gShadow, kStreamThreads, 0, st>>>(v);
+      }
       k_wf_finish<<<gFinish, kStreamThreads, 0, st>>>(v, cur);
       e = cudaGetLastError();
       cur ^= 1u;

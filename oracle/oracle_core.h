@@ -99,8 +99,10 @@ V3 decodeMapColor(const Scene &s, i32 idx, V3 c);
 FirstHit querySceneSoftware(const Scene &s, const Ray &r, Traffic *tr);
 bool intersectScene(const Scene &s, const Ray &r, SurfaceInteraction &si, int bounces,
                     bool doubleSided, Traffic *tr);
+// With a sampler, scenes with alpha (MTC_SCENE_HAS_ALPHA) test each
+// candidate's coverage (intersectionAlphaPasses), drawing from it.
 bool intersectSceneShadow(const Scene &s, const Ray &r, float lightDistance, i32 tri, i32 ins,
-                          Traffic *tr);
+                          Traffic *tr, Sampler *smp = nullptr);
 
 // One path sample for pixel (x, y): rayTrace.compute.ts:1157-1263.
 void tracePixel(const Scene &s, u32 x, u32 y, V4 *outColor, V4 *outNormal, V4 *outAlbedo,

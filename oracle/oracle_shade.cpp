@@ -861,7 +861,7 @@ static Scattering sampleScattering(Ctx &c, SurfaceInteraction &si, const Materia
         if (valid) ucw = selected.lightSelectionPmf * scalarWeightSum / (float(count) * selectedTarget);
       }
       if (valid && !intersectSceneShadow(c.s, selected.ray, selected.maxDistance, selected.triangleIndex,
-                                         si.instanceIndex, c.tr))
+                                         si.instanceIndex, c.tr, &c.smp))
         path.li += selected.contribution * ucw;
       if (!isSurface) {
         result.direction = henyeyGreenstein(-path.ray.d, si.mediumAnisotropy, c.smp.s2(c.smp.bounceDim(6)));
@@ -1172,6 +1172,95 @@ static V4 integrateRgb(Ctx &c, V2 uv, const Ray &ray, Aux &aux) {
   return {path.li.x, path.li.y, path.li.z, path.alpha};
 }
 
+// rayTrace.compute.ts:815-890: the RGB integrator of scenes with alpha
+// (deterministicPrimaryAlpha).  A standard or unlit primary hit with coverage
+// below 1 splits the sample: the back path continues through the surface
+// first, then the front path restarts at the primary vertex with full
+// coverage, and the two are mixed by the coverage.
+static V4 integrateRgbAlpha(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
+  SurfaceInteraction si;
+  Material ma;
+  SurfaceInteraction primarySi;
+  Material primaryMa;
+  Aux primaryAux;
+  bool primaryReady = false, query = true, split = false, front = false;
+  float coverage = 1.0f;
+  V4 back{0, 0, 0, 0};
+  Aux backAux;
+  auto freshPath = [&]() {
+    Path p;
+    p.ray = ray;
+    p.alpha = c.s.u->transmissive_output_alpha_min < 1.0f ? 0.0f : 1.0f;
+    p.beta = v3(1.0f);
+    p.fromEye = true;
+    return p;
+  };
+  Path path = freshPath();
+  const int bounceLimit = std::max(c.s.u->bounces, 0);
+  const int eventLimit = std::min(bounceLimit * 3, 20);
+  int event = 0, depth = 0;
+  bool sampleIgnored = false, isNotTransparent = false;
+  for (int step = 0; step < (20 + 1) * 2 + 2; step++) {
+    if (query) {
+      intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
+      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv);
+      if (c.tr) c.tr->material_fetches++;
+    }
+    query = true;
+    if (!primaryReady) {
+      if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
+        outAux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+        outAux.normal = dot(si.normal, si.position - cameraEye(c.s)) > 0.0f ? -si.normal : si.normal;
+        si.albedoSampled = ma.transmissionWeight > 0.5f;
+      }
+      outAux.isShadowCatcher = false;
+      primarySi = si; primaryMa = ma; primaryAux = outAux;
+      primaryReady = true;
+      coverage = clampf(ma.alpha, 0.0f, 1.0f);
+      split = si.hit && (ma.materialType == 0 || ma.materialType == 2) && coverage < 1.0f;
+      if (split) {
+        path.ray.o = si.position + ray.d * (EPS * 0.02f);
+        si.albedoSampled = false;
+        continue;
+      }
+    } else if (event == 0 && !front && split) {
+      if (si.hit && ma.materialType == 0) {
+        outAux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
+        outAux.normal = dot(si.normal, si.position - cameraEye(c.s)) > 0.0f ? -si.normal : si.normal;
+        si.albedoSampled = ma.transmissionWeight > 0.5f;
+      }
+    }
+    if (event == 0) {
+      isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
+    } else {
+      completeVertex(c, path, depth, si, ma, sampleIgnored);
+    }
+    if (isNotTransparent && event > bounceLimit) path.abort = true;
+    if (!path.abort && event < eventLimit) shadeVertex(c, uv, path, depth, si, ma, outAux, sampleIgnored);
+    if (path.abort || event >= eventLimit) {
+      V4 result = {path.li.x, path.li.y, path.li.z, path.alpha};
+      if (!split || coverage <= 0.0f) return result;
+      if (front) {
+        auto mix3 = [&](V3 a, V3 b) { return a * (1.0f - coverage) + b * coverage; };
+        outAux.albedo = mix3(backAux.albedo, outAux.albedo);
+        V3 n = mix3(backAux.normal, outAux.normal);
+        outAux.normal = dot(n, n) > 1e-12f ? normalize(n) : v3(0.0f);
+        outAux.isBlank = backAux.isBlank && outAux.isBlank;
+        outAux.isShadowCatcher = backAux.isShadowCatcher && outAux.isShadowCatcher;
+        return {back.x * (1.0f - coverage) + result.x * coverage, back.y * (1.0f - coverage) + result.y * coverage,
+                back.z * (1.0f - coverage) + result.z * coverage, back.w * (1.0f - coverage) + result.w * coverage};
+      }
+      back = result; backAux = outAux;
+      front = true; query = false; event = 0; depth = 0; sampleIgnored = false;
+      si = primarySi; ma = primaryMa; ma.alpha = 1.0f; outAux = primaryAux;
+      path = freshPath();
+    } else {
+      event++;
+    }
+  }
+  return {0.0f, 0.0f, 0.0f, 0.0f};
+}
+
 // rayTrace.compute.ts:947-1057: the spectral integrator (independent
 // wavelength paths, shareSpectralPrefix off).  The primary hit is traced once
 // and reused by the three wavelength paths (or one hero wavelength when
@@ -1327,7 +1416,9 @@ void tracePixel(const Scene &s, u32 x, u32 y, V4 *outColor, V4 *outNormal, V4 *o
     cam = {origin, normalize(focus - origin)};
   }
   Aux aux;
-  V4 li = (s.flags & MTC_SCENE_SPECTRAL) ? integrateSpectral(c, coord, cam, aux) : integrateRgb(c, coord, cam, aux);
+  V4 li = (s.flags & MTC_SCENE_SPECTRAL) ? integrateSpectral(c, coord, cam, aux)
+          : (s.flags & MTC_SCENE_HAS_ALPHA) ? integrateRgbAlpha(c, coord, cam, aux)
+                                             : integrateRgb(c, coord, cam, aux);
   if (tr) tr->paths++;
   if (u.clamping > 0.0f) {
     float cl = u.clamping;

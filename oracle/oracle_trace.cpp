@@ -313,9 +313,31 @@ struct TraversalHit {
 
 enum class Mode { Closest, Shadow };
 
-// Returns true when a shadow query found an occluder.
+// intersectionAlphaPasses (intersectionAlpha.wgsl.ts:14-90): whether a
+// shadow candidate on a triangle of `materialIndex` (vertex indices `index`,
+// barycentrics `bary`) occludes.
+static bool intersectionAlphaPasses(const Scene &s, i32 materialIndex, const i32 index[3], V3 bary, Sampler &smp) {
+  const V4 *ma = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  float alpha = ma[9].x;
+  auto surfaceUv = [&]() {
+    V2 uv0 = vertexUv(s, index[0]), uv1 = vertexUv(s, index[1]), uv2 = vertexUv(s, index[2]);
+    V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
+    return V2{uv.x * ma[7].z, uv.y * ma[7].w};
+  };
+  if (ma[5].w == 2.0f && mapValid(s, ma[2].z)) alpha *= sampleMap(s, i32(ma[2].z), surfaceUv()).w;
+  if (mapValid(s, ma[22].z)) alpha *= sampleMap(s, i32(ma[22].z), surfaceUv()).y;
+  const i32 alphaMode = i32(ma[23].w);
+  if (alphaMode == 0) alpha = 1.0f;
+  else if (alphaMode == 1) alpha = alpha >= ma[22].w ? 1.0f : 0.0f;
+  if (alphaMode == 2) return smp.hashedSample(1u) <= alpha;
+  return alpha >= 1.0f;
+}
+
+// Returns true when a shadow query found an occluder.  `alphaSmp`: the
+// shadow hook's coverage test (intersect.wgsl.ts:846-866).
 static bool traverse(const Scene &s, const Ray &ray, int bounces, bool doubleSided, i32 currentTri,
-                     i32 currentIns, Mode mode, TraversalHit &h, Traffic *tr) {
+                     i32 currentIns, Mode mode, TraversalHit &h, Traffic *tr, Sampler *alphaSmp = nullptr) {
+  const float shadowRayTMax = h.tMax;
   i32 tlasStack[MTC_MAX_STACK];
   i32 blasStack[MTC_MAX_STACK];
   int tlasTop = -1;
@@ -432,7 +454,14 @@ static bool traverse(const Scene &s, const Ray &ray, int bounces, bool doubleSid
           h.isHit = true;
           h.hitPosition = o + d * h.tMax;
           h.hitBary = hit.bary;
-          if (mode == Mode::Shadow) return true;
+          if (mode == Mode::Shadow) {
+            const i32 index[3] = {i0, i1, i2};
+            if (alphaSmp && !intersectionAlphaPasses(s, sideMaterial, index, hit.bary, *alphaSmp)) {
+              h.tMax = shadowRayTMax;  // not occluded: never traverse beyond the light
+              continue;
+            }
+            return true;
+          }
           h.triangleIndex = triangleIndex;
           h.insIdx = insIdx;
           h.idx[0] = i0; h.idx[1] = i1; h.idx[2] = i2;
@@ -576,13 +605,14 @@ bool intersectScene(const Scene &s, const Ray &r, SurfaceInteraction &si, int bo
   return si.hit;
 }
 
-// intersect.wgsl.ts:829-879 intersectSceneShadow (no alpha)
-bool intersectSceneShadow(const Scene &s, const Ray &r, float lightDistance, i32 tri, i32 ins, Traffic *tr) {
+// intersect.wgsl.ts:829-879 intersectSceneShadow
+bool intersectSceneShadow(const Scene &s, const Ray &r, float lightDistance, i32 tri, i32 ins, Traffic *tr,
+                          Sampler *smp) {
   if (s.u->is_empty > 0) return false;
   if (tr) tr->shadow_rays++;
   TraversalHit h;
   h.tMax = fminf(fmaxf(lightDistance, 0.0f), RAY_MAX_DISTANCE);
-  return traverse(s, r, 1, true, tri, ins, Mode::Shadow, h, tr);
+  return traverse(s, r, 1, true, tri, ins, Mode::Shadow, h, tr, (s.flags & MTC_SCENE_HAS_ALPHA) ? smp : nullptr);
 }
 
 }  // namespace oracle

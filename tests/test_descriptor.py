@@ -357,7 +357,7 @@ def test_spot_and_triangle_material_rules():
 @pytest.mark.parametrize("name,build", [
     ("displacement map", lambda d: d.add_material(
         extensions=[(59, d.add_texture(1, 1, np.zeros((1, 1, 4), np.uint8)))])),
-    ("opacity", lambda d: d.add_material(opacity=0.5)),
+    ("alpha in a spectral scene", lambda d: d.add_mesh(0, d.add_material(opacity=0.5, extensions=[(15, (0.5,))]))),
     ("vertex colors", lambda d: d.add_geometry(QUAD, QUAD_IDX, colors=np.ones((4, 3), F))),
     ("extension", lambda d: d.add_material(extensions=[(53, (0.1,))])),
     ("unlit", lambda d: d.add_material(extensions=[(52, 1)])),

@@ -108,7 +108,7 @@ def test_rejected_descriptor_keeps_previous_scene(cuda):
             ctx.commit_descriptor(bytes(bad))
         assert e.value.status == abi.MT_ERROR_INVALID_ARGUMENT
         unsupported = room(32, 24)
-        unsupported.add_material(opacity=0.5)
+        unsupported.add_material(extensions=[(52, 1)])                  # unlit
         with pytest.raises(abi.MtError) as e:
             ctx.commit_descriptor(unsupported.to_bytes())
         assert e.value.status == abi.MT_ERROR_UNAVAILABLE

@@ -185,8 +185,8 @@ def test_texture_rejections_of_pixels_udim_and_references():
     rejected(d)
 
 
-@pytest.mark.parametrize("name", ["displacement", "anisotropy map", "coat normal", "alpha map", "udim", "uv1",
-                                  "alpha blend", "projection", "anisotropy"])
+@pytest.mark.parametrize("name", ["displacement", "anisotropy map", "coat normal", "udim", "uv1", "projection",
+                                  "anisotropy"])
 def test_unsupported_texture_features_are_named(name):
     px = np.zeros((10, 10, 4), np.uint8)
     d = base()
@@ -199,10 +199,6 @@ def test_unsupported_texture_features_are_named(name):
         ext = [(70, t)]
     elif name == "coat normal":
         ext = [(74, t)]
-    elif name == "alpha map":
-        ext = [(40, t)]
-    elif name == "alpha blend":
-        ext = [(54, 1)]
     elif name == "projection":
         ext = [(55, 1)]
     elif name == "anisotropy":
