@@ -89,7 +89,10 @@ bool fillJob(const mtc_job_desc &d, JobData &J) {
   const mtc_scene_view *v = &d.scene;
   if (v->struct_size != sizeof(mtc_scene_view) || !v->bvh || !v->instances || !v->attributes || !v->materials ||
       v->material_count == 0 || !v->energy_lut || !v->light_sampling || v->vertex_layout.stride < 4 ||
-      (v->vertex_layout.uv_offset && (v->vertex_layout.uv_offset < 3 || v->vertex_layout.uv_offset + 2 > v->vertex_layout.stride)))
+      (v->vertex_layout.uv_offset && (v->vertex_layout.uv_offset < 3 || v->vertex_layout.uv_offset + 2 > v->vertex_layout.stride)) ||
+      (v->vertex_layout.color_offset &&
+       (v->vertex_layout.color_offset < 3 ||
+        v->vertex_layout.color_offset + (v->vertex_layout.color_float ? 3u : 1u) > v->vertex_layout.stride)))
     return false;
   float w = d.uniform.output_size[0], h = d.uniform.output_size[1];
   if (!(w >= 1.0f && h >= 1.0f && w <= 65536.0f && h <= 65536.0f) || d.uniform.loop_unroll_guard != 4u) return false;
@@ -117,6 +120,8 @@ bool fillJob(const mtc_job_desc &d, JobData &J) {
   J.s.mapCount = v->maps && v->map_texels ? v->map_count : 0;
   J.s.mapTexelCount = v->map_texel_count;
   J.s.vuvOff = v->vertex_layout.uv_offset;
+  J.s.vcolorOff = v->vertex_layout.color_offset;
+  J.s.vcolorFloat = v->vertex_layout.color_float;
   J.u = d.uniform;
   J.cam = d.camera;
   J.outColor = (float4 *)d.out.color;

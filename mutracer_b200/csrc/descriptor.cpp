@@ -20,13 +20,12 @@
 //
 // Malformed descriptors are rejected with MT_ERROR_INVALID_ARGUMENT and a
 // message naming the problem, as the reference's validator does.  Valid
-// descriptors that use what this build does not render (texture slots other
-// than base color, normal and metallic-roughness, UDIM sets, second UV sets,
-// textures the atlas would downscale, material graphs, IES profiles,
-// rect-light textures, background maps, vertex colors, meshes whose
-// triangles use several materials, partial opacity and base-color alpha
-// blending, UV projections, bevel, shadow catchers, unlit materials, most
-// material extensions beyond OpenPBR scalars and colors) are refused with
+// descriptors that use what this build does not render (displacement,
+// anisotropy and coat-normal maps, UDIM sets, second UV sets, textures the
+// atlas would downscale, UV projections, alpha in spectral scenes, material
+// graphs, IES profiles, rect-light textures, background maps, meshes whose
+// triangles use several materials, bevel, shadow catchers, unlit materials,
+// the remaining material extensions) are refused with
 // MT_ERROR_UNAVAILABLE and a message naming the feature.
 //
 // Material textures (scene-records.ts:22-39 decodeTexture, MaterialData.ts
@@ -831,7 +830,7 @@ void decodeScene(const Words &d, SceneHost &s) {
       tangentFrames = true;  // decodeGeometry generates tangents from UVs
     }
     geometryHasUv1 |= d.array("uv1s", u[o + 6], uint64_t(vc) * 2);
-    if (d.array("vertex colors", u[o + 7], uint64_t(vc) * 3)) unsupported("vertex colors");
+    if (d.array("vertex colors", u[o + 7], uint64_t(vc) * 3)) md.colors.assign(d.f + u[o + 7], d.f + u[o + 7] + size_t(vc) * 3);
     tangentFrames |= d.array("tangents", u[o + 8], uint64_t(vc) * 4);
     if (d.array("material indices", u[o + 9], vc)) {
       vertexMaterial[g].assign(u + u[o + 9], u + u[o + 9] + vc);

@@ -559,7 +559,7 @@ MTD void sampleLightChoiceTable(const JobData &J, V3 p, V3 rnd, LightSample &ls)
 
 // --------------------------------------------------------------- material
 // materialBuffer.wgsl.ts:170-257 getMaterial with its texture block
-MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 uv, Material &m) {
+MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 uv, V3 vertexColor, Material &m) {
   // A miss keeps the previous hit's indices (zero before the first hit);
   // clamp so an empty or single-material scene never reads past its buffers.
   if (materialIndex < 0 || uint32_t(materialIndex) >= J.s.matCount) materialIndex = 0;
@@ -637,6 +637,7 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 
   }
   V3 color = v3(1.0f);
   if (instanceIndex >= 0) color = xyz(ld4(J.s.ins + size_t(instanceIndex) * MTC_INSTANCE_VEC4_STRIDE + 9));
+  color = mulv(color, vertexColor);  // getInstanceColor(instanceIndex) * vertexColor
   m.baseColor *= color;
   if (m.materialType == 2) m.emission *= color;
   m.specularRoughness = clampf(m.specularRoughness, ROUGHNESS_MIN, 1.0f);
@@ -653,6 +654,7 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 
 struct SurfaceInteraction {
   V3 position; bool albedoSampled;
   V2 uv;  // primary UV times the material's uvScale (0 without UVs)
+  V3 vertexColor;  // interpolated vertex color (white without colors)
   V3 normal, vertexNormal, shadowOffset, faceNormal; bool hit;
   int32_t triangleIndex, instanceIndex, materialIndex;
   float wavelength; int32_t spectralChannel;
@@ -741,6 +743,18 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
       return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
     };
     uv0 = vuv(i0); uv1 = vuv(i1); uv2 = vuv(i2);
+  }
+  si.vertexColor = v3(1.0f);
+  if (s.vcolorOff) {
+    // vertexColor (vertexAttributes.wgsl.ts:38-43): f32x3, or unpack4x8unorm
+    auto vcol = [&](int32_t i) {
+      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vcolorOff;
+      if (s.vcolorFloat) return V3{asf(__ldg(w)), asf(__ldg(w + 1)), asf(__ldg(w + 2))};
+      const uint32_t c = __ldg(w);
+      return V3{float(c & 255u) / 255.0f, float((c >> 8) & 255u) / 255.0f, float((c >> 16) & 255u) / 255.0f};
+    };
+    const V3 c0 = vcol(i0), c1 = vcol(i1), c2 = vcol(i2);
+    si.vertexColor = c0 * bary.x + c1 * bary.y + c2 * bary.z;
   }
   const float4 *md = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   const float4 r7 = ld4(md + 7);
@@ -1304,6 +1318,7 @@ static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, 
   si.mediumScattering = v3(0.0f); si.mediumAnisotropy = 0.0f;
   si.position = v3(0.0f); si.normal = v3(0.0f); si.vertexNormal = v3(0.0f); si.shadowOffset = v3(0.0f);
   si.uv = v2(0.0f, 0.0f);
+  si.vertexColor = v3(1.0f);
   si.faceNormal = v3(0.0f);
   Path &path = ps.path;
   path.scatteringMediumEntered = false;
@@ -1380,7 +1395,7 @@ static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const Trav
     completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
   }
   Material ma;
-  getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
+  getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
   if (event == 0) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
       ps.aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
@@ -1416,7 +1431,7 @@ static __device__ __noinline__ bool shadeStepAlpha(Ctx &c, PathSample &ps, Spect
   if (sp.frontPending) {
     sp.frontPending = false;
     si = sp.primarySi;
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
     ma.alpha = 1.0f;
   } else {
     si.hit = false;
@@ -1424,7 +1439,7 @@ static __device__ __noinline__ bool shadeStepAlpha(Ctx &c, PathSample &ps, Spect
       si.triangleIndex = h.triangleIndex;
       completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
     }
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
   }
   if (!sp.primaryReady) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
@@ -1524,10 +1539,10 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
       si.triangleIndex = h.triangleIndex;
       completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
     }
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
   } else {
     // The primary material is a pure function of the primary vertex.
-    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, sp.primarySi.uv, ma);
+    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, sp.primarySi.uv, sp.primarySi.vertexColor, ma);
   }
   if (event == 0) {
     if (!sp.primaryReady) {

@@ -25,6 +25,7 @@ struct DevScene {
   const float4 *mapTexels;  // RGBA per texel
   uint32_t mapCount, mapTexelCount;
   uint32_t vuvOff;          // word offset of the f32 UV pair (0: no UVs)
+  uint32_t vcolorOff, vcolorFloat;  // vertex color word(s) (0: white), f32x3 or RGBA8
 };
 
 // One render job: scene, uniforms, outputs (the plain kernel takes one as a

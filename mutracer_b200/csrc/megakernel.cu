@@ -273,7 +273,10 @@ bool validScene(const mtc_scene_view *s) {
          s->vertex_layout.stride >= 4 && s->vertex_layout.normal_offset + (s->vertex_layout.normal_float ? 3u : 1u) <=
                                              s->vertex_layout.stride &&
          (s->vertex_layout.uv_offset == 0 || (s->vertex_layout.uv_offset >= 3 &&
-                                              s->vertex_layout.uv_offset + 2 <= s->vertex_layout.stride));
+                                              s->vertex_layout.uv_offset + 2 <= s->vertex_layout.stride)) &&
+         (s->vertex_layout.color_offset == 0 ||
+          (s->vertex_layout.color_offset >= 3 &&
+           s->vertex_layout.color_offset + (s->vertex_layout.color_float ? 3u : 1u) <= s->vertex_layout.stride));
 }
 
 DevScene toDev(const mtc_scene_view *v) {
@@ -300,6 +303,8 @@ DevScene toDev(const mtc_scene_view *v) {
   s.mapCount = v->maps && v->map_texels ? v->map_count : 0;
   s.mapTexelCount = v->map_texel_count;
   s.vuvOff = v->vertex_layout.uv_offset;
+  s.vcolorOff = v->vertex_layout.color_offset;
+  s.vcolorFloat = v->vertex_layout.color_float;
   return s;
 }
 

@@ -970,12 +970,21 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   s.tlasStack = std::min(64u, std::max(1u, tlas.maxDepth));
   s.blasStack = std::min(64u, blasDepth);
   // Compact vertices (compactVertices.ts:7-27, 67-90): position f32x3 + oct
-  // normal (or f32x3 normal), then an f32 UV pair when any mesh has UVs.
-  bool hasUv = false;
-  for (const MeshData &md : meshes) hasUv |= !md.uvs.empty();
+  // normal (or f32x3 normal), then an f32 UV pair when any mesh has UVs, then
+  // the vertex color when any mesh has colors: RGBA8 in one word, or f32x3
+  // when some component lies outside [0, 1].
+  bool hasUv = false, hasColor = false, colorFloat = false;
+  for (const MeshData &md : meshes) {
+    hasUv |= !md.uvs.empty();
+    hasColor |= !md.colors.empty();
+    for (float c : md.colors)
+      if (!(c >= 0.0f && c <= 1.0f)) colorFloat = true;
+  }
   const uint32_t uvOffset = hasUv ? (normalFloat ? 6u : 4u) : 0u;
   uint32_t stride = (normalFloat ? 6 : 4) + (hasUv ? 2 : 0);
-  s.layout = {stride, 3, normalFloat ? 1u : 0u, uvOffset};
+  const uint32_t colorOffset = hasColor ? stride : 0u;
+  if (hasColor) stride += colorFloat ? 3 : 1;
+  s.layout = {stride, 3, normalFloat ? 1u : 0u, uvOffset, colorOffset, colorFloat ? 1u : 0u};
   s.attributes.assign(size_t(vertexOffset) * stride, 0);
   for (size_t m = 0; m < meshes.size(); m++) {
     const MeshData &md = meshes[m];
@@ -986,6 +995,19 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
       if (normalFloat) std::memcpy(w + 3, &md.normals[size_t(v) * 3], 12);
       else w[3] = octEncode(md.normals[v * 3], md.normals[v * 3 + 1], md.normals[v * 3 + 2]);
       if (uvOffset && !md.uvs.empty()) std::memcpy(w + uvOffset, &md.uvs[size_t(v) * 2], 8);
+      if (colorOffset) {
+        const float *c = md.colors.empty() ? nullptr : &md.colors[size_t(v) * 3];
+        const float r = c ? c[0] : 1.0f, g = c ? c[1] : 1.0f, b = c ? c[2] : 1.0f;
+        if (colorFloat) {
+          std::memcpy(w + colorOffset, &r, 4);
+          std::memcpy(w + colorOffset + 1, &g, 4);
+          std::memcpy(w + colorOffset + 2, &b, 4);
+        } else {
+          // Math.round(x * 255) (round half up) packed R | G << 8 | B << 16 | 0xff << 24
+          auto q = [](float x) { return uint32_t(std::floor(double(x) * 255.0 + 0.5)); };
+          w[colorOffset] = q(r) | q(g) << 8 | q(b) << 16 | 0xff000000u;
+        }
+      }
     }
   }
   // Materials.

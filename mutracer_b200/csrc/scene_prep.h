@@ -208,6 +208,7 @@ struct MeshData {
   std::vector<float> positions, normals;
   std::vector<uint32_t> indices;
   std::vector<float> uvs;  // 2 per vertex, or empty (zero UVs when another mesh has some)
+  std::vector<float> colors;  // 3 per vertex, or empty (white when another mesh has some)
 };
 void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std::vector<Instance> &instances,
                    const std::vector<MaterialDesc> &materials, const std::vector<LightDesc> &lights, int blasBins,

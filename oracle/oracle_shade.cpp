@@ -573,7 +573,7 @@ static void sampleLightChoiceTable(const Scene &s, V3 p, V3 rnd, LightSample &ls
 // --------------------------------------------------------------- material
 // materialBuffer.wgsl.ts:170-257 getMaterial with its texture block
 // (:79-139 and the slots of materialTextureSlots.ts)
-Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv) {
+Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv, V3 vertexColor) {
   const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   Material m;
   m.baseColor = xyz(d[0]);
@@ -694,6 +694,7 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   }
   V3 color = v3(1.0f);
   if (instanceIndex >= 0) color = xyz(s.ins[size_t(instanceIndex) * MTC_INSTANCE_VEC4_STRIDE + 9]);
+  color = color * vertexColor;  // getInstanceColor(instanceIndex) * vertexColor
   m.baseColor *= color;
   if (m.materialType == 2) m.emission *= color;
   m.specularRoughness = clampf(m.specularRoughness, ROUGHNESS_MIN, 1.0f);
@@ -1151,7 +1152,7 @@ static V4 integrateRgb(Ctx &c, V2 uv, const Ray &ray, Aux &aux) {
   bool sampleIgnored = false;
   for (int event = 0; event <= eventLimit; event++) {
     intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-    ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv);
+    ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor);
     if (c.tr) c.tr->material_fetches++;
     if (event == 0) {
       if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
@@ -1203,7 +1204,7 @@ static V4 integrateRgbAlpha(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
   for (int step = 0; step < (20 + 1) * 2 + 2; step++) {
     if (query) {
       intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv);
+      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor);
       if (c.tr) c.tr->material_fetches++;
     }
     query = true;
@@ -1293,7 +1294,7 @@ static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
   for (int step = 0; step < stepLimit; step++) {
     if (!primaryReady || (event != 0 && !path.abort)) {
       intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv);
+      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor);
       if (c.tr) c.tr->material_fetches++;
     }
     if (event == 0) {
@@ -1506,7 +1507,7 @@ int oracle_bsdf(const float *rows, uint32_t features, const float *view, const f
   s.mats = (const om::V4 *)rows;
   s.ins = (const om::V4 *)ins;
   s.u = &u;
-  oracle::Material m = oracle::getMaterial(s, 0, 0, {0.0f, 0.0f});
+  oracle::Material m = oracle::getMaterial(s, 0, 0, {0.0f, 0.0f}, om::v3(1.0f));
   om::V3 v = om::normalize({view[0], view[1], view[2]});
   om::V3 n = {0.0f, 0.0f, 1.0f};
   float ndv = om::dot(v, n);

@@ -268,6 +268,15 @@ static V3 getMatNormal(const Scene &s, i32 materialIndex, V2 uv, V3 normal, V3 d
   return normalize(dpdu * n.x + dpdv * n.y + normal * n.z);
 }
 
+// vertexColor (vertexAttributes.wgsl.ts:38-43): f32x3, or unpack4x8unorm of
+// one RGBA8 word; white without color words.
+static inline V3 vertexColor(const Scene &s, i32 i) {
+  if (!s.vl.color_offset) return v3(1.0f);
+  const u32 *w = s.attr + size_t(i) * s.vl.stride + s.vl.color_offset;
+  if (s.vl.color_float) return {asf(w[0]), asf(w[1]), asf(w[2])};
+  return {float(w[0] & 255u) / 255.0f, float((w[0] >> 8) & 255u) / 255.0f, float((w[0] >> 16) & 255u) / 255.0f};
+}
+
 static inline V2 vertexUv(const Scene &s, i32 i) {
   if (!s.vl.uv_offset) return {0, 0};
   const u32 *w = s.attr + size_t(i) * s.vl.stride + s.vl.uv_offset;
@@ -525,8 +534,11 @@ static void completeSurfaceInteraction(const Scene &s, SurfaceInteraction &si, c
   const V4 *insv = s.ins + size_t(h.insIdx) * MTC_INSTANCE_VEC4_STRIDE;
   si.materialIndex = unpackMaterialIndex(asi(insv[0].z));
   si.hit = true;
-  si.vertexColor = v3(1.0f);
   V3 bary = h.hitBary;
+  si.vertexColor = v3(1.0f);
+  if (s.vl.color_offset)
+    si.vertexColor = vertexColor(s, h.idx[0]) * bary.x + vertexColor(s, h.idx[1]) * bary.y +
+                     vertexColor(s, h.idx[2]) * bary.z;
   V3 n0 = vertexNormal(s, h.idx[0]), n1 = vertexNormal(s, h.idx[1]), n2 = vertexNormal(s, h.idx[2]);
   V3 normal = normalize(n0 * bary.x + n1 * bary.y + n2 * bary.z);
   const V2 uv0 = vertexUv(s, h.idx[0]), uv1 = vertexUv(s, h.idx[1]), uv2 = vertexUv(s, h.idx[2]);

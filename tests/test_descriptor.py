@@ -358,7 +358,7 @@ def test_spot_and_triangle_material_rules():
     ("displacement map", lambda d: d.add_material(
         extensions=[(59, d.add_texture(1, 1, np.zeros((1, 1, 4), np.uint8)))])),
     ("alpha in a spectral scene", lambda d: d.add_mesh(0, d.add_material(opacity=0.5, extensions=[(15, (0.5,))]))),
-    ("vertex colors", lambda d: d.add_geometry(QUAD, QUAD_IDX, colors=np.ones((4, 3), F))),
+
     ("extension", lambda d: d.add_material(extensions=[(53, (0.1,))])),
     ("unlit", lambda d: d.add_material(extensions=[(52, 1)])),
     ("bevel", lambda d: setattr(d, "quality", D.QUALITY_BEVEL)),
@@ -422,3 +422,27 @@ def test_emissive_meshes_enter_the_light_table():
     assert all(abs(p - area * lum / total) < 1e-6 for p in pmfs)
     mat_rows = h.materials.reshape(-1, 26, 4)
     assert np.allclose(mat_rows[lamp, 3, :3], emission.astype(F))
+
+
+def test_vertex_colors_pack_like_compact_vertices():
+    """compactVertices.ts:7-27, 79-88: RGBA8 words (Math.round(c * 255),
+    alpha 255) when every component lies in [0, 1], f32x3 otherwise; meshes
+    without colors are white."""
+    d = base()
+    cols = np.array([[0.0, 0.5, 1.0], [0.2, 0.4, 0.6], [1.0, 1.0, 1.0], [0.1, 0.9, 0.33]], F)
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, colors=cols), 0, transform=D.translate([0, 1, 0]))
+    h = decoded(d)
+    lay = h.bundle.vertex_layout
+    assert (lay.stride, lay.color_offset, lay.color_float) == (5, 4, 0)
+    words = h.attributes.reshape(-1, 5)
+    want = [int(np.floor(np.float64(r) * 255 + 0.5)) | int(np.floor(np.float64(g) * 255 + 0.5)) << 8 |
+            int(np.floor(np.float64(b) * 255 + 0.5)) << 16 | 0xff000000 for r, g, b in cols]
+    assert words[4:, 4].tolist() == want
+    assert (words[:4, 4] == 0xffffffff).all()                      # the base quad: white
+    d = base()
+    d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, colors=cols * F(2)), 0)
+    h = decoded(d)
+    lay = h.bundle.vertex_layout
+    assert (lay.stride, lay.color_offset, lay.color_float) == (7, 4, 1)
+    words = h.attributes.reshape(-1, 7)
+    assert np.array_equal(words[4:, 4:7].view(F), cols * F(2)) and np.array_equal(words[:4, 4:7].view(F), np.ones((4, 3), F))
