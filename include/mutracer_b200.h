@@ -178,6 +178,11 @@ typedef struct mtc_scene_view {
   const void *map_texels;
   uint32_t map_count;
   uint32_t map_texel_count;        /* texels in map_texels (a map reaching past it samples zero) */
+  /* Triangle material plane (triangleMaterial, vertexAttributes.wgsl.ts:51-56;
+   * packTriangleMaterials, compactVertices.ts:93-102): one u32 per bvh vec4,
+   * material index + 1 of the triangle whose record sits at that vec4, 0 for
+   * the instance's material.  NULL: every triangle uses its instance's. */
+  const uint32_t *triangle_materials;
 } mtc_scene_view;
 /* One material map, 3 vec4 (f32 words; integers as their bit patterns):
  *   [0] width (u32), height (u32), first texel (u32), 0
@@ -504,6 +509,7 @@ typedef struct mt_scene_bundle {
   mtc_trace_uniform uniform;       /* settings fields are overwritten by mt_render_settings */
   const float *maps; uint32_t map_count;       /* MTC_MAP_VEC4_ROWS vec4 per map */
   const float *map_texels; uint64_t map_texel_count;
+  const uint32_t *triangle_materials;  /* bvh_vec4_count words or NULL (mtc_scene_view) */
 } mt_scene_bundle;
 
 /* mutracer-context.h:86-100 */

@@ -90,6 +90,7 @@ class SceneView(C.Structure):
         ("blas_offset", C.c_int32), ("energy_lut", C.c_void_p), ("analytic_lights", C.c_void_p),
         ("tlas_stack_size", C.c_uint32), ("blas_stack_size", C.c_uint32),
         ("maps", C.c_void_p), ("map_texels", C.c_void_p), ("map_count", C.c_uint32), ("map_texel_count", C.c_uint32),
+        ("triangle_materials", C.c_void_p),
     ]
 
 
@@ -175,6 +176,7 @@ class SceneBundle(C.Structure):
         ("camera", CameraUniform), ("uniform", TraceUniform),
         ("maps", C.POINTER(C.c_float)), ("map_count", C.c_uint32),
         ("map_texels", C.POINTER(C.c_float)), ("map_texel_count", C.c_uint64),
+        ("triangle_materials", C.POINTER(C.c_uint32)),
     ]
 
 

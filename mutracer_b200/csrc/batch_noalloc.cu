@@ -121,6 +121,7 @@ bool fillJob(const mtc_job_desc &d, JobData &J) {
   J.s.mapTexelCount = v->map_texel_count;
   J.s.vuvOff = v->vertex_layout.uv_offset;
   J.s.vcolorOff = v->vertex_layout.color_offset;
+  J.s.triMats = v->triangle_materials;
   J.s.vcolorFloat = v->vertex_layout.color_float;
   J.u = d.uniform;
   J.cam = d.camera;

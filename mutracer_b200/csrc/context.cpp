@@ -60,7 +60,7 @@ struct DeviceBuffer {
 };
 
 struct SceneResources {
-  DeviceBuffer bvh, ins, attr, mats, env, envDist, lightData, lut, lights, maps, mapTexels;
+  DeviceBuffer bvh, ins, attr, mats, env, envDist, lightData, lut, lights, maps, mapTexels, triMats;
   DeviceBuffer color, normal, albedo, catcher;
   DeviceBuffer average, flag;  // read_pixels staging: averaged image, non-finite flag
   DeviceBuffer stream;         // wavefront state of blocking renders (mtc_stream_run)
@@ -275,6 +275,7 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   up(r->lights, b->analytic_lights, b->lights_count ? size_t(b->lights_count) * MTC_LIGHT_VEC4_ROWS * 16 : 0);
   up(r->maps, b->maps, size_t(b->map_count) * MTC_MAP_VEC4_ROWS * 16);
   up(r->mapTexels, b->map_texels, size_t(b->map_texel_count) * 16);
+  up(r->triMats, b->triangle_materials, b->triangle_materials ? size_t(b->bvh_vec4_count) * 4 : 0);
   for (DeviceBuffer *d : {&r->color, &r->normal, &r->albedo, &r->catcher}) {
     size_t bytes = px * 16 * (d == &r->catcher ? 3 : 1);
     if (e == cudaSuccess) e = d->reserve(bytes);
@@ -307,6 +308,7 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   v.maps = b->map_count ? r->maps.data() : nullptr; v.map_count = b->map_count;
   v.map_texels = b->map_texel_count ? r->mapTexels.data() : nullptr;
   v.map_texel_count = uint32_t(b->map_texel_count);
+  v.triangle_materials = b->triangle_materials ? static_cast<const uint32_t *>(r->triMats.data()) : nullptr;
   r->width = b->width; r->height = b->height;
   // Publish: accumulation restarts.
   c->scene = std::move(r);

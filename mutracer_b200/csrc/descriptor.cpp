@@ -662,8 +662,16 @@ void packMaterialMaps(const Words &d, const std::vector<TextureRecord> &records,
   }
 }
 
-void collectEmissive(const MeshData &md, const double *m, uint32_t material, double luminanceValue, SceneHost &s) {
+// collectEmissiveTriangles (lightSampling.ts:240-320) for one instance:
+// each triangle with an emitting material (its per-vertex material, else the
+// instance's) in world space.
+void collectEmissive(const MeshData &md, const double *m, uint32_t instanceMaterial,
+                     const std::vector<double> &samplingLuminance, SceneHost &s) {
   for (size_t t = 0; t + 2 < md.indices.size(); t += 3) {
+    const uint32_t material =
+        md.vertexMaterials.empty() ? instanceMaterial : uint32_t(md.vertexMaterials[md.indices[t]]);
+    const double luminanceValue = samplingLuminance[material];
+    if (!(luminanceValue > 1e-8)) continue;
     EmissiveTriangle tri;
     for (int c = 0; c < 3; c++) {
       const float *p = &md.positions[size_t(md.indices[t + c]) * 3];
@@ -842,6 +850,8 @@ void decodeScene(const Words &d, SceneHost &s) {
   }
   // Meshes and batches -> instances.
   std::vector<Instance> instances;
+  std::vector<MeshData> blasMeshes = meshData;  // one BLAS per geometry, plus per-table variants
+  std::map<std::pair<uint32_t, std::vector<int32_t>>, uint32_t> blasOf;
   for (uint32_t i = 0; i < meshes; i++) {
     const uint32_t o = u[10] + i * kMeshWords;
     const uint32_t g = u[o], flags = u[o + 20];
@@ -849,43 +859,67 @@ void decodeScene(const Words &d, SceneHost &s) {
     if (flags & ~1u) reject(at("mesh", i) + ": only flag bit 0 (hidden) is defined");
     double world[16];
     d.matrix(o + 4, "mesh", world);
-    // decodeMeshMaterials: the table, else material_index.
+    // decodeMeshMaterials: the table, else material_index.  The instance
+    // record carries the first (materialsIndices[0], bvhAccel.ts:344);
+    // per-vertex material indices select table entries per triangle through
+    // the triangle material plane.  A geometry used with different tables
+    // gets one BLAS per table (scenePreparation.ts:246-255).
     const uint32_t tableCount = u[o + 3];
-    uint32_t material;
+    std::vector<uint32_t> table;
     if (tableCount) {
       if (!d.array("material table", u[o + 2], tableCount)) reject(at("mesh", i) + ": material table missing");
-      std::vector<uint32_t> used;
-      const std::vector<uint32_t> &vm = vertexMaterial[g];
-      const std::vector<uint32_t> &idx = meshData[g].indices;
-      if (vm.empty()) used.push_back(0);
-      else
-        for (size_t t = 0; t < idx.size(); t += 3) used.push_back(vm[idx[t]]);
-      uint32_t first = used.empty() ? 0 : used[0];
-      for (uint32_t k : used) {
-        if (k >= tableCount) reject(at("mesh", i) + ": per-vertex material index past its material table");
-        if (k != first) unsupported("meshes whose triangles use several materials");
-      }
-      material = u[u[o + 2] + first];
-      for (uint32_t k = 0; k < tableCount; k++)
-        if (u[u[o + 2] + k] >= materials) reject(at("mesh", i) + ": material table entry out of range");
+      table.assign(u + u[o + 2], u + u[o + 2] + tableCount);
+      for (uint32_t k : table)
+        if (k >= materials) reject(at("mesh", i) + ": material table entry out of range");
     } else {
-      material = u[o + 1];
+      table.push_back(u[o + 1]);
+      if (table[0] >= materials) reject(at("mesh", i) + ": material index out of range");
     }
-    if (material >= materials) reject(at("mesh", i) + ": material index out of range");
+    const uint32_t material = table[0];
+    uint32_t blas = g;
+    std::vector<uint32_t> usedMaterials;
+    const std::vector<uint32_t> &vm = vertexMaterial[g];
+    if (vm.empty()) {
+      usedMaterials.push_back(material);
+    } else {
+      // localMaterialIndex (materialIndices.ts:5-15): an index past the
+      // mesh's materials falls back to its first (a table rejects it above).
+      std::vector<int32_t> global(vm.size());
+      for (size_t v = 0; v < vm.size(); v++) {
+        if (tableCount && vm[v] >= tableCount)
+          reject(at("mesh", i) + ": per-vertex material index past its material table");
+        global[v] = int32_t(table[vm[v] < table.size() ? vm[v] : 0]);
+      }
+      for (size_t t = 0; t < meshData[g].indices.size(); t += 3)
+        usedMaterials.push_back(uint32_t(global[meshData[g].indices[t]]));
+      auto key = std::make_pair(g, global);
+      auto found = blasOf.find(key);
+      if (found != blasOf.end()) {
+        blas = found->second;
+      } else {
+        if (!blasMeshes[g].vertexMaterials.empty()) {  // another table: its own BLAS
+          blas = uint32_t(blasMeshes.size());
+          blasMeshes.push_back(meshData[g]);
+        }
+        blasMeshes[blas].vertexMaterials = global;
+        blasOf.emplace(std::move(key), blas);
+      }
+    }
     if (flags & 1) continue;                        // hidden mesh or batch
     // Vertex tangents orient anisotropic lobes (openpbr_make_basis); this
     // build shades them in the normal's own frame.
-    if (tangentFrames && mats[material].specularAnisotropy > 0)
-      unsupported("anisotropic materials in a scene with vertex tangents or UVs");
+    for (uint32_t um : usedMaterials)
+      if (tangentFrames && mats[um].specularAnisotropy > 0)
+        unsupported("anisotropic materials in a scene with vertex tangents or UVs");
     if (meshData[g].indices.empty()) continue;      // nothing to intersect
     auto push = [&](const double *m, const float *color) {
       Instance ins;
-      ins.blasIndex = g;
+      ins.blasIndex = blas;
       std::memcpy(ins.transform, m, sizeof(ins.transform));
       ins.material = int32_t(255 + (material << 8));
       if (color) setColor(ins.color, color);
       instances.push_back(ins);
-      if (samplingLuminance[material] > 1e-8) collectEmissive(meshData[g], m, material, samplingLuminance[material], s);
+      collectEmissive(blasMeshes[blas], m, material, samplingLuminance, s);
     };
     if (!u[23]) {
       push(world, nullptr);
@@ -930,14 +964,14 @@ void decodeScene(const Words &d, SceneHost &s) {
       mats[i].maps[slot] = index;
     }
   if (mapTextures.empty()) {
-    for (MeshData &md : meshData) md.uvs.clear();  // nothing samples them
+    for (MeshData &md : blasMeshes) md.uvs.clear();  // nothing samples them
   } else {
     packMaterialMaps(d, textureRecords, mapTextures, geometryHasUv1, s);
   }
   // Lights.
   std::vector<LightDesc> lightList;
   for (uint32_t i = 0; i < lights; i++) lightList.push_back(decodeLight(d, u[12] + i * lightWords, version, i));
-  assembleScene(s, meshData, instances, mats, lightList, 8, 8, false);
+  assembleScene(s, blasMeshes, instances, mats, lightList, 8, 8, false);
   if ((s.flags & MTC_SCENE_SPECTRAL) && (s.flags & MTC_SCENE_HAS_ALPHA))
     unsupported("alpha coverage in a dispersive (spectral) scene");
   decodeCamera(d, u[14], width, height, s.camera);

@@ -756,8 +756,14 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
     const V3 c0 = vcol(i0), c1 = vcol(i1), c2 = vcol(i2);
     si.vertexColor = c0 * bary.x + c1 * bary.y + c2 * bary.z;
   }
+  // fetchAttributes reads uvScale from the instance's material, then
+  // resolves the triangle's own (resolveSurfaceMaterialIndex).
+  const float4 r7 = ld4(s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS + 7);
+  if (s.triMats) {
+    const uint32_t tm = __ldg(s.triMats + h.triangleIndex);
+    if (tm && tm - 1u < s.matCount) si.materialIndex = int32_t(tm - 1u);
+  }
   const float4 *md = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
-  const float4 r7 = ld4(md + 7);
   si.uv = {(bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x) * r7.z,
            (bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y) * r7.w};
   V3 mapped = normal;

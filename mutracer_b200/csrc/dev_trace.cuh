@@ -26,6 +26,7 @@ struct DevScene {
   uint32_t mapCount, mapTexelCount;
   uint32_t vuvOff;          // word offset of the f32 UV pair (0: no UVs)
   uint32_t vcolorOff, vcolorFloat;  // vertex color word(s) (0: white), f32x3 or RGBA8
+  const uint32_t *triMats;  // material + 1 per bvh vec4 (null: instance materials only)
 };
 
 // One render job: scene, uniforms, outputs (the plain kernel takes one as a
@@ -280,8 +281,12 @@ MTD bool mapValid(const DevScene &s, float index) { return index >= 0.0f && inde
 // material's alpha times the base color's alpha (map alpha usage "alpha") and
 // the alpha map's g at the hit's UV, then resolved by the alpha mode: opaque
 // occludes, mask compares with the cutoff, blend draws hashedSample(1).
-static __device__ __noinline__ bool alphaPasses(const DevScene &s, int32_t material, int32_t i0, int32_t i1,
-                                                int32_t i2, V3 bary, Sampler &smp) {
+static __device__ __noinline__ bool alphaPasses(const DevScene &s, int32_t material, int32_t record, int32_t i0,
+                                                int32_t i1, int32_t i2, V3 bary, Sampler &smp) {
+  if (s.triMats) {  // triangleMaterial (vertexAttributes.wgsl.ts:51-56)
+    const uint32_t m = __ldg(s.triMats + record);
+    if (m && m - 1u < s.matCount) material = int32_t(m - 1u);
+  }
   const float4 *d = s.mats + size_t(material) * MTC_MATERIAL_VEC4_ROWS;
   const float4 r2 = ld4(d + 2), r5 = ld4(d + 5), r22 = ld4(d + 22);
   float alpha = ld4(d + 9).x;
@@ -437,8 +442,8 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
           h.tMax = t;
           h.hitBary = bary;
           if (shadow) {
-            if (kAlpha && !alphaPasses(s, sideMaterial, asi(r3.x) + vertexOffset, asi(r3.y) + vertexOffset,
-                                       asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
+            if (kAlpha && !alphaPasses(s, sideMaterial, triangleIndex, asi(r3.x) + vertexOffset,
+                                       asi(r3.y) + vertexOffset, asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
               h.tMax = tMaxInit;
               continue;
             }
@@ -619,8 +624,8 @@ struct RayTraversal {
       h.hitBary = bary;
       if (shadow) {
         if (kAlpha && alphaSmp &&
-            !alphaPasses(*alphaScene, sideMaterial, asi(r3.x) + vertexOffset, asi(r3.y) + vertexOffset,
-                         asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
+            !alphaPasses(*alphaScene, sideMaterial, triangleIndex, asi(r3.x) + vertexOffset,
+                         asi(r3.y) + vertexOffset, asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
           h.tMax = tMaxInit;
           continue;
         }

@@ -90,6 +90,7 @@ int mtp_scene_bundle(void *scene, mt_scene_bundle *b) {
   b->map_count = uint32_t(s.maps.size() / (MTC_MAP_VEC4_ROWS * 4));
   b->map_texels = s.mapTexels.empty() ? nullptr : s.mapTexels.data();
   b->map_texel_count = s.mapTexels.size() / 4;
+  b->triangle_materials = s.triangleMaterials.empty() ? nullptr : s.triangleMaterials.data();
   return MT_OK;
 }
 

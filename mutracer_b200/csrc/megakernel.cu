@@ -304,6 +304,7 @@ DevScene toDev(const mtc_scene_view *v) {
   s.mapTexelCount = v->map_texel_count;
   s.vuvOff = v->vertex_layout.uv_offset;
   s.vcolorOff = v->vertex_layout.color_offset;
+  s.triMats = v->triangle_materials;
   s.vcolorFloat = v->vertex_layout.color_float;
   return s;
 }

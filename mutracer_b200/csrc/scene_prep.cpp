@@ -391,8 +391,28 @@ void setBlasLayout(SceneHost &s, uint32_t layout) {
   s.bvh.swap(bvh);
   s.blasOffsets = offsets;
   s.blasLayout = layout;
+  buildTrianglePlane(s);  // records moved
   if (layout == 2) s.flags |= MTC_SCENE_BLAS_GPU_LAYOUT;
   else s.flags &= ~uint32_t(MTC_SCENE_BLAS_GPU_LAYOUT);
+}
+
+void buildTrianglePlane(SceneHost &s) {
+  s.triangleMaterials.clear();
+  bool any = false;
+  for (const auto &vm : s.sourceVertexMaterials) any |= !vm.empty();
+  if (!any) return;
+  s.triangleMaterials.assign(s.bvh.size() / 4, 0u);
+  for (size_t m = 0; m < s.blasOffsets.size() && m < s.sourceVertexMaterials.size(); m++) {
+    const std::vector<int32_t> &vm = s.sourceVertexMaterials[m];
+    if (vm.empty()) continue;
+    const size_t begin = size_t(s.tlasVec4) + s.blasOffsets[m];
+    const size_t end = m + 1 < s.blasOffsets.size() ? size_t(s.tlasVec4) + s.blasOffsets[m + 1] : s.bvh.size() / 4;
+    for (size_t r = begin; r < end; r++) {
+      uint32_t vertex;
+      std::memcpy(&vertex, &s.bvh[r * 4], 4);
+      if (vertex < vm.size()) s.triangleMaterials[r] = uint32_t(vm[vertex]) + 1u;
+    }
+  }
 }
 
 // gl-matrix mat4 invert (cofactor expansion), float64, as called by
@@ -958,15 +978,18 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   s.sourceInstances = instances;
   s.sourcePositions.clear();
   s.sourceIndices.clear();
+  s.sourceVertexMaterials.clear();
   for (const MeshData &md : meshes) {
     s.sourcePositions.push_back(md.positions);
     s.sourceIndices.push_back(md.indices);
+    s.sourceVertexMaterials.push_back(md.vertexMaterials);
   }
   s.blasBins = uint32_t(blasBins);
   s.tlasVec4 = uint32_t(tlas.buffer.size() / 4);
   s.bvh = tlas.buffer;
   for (const Blas &b : s.blases) s.bvh.insert(s.bvh.end(), b.buffer.begin(), b.buffer.end());
   s.instances = tlas.instances;
+  buildTrianglePlane(s);
   s.tlasStack = std::min(64u, std::max(1u, tlas.maxDepth));
   s.blasStack = std::min(64u, blasDepth);
   // Compact vertices (compactVertices.ts:7-27, 67-90): position f32x3 + oct

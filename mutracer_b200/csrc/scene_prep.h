@@ -159,6 +159,8 @@ struct SceneHost {
   mtc_vertex_layout layout{4, 3, 0, 0};
   std::vector<float> materials;
   std::vector<float> lights;         // 24 floats per light
+  std::vector<uint32_t> triangleMaterials;  // material + 1 per bvh vec4, or empty
+  std::vector<std::vector<int32_t>> sourceVertexMaterials;  // per BLAS (MeshData::vertexMaterials)
   std::vector<float> maps;           // MTC_MAP_VEC4_ROWS * 4 floats per map
   std::vector<float> mapTexels;      // RGBA f32 per texel, maps back to back
   std::vector<float> lightSampling;  // RGBA32F texels
@@ -190,6 +192,12 @@ void setBlasLayout(SceneHost &s, uint32_t layout);
 // index) (right min, leaf count) (right max, first record), node k at vec4
 // 4k, leaf primitive records after the nodes.
 std::vector<float> blasToGpuLayout(const std::vector<float> &bvh2);
+// packTriangleMaterials (compactVertices.ts:93-102) over every BLAS of `s`:
+// for each vec4 of a BLAS whose first word, read as a vertex index, lies
+// inside the BLAS's vertices, that vertex's material + 1 (the triangle
+// records; other vec4s are never read).  Empty when no BLAS has per-vertex
+// materials.
+void buildTrianglePlane(SceneHost &s);
 // refitBLAS (bvhAccel.ts:800-870) on a layout-0 BLAS in place; returns the
 // summed node surface area in post order.  Throws on offsets that leave the
 // buffer or break the depth-first order.
@@ -209,6 +217,9 @@ struct MeshData {
   std::vector<uint32_t> indices;
   std::vector<float> uvs;  // 2 per vertex, or empty (zero UVs when another mesh has some)
   std::vector<float> colors;  // 3 per vertex, or empty (white when another mesh has some)
+  // Global material index per vertex (a triangle takes its first vertex's),
+  // or empty: every triangle uses its instance's material.
+  std::vector<int32_t> vertexMaterials;
 };
 void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std::vector<Instance> &instances,
                    const std::vector<MaterialDesc> &materials, const std::vector<LightDesc> &lights, int blasBins,

@@ -76,6 +76,8 @@ class SceneHost:
             else np.zeros(0, np.float32)
         self.map_texels = _np(b.map_texels, b.map_texel_count * 4, np.float32) if b.map_texel_count \
             else np.zeros(0, np.float32)
+        self.triangle_materials = _np(b.triangle_materials, b.bvh_vec4_count, np.uint32) \
+            if b.triangle_materials else None
 
     @property
     def uniform(self):
@@ -122,6 +124,7 @@ class SceneHost:
         v.maps = C.cast(b.maps, C.c_void_p) if b.map_count else None
         v.map_texels = C.cast(b.map_texels, C.c_void_p) if b.map_texel_count else None
         v.map_count, v.map_texel_count = b.map_count, b.map_texel_count
+        v.triangle_materials = C.cast(b.triangle_materials, C.c_void_p) if b.triangle_materials else None
         return v
 
     def refit_inputs(self):
@@ -202,6 +205,7 @@ class DeviceScene:
         self.lights = up(host.lights)
         self.maps = up(host.maps)
         self.map_texels = up(host.map_texels)
+        self.triangle_materials = up(host.triangle_materials) if host.triangle_materials is not None else None
         b = host.bundle
         v = abi.SceneView()
         v.struct_size = C.sizeof(abi.SceneView)
@@ -230,6 +234,7 @@ class DeviceScene:
         v.tlas_stack_size, v.blas_stack_size = b.tlas_stack_size, b.blas_stack_size
         v.maps, v.map_texels = ptr(self.maps), ptr(self.map_texels)
         v.map_count, v.map_texel_count = b.map_count, b.map_texel_count
+        v.triangle_materials = ptr(self.triangle_materials)
         self.view = v
         self.uniform = abi.TraceUniform.from_buffer_copy(b.uniform)
         self.camera = abi.CameraUniform.from_buffer_copy(b.camera)
@@ -239,4 +244,4 @@ class DeviceScene:
     def device_bytes(self):
         return sum(t.numel() * t.element_size() for t in (self.bvh, self.instances, self.attributes,
                    self.materials, self.env_map, self.env_distribution, self.light_sampling, self.energy_lut,
-                   self.lights, self.maps, self.map_texels) if t is not None)
+                   self.lights, self.maps, self.map_texels, self.triangle_materials) if t is not None)

@@ -28,6 +28,8 @@ static Scene makeScene(const mtc_scene_view *sv, const mtc_trace_uniform *u, con
   s.mapTexels = (const V4 *)sv->map_texels;
   s.mapCount = sv->maps && sv->map_texels ? sv->map_count : 0;
   s.mapTexelCount = sv->map_texel_count;
+  s.triMats = sv->triangle_materials;
+  s.matCount = sv->material_count;
   s.flags = sv->flags;
   s.tlasStack = sv->tlas_stack_size;
   s.blasStack = sv->blas_stack_size;

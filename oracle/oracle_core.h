@@ -37,6 +37,8 @@ struct Scene {
   // Material maps: MTC_MAP_VEC4_ROWS vec4 per map, texels RGBA f32.
   const V4 *maps = nullptr, *mapTexels = nullptr;
   u32 mapCount = 0, mapTexelCount = 0;
+  const u32 *triMats = nullptr;  // triangle material plane (material + 1 per bvh vec4), or null
+  u32 matCount = 0;
   mtc_vertex_layout vl{};
   u32 flags = 0;
   u32 tlasStack = 64, blasStack = 64;

@@ -325,7 +325,17 @@ enum class Mode { Closest, Shadow };
 // intersectionAlphaPasses (intersectionAlpha.wgsl.ts:14-90): whether a
 // shadow candidate on a triangle of `materialIndex` (vertex indices `index`,
 // barycentrics `bary`) occludes.
-static bool intersectionAlphaPasses(const Scene &s, i32 materialIndex, const i32 index[3], V3 bary, Sampler &smp) {
+// triangleMaterial (vertexAttributes.wgsl.ts:51-56): the plane's material of
+// the triangle record, else the instance's (`fallback`).
+static i32 triangleMaterial(const Scene &s, i32 fallback, i32 record) {
+  if (!s.triMats) return fallback;
+  const u32 m = s.triMats[record];
+  return m && m - 1u < s.matCount ? i32(m - 1u) : fallback;
+}
+
+static bool intersectionAlphaPasses(const Scene &s, i32 initialMaterialIndex, i32 record, const i32 index[3], V3 bary,
+                                    Sampler &smp) {
+  const i32 materialIndex = triangleMaterial(s, initialMaterialIndex, record);
   const V4 *ma = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   float alpha = ma[9].x;
   auto surfaceUv = [&]() {
@@ -465,7 +475,7 @@ static bool traverse(const Scene &s, const Ray &ray, int bounces, bool doubleSid
           h.hitBary = hit.bary;
           if (mode == Mode::Shadow) {
             const i32 index[3] = {i0, i1, i2};
-            if (alphaSmp && !intersectionAlphaPasses(s, sideMaterial, index, hit.bary, *alphaSmp)) {
+            if (alphaSmp && !intersectionAlphaPasses(s, sideMaterial, triangleIndex, index, hit.bary, *alphaSmp)) {
               h.tMax = shadowRayTMax;  // not occluded: never traverse beyond the light
               continue;
             }
@@ -542,9 +552,13 @@ static void completeSurfaceInteraction(const Scene &s, SurfaceInteraction &si, c
   V3 n0 = vertexNormal(s, h.idx[0]), n1 = vertexNormal(s, h.idx[1]), n2 = vertexNormal(s, h.idx[2]);
   V3 normal = normalize(n0 * bary.x + n1 * bary.y + n2 * bary.z);
   const V2 uv0 = vertexUv(s, h.idx[0]), uv1 = vertexUv(s, h.idx[1]), uv2 = vertexUv(s, h.idx[2]);
+  // uvScale comes from the instance's material (fetchAttributes' `material`),
+  // read before the triangle's own material is resolved.
+  const V4 *im = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
+  si.materialIndex = triangleMaterial(s, si.materialIndex, h.triangleIndex);
   const V4 *dm = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
-  uv = {uv.x * dm[7].z, uv.y * dm[7].w};
+  uv = {uv.x * im[7].z, uv.y * im[7].w};
   const V2 duv1 = {uv0.x - uv2.x, uv0.y - uv2.y}, duv2 = {uv1.x - uv2.x, uv1.y - uv2.y};
   if (dm[24].x >= 0.0f || dm[24].y != 0.0f || dm[25].x != 0.0f) {
     V3 dp1 = h.tri[0] - h.tri[2];

@@ -370,19 +370,42 @@ def test_unsupported_features_are_named(name, build):
     assert "not supported" in msg
 
 
-def test_multi_material_mesh_is_unsupported_but_uniform_table_is_fine():
+def test_multi_material_meshes_use_the_triangle_material_plane():
+    """decodeMeshMaterials + packTriangleMaterials: the instance record
+    carries the table's first material; every triangle record's plane word
+    holds its vertices' table entry + 1; a geometry shared by meshes with
+    different tables gets one BLAS per table."""
+    d = D.Descriptor(16, 16)
+    g = d.add_geometry(np.concatenate([QUAD, QUAD + F(3)]), QUAD_IDX + [i + 4 for i in QUAD_IDX],
+                       material_indices=[0, 0, 0, 0, 1, 1, 1, 1])
+    a, b, c = d.add_material(base_color=(1, 0, 0)), d.add_material(base_color=(0, 1, 0)), d.add_material()
+    d.add_mesh(g, a, material_table=[a, b])
+    d.add_mesh(g, a, material_table=[c, a], transform=D.translate([0, 5, 0]))
+    d.add_mesh(g, a, material_table=[a, b], transform=D.translate([0, 9, 0]))   # shares the first BLAS
+    h = decoded(d)
+    ins = h.instances.reshape(-1, 40)
+    assert sorted(int(x) for x in ins[:, 2].view(np.int32)) == [255 + (a << 8), 255 + (a << 8), 255 + (c << 8)]
+    plane = h.triangle_materials
+    assert plane is not None and plane.size == h.bundle.bvh_vec4_count
+    info = h.info
+    assert info.blases == 2
+    # every triangle record (first word < 8 inside a BLAS) carries its table entry
+    words = h.bvh.reshape(-1, 4).view(np.uint32)
+    tl = h.uniform.blas_offset
+    recs = [r for r in range(tl, len(words)) if plane[r]]
+    assert set(int(plane[r]) for r in recs) == {a + 1, b + 1, c + 1}
+    assert not plane[:tl].any()
+    # uniform per-vertex indices: every triangle takes the table entry
     d = D.Descriptor(16, 16)
     g = d.add_geometry(QUAD, QUAD_IDX, material_indices=[1, 1, 1, 1])
     a, b = d.add_material(base_color=(1, 0, 0)), d.add_material(base_color=(0, 1, 0))
     d.add_mesh(g, a, material_table=[a, b])
     h = decoded(d)
-    assert int(h.instances.reshape(-1, 40)[0, 2:3].view(np.int32)[0]) == 255 + (1 << 8)
-    d = D.Descriptor(16, 16)
-    g = d.add_geometry(np.concatenate([QUAD, QUAD + F(3)]), QUAD_IDX + [i + 4 for i in QUAD_IDX],
-                       material_indices=[0, 0, 0, 0, 1, 1, 1, 1])
-    a, b = d.add_material(), d.add_material()
-    d.add_mesh(g, a, material_table=[a, b])
-    assert "several materials" in rejected(d, abi.MT_ERROR_UNAVAILABLE)
+    assert int(h.instances.reshape(-1, 40)[0, 2:3].view(np.int32)[0]) == 255 + (a << 8)
+    assert set(int(x) for x in h.triangle_materials if x) == {b + 1}
+    # no per-vertex materials: no plane
+    assert decoded(base()).triangle_materials is None
+
 
 
 def test_emissive_meshes_enter_the_light_table():
