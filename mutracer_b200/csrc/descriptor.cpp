@@ -456,9 +456,7 @@ DecodedMaterial decodeMaterial(const Words &d, uint32_t o, uint32_t version, uin
       case 42: scalar(md.alphaCutoff); break;
       case 45: pair(md.normalScale); break;
       case 54: mapAlphaUsage = choice(3); break;  // opaque, alpha, transmission
-      case 55:
-        if (choice(4) != 0) unsupported("UV projections");
-        break;
+      case 55: md.uvProjection = int(choice(4)); break;  // none, spherical, cylindrical, triplanar
       case 56: pair(md.uvScale); break;  // uvProjectionScale scales the UVs of every map
       case 51: case 52: {
         bool on = false;

@@ -764,8 +764,13 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
     if (tm && tm - 1u < s.matCount) si.materialIndex = int32_t(tm - 1u);
   }
   const float4 *md = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
-  si.uv = {(bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x) * r7.z,
-           (bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y) * r7.w};
+  // UV projection of the instance's material, from the local position and
+  // normal (intersect.wgsl.ts:1311-1322); triplanar UVs repeat.
+  const int projection = int(r7.x);
+  V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
+  if (projection > 0) uv = projectUV(projection, position, normal);
+  si.uv = {uv.x * r7.z, uv.y * r7.w};
+  if (projection == 3) si.uv = {si.uv.x - floorf(si.uv.x), si.uv.y - floorf(si.uv.y)};
   V3 mapped = normal;
   const float4 r1 = ld4(md + 1);
   const bool normalMapped = mapValid(s, r1.y);

@@ -272,6 +272,23 @@ static __device__ __noinline__ float4 sampleMap(const DevScene &s, int idx, V2 u
   };
   return mix4(mix4(t00, t10, wx), mix4(t01, t11, wx), wy);
 }
+// projectUV (uvProjection.wgsl.ts): procedural UVs from a local-space
+// position and normal; 1 spherical, 2 cylindrical, 3 triplanar.
+MTD V2 projectUV(int type, V3 pos, V3 normal) {
+  if (type == 3) {
+    const V3 a = {fabsf(normal.x), fabsf(normal.y), fabsf(normal.z)};
+    if (a.x > a.y && a.x > a.z) return {pos.y, pos.z};
+    if (a.y > a.x && a.y > a.z) return {pos.x, pos.z};
+    return {pos.x, pos.y};
+  }
+  if (type == 1) {
+    const V3 n = normalize(pos);
+    return {atan2f(n.x, n.z) / (2.0f * PI) + 0.5f, 1.0f - acosf(n.y) / PI};
+  }
+  if (type == 2) return {atan2f(pos.z, pos.x) / (2.0f * PI) + 0.5f, pos.y};
+  return {0.0f, 0.0f};
+}
+
 // A material's map index names a map of this scene (an index past the map
 // table, like -1, means no map).
 MTD bool mapValid(const DevScene &s, float index) { return index >= 0.0f && index < float(s.mapCount); }
@@ -282,7 +299,8 @@ MTD bool mapValid(const DevScene &s, float index) { return index >= 0.0f && inde
 // the alpha map's g at the hit's UV, then resolved by the alpha mode: opaque
 // occludes, mask compares with the cutoff, blend draws hashedSample(1).
 static __device__ __noinline__ bool alphaPasses(const DevScene &s, int32_t material, int32_t record, int32_t i0,
-                                                int32_t i1, int32_t i2, V3 bary, Sampler &smp) {
+                                                int32_t i1, int32_t i2, V3 bary, V3 hitPosition, V3 hitNormal,
+                                                Sampler &smp) {
   if (s.triMats) {  // triangleMaterial (vertexAttributes.wgsl.ts:51-56)
     const uint32_t m = __ldg(s.triMats + record);
     if (m && m - 1u < s.matCount) material = int32_t(m - 1u);
@@ -301,8 +319,11 @@ static __device__ __noinline__ bool alphaPasses(const DevScene &s, int32_t mater
       uv0 = vuv(i0); uv1 = vuv(i1); uv2 = vuv(i2);
     }
     const float4 r7 = ld4(d + 7);
-    const V2 uv = {(bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x) * r7.z,
-                   (bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y) * r7.w};
+    const int projection = int(r7.x);
+    V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
+    if (projection > 0) uv = projectUV(projection, hitPosition, hitNormal);
+    uv = {uv.x * r7.z, uv.y * r7.w};
+    if (projection == 3) uv = {uv.x - floorf(uv.x), uv.y - floorf(uv.y)};
     if (baseAlpha) alpha *= sampleMap(s, int(r2.z), uv).w;
     if (alphaMap) alpha *= sampleMap(s, int(r22.z), uv).y;
   }
@@ -443,7 +464,8 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
           h.hitBary = bary;
           if (shadow) {
             if (kAlpha && !alphaPasses(s, sideMaterial, triangleIndex, asi(r3.x) + vertexOffset,
-                                       asi(r3.y) + vertexOffset, asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
+                                       asi(r3.y) + vertexOffset, asi(r3.z) + vertexOffset, bary, o + d * t,
+                                       candidateNormal, *alphaSmp)) {
               h.tMax = tMaxInit;
               continue;
             }
@@ -625,7 +647,8 @@ struct RayTraversal {
       if (shadow) {
         if (kAlpha && alphaSmp &&
             !alphaPasses(*alphaScene, sideMaterial, triangleIndex, asi(r3.x) + vertexOffset,
-                         asi(r3.y) + vertexOffset, asi(r3.z) + vertexOffset, bary, *alphaSmp)) {
+                         asi(r3.y) + vertexOffset, asi(r3.z) + vertexOffset, bary, o + d * t, candidateNormal,
+                         *alphaSmp)) {
           h.tMax = tMaxInit;
           continue;
         }

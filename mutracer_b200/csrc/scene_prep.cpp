@@ -575,7 +575,7 @@ void packMaterial(const MaterialDesc &m, float *r) {
   row(5)[3] = float(m.mapAlphaUsage);
   row(6)[0] = float(m.maps[kMapCoatWeight]); row(6)[1] = float(m.maps[kMapCoatRoughness]);
   row(6)[2] = float(m.maps[kMapCoatNormal]); row(6)[3] = float(m.maps[kMapFuzzColor]);
-  row(7)[0] = 0.0f; row(7)[1] = float(m.maps[kMapDisplacement]); row(7)[2] = m.uvScale[0]; row(7)[3] = m.uvScale[1];
+  row(7)[0] = float(m.uvProjection); row(7)[1] = float(m.maps[kMapDisplacement]); row(7)[2] = m.uvScale[0]; row(7)[3] = m.uvScale[1];
   row(9)[0] = m.opacity; row(9)[1] = float(m.maps[kMapThinFilm]); row(9)[2] = m.thinFilmIor;
   row(9)[3] = float(m.maps[kMapTransmission]);
   row(10)[0] = m.baseWeight; row(10)[1] = m.diffuseRoughness; row(10)[2] = m.specularWeight; row(10)[3] = m.subsurfaceWeight;

@@ -90,6 +90,7 @@ struct MaterialDesc {
   int maps[kMapSlots] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
   float normalScale[2] = {1, 1};
   float uvScale[2] = {1, 1};     // uvProjectionScale: multiplies the interpolated UV
+  int uvProjection = 0;          // uvProjectionConstants: 0 none, 1 spherical, 2 cylindrical, 3 triplanar
   int mapAlphaUsage = 0;         // mapAlphaUsageConstants: 0 opaque, 2 alpha, 3 transmission
   float thinFilmThicknessMinimum = 0.0f;
   int thinFilmMapChannel = 0;    // r, g, b, a

@@ -325,6 +325,22 @@ enum class Mode { Closest, Shadow };
 // intersectionAlphaPasses (intersectionAlpha.wgsl.ts:14-90): whether a
 // shadow candidate on a triangle of `materialIndex` (vertex indices `index`,
 // barycentrics `bary`) occludes.
+// projectUV (uvProjection.wgsl.ts): 1 spherical, 2 cylindrical, 3 triplanar.
+static V2 projectUV(i32 type, V3 pos, V3 normal) {
+  if (type == 3) {
+    const V3 a = {std::fabs(normal.x), std::fabs(normal.y), std::fabs(normal.z)};
+    if (a.x > a.y && a.x > a.z) return {pos.y, pos.z};
+    if (a.y > a.x && a.y > a.z) return {pos.x, pos.z};
+    return {pos.x, pos.y};
+  }
+  if (type == 1) {
+    const V3 n = normalize(pos);
+    return {std::atan2(n.x, n.z) / (2.0f * PI) + 0.5f, 1.0f - std::acos(n.y) / PI};
+  }
+  if (type == 2) return {std::atan2(pos.z, pos.x) / (2.0f * PI) + 0.5f, pos.y};
+  return {0.0f, 0.0f};
+}
+
 // triangleMaterial (vertexAttributes.wgsl.ts:51-56): the plane's material of
 // the triangle record, else the instance's (`fallback`).
 static i32 triangleMaterial(const Scene &s, i32 fallback, i32 record) {
@@ -334,14 +350,18 @@ static i32 triangleMaterial(const Scene &s, i32 fallback, i32 record) {
 }
 
 static bool intersectionAlphaPasses(const Scene &s, i32 initialMaterialIndex, i32 record, const i32 index[3], V3 bary,
-                                    Sampler &smp) {
+                                    V3 hitPosition, V3 hitNormal, Sampler &smp) {
   const i32 materialIndex = triangleMaterial(s, initialMaterialIndex, record);
   const V4 *ma = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   float alpha = ma[9].x;
   auto surfaceUv = [&]() {
     V2 uv0 = vertexUv(s, index[0]), uv1 = vertexUv(s, index[1]), uv2 = vertexUv(s, index[2]);
     V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
-    return V2{uv.x * ma[7].z, uv.y * ma[7].w};
+    const i32 projection = i32(ma[7].x);
+    if (projection > 0) uv = projectUV(projection, hitPosition, hitNormal);
+    uv = {uv.x * ma[7].z, uv.y * ma[7].w};
+    if (projection == 3) uv = {uv.x - std::floor(uv.x), uv.y - std::floor(uv.y)};
+    return uv;
   };
   if (ma[5].w == 2.0f && mapValid(s, ma[2].z)) alpha *= sampleMap(s, i32(ma[2].z), surfaceUv()).w;
   if (mapValid(s, ma[22].z)) alpha *= sampleMap(s, i32(ma[22].z), surfaceUv()).y;
@@ -475,7 +495,8 @@ static bool traverse(const Scene &s, const Ray &ray, int bounces, bool doubleSid
           h.hitBary = hit.bary;
           if (mode == Mode::Shadow) {
             const i32 index[3] = {i0, i1, i2};
-            if (alphaSmp && !intersectionAlphaPasses(s, sideMaterial, triangleIndex, index, hit.bary, *alphaSmp)) {
+            if (alphaSmp && !intersectionAlphaPasses(s, sideMaterial, triangleIndex, index, hit.bary, h.hitPosition,
+                                                     candidateNormal, *alphaSmp)) {
               h.tMax = shadowRayTMax;  // not occluded: never traverse beyond the light
               continue;
             }
@@ -558,7 +579,10 @@ static void completeSurfaceInteraction(const Scene &s, SurfaceInteraction &si, c
   si.materialIndex = triangleMaterial(s, si.materialIndex, h.triangleIndex);
   const V4 *dm = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
+  const i32 projection = i32(im[7].x);  // intersect.wgsl.ts:1311-1322, local position and normal
+  if (projection > 0) uv = projectUV(projection, si.position, normal);
   uv = {uv.x * im[7].z, uv.y * im[7].w};
+  if (projection == 3) uv = {uv.x - std::floor(uv.x), uv.y - std::floor(uv.y)};
   const V2 duv1 = {uv0.x - uv2.x, uv0.y - uv2.y}, duv2 = {uv1.x - uv2.x, uv1.y - uv2.y};
   if (dm[24].x >= 0.0f || dm[24].y != 0.0f || dm[25].x != 0.0f) {
     V3 dp1 = h.tri[0] - h.tri[2];

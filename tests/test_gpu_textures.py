@@ -243,3 +243,42 @@ def test_every_slot_scene_oracle_parity(cuda):
     assert np.isfinite(gpu).all()
     assert rel_mse <= REL_MSE_BAR, rel_mse
     assert luma <= LUMA_BAR, luma
+
+
+def projection_room(width=96, height=72):
+    """Spherical, cylindrical and triplanar projected checkers on spheres, and
+    a triplanar-projected cutout (base-color alpha under mask mode) casting a
+    patterned shadow: projected UVs at surface hits and in the shadow rays'
+    coverage test."""
+    d = D.Descriptor(width, height)
+    yy, xx = np.mgrid[0:8, 0:8]
+    checker = np.zeros((8, 8, 4), np.uint8)
+    checker[(xx + yy) % 2 == 0] = [230, 210, 170, 255]
+    checker[(xx + yy) % 2 == 1] = [40, 70, 140, 0]
+    tex = d.add_texture(8, 8, checker)
+    floor = d.add_geometry(QUAD * F(3), QUAD_IDX)
+    spos, suv, sidx = uv_sphere(32, 16, 0.45)
+    sphere = d.add_geometry(spos, sidx)                              # no UVs: projections only
+    panel = d.add_geometry(np.array([[-.8, 0, -.6], [.8, 0, -.6], [.8, 0, .6], [-.8, 0, .6]], F), QUAD_IDX)
+    d.add_mesh(floor, d.add_material(base_color=(0.7, 0.7, 0.7), roughness=0.8))
+    for k, proj in enumerate((1, 2, 3)):
+        m = d.add_material(base_color=(1, 1, 1), roughness=0.4, textures=(tex, NONE, NONE, NONE),
+                           extensions=[(55, proj), (56, (2.0, 3.0))])
+        d.add_mesh(sphere, m, transform=D.translate([-1.1 + 1.1 * k, 0.45, 0]))
+    cutout = d.add_material(base_color=(1, 1, 1), roughness=0.5, textures=(tex, NONE, NONE, NONE),
+                            extensions=[(55, 3), (56, (1.5, 1.5)), (54, 1), (41, 2), (42, (0.5,))])
+    d.add_mesh(panel, cutout, transform=D.translate([0, 1.6, 0.2]))
+    d.add_light(D.LIGHT_RECT, intensity=8, size=0.8, height_or_inner=0.8, transform=D.look_at([0, 2.8, 0.3], [0, 0, 0]))
+    d.set_camera(fov=45, transform=D.look_at([0, 1.4, 3.8], [0, 0.5, 0]))
+    return d
+
+
+def test_projection_scene_oracle_parity(cuda):
+    st, msg, host = D.decode(projection_room().to_bytes())
+    assert st == abi.MT_OK, msg
+    assert host.bundle.flags & abi.MTC_SCENE_HAS_ALPHA and host.bundle.vertex_layout.uv_offset == 0
+    gpu, ref, _, _ = _render_pair(cuda, host, 32)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert np.isfinite(gpu).all()
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma

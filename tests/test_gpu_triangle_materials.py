@@ -1,7 +1,8 @@
-"""Per-triangle materials on a B200: the device image of a mesh whose halves
-select different table entries is bit-identical to the split meshes' image,
-in the BVH2 and BVH_GPU layouts and through the batch entry point, the
-wavefront engine and mt_context_commit; image parity against the oracle."""
+"""Per-triangle materials and vertex colors on a B200: the device image of a
+mesh whose halves select different table entries is bit-identical to the
+split meshes' image, in the BVH2 and BVH_GPU layouts and through the batch
+entry point, the wavefront engine and mt_context_commit; image parity against
+the oracle, with RGBA8 and float vertex colors on the floor."""
 import ctypes as C
 
 import numpy as np
@@ -58,8 +59,11 @@ def test_multi_material_mesh_equals_split_meshes(cuda):
         ctx.destroy()
 
 
-def test_multi_material_oracle_parity(cuda):
-    host = decode(halves(True, 96, 72, emissive=True))
+@pytest.mark.parametrize("colors", [None, "rgba8", "float"])
+def test_multi_material_oracle_parity(cuda, colors):
+    host = decode(halves(True, 96, 72, emissive=True, colors=colors))
+    if colors:
+        assert host.bundle.vertex_layout.color_offset and host.bundle.vertex_layout.color_float == (colors == "float")
     gpu, ref, _, _ = _render_pair(cuda, host, 32)
     rel_mse, luma = _image_metrics(gpu, ref)
     assert rel_mse <= REL_MSE_BAR, rel_mse

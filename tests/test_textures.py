@@ -185,8 +185,7 @@ def test_texture_rejections_of_pixels_udim_and_references():
     rejected(d)
 
 
-@pytest.mark.parametrize("name", ["displacement", "anisotropy map", "coat normal", "udim", "uv1", "projection",
-                                  "anisotropy"])
+@pytest.mark.parametrize("name", ["displacement", "anisotropy map", "coat normal", "udim", "uv1", "anisotropy"])
 def test_unsupported_texture_features_are_named(name):
     px = np.zeros((10, 10, 4), np.uint8)
     d = base()
@@ -199,8 +198,6 @@ def test_unsupported_texture_features_are_named(name):
         ext = [(70, t)]
     elif name == "coat normal":
         ext = [(74, t)]
-    elif name == "projection":
-        ext = [(55, 1)]
     elif name == "anisotropy":
         ext = [(9, (0.5,))]
     d.add_mesh(g, d.add_material(textures=tuple(slots), extensions=ext))
@@ -353,3 +350,31 @@ def test_emissive_triangles_carry_corner_uvs():
         assert np.array_equal(tri[k, 3:6].reshape(-1)[:6], want)
         assert np.array_equal(tri[k, 3:6].reshape(-1)[6:], want)      # secondary set repeats the primary
     assert h.materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)[lamp, 3, 3] == 0
+
+
+@pytest.mark.parametrize("projection", [1, 2, 3])
+def test_uv_projection_packs_and_renders(projection):
+    """uvProjection (ext 55) lands in row 7.x with uvProjectionScale in 7.zw;
+    the oracle renders a projected checker finitely and differently from
+    plain UVs."""
+    px = np.zeros((8, 8, 4), np.uint8)
+    yy, xx = np.mgrid[0:8, 0:8]
+    px[(xx + yy) % 2 == 0] = [255, 255, 255, 255]
+    px[(xx + yy) % 2 == 1] = [20, 20, 20, 255]
+
+    def scene(proj):
+        d = base()
+        t = d.add_texture(8, 8, px)
+        ext = [(56, (2.0, 2.0))] + ([(55, proj)] if proj else [])
+        m = d.add_material(textures=(t, NONE, NONE, NONE), extensions=ext)
+        d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV), m, transform=D.translate([0, 0.3, 0], 0.8))
+        return d, m
+    d, m = scene(projection)
+    h = decoded(d)
+    assert h.materials.reshape(-1, abi.MTC_MATERIAL_VEC4_ROWS, 4)[m, 7].tolist() == [projection, -1, 2, 2]
+    acc = oracle_lib.Accum(h.width, h.height)
+    oracle_lib.trace(h, acc, 4)
+    h0 = decoded(scene(0)[0])
+    acc0 = oracle_lib.Accum(h0.width, h0.height)
+    oracle_lib.trace(h0, acc0, 4)
+    assert np.isfinite(acc.color).all() and not np.array_equal(acc.color, acc0.color)

@@ -15,13 +15,19 @@ QUAD = np.array([[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], F)
 QUAD_IDX = [0, 2, 1, 0, 3, 2]
 
 
-def halves(multi, width=32, height=24, emissive=False):
+def halves(multi, width=32, height=24, emissive=False, colors=None):
+    """colors: None, "rgba8" (vertex colors in [0, 1]) or "float" (some above 1)."""
     d = D.Descriptor(width, height)
+    floor_colors = None
+    if colors is not None:
+        floor_colors = np.array([[1, 0.2, 0.2], [0.2, 1, 0.2], [0.2, 0.2, 1], [1, 1, 0.2]], F)
+        if colors == "float":
+            floor_colors = floor_colors * F(1.5)
     left, right = QUAD * F(0.5) + F([-0.6, 0, 0]), QUAD * F(0.5) + F([0.6, 0, 0])
     red = d.add_material(base_color=(0.8, 0.1, 0.1), roughness=0.5)
     green = d.add_material(base_color=(0.1, 0.8, 0.1), roughness=0.2, metalness=1.0,
                            emission_color=(1, 1, 1), emission_luminance=2.0 if emissive else 0.0)
-    d.add_mesh(d.add_geometry(QUAD * F(3) + F([0, -0.01, 0]), QUAD_IDX), d.add_material())
+    d.add_mesh(d.add_geometry(QUAD * F(3) + F([0, -0.01, 0]), QUAD_IDX, colors=floor_colors), d.add_material())
     if multi:
         g = d.add_geometry(np.concatenate([left, right]), QUAD_IDX + [i + 4 for i in QUAD_IDX],
                            material_indices=[0] * 4 + [1] * 4)
