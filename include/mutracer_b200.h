@@ -132,7 +132,8 @@ typedef struct mtc_camera_uniform {
 /* Compact vertex layout of attrBuffers (src/renderer/compactVertices.ts:7-28):
  * u32 words, position f32x3 at word 0, normal at normal_offset (oct-encoded
  * u32, or f32x3 when normal_float != 0), the primary UV set (f32x2) at
- * uv_offset when nonzero (UV_OFF; 0 = no UVs), the vertex color at
+ * uv_offset when nonzero (UV_OFF; 0 = no UVs), the secondary UV set at
+ * uv1_offset when nonzero (UV1_OFF; 0 = the primary set), the vertex color at
  * color_offset when nonzero (COLOR_OFF: RGBA8 in one word, or f32x3 when
  * color_float != 0; 0 = white).  Tangent words may be present in the stride
  * and are not read. */
@@ -143,6 +144,8 @@ typedef struct mtc_vertex_layout {
   uint32_t uv_offset;
   uint32_t color_offset;
   uint32_t color_float;
+  uint32_t uv1_offset;
+  uint32_t _pad;
 } mtc_vertex_layout;
 
 /* Device-side view of the bind groups (all pointers are device pointers). */

@@ -75,7 +75,8 @@ class CameraUniform(C.Structure):
 
 class VertexLayout(C.Structure):
     _fields_ = [("stride", C.c_uint32), ("normal_offset", C.c_uint32), ("normal_float", C.c_uint32),
-                ("uv_offset", C.c_uint32), ("color_offset", C.c_uint32), ("color_float", C.c_uint32)]
+                ("uv_offset", C.c_uint32), ("color_offset", C.c_uint32), ("color_float", C.c_uint32),
+                ("uv1_offset", C.c_uint32), ("_pad", C.c_uint32)]
 
 
 class SceneView(C.Structure):

@@ -90,6 +90,7 @@ bool fillJob(const mtc_job_desc &d, JobData &J) {
   if (v->struct_size != sizeof(mtc_scene_view) || !v->bvh || !v->instances || !v->attributes || !v->materials ||
       v->material_count == 0 || !v->energy_lut || !v->light_sampling || v->vertex_layout.stride < 4 ||
       (v->vertex_layout.uv_offset && (v->vertex_layout.uv_offset < 3 || v->vertex_layout.uv_offset + 2 > v->vertex_layout.stride)) ||
+      (v->vertex_layout.uv1_offset && (v->vertex_layout.uv1_offset < 3 || v->vertex_layout.uv1_offset + 2 > v->vertex_layout.stride)) ||
       (v->vertex_layout.color_offset &&
        (v->vertex_layout.color_offset < 3 ||
         v->vertex_layout.color_offset + (v->vertex_layout.color_float ? 3u : 1u) > v->vertex_layout.stride)))
@@ -121,6 +122,7 @@ bool fillJob(const mtc_job_desc &d, JobData &J) {
   J.s.mapTexelCount = v->map_texel_count;
   J.s.vuvOff = v->vertex_layout.uv_offset;
   J.s.vcolorOff = v->vertex_layout.color_offset;
+  J.s.vuv1Off = v->vertex_layout.uv1_offset;
   J.s.triMats = v->triangle_materials;
   J.s.vcolorFloat = v->vertex_layout.color_float;
   J.u = d.uniform;

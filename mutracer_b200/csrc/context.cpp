@@ -242,6 +242,8 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
       (b->env_map && !b->env_distribution) || (b->lights_count && !b->analytic_lights) ||
       (b->vertex_layout.uv_offset && (b->vertex_layout.uv_offset < 3 ||
                                       b->vertex_layout.uv_offset + 2 > b->vertex_layout.stride)) ||
+      (b->vertex_layout.uv1_offset && (b->vertex_layout.uv1_offset < 3 ||
+                                       b->vertex_layout.uv1_offset + 2 > b->vertex_layout.stride)) ||
       (b->vertex_layout.color_offset &&
        (b->vertex_layout.color_offset < 3 ||
         b->vertex_layout.color_offset + (b->vertex_layout.color_float ? 3u : 1u) > b->vertex_layout.stride)) ||

@@ -606,14 +606,13 @@ bool atlasKeepsFullSize(const std::vector<TextureRecord> &sources, uint32_t byte
 // one record of MTC_MAP_VEC4_ROWS vec4 per map and the texels of each
 // distinct pixel source (writeRawAtlasPlacement at unit scale).
 void packMaterialMaps(const Words &d, const std::vector<TextureRecord> &records, const std::vector<uint32_t> &maps,
-                      bool geometryHasUv1, SceneHost &s) {
+                      SceneHost &s) {
   bool floatStorage = false;
   std::vector<TextureRecord> sources;
   std::set<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>> seen;
   for (uint32_t t : maps) {
     const TextureRecord &r = records[t];
     if (r.udim) unsupported("UDIM texture sets");
-    if (r.uvChannel == 1 && geometryHasUv1) unsupported("textures on a second UV set");
     floatStorage |= r.storage == 1;
     if (seen.insert(r.source()).second) sources.push_back(r);
   }
@@ -690,11 +689,19 @@ void collectEmissive(const MeshData &md, const double *m, uint32_t instanceMater
     cr[2] = float(double(e0[0]) * e1[1] - double(e0[1]) * e1[0]);
     const double area = 0.5 * std::sqrt(double(cr[0]) * cr[0] + double(cr[1]) * cr[1] + double(cr[2]) * cr[2]);
     if (!(area > 1e-10) || !std::isfinite(area)) continue;
-    if (!md.uvs.empty())
-      for (int c = 0; c < 3; c++) {
-        tri.uv[c * 2] = md.uvs[size_t(md.indices[t + c]) * 2];
-        tri.uv[c * 2 + 1] = md.uvs[size_t(md.indices[t + c]) * 2 + 1];
+    // collectEmissiveTriangles: uv, and uv1 ?? uv (lightSampling.ts:264, 290-299)
+    const std::vector<float> &second = md.uv1s.empty() ? md.uvs : md.uv1s;
+    for (int c = 0; c < 3; c++) {
+      const size_t v = md.indices[t + c];
+      if (!md.uvs.empty()) {
+        tri.uv[c * 2] = md.uvs[v * 2];
+        tri.uv[c * 2 + 1] = md.uvs[v * 2 + 1];
       }
+      if (!second.empty()) {
+        tri.uv1[c * 2] = second[v * 2];
+        tri.uv1[c * 2 + 1] = second[v * 2 + 1];
+      }
+    }
     tri.area = area;
     tri.luminance = luminanceValue;
     tri.material = int32_t(material);
@@ -810,7 +817,7 @@ void decodeScene(const Words &d, SceneHost &s) {
   // Geometries.
   std::vector<MeshData> meshData(geometries);
   std::vector<std::vector<uint32_t>> vertexMaterial(geometries);
-  bool geometryHasUv1 = false, tangentFrames = false;
+  bool tangentFrames = false;
   for (uint32_t g = 0; g < geometries; g++) {
     const uint32_t o = u[9] + g * kGeometryWords;
     const uint32_t vc = u[o], ic = u[o + 1];
@@ -835,7 +842,7 @@ void decodeScene(const Words &d, SceneHost &s) {
       md.uvs.assign(d.f + u[o + 5], d.f + u[o + 5] + size_t(vc) * 2);
       tangentFrames = true;  // decodeGeometry generates tangents from UVs
     }
-    geometryHasUv1 |= d.array("uv1s", u[o + 6], uint64_t(vc) * 2);
+    if (d.array("uv1s", u[o + 6], uint64_t(vc) * 2)) md.uv1s.assign(d.f + u[o + 6], d.f + u[o + 6] + size_t(vc) * 2);
     if (d.array("vertex colors", u[o + 7], uint64_t(vc) * 3)) md.colors.assign(d.f + u[o + 7], d.f + u[o + 7] + size_t(vc) * 3);
     tangentFrames |= d.array("tangents", u[o + 8], uint64_t(vc) * 4);
     if (d.array("material indices", u[o + 9], vc)) {
@@ -962,9 +969,12 @@ void decodeScene(const Words &d, SceneHost &s) {
       mats[i].maps[slot] = index;
     }
   if (mapTextures.empty()) {
-    for (MeshData &md : blasMeshes) md.uvs.clear();  // nothing samples them
+    for (MeshData &md : blasMeshes) {  // nothing samples them
+      md.uvs.clear();
+      md.uv1s.clear();
+    }
   } else {
-    packMaterialMaps(d, textureRecords, mapTextures, geometryHasUv1, s);
+    packMaterialMaps(d, textureRecords, mapTextures, s);
   }
   // Lights.
   std::vector<LightDesc> lightList;

@@ -150,17 +150,22 @@ MTD V3 mulv(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
 // times the sRGB-decoded emissive map and, for standard materials, the coat
 // weight map's single coat passage.  `uv` is the caller's (the surface's
 // scaled UV, or a light sample's unscaled one).
-static __device__ __noinline__ V3 materialEmission(const DevScene &s, const float4 *d, V2 uv) {
+// getMapUvSet (materialBuffer.wgsl.ts:329-331): a map on UV set 1 samples the
+// secondary coordinates.
+MTD V2 mapUvSet(const DevScene &s, int idx, V2 uv, V2 uv1) {
+  return ld4(s.maps + size_t(idx) * MTC_MAP_VEC4_ROWS + 2).x > 0.5f ? uv1 : uv;
+}
+static __device__ __noinline__ V3 materialEmission(const DevScene &s, const float4 *d, V2 uv, V2 uv1) {
   const float4 r3 = ld4(d + 3);
   V3 emission = xyz(r3);
   const int emissive = int(r3.w), coatWeightMap = int(ld4(d + 6).x);
   if (mapValid(s, r3.w)) {
-    const float4 t = sampleMap(s, emissive, uv);
+    const float4 t = sampleMap(s, emissive, mapUvSet(s, emissive, uv, uv1));
     emission = mulv(emission, decodeMapColor(s, emissive, {t.x, t.y, t.z}));
   }
   if (mapValid(s, ld4(d + 6).x) && ld4(d).w == 0.0f) {
     const float4 r16 = ld4(d + 16);
-    const float w = clampf(r16.w, 0.0f, 1.0f) * sampleMap(s, coatWeightMap, uv).x;
+    const float w = clampf(r16.w, 0.0f, 1.0f) * sampleMap(s, coatWeightMap, mapUvSet(s, coatWeightMap, uv, uv1)).x;
     const V3 c = {sqrtf(fmaxf(r16.x, 0.0f)), sqrtf(fmaxf(r16.y, 0.0f)), sqrtf(fmaxf(r16.z, 0.0f))};
     emission = mulv(emission, V3{(1.0f - w) + c.x * w, (1.0f - w) + c.y * w, (1.0f - w) + c.z * w});
   }
@@ -180,12 +185,13 @@ MTD bool materialHasMaps(float4 r2, float4 r3, float4 r6, float4 r9, float4 r18,
 // resolution that sits between the alpha and transmission maps touches only
 // alpha, so the caller resolves it after this.  Out of line: only materials
 // with maps call it.
-static __device__ __noinline__ void applyMaterialMaps(const DevScene &s, const float4 *d, V2 uv, Material &m) {
-  m.emission = materialEmission(s, d, uv);
+static __device__ __noinline__ void applyMaterialMaps(const DevScene &s, const float4 *d, V2 uv, V2 uv1,
+                                                      Material &m) {
+  m.emission = materialEmission(s, d, uv, uv1);
   const float4 r2 = ld4(d + 2), r5 = ld4(d + 5), r6 = ld4(d + 6), r9 = ld4(d + 9), r22 = ld4(d + 22);
   auto slot = [&](float index, float4 &t) {
     if (!mapValid(s, index)) return false;
-    t = sampleMap(s, int(index), uv);
+    t = sampleMap(s, int(index), mapUvSet(s, int(index), uv, uv1));
     return true;
   };
   float4 t;
@@ -514,9 +520,9 @@ MTD void sampleEmissiveTriangle(const JobData &J, int index, V3 p, V2 rnd, Light
   const float4 *md = J.s.mats + size_t(int(c.w)) * MTC_MATERIAL_VEC4_ROWS;
   const float4 r3 = ld4(md + 3);
   if (mapValid(J.s, r3.w) || mapValid(J.s, ld4(md + 6).x)) {
-    const float4 uv01 = ld4(t + 3), uv2 = ld4(t + 4);
-    ls.emission = materialEmission(J.s, md, V2{bc.x * uv01.x + bc.y * uv01.z + bc.z * uv2.x,
-                                               bc.x * uv01.y + bc.y * uv01.w + bc.z * uv2.y});
+    const float4 d3 = ld4(t + 3), d4 = ld4(t + 4), d5 = ld4(t + 5);  // uv0 uv1 | uv2 uv1_0 | uv1_1 uv1_2
+    ls.emission = materialEmission(J.s, md, V2{bc.x * d3.x + bc.y * d3.z + bc.z * d4.x, bc.x * d3.y + bc.y * d3.w + bc.z * d4.y},
+                                   V2{bc.x * d4.z + bc.y * d5.x + bc.z * d5.z, bc.x * d4.w + bc.y * d5.y + bc.z * d5.w});
   } else {
     ls.emission = xyz(r3);
   }
@@ -559,7 +565,8 @@ MTD void sampleLightChoiceTable(const JobData &J, V3 p, V3 rnd, LightSample &ls)
 
 // --------------------------------------------------------------- material
 // materialBuffer.wgsl.ts:170-257 getMaterial with its texture block
-MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 uv, V3 vertexColor, Material &m) {
+MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 uv, V2 uv1, V3 vertexColor,
+                     Material &m) {
   // A miss keeps the previous hit's indices (zero before the first hit);
   // clamp so an empty or single-material scene never reads past its buffers.
   if (materialIndex < 0 || uint32_t(materialIndex) >= J.s.matCount) materialIndex = 0;
@@ -608,7 +615,7 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 
   m.coatAnisotropy = clampf(r17.y, 0.0f, 1.0f);
   m.coatIor = fmaxf(r17.z, 1.0f);
   m.coatDarkening = clampf(r17.w, 0.0f, 1.0f);
-  if (materialHasMaps(r2, r3, r6, r9, r18, r19, r21, r22)) applyMaterialMaps(J.s, d, uv, m);
+  if (materialHasMaps(r2, r3, r6, r9, r18, r19, r21, r22)) applyMaterialMaps(J.s, d, uv, uv1, m);
   if (m.alphaMode == 0) m.alpha = 1.0f;
   else if (m.alphaMode == 1) m.alpha = m.alpha >= r22.w ? 1.0f : 0.0f;
   m.anisotropyDirection = {1.0f, 0.0f};
@@ -654,6 +661,7 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 
 struct SurfaceInteraction {
   V3 position; bool albedoSampled;
   V2 uv;  // primary UV times the material's uvScale (0 without UVs)
+  V2 uv1;  // secondary UV times uvScale (the primary set without UV1 words)
   V3 vertexColor;  // interpolated vertex color (white without colors)
   V3 normal, vertexNormal, shadowOffset, faceNormal; bool hit;
   int32_t triangleIndex, instanceIndex, materialIndex;
@@ -768,8 +776,22 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
   // normal (intersect.wgsl.ts:1311-1322); triplanar UVs repeat.
   const int projection = int(r7.x);
   V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
-  if (projection > 0) uv = projectUV(projection, position, normal);
+  // vertexUv1 reads UV1_OFF, which aliases UV_OFF without secondary words
+  V2 second = uv;
+  if (s.vuv1Off) {
+    auto vuv1 = [&](int32_t i) {
+      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vuv1Off;
+      return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
+    };
+    const V2 a = vuv1(i0), b = vuv1(i1), c = vuv1(i2);
+    second = {bary.x * a.x + bary.y * b.x + bary.z * c.x, bary.x * a.y + bary.y * b.y + bary.z * c.y};
+  }
+  if (projection > 0) {
+    uv = projectUV(projection, position, normal);
+    second = uv;
+  }
   si.uv = {uv.x * r7.z, uv.y * r7.w};
+  si.uv1 = {second.x * r7.z, second.y * r7.w};
   if (projection == 3) si.uv = {si.uv.x - floorf(si.uv.x), si.uv.y - floorf(si.uv.y)};
   V3 mapped = normal;
   const float4 r1 = ld4(md + 1);
@@ -1329,6 +1351,7 @@ static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, 
   si.mediumScattering = v3(0.0f); si.mediumAnisotropy = 0.0f;
   si.position = v3(0.0f); si.normal = v3(0.0f); si.vertexNormal = v3(0.0f); si.shadowOffset = v3(0.0f);
   si.uv = v2(0.0f, 0.0f);
+  si.uv1 = v2(0.0f, 0.0f);
   si.vertexColor = v3(1.0f);
   si.faceNormal = v3(0.0f);
   Path &path = ps.path;
@@ -1406,7 +1429,7 @@ static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const Trav
     completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
   }
   Material ma;
-  getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
+  getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
   if (event == 0) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
       ps.aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
@@ -1442,7 +1465,7 @@ static __device__ __noinline__ bool shadeStepAlpha(Ctx &c, PathSample &ps, Spect
   if (sp.frontPending) {
     sp.frontPending = false;
     si = sp.primarySi;
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
     ma.alpha = 1.0f;
   } else {
     si.hit = false;
@@ -1450,7 +1473,7 @@ static __device__ __noinline__ bool shadeStepAlpha(Ctx &c, PathSample &ps, Spect
       si.triangleIndex = h.triangleIndex;
       completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
     }
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
   }
   if (!sp.primaryReady) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
@@ -1550,10 +1573,10 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
       si.triangleIndex = h.triangleIndex;
       completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
     }
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
   } else {
     // The primary material is a pure function of the primary vertex.
-    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, sp.primarySi.uv, sp.primarySi.vertexColor, ma);
+    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, sp.primarySi.uv, sp.primarySi.uv1, sp.primarySi.vertexColor, ma);
   }
   if (event == 0) {
     if (!sp.primaryReady) {

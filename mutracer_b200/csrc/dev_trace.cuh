@@ -26,6 +26,7 @@ struct DevScene {
   uint32_t mapCount, mapTexelCount;
   uint32_t vuvOff;          // word offset of the f32 UV pair (0: no UVs)
   uint32_t vcolorOff, vcolorFloat;  // vertex color word(s) (0: white), f32x3 or RGBA8
+  uint32_t vuv1Off;         // secondary UV pair (0: the primary pair)
   const uint32_t *triMats;  // material + 1 per bvh vec4 (null: instance materials only)
 };
 

@@ -274,6 +274,8 @@ bool validScene(const mtc_scene_view *s) {
                                              s->vertex_layout.stride &&
          (s->vertex_layout.uv_offset == 0 || (s->vertex_layout.uv_offset >= 3 &&
                                               s->vertex_layout.uv_offset + 2 <= s->vertex_layout.stride)) &&
+         (s->vertex_layout.uv1_offset == 0 || (s->vertex_layout.uv1_offset >= 3 &&
+                                               s->vertex_layout.uv1_offset + 2 <= s->vertex_layout.stride)) &&
          (s->vertex_layout.color_offset == 0 ||
           (s->vertex_layout.color_offset >= 3 &&
            s->vertex_layout.color_offset + (s->vertex_layout.color_float ? 3u : 1u) <= s->vertex_layout.stride));
@@ -304,6 +306,7 @@ DevScene toDev(const mtc_scene_view *v) {
   s.mapTexelCount = v->map_texel_count;
   s.vuvOff = v->vertex_layout.uv_offset;
   s.vcolorOff = v->vertex_layout.color_offset;
+  s.vuv1Off = v->vertex_layout.uv1_offset;
   s.triMats = v->triangle_materials;
   s.vcolorFloat = v->vertex_layout.color_float;
   return s;

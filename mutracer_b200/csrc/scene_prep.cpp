@@ -996,18 +996,21 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
   // normal (or f32x3 normal), then an f32 UV pair when any mesh has UVs, then
   // the vertex color when any mesh has colors: RGBA8 in one word, or f32x3
   // when some component lies outside [0, 1].
-  bool hasUv = false, hasColor = false, colorFloat = false;
+  bool hasUv = false, hasUv1 = false, hasColor = false, colorFloat = false;
   for (const MeshData &md : meshes) {
-    hasUv |= !md.uvs.empty();
+    hasUv |= !md.uvs.empty() || !md.uv1s.empty();
+    hasUv1 |= !md.uv1s.empty();
     hasColor |= !md.colors.empty();
     for (float c : md.colors)
       if (!(c >= 0.0f && c <= 1.0f)) colorFloat = true;
   }
   const uint32_t uvOffset = hasUv ? (normalFloat ? 6u : 4u) : 0u;
   uint32_t stride = (normalFloat ? 6 : 4) + (hasUv ? 2 : 0);
+  const uint32_t uv1Offset = hasUv1 ? stride : 0u;  // UV1_OFF; absent: it aliases UV_OFF
+  if (hasUv1) stride += 2;
   const uint32_t colorOffset = hasColor ? stride : 0u;
   if (hasColor) stride += colorFloat ? 3 : 1;
-  s.layout = {stride, 3, normalFloat ? 1u : 0u, uvOffset, colorOffset, colorFloat ? 1u : 0u};
+  s.layout = {stride, 3, normalFloat ? 1u : 0u, uvOffset, colorOffset, colorFloat ? 1u : 0u, uv1Offset, 0u};
   s.attributes.assign(size_t(vertexOffset) * stride, 0);
   for (size_t m = 0; m < meshes.size(); m++) {
     const MeshData &md = meshes[m];
@@ -1018,6 +1021,9 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
       if (normalFloat) std::memcpy(w + 3, &md.normals[size_t(v) * 3], 12);
       else w[3] = octEncode(md.normals[v * 3], md.normals[v * 3 + 1], md.normals[v * 3 + 2]);
       if (uvOffset && !md.uvs.empty()) std::memcpy(w + uvOffset, &md.uvs[size_t(v) * 2], 8);
+      // packCompactVertices: uv1 = geometry.uv1 ?? uv
+      const std::vector<float> &second = md.uv1s.empty() ? md.uvs : md.uv1s;
+      if (uv1Offset && !second.empty()) std::memcpy(w + uv1Offset, &second[size_t(v) * 2], 8);
       if (colorOffset) {
         const float *c = md.colors.empty() ? nullptr : &md.colors[size_t(v) * 3];
         const float r = c ? c[0] : 1.0f, g = c ? c[1] : 1.0f, b = c ? c[2] : 1.0f;
@@ -1090,7 +1096,10 @@ void assembleScene(SceneHost &s, const std::vector<MeshData> &meshes, const std:
     d[0] = t.p[0]; d[1] = t.p[1]; d[2] = t.p[2]; d[3] = emissivePmf[i];
     d[4] = t.p[3]; d[5] = t.p[4]; d[6] = t.p[5]; d[7] = float(t.area);
     d[8] = t.p[6]; d[9] = t.p[7]; d[10] = t.p[8]; d[11] = float(t.material);
-    for (int k = 0; k < 6; k++) d[12 + k] = d[18 + k] = t.uv[k];
+    for (int k = 0; k < 6; k++) {
+      d[12 + k] = t.uv[k];
+      d[18 + k] = t.uv1[k];
+    }
   }
   std::memcpy(s.lightSampling.data() + size_t(emissiveTexels) * 4, alias.words.data(), alias.words.size() * 4);
   // Analytic light records (wgpuSceneUniform.ts:70-152).

@@ -144,7 +144,8 @@ void buildEnergyLut(std::vector<float> &lut);
 // corners (f32), area and sampling luminance (float64), material index.
 struct EmissiveTriangle {
   float p[9];
-  float uv[6] = {0, 0, 0, 0, 0, 0};  // corner UVs (the secondary set repeats them)
+  float uv[6] = {0, 0, 0, 0, 0, 0};   // corner UVs
+  float uv1[6] = {0, 0, 0, 0, 0, 0};  // corner secondary UVs (the primary ones without a secondary set)
   double area = 0.0, luminance = 0.0;
   int32_t material = 0;
 };
@@ -217,6 +218,7 @@ struct MeshData {
   std::vector<float> positions, normals;
   std::vector<uint32_t> indices;
   std::vector<float> uvs;  // 2 per vertex, or empty (zero UVs when another mesh has some)
+  std::vector<float> uv1s;  // secondary set, 2 per vertex, or empty (the primary set stands in)
   std::vector<float> colors;  // 3 per vertex, or empty (white when another mesh has some)
   // Global material index per vertex (a triangle takes its first vertex's),
   // or empty: every triangle uses its instance's material.

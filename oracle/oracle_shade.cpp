@@ -494,18 +494,23 @@ static void sampleAnalyticLight(const Light &L, V3 p, V2 rnd, LightSample &ls) {
 }
 // sampleLight.wgsl.ts:319-357 (material emission without maps)
 // getMaterialEmission (materialBuffer.wgsl.ts:381-403).
-V3 getMaterialEmission(const Scene &s, i32 materialIndex, V2 uv) {
+// getMapUvSet (materialBuffer.wgsl.ts:329-331).
+static V2 getMapUvSet(const Scene &s, i32 idx, V2 uv, V2 uv1) {
+  return s.maps[size_t(idx) * MTC_MAP_VEC4_ROWS + 2].x > 0.5f ? uv1 : uv;
+}
+
+V3 getMaterialEmission(const Scene &s, i32 materialIndex, V2 uv, V2 uv1) {
   const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   V3 emission = xyz(d[3]);
   const i32 emissiveMapIndex = i32(d[3].w);
   if (mapValid(s, d[3].w)) {
-    V4 t = sampleMap(s, emissiveMapIndex, uv);
+    V4 t = sampleMap(s, emissiveMapIndex, getMapUvSet(s, emissiveMapIndex, uv, uv1));
     emission = emission * decodeMapColor(s, emissiveMapIndex, {t.x, t.y, t.z});
   }
   if (d[0].w == 0.0f) {
     const i32 coatWeightMapIndex = i32(d[6].x);
     if (mapValid(s, d[6].x)) {
-      const float coatWeight = clampf(d[16].w, 0.0f, 1.0f) * sampleMap(s, coatWeightMapIndex, uv).x;
+      const float coatWeight = clampf(d[16].w, 0.0f, 1.0f) * sampleMap(s, coatWeightMapIndex, getMapUvSet(s, coatWeightMapIndex, uv, uv1)).x;
       const V3 c = {std::sqrt(fmaxf(d[16].x, 0.0f)), std::sqrt(fmaxf(d[16].y, 0.0f)), std::sqrt(fmaxf(d[16].z, 0.0f))};
       emission = emission * V3{1.0f * (1.0f - coatWeight) + c.x * coatWeight, 1.0f * (1.0f - coatWeight) + c.y * coatWeight,
                                1.0f * (1.0f - coatWeight) + c.z * coatWeight};
@@ -532,7 +537,8 @@ static void sampleEmissiveTriangle(const Scene &s, i32 index, V3 p, V2 rnd, Ligh
   if (cl <= 0.0f) { ls.emission = v3(0.0f); ls.pdf = 0.0f; return; }
   // getMaterialEmission at the unscaled barycentric UV (sampleLight.wgsl.ts:331-358)
   V2 uv = {b.x * t[3].x + b.y * t[3].z + b.z * t[4].x, b.x * t[3].y + b.y * t[3].w + b.z * t[4].y};
-  ls.emission = getMaterialEmission(s, materialIndex, uv);
+  V2 uv1 = {b.x * t[4].z + b.y * t[5].x + b.z * t[5].z, b.x * t[4].w + b.y * t[5].y + b.z * t[5].w};
+  ls.emission = getMaterialEmission(s, materialIndex, uv, uv1);
   ls.selectionPmf = selectionPmf;
   ls.pdf = selectionPmf * (ls.dist * ls.dist) / fmaxf(area * cl, 1e-8f);
 }
@@ -573,7 +579,7 @@ static void sampleLightChoiceTable(const Scene &s, V3 p, V3 rnd, LightSample &ls
 // --------------------------------------------------------------- material
 // materialBuffer.wgsl.ts:170-257 getMaterial with its texture block
 // (:79-139 and the slots of materialTextureSlots.ts)
-Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv, V3 vertexColor) {
+Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv, V2 uv1, V3 vertexColor) {
   const V4 *d = s.mats + size_t(materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   Material m;
   m.baseColor = xyz(d[0]);
@@ -581,7 +587,7 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   m.specularRoughness = d[1].x;
   m.baseMetalness = d[2].x;
   m.specularAnisotropy = clampf(d[2].y, 0.0f, 1.0f);
-  m.emission = getMaterialEmission(s, materialIndex, uv);
+  m.emission = getMaterialEmission(s, materialIndex, uv, uv1);
   m.inside = false;
   m.specularIor = d[4].x;
   m.transmissionWeight = d[4].y;
@@ -616,7 +622,7 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   m.coatDarkening = clampf(d[17].w, 0.0f, 1.0f);
   const i32 diffuseMapIndex = i32(d[2].z);
   if (mapValid(s, d[2].z)) {
-    V4 t = sampleMap(s, diffuseMapIndex, uv);
+    V4 t = sampleMap(s, diffuseMapIndex, getMapUvSet(s, diffuseMapIndex, uv, uv1));
     m.baseColor = m.baseColor * decodeMapColor(s, diffuseMapIndex, {t.x, t.y, t.z});
     // mapAlphaUsageConstants (materialConstants.ts:2): 3 transmission, 2 alpha
     if (d[5].w == 3.0f) m.transmissionWeight = 1.0f - t.w;
@@ -626,7 +632,7 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   auto simple = [&](float index, float &target, int channel) {
     if (!mapValid(s, index)) return;
     const i32 idx = i32(index);
-    V4 t = sampleMap(s, idx, uv);
+    V4 t = sampleMap(s, idx, getMapUvSet(s, idx, uv, uv1));
     target *= channel == 0 ? t.x : channel == 1 ? t.y : channel == 2 ? t.z : t.w;
   };
   simple(d[22].z, m.alpha, 1);  // alphaMap: g
@@ -636,7 +642,7 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   simple(d[9].w, m.transmissionWeight, 0);  // transmissionMap: r
   const i32 mrtMapIndex = i32(d[2].w);
   if (mapValid(s, d[2].w)) {
-    V4 t = sampleMap(s, mrtMapIndex, uv);
+    V4 t = sampleMap(s, mrtMapIndex, getMapUvSet(s, mrtMapIndex, uv, uv1));
     m.baseMetalness *= t.z;
     m.specularRoughness *= t.y;
   }
@@ -645,7 +651,7 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   const i32 thinFilmMapIndex = i32(d[9].y);
   if (mapValid(s, d[9].y)) {
     // thinFilmTextureSample (materialTextureSlots.ts:214-228)
-    V4 t = sampleMap(s, thinFilmMapIndex, uv);
+    V4 t = sampleMap(s, thinFilmMapIndex, getMapUvSet(s, thinFilmMapIndex, uv, uv1));
     if (d[25].z == 0.0f && d[25].w == 0.0f) {
       m.thinFilmThickness *= t.x;
     } else {
@@ -658,14 +664,14 @@ Material getMaterial(const Scene &s, i32 materialIndex, i32 instanceIndex, V2 uv
   simple(d[6].y, m.coatRoughness, 1);   // coatRoughnessMap: g
   const i32 fuzzColorMapIndex = i32(d[6].w);
   if (mapValid(s, d[6].w)) {
-    V4 t = sampleMap(s, fuzzColorMapIndex, uv);
+    V4 t = sampleMap(s, fuzzColorMapIndex, getMapUvSet(s, fuzzColorMapIndex, uv, uv1));
     m.fuzzColor = m.fuzzColor * decodeMapColor(s, fuzzColorMapIndex, {t.x, t.y, t.z});
   }
   simple(d[18].w, m.fuzzRoughness, 3);  // fuzzRoughnessMap: a
   simple(d[19].w, m.specularWeight, 3); // specularWeightMap: a
   const i32 specularColorMapIndex = i32(d[21].w);
   if (mapValid(s, d[21].w)) {
-    V4 t = sampleMap(s, specularColorMapIndex, uv);
+    V4 t = sampleMap(s, specularColorMapIndex, getMapUvSet(s, specularColorMapIndex, uv, uv1));
     m.specularColor = m.specularColor * decodeMapColor(s, specularColorMapIndex, {t.x, t.y, t.z});
   }
   m.anisotropyDirection = {1.0f, 0.0f};
@@ -1152,7 +1158,7 @@ static V4 integrateRgb(Ctx &c, V2 uv, const Ray &ray, Aux &aux) {
   bool sampleIgnored = false;
   for (int event = 0; event <= eventLimit; event++) {
     intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-    ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor);
+    ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor);
     if (c.tr) c.tr->material_fetches++;
     if (event == 0) {
       if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
@@ -1204,7 +1210,7 @@ static V4 integrateRgbAlpha(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
   for (int step = 0; step < (20 + 1) * 2 + 2; step++) {
     if (query) {
       intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor);
+      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor);
       if (c.tr) c.tr->material_fetches++;
     }
     query = true;
@@ -1294,7 +1300,7 @@ static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
   for (int step = 0; step < stepLimit; step++) {
     if (!primaryReady || (event != 0 && !path.abort)) {
       intersectScene(c.s, path.ray, si, depth, event != 0, c.tr);
-      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.vertexColor);
+      ma = getMaterial(c.s, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor);
       if (c.tr) c.tr->material_fetches++;
     }
     if (event == 0) {
@@ -1507,7 +1513,7 @@ int oracle_bsdf(const float *rows, uint32_t features, const float *view, const f
   s.mats = (const om::V4 *)rows;
   s.ins = (const om::V4 *)ins;
   s.u = &u;
-  oracle::Material m = oracle::getMaterial(s, 0, 0, {0.0f, 0.0f}, om::v3(1.0f));
+  oracle::Material m = oracle::getMaterial(s, 0, 0, {0.0f, 0.0f}, {0.0f, 0.0f}, om::v3(1.0f));
   om::V3 v = om::normalize({view[0], view[1], view[2]});
   om::V3 n = {0.0f, 0.0f, 1.0f};
   float ndv = om::dot(v, n);

@@ -579,9 +579,23 @@ static void completeSurfaceInteraction(const Scene &s, SurfaceInteraction &si, c
   si.materialIndex = triangleMaterial(s, si.materialIndex, h.triangleIndex);
   const V4 *dm = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
   V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
+  // vertexUv1 reads UV1_OFF, which aliases UV_OFF without secondary words
+  V2 secondary = uv;
+  if (s.vl.uv1_offset) {
+    auto vuv1 = [&](i32 i) {
+      const u32 *w = s.attr + size_t(i) * s.vl.stride + s.vl.uv1_offset;
+      return V2{asf(w[0]), asf(w[1])};
+    };
+    const V2 a = vuv1(h.idx[0]), b = vuv1(h.idx[1]), c = vuv1(h.idx[2]);
+    secondary = {bary.x * a.x + bary.y * b.x + bary.z * c.x, bary.x * a.y + bary.y * b.y + bary.z * c.y};
+  }
   const i32 projection = i32(im[7].x);  // intersect.wgsl.ts:1311-1322, local position and normal
-  if (projection > 0) uv = projectUV(projection, si.position, normal);
+  if (projection > 0) {
+    uv = projectUV(projection, si.position, normal);
+    secondary = uv;
+  }
   uv = {uv.x * im[7].z, uv.y * im[7].w};
+  secondary = {secondary.x * im[7].z, secondary.y * im[7].w};
   if (projection == 3) uv = {uv.x - std::floor(uv.x), uv.y - std::floor(uv.y)};
   const V2 duv1 = {uv0.x - uv2.x, uv0.y - uv2.y}, duv2 = {uv1.x - uv2.x, uv1.y - uv2.y};
   if (dm[24].x >= 0.0f || dm[24].y != 0.0f || dm[25].x != 0.0f) {
@@ -623,7 +637,7 @@ static void completeSurfaceInteraction(const Scene &s, SurfaceInteraction &si, c
     si.shadowOffset = smoothNormal * hh;
   }
   si.uv = uv;
-  si.uv1 = uv;  // no secondary UV set: vertexUv1 aliases the primary one
+  si.uv1 = secondary;
   si.normal = getMatNormal(s, si.materialIndex, uv, normal, h.tri[0] - h.tri[2], h.tri[1] - h.tri[2], duv1, duv2);
   const V4 *w2l = insv + 1;
   const V4 *l2w = insv + 5;

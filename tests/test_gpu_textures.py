@@ -282,3 +282,40 @@ def test_projection_scene_oracle_parity(cuda):
     assert np.isfinite(gpu).all()
     assert rel_mse <= REL_MSE_BAR, rel_mse
     assert luma <= LUMA_BAR, luma
+
+
+def uv1_room(width=96, height=72):
+    """Maps on the secondary UV set: a floor whose base color reads UV1 and
+    roughness reads UV0, and a lamp whose emissive map reads UV1 (also at its
+    NEE light samples)."""
+    d = D.Descriptor(width, height)
+    yy, xx = np.mgrid[0:8, 0:8]
+    checker = np.zeros((8, 8, 4), np.uint8)
+    checker[(xx + yy) % 2 == 0] = [230, 200, 150, 255]
+    checker[(xx + yy) % 2 == 1] = [40, 60, 120, 255]
+    base_tex = d.add_texture(8, 8, checker, uv_channel=1)
+    rough = np.zeros((8, 8, 4), np.uint8)
+    rough[..., 1] = (np.arange(8) * 30 + 20)[None, :]
+    rough_tex = d.add_texture(8, 8, rough)
+    glow_tex = d.add_texture(8, 8, checker, uv_channel=1, wrap_s=2, wrap_t=2)
+    uv1 = np.array([[0, 0], [4, 0], [4, 4], [0, 4]], F)
+    floor = d.add_geometry(QUAD * F(3), QUAD_IDX, uvs=QUAD_UV, uv1s=uv1)
+    lamp_geo = d.add_geometry(np.array([[-.6, 0, -.4], [.6, 0, -.4], [.6, 0, .4], [-.6, 0, .4]], F), QUAD_IDX,
+                              uvs=QUAD_UV, uv1s=uv1 * F(0.5))
+    d.add_mesh(floor, d.add_material(base_color=(1, 1, 1), roughness=0.9, textures=(base_tex, NONE, NONE, NONE),
+                                     extensions=[(47, rough_tex)]))
+    lamp = d.add_material(emission_color=(1, 1, 1), emission_luminance=4.0, textures=(NONE, NONE, NONE, glow_tex))
+    d.add_mesh(lamp_geo, lamp, transform=[1, 0, 0, 0, 0, -1, 0, 0, 0, 0, -1, 0, 0, 2.2, 0, 1])
+    d.set_camera(fov=50, transform=D.look_at([0, 1.6, 3.6], [0, 0.2, 0]))
+    return d
+
+
+def test_secondary_uv_scene_oracle_parity(cuda):
+    st, msg, host = D.decode(uv1_room().to_bytes())
+    assert st == abi.MT_OK, msg
+    assert host.bundle.vertex_layout.uv1_offset == 6
+    gpu, ref, _, _ = _render_pair(cuda, host, 32)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert np.isfinite(gpu).all()
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma

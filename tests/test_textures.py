@@ -185,7 +185,7 @@ def test_texture_rejections_of_pixels_udim_and_references():
     rejected(d)
 
 
-@pytest.mark.parametrize("name", ["displacement", "anisotropy map", "coat normal", "udim", "uv1", "anisotropy"])
+@pytest.mark.parametrize("name", ["displacement", "anisotropy map", "coat normal", "udim", "anisotropy"])
 def test_unsupported_texture_features_are_named(name):
     px = np.zeros((10, 10, 4), np.uint8)
     d = base()
@@ -378,3 +378,33 @@ def test_uv_projection_packs_and_renders(projection):
     acc0 = oracle_lib.Accum(h0.width, h0.height)
     oracle_lib.trace(h0, acc0, 4)
     assert np.isfinite(acc.color).all() and not np.array_equal(acc.color, acc0.color)
+
+
+def test_secondary_uv_set_layout_and_sampling():
+    """compactVertexLayout / packCompactVertices: UV1 words follow the UV
+    pair when any geometry has them, geometries without UV1 repeat their
+    primary UVs there (uv1 ?? uv); a map on uv_channel 1 samples them."""
+    px = np.zeros((2, 2, 4), np.uint8)
+    px[0, 0] = px[1, 1] = [255, 255, 255, 255]
+    uv1 = np.array([[0.5, 0.5], [0.75, 0.5], [0.75, 0.75], [0.5, 0.75]], F)
+
+    def scene(channel):
+        d = base()
+        t = d.add_texture(2, 2, px, uv_channel=channel)
+        m = d.add_material(textures=(t, NONE, NONE, NONE))
+        d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV, uv1s=uv1), m, transform=D.translate([0, 0.6, 0]))
+        d.add_mesh(d.add_geometry(QUAD, QUAD_IDX, uvs=QUAD_UV), m, transform=D.translate([0, 0.3, 0]))
+        return d
+    h = decoded(scene(1))
+    lay = h.bundle.vertex_layout
+    assert (lay.stride, lay.uv_offset, lay.uv1_offset) == (8, 4, 6)
+    words = h.attributes.reshape(-1, 8)
+    assert np.array_equal(words[4:8, 6:8].view(F), uv1)              # the UV1 geometry
+    assert np.array_equal(words[8:12, 6:8].view(F), QUAD_UV)         # uv1 ?? uv
+    renders = []
+    for channel in (0, 1):
+        hh = decoded(scene(channel))
+        acc = oracle_lib.Accum(hh.width, hh.height)
+        oracle_lib.trace(hh, acc, 4)
+        renders.append(acc.color.copy())
+    assert np.isfinite(renders[1]).all() and not np.array_equal(renders[0], renders[1])
