@@ -660,9 +660,6 @@ MTD void getMaterial(const JobData &J, int materialIndex, int instanceIndex, V2 
 // ------------------------------------------------------------- surface hit
 struct SurfaceInteraction {
   V3 position; bool albedoSampled;
-  V2 uv;  // primary UV times the material's uvScale (0 without UVs)
-  V2 uv1;  // secondary UV times uvScale (the primary set without UV1 words)
-  V3 vertexColor;  // interpolated vertex color (white without colors)
   V3 normal, vertexNormal, shadowOffset, faceNormal; bool hit;
   int32_t triangleIndex, instanceIndex, materialIndex;
   float wavelength; int32_t spectralChannel;
@@ -698,7 +695,18 @@ static __device__ __noinline__ V3 applyNormalMap(const DevScene &s, int idx, flo
 // fetchAttributes + completeSurfaceInteraction (intersect.wgsl.ts:1233-1419,
 // 1539-1601) for compact vertices with an optional primary UV pair (no
 // tangent words, no UV projection).
-MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, const TraversalHit &h, V3 rayO, V3 rayD) {
+// The surface's texture coordinates and vertex color, which only the
+// material fetch reads.  They live beside the path sample (SpectralState)
+// rather than in its SurfaceInteraction, so the wavefront's per-step copy of
+// a slot's path sample stays as small as before textures.
+struct SurfaceTexcoords {
+  V2 uv;           // primary UV times the material's uvScale (0 without UVs)
+  V2 uv1;          // secondary UV times uvScale (the primary set without UV1 words)
+  V3 vertexColor;  // interpolated vertex color (white without colors)
+};
+
+MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, SurfaceTexcoords &tex,
+                                    const TraversalHit &h, V3 rayO, V3 rayD) {
   const DevScene &s = J.s;
   const float4 *insv = s.ins + size_t(h.insIdx) * MTC_INSTANCE_VEC4_STRIDE;
   float4 insData = ld4(insv);
@@ -752,7 +760,7 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
     };
     uv0 = vuv(i0); uv1 = vuv(i1); uv2 = vuv(i2);
   }
-  si.vertexColor = v3(1.0f);
+  tex.vertexColor = v3(1.0f);
   if (s.vcolorOff) {
     // vertexColor (vertexAttributes.wgsl.ts:38-43): f32x3, or unpack4x8unorm
     auto vcol = [&](int32_t i) {
@@ -762,7 +770,7 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
       return V3{float(c & 255u) / 255.0f, float((c >> 8) & 255u) / 255.0f, float((c >> 16) & 255u) / 255.0f};
     };
     const V3 c0 = vcol(i0), c1 = vcol(i1), c2 = vcol(i2);
-    si.vertexColor = c0 * bary.x + c1 * bary.y + c2 * bary.z;
+    tex.vertexColor = c0 * bary.x + c1 * bary.y + c2 * bary.z;
   }
   // fetchAttributes reads uvScale from the instance's material, then
   // resolves the triangle's own (resolveSurfaceMaterialIndex).
@@ -790,14 +798,14 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, co
     uv = projectUV(projection, position, normal);
     second = uv;
   }
-  si.uv = {uv.x * r7.z, uv.y * r7.w};
-  si.uv1 = {second.x * r7.z, second.y * r7.w};
-  if (projection == 3) si.uv = {si.uv.x - floorf(si.uv.x), si.uv.y - floorf(si.uv.y)};
+  tex.uv = {uv.x * r7.z, uv.y * r7.w};
+  tex.uv1 = {second.x * r7.z, second.y * r7.w};
+  if (projection == 3) tex.uv = {tex.uv.x - floorf(tex.uv.x), tex.uv.y - floorf(tex.uv.y)};
   V3 mapped = normal;
   const float4 r1 = ld4(md + 1);
   const bool normalMapped = mapValid(s, r1.y);
   if (normalMapped)
-    mapped = applyNormalMap(s, int(r1.y), make_float2(r1.z, r1.w), si.uv, normal, p0 - p2, p1 - p2,
+    mapped = applyNormalMap(s, int(r1.y), make_float2(r1.z, r1.w), tex.uv, normal, p0 - p2, p1 - p2,
                             V2{uv0.x - uv2.x, uv0.y - uv2.y}, V2{uv1.x - uv2.x, uv1.y - uv2.y});
   auto nt = [&](V3 v) { return V3{dot(xyz(w0), v), dot(xyz(w1), v), dot(xyz(w2), v)}; };
   si.faceNormal = normalize(nt(h.hitNormal));
@@ -1297,6 +1305,9 @@ struct SpectralState {
   bool split, front, frontPending;
   float4 back;
   Aux backAux;
+  // Texture coordinates of the current surface (kept from the last hit on a
+  // miss, like the rest of the surface interaction) and of the primary one.
+  SurfaceTexcoords tex, primaryTex;
 };
 
 // The alpha-split integrator runs for RGB scenes with a non-opaque material.
@@ -1350,9 +1361,7 @@ static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, 
   si.wavelength = 0.0f; si.spectralChannel = 0; si.mediumType = 0; si.mediumExtinction = v3(0.0f);
   si.mediumScattering = v3(0.0f); si.mediumAnisotropy = 0.0f;
   si.position = v3(0.0f); si.normal = v3(0.0f); si.vertexNormal = v3(0.0f); si.shadowOffset = v3(0.0f);
-  si.uv = v2(0.0f, 0.0f);
-  si.uv1 = v2(0.0f, 0.0f);
-  si.vertexColor = v3(1.0f);
+  sp.tex = {v2(0.0f, 0.0f), v2(0.0f, 0.0f), v3(1.0f)};
   si.faceNormal = v3(0.0f);
   Path &path = ps.path;
   path.scatteringMediumEntered = false;
@@ -1417,7 +1426,7 @@ MTD void traceExtension(const JobData &J, const PathSample &ps, TraversalHit &h,
 // known: surface interaction, material, primary guides or completeVertex,
 // shadeVertex.  Returns true when the path has ended.  Out of line so that
 // the megakernel and the wavefront shading kernel run one compiled copy.
-static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const TraversalHit &h) {
+static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, SpectralState &sp, const TraversalHit &h) {
   Path &path = ps.path;
   SurfaceInteraction &si = ps.si;
   const int bounceLimit = max(c.J.u.bounces, 0);
@@ -1426,10 +1435,10 @@ static __device__ __noinline__ bool shadeStep(Ctx &c, PathSample &ps, const Trav
   si.hit = false;
   if (h.insIdx >= 0) {
     si.triangleIndex = h.triangleIndex;
-    completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
+    completeSurfaceInteraction(c.J, si, sp.tex, h, path.ray.o, path.ray.d);
   }
   Material ma;
-  getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
+  getMaterial(c.J, si.materialIndex, si.instanceIndex, sp.tex.uv, sp.tex.uv1, sp.tex.vertexColor, ma);
   if (event == 0) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
       ps.aux.albedo = ma.transmissionWeight > 0.5f ? v3(1.0f) : ma.baseColor;
@@ -1465,15 +1474,16 @@ static __device__ __noinline__ bool shadeStepAlpha(Ctx &c, PathSample &ps, Spect
   if (sp.frontPending) {
     sp.frontPending = false;
     si = sp.primarySi;
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
+    sp.tex = sp.primaryTex;
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, sp.tex.uv, sp.tex.uv1, sp.tex.vertexColor, ma);
     ma.alpha = 1.0f;
   } else {
     si.hit = false;
     if (h.insIdx >= 0) {
       si.triangleIndex = h.triangleIndex;
-      completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
+      completeSurfaceInteraction(c.J, si, sp.tex, h, path.ray.o, path.ray.d);
     }
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, sp.tex.uv, sp.tex.uv1, sp.tex.vertexColor, ma);
   }
   if (!sp.primaryReady) {
     if (si.hit && (ma.materialType == 0 || ma.materialType == 2)) {
@@ -1482,6 +1492,7 @@ static __device__ __noinline__ bool shadeStepAlpha(Ctx &c, PathSample &ps, Spect
       si.albedoSampled = ma.transmissionWeight > 0.5f;
     }
     sp.primarySi = si;
+    sp.primaryTex = sp.tex;
     sp.primaryAux = ps.aux;
     sp.primaryReady = true;
     sp.coverage = clampf(ma.alpha, 0.0f, 1.0f);
@@ -1571,12 +1582,13 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
     si.hit = false;
     if (h.insIdx >= 0) {
       si.triangleIndex = h.triangleIndex;
-      completeSurfaceInteraction(c.J, si, h, path.ray.o, path.ray.d);
+      completeSurfaceInteraction(c.J, si, sp.tex, h, path.ray.o, path.ray.d);
     }
-    getMaterial(c.J, si.materialIndex, si.instanceIndex, si.uv, si.uv1, si.vertexColor, ma);
+    getMaterial(c.J, si.materialIndex, si.instanceIndex, sp.tex.uv, sp.tex.uv1, sp.tex.vertexColor, ma);
   } else {
     // The primary material is a pure function of the primary vertex.
-    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, sp.primarySi.uv, sp.primarySi.uv1, sp.primarySi.vertexColor, ma);
+    getMaterial(c.J, sp.primarySi.materialIndex, sp.primarySi.instanceIndex, sp.primaryTex.uv, sp.primaryTex.uv1,
+                sp.primaryTex.vertexColor, ma);
   }
   if (event == 0) {
     if (!sp.primaryReady) {
@@ -1586,6 +1598,7 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
         si.albedoSampled = ma.transmissionWeight > 0.5f;
       }
       sp.primarySi = si;
+      sp.primaryTex = sp.tex;
       sp.primaryReady = true;
       sp.dispersivePrimary = si.hit && ma.transmissionWeight > 0.001f && ma.transmissionDispersionScale > 0.001f;
       sp.wavelengthSample = c.smp.s1(2u);  // CAMERA_WAVELENGTH, sobol.wgsl.ts:5
@@ -1676,7 +1689,7 @@ MTD bool stepPath(Ctx &c, PathSample &ps, SpectralState &sp) {
   const bool spectral = isSpectral(c.J), split = alphaSplit(c.J);
   const bool reuse = spectral ? reusesPrimary(c.J, ps, sp.primaryReady) : split && sp.frontPending;
   if (!reuse) traceExtension<kGpuLayout>(c.J, ps, h, c.cnt);
-  return spectral ? shadeStepSpectral(c, ps, sp, h) : split ? shadeStepAlpha(c, ps, sp, h) : shadeStep(c, ps, h);
+  return spectral ? shadeStepSpectral(c, ps, sp, h) : split ? shadeStepAlpha(c, ps, sp, h) : shadeStep(c, ps, sp, h);
 }
 
 // The deferred NEE visibility test of sampleScattering (sampleMaterial.wgsl.ts
