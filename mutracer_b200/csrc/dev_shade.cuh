@@ -705,6 +705,63 @@ struct SurfaceTexcoords {
   V3 vertexColor;  // interpolated vertex color (white without colors)
 };
 
+// The attribute half of fetchAttributes (intersect.wgsl.ts:1250-1322,
+// 1408-1418) that only scenes with UVs, vertex colors, maps or UV projections
+// need: interpolated (or projected) UV sets times the instance material's
+// `r7` uvScale, the vertex color, and the normal map of `material`, whose
+// bent local normal goes to `mapped` (returns whether one applied).  Out of
+// line, so scenes without such data keep a lean surface completion.
+static __device__ __noinline__ bool surfaceTexcoords(const DevScene &s, int32_t material, float4 r7, int32_t i0,
+                                                     int32_t i1, int32_t i2, V3 bary, V3 position, V3 normal,
+                                                     V3 p0, V3 p1, V3 p2, SurfaceTexcoords &tex, V3 &mapped) {
+  V2 uv0 = {0.0f, 0.0f}, uv1 = uv0, uv2 = uv0;
+  if (s.vuvOff) {
+    auto vuv = [&](int32_t i) {
+      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vuvOff;
+      return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
+    };
+    uv0 = vuv(i0); uv1 = vuv(i1); uv2 = vuv(i2);
+  }
+  tex.vertexColor = v3(1.0f);
+  if (s.vcolorOff) {
+    // vertexColor (vertexAttributes.wgsl.ts:38-43): f32x3, or unpack4x8unorm
+    auto vcol = [&](int32_t i) {
+      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vcolorOff;
+      if (s.vcolorFloat) return V3{asf(__ldg(w)), asf(__ldg(w + 1)), asf(__ldg(w + 2))};
+      const uint32_t c = __ldg(w);
+      return V3{float(c & 255u) / 255.0f, float((c >> 8) & 255u) / 255.0f, float((c >> 16) & 255u) / 255.0f};
+    };
+    const V3 c0 = vcol(i0), c1 = vcol(i1), c2 = vcol(i2);
+    tex.vertexColor = c0 * bary.x + c1 * bary.y + c2 * bary.z;
+  }
+  // UV projection (intersect.wgsl.ts:1311-1322) from the local position and
+  // normal; triplanar UVs repeat.
+  const int projection = int(r7.x);
+  V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
+  // vertexUv1 reads UV1_OFF, which aliases UV_OFF without secondary words
+  V2 second = uv;
+  if (s.vuv1Off) {
+    auto vuv1 = [&](int32_t i) {
+      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vuv1Off;
+      return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
+    };
+    const V2 a = vuv1(i0), b = vuv1(i1), c = vuv1(i2);
+    second = {bary.x * a.x + bary.y * b.x + bary.z * c.x, bary.x * a.y + bary.y * b.y + bary.z * c.y};
+  }
+  if (projection > 0) {
+    uv = projectUV(projection, position, normal);
+    second = uv;
+  }
+  tex.uv = {uv.x * r7.z, uv.y * r7.w};
+  tex.uv1 = {second.x * r7.z, second.y * r7.w};
+  if (projection == 3) tex.uv = {tex.uv.x - floorf(tex.uv.x), tex.uv.y - floorf(tex.uv.y)};
+  const float4 r1 = ld4(s.mats + size_t(material) * MTC_MATERIAL_VEC4_ROWS + 1);
+  if (!mapValid(s, r1.y)) return false;
+  mapped = applyNormalMap(s, int(r1.y), make_float2(r1.z, r1.w), tex.uv, normal, p0 - p2, p1 - p2,
+                          V2{uv0.x - uv2.x, uv0.y - uv2.y}, V2{uv1.x - uv2.x, uv1.y - uv2.y});
+  return true;
+}
+
 MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, SurfaceTexcoords &tex,
                                     const TraversalHit &h, V3 rayO, V3 rayD) {
   const DevScene &s = J.s;
@@ -752,61 +809,19 @@ MTD void completeSurfaceInteraction(const JobData &J, SurfaceInteraction &si, Su
   V3 shadowOffset = smoothNormal * hh;
   // UVs (intersect.wgsl.ts:1274-1319, 1408-1418): interpolated, times the
   // instance material's uvScale; a normal map bends the shading normal.
-  V2 uv0 = {0.0f, 0.0f}, uv1 = uv0, uv2 = uv0;
-  if (s.vuvOff) {
-    auto vuv = [&](int32_t i) {
-      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vuvOff;
-      return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
-    };
-    uv0 = vuv(i0); uv1 = vuv(i1); uv2 = vuv(i2);
-  }
-  tex.vertexColor = v3(1.0f);
-  if (s.vcolorOff) {
-    // vertexColor (vertexAttributes.wgsl.ts:38-43): f32x3, or unpack4x8unorm
-    auto vcol = [&](int32_t i) {
-      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vcolorOff;
-      if (s.vcolorFloat) return V3{asf(__ldg(w)), asf(__ldg(w + 1)), asf(__ldg(w + 2))};
-      const uint32_t c = __ldg(w);
-      return V3{float(c & 255u) / 255.0f, float((c >> 8) & 255u) / 255.0f, float((c >> 16) & 255u) / 255.0f};
-    };
-    const V3 c0 = vcol(i0), c1 = vcol(i1), c2 = vcol(i2);
-    tex.vertexColor = c0 * bary.x + c1 * bary.y + c2 * bary.z;
-  }
-  // fetchAttributes reads uvScale from the instance's material, then
-  // resolves the triangle's own (resolveSurfaceMaterialIndex).
+  // fetchAttributes reads uvScale and the UV projection from the instance's
+  // material, then resolves the triangle's own (resolveSurfaceMaterialIndex).
   const float4 r7 = ld4(s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS + 7);
   if (s.triMats) {
     const uint32_t tm = __ldg(s.triMats + h.triangleIndex);
     if (tm && tm - 1u < s.matCount) si.materialIndex = int32_t(tm - 1u);
   }
-  const float4 *md = s.mats + size_t(si.materialIndex) * MTC_MATERIAL_VEC4_ROWS;
-  // UV projection of the instance's material, from the local position and
-  // normal (intersect.wgsl.ts:1311-1322); triplanar UVs repeat.
-  const int projection = int(r7.x);
-  V2 uv = {bary.x * uv0.x + bary.y * uv1.x + bary.z * uv2.x, bary.x * uv0.y + bary.y * uv1.y + bary.z * uv2.y};
-  // vertexUv1 reads UV1_OFF, which aliases UV_OFF without secondary words
-  V2 second = uv;
-  if (s.vuv1Off) {
-    auto vuv1 = [&](int32_t i) {
-      const uint32_t *w = s.attr + size_t(i) * s.vstride + s.vuv1Off;
-      return V2{asf(__ldg(w)), asf(__ldg(w + 1))};
-    };
-    const V2 a = vuv1(i0), b = vuv1(i1), c = vuv1(i2);
-    second = {bary.x * a.x + bary.y * b.x + bary.z * c.x, bary.x * a.y + bary.y * b.y + bary.z * c.y};
-  }
-  if (projection > 0) {
-    uv = projectUV(projection, position, normal);
-    second = uv;
-  }
-  tex.uv = {uv.x * r7.z, uv.y * r7.w};
-  tex.uv1 = {second.x * r7.z, second.y * r7.w};
-  if (projection == 3) tex.uv = {tex.uv.x - floorf(tex.uv.x), tex.uv.y - floorf(tex.uv.y)};
   V3 mapped = normal;
-  const float4 r1 = ld4(md + 1);
-  const bool normalMapped = mapValid(s, r1.y);
-  if (normalMapped)
-    mapped = applyNormalMap(s, int(r1.y), make_float2(r1.z, r1.w), tex.uv, normal, p0 - p2, p1 - p2,
-                            V2{uv0.x - uv2.x, uv0.y - uv2.y}, V2{uv1.x - uv2.x, uv1.y - uv2.y});
+  bool normalMapped = false;
+  // Only maps and vertex colors read `tex`; without them it keeps the
+  // sample's initial zero UVs and white.
+  if (s.vuvOff | s.vuv1Off | s.vcolorOff | s.mapCount || r7.x > 0.0f)
+    normalMapped = surfaceTexcoords(s, si.materialIndex, r7, i0, i1, i2, bary, position, normal, p0, p1, p2, tex, mapped);
   auto nt = [&](V3 v) { return V3{dot(xyz(w0), v), dot(xyz(w1), v), dot(xyz(w2), v)}; };
   si.faceNormal = normalize(nt(h.hitNormal));
   si.vertexNormal = normalize(nt(normal));
