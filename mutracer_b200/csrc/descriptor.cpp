@@ -21,8 +21,8 @@
 // Malformed descriptors are rejected with MT_ERROR_INVALID_ARGUMENT and a
 // message naming the problem, as the reference's validator does.  Valid
 // descriptors that use what this build does not render (displacement,
-// anisotropy and coat-normal maps, UDIM sets, second UV sets, textures the
-// atlas would downscale, UV projections, alpha in spectral scenes, material
+// anisotropy and coat-normal maps, UDIM sets, textures the atlas would
+// downscale, alpha in spectral scenes, material
 // graphs, IES profiles, rect-light textures, background maps, meshes whose
 // triangles use several materials, bevel, shadow catchers, unlit materials,
 // the remaining material extensions) are refused with
