@@ -457,13 +457,12 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
     uint32_t s = v.finishQueue[t];
     Slot &sl = v.slots[s];
     const JobData &J = v.jobs[sl.job];
-    // In place: the slot is this thread's alone, and a register copy of the
-    // whole path sample costs more than the few fields touched here.
-    PathSample &ps = sl.ps;
+    PathSample ps = sl.ps;
     if ((isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) ||
         (alphaSplit(J) && !finishAlphaSplit(J, ps, v.spectral[s]))) {
       // The next wavelength path, or the front path, of this sample starts
       // at event 0.
+      sl.ps = ps;
       enqueueRay(v, cur ^ 1u, s);
       continue;
     }
@@ -474,6 +473,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
       sl.left--;
       Ctx c{J, Sampler(), bsdfContext(J), Counters(), ShadowQuery()};
       beginSample(c, sl.x, sl.y, ps, v.spectral[s]);
+      sl.ps = ps;
       sl.smp = c.smp;
       again = true;
     } else {
