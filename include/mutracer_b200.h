@@ -207,10 +207,19 @@ typedef struct mtc_scene_view {
  * bit 2 (layout code 2) of the reference's blasLayoutMask: set it when any
  * instance record carries BLAS layout code 2 (BVH_GPU); without it such
  * instances are not traversed, as in a shader compiled without that layout.
- * BVH2 (layout code 0) is always traversed. */
+ * BVH2 (layout code 0) is always traversed.
+ * A SPECTRAL scene with three dispersion wavelengths shares each sample's
+ * path prefix: the first wavelength path runs in RGB until it meets a
+ * dispersive transmissive surface, where it forks into the three wavelength
+ * paths (the reference's shareSpectralPrefix, spectralPrefix.wgsl.ts, its
+ * default whenever dispersionWavelengths is 3: WGPURayTracePass.ts:2113,2122,
+ * scene-core.ts:689).  SPECTRAL_INDEPENDENT selects the variant without
+ * sharing, where every wavelength path is spectral from the camera (the
+ * reference's shader compiled with shareSpectralPrefix off). */
 enum { MTC_SCENE_HAS_MEDIUM = 1u, MTC_SCENE_SPECTRAL = 2u,
        MTC_SCENE_PATTERN_SHIFT = 4u, MTC_SCENE_PATTERN_MASK = 0x30u,
-       MTC_SCENE_BLAS_GPU_LAYOUT = 0x100u, MTC_SCENE_HAS_ALPHA = 0x200u };
+       MTC_SCENE_BLAS_GPU_LAYOUT = 0x100u, MTC_SCENE_HAS_ALPHA = 0x200u,
+       MTC_SCENE_SPECTRAL_INDEPENDENT = 0x400u };
 
 /* G3 accumulation outputs (rayTrace.compute.ts:294-299; never overwritten,
  * always accumulated).  shadow_catcher holds 3 vec4 per pixel
@@ -397,10 +406,14 @@ typedef struct mtc_batch_config {
  * pointers) to completion in one persistent launch.  `queue_state` is
  * caller-provided device scratch of mtc_batch_scratch_bytes(job_count) bytes
  * that receives the job table and the work-queue counter (reset by the call
- * on `stream`).  status_out (device, may be NULL) is set to 0.  Work is
+ * on `stream`).  status_out (device, may be NULL) is cleared on `stream`; the
+ * kernel then sets MTC_BATCH_STATUS_GUARD_EXHAUSTED in it if a warp's work
+ * loop reached its iteration bound before the queue drained (a corrupted
+ * table: the warp stops instead of spinning).  Work is
  * pulled with one atomic per warp tile (config->items_per_fetch tiles); every
  * sample of a tile runs in order on one warp, so each job's outputs are
  * bit-identical to running it alone through mtc_trace_samples. */
+#define MTC_BATCH_STATUS_GUARD_EXHAUSTED 1u
 size_t mtc_batch_scratch_bytes(uint32_t capacity);
 mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count,
                           const mtc_batch_config *config, void *queue_state,
@@ -472,9 +485,12 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity,
  * inside the library's device image, sized for MTC_BATCH_NOALLOC_MAX_JOBS
  * jobs, so the call allocates nothing; a larger job_count returns
  * MT_ERROR_INVALID_ARGUMENT.  The caller still passes the jobs with their
- * scene buffers and accumulation outputs.  The first call on a device looks
- * up that array's device address (cudaGetSymbolAddress) with the device
- * current; make that first call before any stream capture.  Every call on a
+ * scene buffers and accumulation outputs.  Jobs and `config` follow the rules
+ * of mtc_trace_batch (same validation, every config field applied), and
+ * status_out is used the same way.  The first call on a device (and the first
+ * after its primary context was reset) looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current; make that first call
+ * before any stream capture.  Every call on a
  * device shares the one array (each call rewrites the table and clears the
  * counter), so calls whose work overlaps on the same device race: serialise
  * them, for example on one stream.  The array stays resident on every device

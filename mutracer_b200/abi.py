@@ -31,6 +31,7 @@ MTC_SCENE_PATTERN_SHIFT = 4
 MTC_SCENE_PATTERN_MASK = 0x30
 MTC_SCENE_BLAS_GPU_LAYOUT = 0x100
 MTC_SCENE_HAS_ALPHA = 0x200
+MTC_SCENE_SPECTRAL_INDEPENDENT = 0x400
 MTC_FEATURE_USE_ENVMAP = 1
 MTC_INSTANCE_VEC4_STRIDE = 10
 MTC_MATERIAL_VEC4_ROWS = 26
@@ -40,6 +41,7 @@ MTC_ENERGY_LUT_WIDTH = 32
 MTC_ENERGY_LUT_HEIGHT = 2177
 MTC_REGROUP_OFF = 0xFFFFFFFF
 MTC_BATCH_NOALLOC_MAX_JOBS = 64
+MTC_BATCH_STATUS_GUARD_EXHAUSTED = 1
 
 
 class MtError(RuntimeError):

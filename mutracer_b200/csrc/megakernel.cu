@@ -15,7 +15,7 @@
 #include <cstring>
 #include <vector>
 
-#include "dev_shade.cuh"
+#include "batch_table.cuh"
 #include "js_minmax.h"
 
 using namespace mt;
@@ -23,7 +23,6 @@ using namespace mt;
 namespace {
 
 constexpr int kTileW = 16, kTileH = 8;       // plain kernel CTA tile
-constexpr int kWarpTileW = 8, kWarpTileH = 4;  // batched kernel warp tile
 
 __device__ __forceinline__ void flushCounters(const Counters &cnt, uint32_t paths, mtc_counters *out) {
   if (!out) return;
@@ -57,51 +56,14 @@ __global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
   flushCounters(cnt, paths, counters);
 }
 
-// Header of a batched job table (host table and device scratch alike); the
-// JobData entries follow at kBatchTableOffset.  The kernel reads the job
-// count and item total from it, so a captured launch can be replayed after
-// the host table is rewritten with other jobs.
-struct BatchHeader {
-  uint32_t jobCount, totalItems, tileW, flagsUnion, _pad[60];
-};
-static_assert(sizeof(BatchHeader) == 256, "batch header size");
-constexpr size_t kBatchTableOffset = sizeof(BatchHeader);
-
-// Persistent batched kernel.  queue[0] is the next work item; items are
-// warp tiles (tileW x 32/tileW pixels) laid out job after job
-// (JobData.firstItem / .items).  A warp takes `grain` consecutive items per
-// atomic.  The loop ends when the counter passes the item total, so every
-// warp exits.
+// Persistent batched kernel over a job table (batch_table.cuh).
 template <bool kGpuLayout>
 __global__ void __launch_bounds__(128)
-    k_batch(const BatchHeader *__restrict__ header, uint32_t *queue, mtc_counters *counters, uint32_t grain) {
-  const JobData *__restrict__ jobs =
-      reinterpret_cast<const JobData *>(reinterpret_cast<const char *>(header) + kBatchTableOffset);
-  const uint32_t job_count = header->jobCount, total_items = header->totalItems, tileW = header->tileW;
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t lx = lane % tileW, ly = lane / tileW, tileH = 32u / tileW;
+    k_batch(const BatchHeader *__restrict__ header, uint32_t *queue, mtc_counters *counters, uint32_t grain,
+            uint32_t *status) {
   Counters cnt;
   uint32_t paths = 0;
-  for (uint32_t guard = 0; guard < total_items + 1u; guard++) {
-    uint32_t first = 0;
-    if (lane == 0) first = atomicAdd(queue, grain);
-    first = __shfl_sync(0xffffffffu, first, 0);
-    if (first >= total_items) break;
-    const uint32_t last = min(first + grain, total_items);
-    uint32_t j = 0;
-    for (uint32_t item = first; item < last; item++) {
-      // Jobs are few; a forward scan of the prefix table finds the owner.
-      while (j + 1 < job_count && jobs[j + 1].firstItem <= item) j++;
-      const JobData &J = jobs[j];
-      uint32_t local = item - J.firstItem;
-      uint32_t tx = local % J.tilesX, ty = local / J.tilesX;
-      uint32_t x = tx * tileW + lx, y = ty * tileH + ly;
-      if (x < J.width && y < J.height) {
-        tracePixelSamples<kGpuLayout>(J, x, y, J.samples, cnt);
-        paths += J.samples;
-      }
-    }
-  }
+  batchWorkLoop<kGpuLayout>(header, queue, grain, status, cnt, paths);
   flushCounters(cnt, paths, counters);
 }
 
@@ -267,106 +229,6 @@ mt_status cudaStatus(cudaError_t e) {
   return MT_ERROR;
 }
 
-bool validScene(const mtc_scene_view *s) {
-  return s && s->struct_size == sizeof(mtc_scene_view) && s->bvh && s->instances && s->attributes && s->materials &&
-         s->material_count > 0 && s->energy_lut && s->light_sampling &&
-         s->vertex_layout.stride >= 4 && s->vertex_layout.normal_offset + (s->vertex_layout.normal_float ? 3u : 1u) <=
-                                             s->vertex_layout.stride &&
-         (s->vertex_layout.uv_offset == 0 || (s->vertex_layout.uv_offset >= 3 &&
-                                              s->vertex_layout.uv_offset + 2 <= s->vertex_layout.stride)) &&
-         (s->vertex_layout.uv1_offset == 0 || (s->vertex_layout.uv1_offset >= 3 &&
-                                               s->vertex_layout.uv1_offset + 2 <= s->vertex_layout.stride)) &&
-         (s->vertex_layout.color_offset == 0 ||
-          (s->vertex_layout.color_offset >= 3 &&
-           s->vertex_layout.color_offset + (s->vertex_layout.color_float ? 3u : 1u) <= s->vertex_layout.stride));
-}
-
-DevScene toDev(const mtc_scene_view *v) {
-  DevScene s;
-  s.bvh = (const float4 *)v->bvh;
-  s.ins = (const float4 *)v->instances;
-  s.attr = (const uint32_t *)v->attributes;
-  s.mats = (const float4 *)v->materials;
-  s.env = (const float4 *)v->env_map;
-  s.envDist = (const float2 *)v->env_distribution;
-  s.lightData = (const float4 *)v->light_sampling;
-  s.lut = (const float *)v->energy_lut;
-  s.lights = (const float4 *)v->analytic_lights;
-  s.envW = v->env_width;
-  s.envH = v->env_height;
-  s.vstride = v->vertex_layout.stride;
-  s.vnormalOff = v->vertex_layout.normal_offset;
-  s.vnormalFloat = v->vertex_layout.normal_float;
-  s.flags = v->flags;
-  s.insCount = v->instance_count;
-  s.matCount = v->material_count;
-  s.maps = (const float4 *)v->maps;
-  s.mapTexels = (const float4 *)v->map_texels;
-  s.mapCount = v->maps && v->map_texels ? v->map_count : 0;
-  s.mapTexelCount = v->map_texel_count;
-  s.vuvOff = v->vertex_layout.uv_offset;
-  s.vcolorOff = v->vertex_layout.color_offset;
-  s.vuv1Off = v->vertex_layout.uv1_offset;
-  s.triMats = v->triangle_materials;
-  s.vcolorFloat = v->vertex_layout.color_float;
-  return s;
-}
-
-bool validUniform(const mtc_trace_uniform *u) {
-  if (!u) return false;
-  float w = u->output_size[0], h = u->output_size[1];
-  return w >= 1.0f && h >= 1.0f && w <= 65536.0f && h <= 65536.0f && u->loop_unroll_guard == 4u;
-}
-
-JobData makeJob(const mtc_scene_view *scene, const mtc_camera_uniform *camera, const mtc_trace_uniform *uniform,
-                const mtc_outputs *out, uint32_t samples) {
-  JobData J;
-  std::memset(&J, 0, sizeof(J));
-  J.s = toDev(scene);
-  J.u = *uniform;
-  J.cam = *camera;
-  J.outColor = (float4 *)out->color;
-  J.outNormal = (float4 *)out->normal;
-  J.outAlbedo = (float4 *)out->albedo;
-  J.outCatcher = (float4 *)out->shadow_catcher;
-  J.samples = samples;
-  J.width = uint32_t(uniform->output_size[0]);
-  J.height = uint32_t(uniform->output_size[1]);
-  J.tilesX = (J.width + kWarpTileW - 1) / kWarpTileW;
-  J.tilesY = (J.height + kWarpTileH - 1) / kWarpTileH;
-  J.items = J.tilesX * J.tilesY;
-  return J;
-}
-
-struct BatchShape {
-  uint32_t blockThreads, tileW, tileH, ctasPerSm, grain;
-};
-// Resolves a (possibly NULL) mtc_batch_config to launch parameters; false for
-// out-of-range values.
-bool batchShape(const mtc_batch_config *c, BatchShape &out) {
-  out = BatchShape{128u, 8u, 4u, 2u, 1u};
-  if (!c) return true;
-  if (c->struct_size != sizeof(mtc_batch_config)) return false;
-  if (c->block_threads) {
-    if (c->block_threads > 128u || c->block_threads % 32u) return false;
-    out.blockThreads = c->block_threads;
-  }
-  if (c->tile_width) {
-    if (c->tile_width > 32u || (32u % c->tile_width)) return false;
-    out.tileW = c->tile_width;
-    out.tileH = 32u / c->tile_width;
-  }
-  if (c->ctas_per_sm) {
-    if (c->ctas_per_sm > 32u) return false;
-    out.ctasPerSm = c->ctas_per_sm;
-  }
-  if (c->items_per_fetch) {
-    if (c->items_per_fetch > 16u) return false;
-    out.grain = c->items_per_fetch;
-  }
-  return true;
-}
-
 }  // namespace
 
 extern "C" {
@@ -376,8 +238,7 @@ uint32_t mtc_abi_version(void) { return MTC_ABI_VERSION; }
 mt_status mtc_trace_samples(const mtc_scene_view *scene, const mtc_camera_uniform *camera,
                             const mtc_trace_uniform *uniform, const mtc_outputs *out, uint32_t samples,
                             mtc_counters *counters, void *stream) {
-  if (!validScene(scene) || !camera || !validUniform(uniform) || !out || !out->color || !out->normal ||
-      !out->albedo || !out->shadow_catcher)
+  if (!validScene(scene) || !camera || !validUniform(uniform) || !validOutputs(out))
     return MT_ERROR_INVALID_ARGUMENT;
   if (samples == 0) return MT_OK;
   JobData J = makeJob(scene, camera, uniform, out, samples);
@@ -438,39 +299,18 @@ mt_status mtc_batch_prepare(const mtc_job_desc *jobs, uint32_t job_count, const 
   if ((!jobs && job_count) || !table) return MT_ERROR_INVALID_ARGUMENT;
   BatchShape shape;
   if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
-  char *base = static_cast<char *>(table);
-  uint64_t total = 0;
-  for (uint32_t j = 0; j < job_count; j++) {
-    const mtc_job_desc &d = jobs[j];
-    if (!validScene(&d.scene) || !validUniform(&d.uniform) || !d.out.color || !d.out.normal || !d.out.albedo ||
-        !d.out.shadow_catcher)
-      return MT_ERROR_INVALID_ARGUMENT;
-    JobData J = makeJob(&d.scene, &d.camera, &d.uniform, &d.out, d.samples);
-    J.tilesX = (J.width + shape.tileW - 1) / shape.tileW;
-    J.tilesY = (J.height + shape.tileH - 1) / shape.tileH;
-    J.items = d.samples ? J.tilesX * J.tilesY : 0u;
-    J.firstItem = uint32_t(total);
-    total += J.items;
-    if (total >= 0x7fffffffull) return MT_ERROR_INVALID_ARGUMENT;
-    std::memcpy(base + kBatchTableOffset + size_t(j) * sizeof(JobData), &J, sizeof(J));
-  }
-  BatchHeader h;
-  std::memset(&h, 0, sizeof(h));
-  h.jobCount = job_count;
-  h.totalItems = uint32_t(total);
-  h.tileW = shape.tileW;
-  for (uint32_t j = 0; j < job_count; j++) h.flagsUnion |= jobs[j].scene.flags;
-  std::memcpy(base, &h, sizeof(h));
-  if (total_items) *total_items = uint32_t(total);
-  return MT_OK;
+  return writeBatchTable(jobs, job_count, shape, table, total_items);
 }
 
-mt_status mtc_batch_launch(const void *table, uint32_t capacity, const mtc_batch_config *config, void *queue_state,
-                           mtc_counters *counters, void *stream) {
-  if (!table || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
-  BatchShape shape;
-  if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
+}  // extern "C"
+
+namespace {
+
+// Copies the host table into `queue_state`, clears the work counter and
+// launches k_batch; `status` (device, may be NULL) collects the kernel's
+// status bits.
+mt_status launchBatch(const void *table, uint32_t capacity, const BatchShape &shape, void *queue_state,
+                      uint32_t *status, mtc_counters *counters, cudaStream_t st) {
   char *scratch = (char *)queue_state;
   size_t bytes = mtc_batch_table_bytes(capacity);
   uint32_t *queue = (uint32_t *)(scratch + (bytes + 255) / 256 * 256);
@@ -486,19 +326,34 @@ mt_status mtc_batch_launch(const void *table, uint32_t capacity, const mtc_batch
   // The host copy of the header decides the BLAS-layout specialisation.
   uint32_t flagsUnion = static_cast<const BatchHeader *>(table)->flagsUnion;
   if (flagsUnion & MTC_SCENE_BLAS_GPU_LAYOUT)
-    k_batch<true><<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain);
+    k_batch<true><<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain,
+                                                       status);
   else
-    k_batch<false><<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain);
+    k_batch<false><<<grid, shape.blockThreads, 0, st>>>((const BatchHeader *)scratch, queue, counters, shape.grain,
+                                                        status);
   return cudaStatus(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" {
+
+mt_status mtc_batch_launch(const void *table, uint32_t capacity, const mtc_batch_config *config, void *queue_state,
+                           mtc_counters *counters, void *stream) {
+  if (!table || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
+  BatchShape shape;
+  if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
+  return launchBatch(table, capacity, shape, queue_state, nullptr, counters, (cudaStream_t)stream);
 }
 
 mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count, const mtc_batch_config *config,
                           void *queue_state, uint32_t *status_out, mtc_counters *counters, void *stream) {
   if ((!jobs && job_count) || !queue_state) return MT_ERROR_INVALID_ARGUMENT;
-  if (config && config->struct_size != sizeof(mtc_batch_config)) return MT_ERROR_INVALID_ARGUMENT;
+  BatchShape shape;
+  if (!batchShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
   if (job_count == 0) return MT_OK;
   std::vector<char> table(mtc_batch_table_bytes(job_count));
-  mt_status st = mtc_batch_prepare(jobs, job_count, config, table.data(), nullptr);
+  mt_status st = writeBatchTable(jobs, job_count, shape, table.data(), nullptr);
   if (st != MT_OK) return st;
   if (status_out) {
     cudaError_t e = cudaMemsetAsync(status_out, 0, sizeof(uint32_t), (cudaStream_t)stream);
@@ -506,7 +361,7 @@ mt_status mtc_trace_batch(const mtc_job_desc *jobs, uint32_t job_count, const mt
   }
   // cudaMemcpyAsync from pageable memory has finished reading the table
   // when it returns, so the vector may go out of scope.
-  return mtc_batch_launch(table.data(), job_count, config, queue_state, counters, stream);
+  return launchBatch(table.data(), job_count, shape, queue_state, status_out, counters, (cudaStream_t)stream);
 }
 
 mt_status mtc_refit_tlas(void *tlas, uint64_t tlas_vec4_count, void *instances, uint32_t instance_count,

@@ -708,125 +708,20 @@ void makeAnalyticSky(Environment &env, uint32_t W, uint32_t H, uint64_t seed) {
 }
 
 // ------------------------------------------------------------ energy LUT
-// GGX single-scattering directional albedo tables in the row layout of
-// decodeOpenPbrEnergyLut.ts:20-33, tabulated here by stratified VNDF
-// quadrature (the reference ships Adobe's tabulation of the same integrals).
-namespace {
-struct D3 { double x, y, z; };
-inline D3 norm3(D3 v) { double l = std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z); return {v.x / l, v.y / l, v.z / l}; }
-inline double dot3(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-inline double smithG1(D3 v, double a) {
-  double nz = std::fabs(v.z);
-  if (nz <= 1e-12) return 0.0;
-  double t2 = a * a * (v.x * v.x + v.y * v.y) / (nz * nz);
-  return 2.0 / (1.0 + std::sqrt(1.0 + t2));
-}
-inline D3 vndf(D3 v, double a, double u1, double u2) {
-  D3 vh = norm3({a * v.x, a * v.y, v.z});
-  double lensq = vh.x * vh.x + vh.y * vh.y;
-  D3 T1 = lensq > 0 ? D3{-vh.y / std::sqrt(lensq), vh.x / std::sqrt(lensq), 0} : D3{1, 0, 0};
-  D3 T2 = {vh.y * T1.z - vh.z * T1.y, vh.z * T1.x - vh.x * T1.z, vh.x * T1.y - vh.y * T1.x};
-  double r = std::sqrt(u1), phi = 2.0 * M_PI * u2;
-  double t1 = r * std::cos(phi), t2 = r * std::sin(phi);
-  double s = 0.5 * (1.0 + vh.z);
-  t2 = (1.0 - s) * std::sqrt(std::max(0.0, 1.0 - t1 * t1)) + s * t2;
-  double t3 = std::sqrt(std::max(0.0, 1.0 - t1 * t1 - t2 * t2));
-  D3 nh = {t1 * T1.x + t2 * T2.x + t3 * vh.x, t1 * T1.y + t2 * T2.y + t3 * vh.y, t1 * T1.z + t2 * T2.z + t3 * vh.z};
-  return norm3({a * nh.x, a * nh.y, std::max(1e-9, nh.z)});
-}
-inline double fresnelD(double ci, double eta) {  // eta = etaI / etaT
-  ci = std::min(1.0, std::fabs(ci));
-  double st2 = eta * eta * std::max(0.0, 1.0 - ci * ci);
-  if (st2 >= 1.0) return 1.0;
-  double ct = std::sqrt(std::max(0.0, 1.0 - st2));
-  double rs = (ci - eta * ct) / (ci + eta * ct), rp = (eta * ci - ct) / (eta * ci + ct);
-  return 0.5 * (rs * rs + rp * rp);
-}
-double iorOfIndex(int i) { return i <= 15 ? 1.0 / (1.0 + (15 - i) * 0.1) : 1.0 + (i - 16) * 0.1; }
-// Reflection albedo with Fresnel (mode 0), ideal metal (1), or the (R, T)
-// albedos of a rough dielectric interface (mode 2).
-void albedo(double etaTI, double alpha, double mu, int mode, double &R, double &T) {
-  const int N = 24;
-  double a = std::max(alpha, 1e-4);
-  mu = std::max(mu, 1e-3);
-  D3 v = {std::sqrt(std::max(0.0, 1.0 - mu * mu)), 0.0, mu};
-  double g1v = smithG1(v, a);
-  R = 0.0; T = 0.0;
-  for (int i = 0; i < N; i++)
-    for (int j = 0; j < N; j++) {
-      D3 h = vndf(v, a, (i + 0.5) / N, (j + 0.5) / N);
-      double vh = dot3(v, h);
-      D3 l = {2 * vh * h.x - v.x, 2 * vh * h.y - v.y, 2 * vh * h.z - v.z};
-      double F = mode == 1 ? 1.0 : fresnelD(vh, 1.0 / etaTI);
-      if (l.z > 0) R += F * smithG1(l, a) / std::max(g1v, 1e-12) * g1v;
-      if (mode == 2) {
-        double eta = 1.0 / etaTI;
-        double k = 1.0 - eta * eta * (1.0 - vh * vh);
-        if (k > 0) {
-          D3 t = {-v.x * eta + h.x * (eta * vh - std::sqrt(k)), -v.y * eta + h.y * (eta * vh - std::sqrt(k)),
-                  -v.z * eta + h.z * (eta * vh - std::sqrt(k))};
-          if (t.z < 0) T += (1.0 - F) * smithG1(t, a);
-        }
-      }
-    }
-  R /= double(N) * N;
-  T /= double(N) * N;
-}
-}  // namespace
+// Adobe's OpenPBR energy-compensation tables (Apache License 2.0, Copyright
+// 2026 Adobe; adobe/openpbr-bsdf), decoded from the reference's
+// openPbrEnergyLut.ts by decodeOpenPbrEnergyLut.ts:35-83 into the 32 x 2177
+// float32 rows the BSDF samples.  The build embeds the decoded table
+// (csrc/openpbr_energy_lut.f32, written by csrc/gen_energy_lut.py) as
+// little-endian float32 bit patterns.
+extern "C" const uint32_t mtp_openpbr_energy_lut_bits[];
+extern "C" const uint64_t mtp_openpbr_energy_lut_count;
 
 void buildEnergyLut(std::vector<float> &lut) {
-  lut.assign(size_t(MTC_ENERGY_LUT_WIDTH) * MTC_ENERGY_LUT_HEIGHT, 0.0f);
-  auto at = [&](int row, int col) -> float & { return lut[size_t(row) * 32 + col]; };
-  std::vector<std::thread> pool;
-  unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  for (unsigned t = 0; t < nt; t++) {
-    pool.emplace_back([&, t] {
-      for (int ia = int(t); ia < 32 * 32; ia += int(nt)) {
-        int i = ia / 32, a = ia % 32;
-        double ior = iorOfIndex(i), alpha = (a / 31.0) * (a / 31.0);
-        double avgOpaque = 0.0, avgLoss = 0.0, avgR = 0.0, avgT = 0.0;
-        double prevO = 0.0, prevL = 0.0;
-        for (int c = 0; c < 32; c++) {
-          double mu = c / 31.0, R, T, R2, T2;
-          albedo(ior, alpha, mu, 0, R, T);
-          albedo(ior, alpha, mu, 2, R2, T2);
-          double opaque = std::min(1.0, std::max(0.0, 1.0 - R));
-          double loss = std::min(1.0, std::max(0.0, 1.0 - R2 - T2));
-          at(i * 32 + a, c) = float(opaque);
-          at(1089 + i * 32 + a, c) = float(loss);
-          if (c > 0) {
-            double h = 1.0 / 31.0;
-            avgOpaque += h * ((c - 1) * h * (prevO + opaque) + h * (prevO + 2 * opaque) / 3.0);
-            avgLoss += h * ((c - 1) * h * (prevL + loss) + h * (prevL + 2 * loss) / 3.0);
-          }
-          avgR += R2 * mu; avgT += T2 * mu;
-          prevO = opaque; prevL = loss;
-        }
-        at(1024 + i, a) = float(avgOpaque);
-        at(2113 + i, a) = float(avgLoss);
-        at(2145 + i, a) = float(avgR + avgT > 0 ? avgR / (avgR + avgT) : 0.5);
-      }
-    });
-  }
-  for (auto &th : pool) th.join();
-  for (int r = 0; r < 32; r++) {
-    double alpha = (r / 31.0) * (r / 31.0);
-    for (int c = 0; c < 32; c++) {
-      double R, T;
-      albedo(1.5, alpha, c / 31.0, 1, R, T);
-      at(1056 + r, c) = float(std::min(1.0, std::max(0.0, 1.0 - R)));
-    }
-  }
-  // Metal averages from the piecewise-linear rows (decodeOpenPbrEnergyLut.ts:72-81).
-  for (int r = 0; r < 32; r++) {
-    const double h = 1.0 / 31.0;
-    double avg = 0.0;
-    for (int i = 0; i < 31; i++) {
-      double a = at(1056 + r, i), b = at(1056 + r, i + 1);
-      avg += h * (i * h * (a + b) + h * (a + 2 * b) / 3.0);
-    }
-    at(1088, r) = float(avg);
-  }
+  const size_t n = size_t(MTC_ENERGY_LUT_WIDTH) * MTC_ENERGY_LUT_HEIGHT;
+  if (mtp_openpbr_energy_lut_count != n) throw std::runtime_error("embedded energy LUT has the wrong size");
+  lut.resize(n);
+  std::memcpy(lut.data(), mtp_openpbr_energy_lut_bits, n * sizeof(float));
 }
 
 // ---------------------------------------------------------------- lights
