@@ -172,8 +172,10 @@ def measured_traffic(form, args, host, spp):
     return None, None
 
 
-def cpu_baseline(host, spp, seconds):
-    """The CPU oracle on all host cores over a bounded row sample (full spp)."""
+def cpu_baseline(host, spp, seconds, keep=None):
+    """The CPU oracle on all host cores over a bounded row sample (full spp).
+    With `keep` (a dict), the oracle accumulation and the rows it rendered are
+    left there for the parity check."""
     from tests import oracle_lib
     acc = oracle_lib.Accum(host.width, host.height)
     # Rows in a strided order (0, 37, 74, ...) so the sample covers the whole
@@ -189,9 +191,34 @@ def cpu_baseline(host, spp, seconds):
         rows += 1
         elapsed = time.perf_counter() - t0
     mp = done_paths / elapsed / 1e6
+    if keep is not None:
+        keep["acc"], keep["rows"] = acc, order[:rows]
     return {"value": round(mp, 4), "unit": "Mpaths/s", "cores": oracle_lib.threads(), "kind": "port",
             "sample": f"{rows} rows (stride {stride}) of {host.width}x{host.height} at {spp} spp "
                       f"({done_paths} path samples, {elapsed:.1f} s)"}
+
+
+def row_parity(gpu_color, gpu_normal, oracle_acc, rows, width, height):
+    """Image parity of the timed GPU image against the CPU oracle on the rows
+    the oracle rendered (same seed, same spp): relative MSE of the resolved
+    HDR rows and relative mean-luminance difference, against the bars
+    relMSE <= 1e-3 and luminance within 0.5 %."""
+    rows = np.asarray(sorted(rows), dtype=np.int64)
+    g = gpu_color.reshape(height, width, 4)[rows, :, :3].astype(np.float64)
+    gn = np.maximum(gpu_normal.reshape(height, width, 4)[rows, :, 3:4], 1.0)
+    o = oracle_acc.color.reshape(height, width, 4)[rows, :, :3].astype(np.float64)
+    on = np.maximum(oracle_acc.normal.reshape(height, width, 4)[rows, :, 3:4], 1.0)
+    a, b = g / gn, o / on
+    rel = float(((a - b) ** 2).sum() / max(float((b ** 2).sum()), 1e-30))
+    w = np.array([0.2126, 0.7152, 0.0722])
+    la, lb = float((a @ w).mean()), float((b @ w).mean())
+    luma = abs(la - lb) / max(lb, 1e-30)
+    counts = bool(np.array_equal(gpu_normal.reshape(height, width, 4)[rows, :, 3],
+                                 oracle_acc.normal.reshape(height, width, 4)[rows, :, 3]))
+    return {"rows": int(len(rows)), "pixels": int(len(rows) * width), "rel_mse": float(f"{rel:.3e}"),
+            "luma_rel": float(f"{luma:.3e}"), "sample_counts_equal": counts,
+            "pass": bool(rel <= 1e-3 and luma <= 0.005 and counts),
+            "bars": "relMSE <= 1e-3, mean luminance within 0.5 %, same per-pixel sample counts"}
 
 
 def workload_desc(name, host, spp):
@@ -349,7 +376,12 @@ def run_b200(args):
     # The CPU baseline and the single-GPU batched and served forms run at N=1.
     if world == 1:
         try:
-            result["cpu_baseline"] = cpu_baseline(host, spp, args.cpu_seconds)
+            keep = {}
+            result["cpu_baseline"] = cpu_baseline(host, spp, args.cpu_seconds, keep)
+            # The oracle rows double as the parity check of the timed image
+            # (the last timed step's accumulation, same seed and spp).
+            result["parity"] = row_parity(acc.color.cpu().numpy(), acc.normal.cpu().numpy(), keep["acc"],
+                                          keep["rows"], host.width, host.height)
         except Exception as exc:
             result["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     if not args.no_batch and world == 1:
@@ -379,7 +411,7 @@ def e2e_context(host, spp, steps):
     h2d = (b.bvh_vec4_count * 16 + b.instance_count * 160 + b.attribute_words * 4 + b.material_count * 416
            + b.env_width * b.env_height * 16 + (b.env_width + 2) * (b.env_height + 1) * 8
            + b.light_sampling_texels * 16 + 32 * 2177 * 4 + b.lights_count * 96)
-    d2h = host.width * host.height * 16 * 2
+    d2h = host.width * host.height * 16  # read_pixels: one averaged f32 RGBA image
     out = np.empty((host.height, host.width, 4), np.float32)
     ctx.commit(host)
     ctx.render(1)

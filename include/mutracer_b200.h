@@ -556,10 +556,32 @@ typedef struct mt_job_snapshot {
   uint32_t requested_samples, submitted_samples, completed_samples, base_samples;
 } mt_job_snapshot;
 
+/* mutracer-status.h:68 */
+typedef enum mt_backend { MT_BACKEND_SOFTWARE = 0, MT_BACKEND_HWRT = 1 } mt_backend;
+/* mutracer-context.h:73 (native/host/src/context.rs:697-716).  backend is
+ * MT_BACKEND_SOFTWARE or MT_BACKEND_HWRT (the mt_context_create default);
+ * other values return MT_ERROR_INVALID_ARGUMENT, no CUDA device
+ * MT_ERROR_UNAVAILABLE.  B200 has no ray-tracing cores: every context
+ * traverses in software (the CUDA kernels), whichever backend is asked for. */
+int32_t mt_context_create_with_backend(uint32_t backend, mt_context *output, char *error,
+                                       size_t capacity);
+/* mutracer-context.h:79 (context.rs:3516-3555).  After a commit: *active is
+ * the backend used (always MT_BACKEND_SOFTWARE) and `reason` (caller storage,
+ * reason_capacity >= 1, always NUL terminated) says why it differs from an
+ * HWRT request, or is empty.  NULL outputs return MT_ERROR_INVALID_ARGUMENT;
+ * no healthy committed scene MT_ERROR_INVALID_STATE. */
+int32_t mt_context_backend(mt_context handle, uint32_t *active, char *reason, size_t reason_capacity,
+                           char *error, size_t capacity);
 /* mutracer-context.h:77 */
 int32_t mt_context_create(mt_context *output, char *error, size_t capacity);
-/* mutracer-context.h:81 */
+/* mutracer-context.h:81: also cancels a commit in preparation. */
 int32_t mt_context_destroy(mt_context handle, char *error, size_t capacity);
+/* mutracer-context.h:87 (context.rs:1409-1424).  Idempotent: a commit in
+ * preparation on another thread returns MT_ERROR_CANCELLED after its current
+ * preparation step (descriptor decode and buffer building, or the start of
+ * publication) and keeps the previous scene; without one it has no effect.
+ * A second commit while one is in preparation returns MT_ERROR_INVALID_STATE. */
+int32_t mt_context_cancel_commit(mt_context handle, char *error, size_t capacity);
 /* mutracer-context.h:101 */
 int32_t mt_render_settings_default(mt_render_settings *output);
 /* mutracer-context.h:91 (commit) and :102-103 (commit_with_settings): the
@@ -570,10 +592,11 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *bundl
 /* mutracer-context.h:94 and :132-133: commit a scene descriptor v8 (the
  * byte layout of native/docs/scene-format.md).  A malformed descriptor returns
  * MT_ERROR_INVALID_ARGUMENT with a message naming the problem; a valid one
- * that uses a feature this build does not render (texture maps, material
- * graphs, IES profiles, background maps, vertex colors, multi-material
- * meshes, partial opacity, bevel) returns
- * MT_ERROR_UNAVAILABLE naming the feature.  Either way the previously
+ * that uses a feature this build does not render (displacement, anisotropy
+ * and coat-normal maps, UDIM sets, textures the atlas would downscale,
+ * material graphs, IES profiles, rect-light textures, background maps,
+ * bevel, shadow-catcher and unlit materials, alpha in a dispersive scene)
+ * returns MT_ERROR_UNAVAILABLE naming the feature.  Either way the previously
  * committed scene stays.  commit uses mt_render_settings_default. */
 int32_t mt_context_commit(mt_context handle, const uint8_t *input, size_t length, char *error,
                           size_t capacity);
@@ -592,9 +615,21 @@ int32_t mt_context_wait(mt_context handle, uint32_t timeout_ms, char *error, siz
 int32_t mt_context_info(mt_context handle, mt_context_snapshot *info, char *error,
                         size_t capacity);
 /* mutracer-context.h:114-115: f32 RGBA, bottom row first, divided by the
- * per-pixel completed sample count. pixels=NULL,size=0 queries the size. */
+ * per-pixel completed sample count. pixels=NULL,size=0 queries the size.
+ * Checked in the reference's order: NULL written, unknown handle, no healthy
+ * scene, an active job (MT_ERROR_INVALID_STATE), unknown kind, no completed
+ * samples (MT_ERROR_INVALID_STATE), then the size query and destination. */
 int32_t mt_context_read_pixels(mt_context handle, uint32_t kind, void *pixels, size_t size,
                                size_t *written, char *error, size_t capacity);
+/* mutracer-debug.h:24-25 (debug and validation only, as in the reference):
+ * commits the descriptor into a fresh context with the default settings
+ * (Sobol, seed 12345, 6 bounces), renders `samples` (1..16384) samples and
+ * writes render.rgba32f, normal.rgba32f, albedo.rgba32f (little-endian f32
+ * RGBA, bottom row first), render.png (Reinhard + sRGB preview) and
+ * result.json into output_directory.  A rejected descriptor returns the
+ * commit's status; MT_ERROR_BUSY while another probe runs. */
+int32_t mt_probe_render_scene(const uint8_t *input, size_t length, const char *output_directory,
+                              uint32_t samples, char *error, size_t error_capacity);
 /* mutracer-context.h:181-185 */
 int32_t mt_context_submit(mt_context handle, uint32_t additional_samples, mt_render_job *job,
                           char *error, size_t capacity);

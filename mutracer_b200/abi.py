@@ -42,6 +42,8 @@ MTC_ENERGY_LUT_HEIGHT = 2177
 MTC_REGROUP_OFF = 0xFFFFFFFF
 MTC_BATCH_NOALLOC_MAX_JOBS = 64
 MTC_BATCH_STATUS_GUARD_EXHAUSTED = 1
+MT_BACKEND_SOFTWARE = 0
+MT_BACKEND_HWRT = 1
 
 
 class MtError(RuntimeError):
@@ -265,6 +267,11 @@ def _declare(lib):
         "mtp_env_distribution": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P]),
         "mt_render_settings_default": (C.c_int32, [C.POINTER(RenderSettings)]),
         "mt_context_create": (C.c_int32, [C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]),
+        "mt_context_create_with_backend": (C.c_int32, [C.c_uint32, C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]),
+        "mt_context_backend": (C.c_int32, [C.c_uint64, C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t, C.c_char_p,
+                                           C.c_size_t]),
+        "mt_context_cancel_commit": (C.c_int32, [C.c_uint64, C.c_char_p, C.c_size_t]),
+        "mt_probe_render_scene": (C.c_int32, [P, C.c_size_t, C.c_char_p, C.c_uint32, C.c_char_p, C.c_size_t]),
         "mt_context_destroy": (C.c_int32, [C.c_uint64, C.c_char_p, C.c_size_t]),
         "mt_context_commit_bundle": (C.c_int32, [C.c_uint64, C.POINTER(SceneBundle), C.POINTER(RenderSettings),
                                                  C.c_char_p, C.c_size_t]),

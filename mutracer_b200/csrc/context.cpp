@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -16,6 +17,9 @@
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <sys/stat.h>
+#include <cerrno>
 
 #include "../../include/mutracer_b200.h"
 #include "mtp_api.h"
@@ -86,7 +90,11 @@ struct Context {
   uint32_t samples = 0;  // completed samples
   bool failed = false;
   uint32_t lastCommit = MT_COMMIT_NONE;
+  uint32_t backend = MT_BACKEND_SOFTWARE;  // requested at creation
   std::unique_ptr<Job> job;
+  // A commit in preparation, and a cancellation request for it
+  // (mt_context_cancel_commit); both are read without the context lock.
+  std::atomic<bool> committing{false}, cancelCommit{false};
   ~Context() {
     if (stream) cudaStreamSynchronize(stream);
     scene.reset();
@@ -122,6 +130,35 @@ int32_t failContext(Context &c, cudaError_t e, char *error, size_t capacity) {
   setError(error, capacity, std::string("CUDA failure: ") + cudaGetErrorString(e));
   cudaGetLastError();
   return MT_ERROR_CONTEXT_FAILED;
+}
+
+// Marks a commit in preparation for its lifetime (mutracer-context.h:86-88,
+// 114-119): a second commit meanwhile is refused, and a cancellation request
+// made during it is seen at its next preparation step.
+class CommitGuard {
+ public:
+  explicit CommitGuard(Context &c) : c_(c) {
+    bool expected = false;
+    owned_ = c.committing.compare_exchange_strong(expected, true);
+    if (owned_) c.cancelCommit.store(false);
+  }
+  ~CommitGuard() {
+    if (owned_) {
+      c_.cancelCommit.store(false);
+      c_.committing.store(false);
+    }
+  }
+  bool owned() const { return owned_; }
+
+ private:
+  Context &c_;
+  bool owned_ = false;
+};
+
+int32_t commitCancelled(Context &c, char *error, size_t capacity) {
+  if (!c.cancelCommit.load()) return MT_OK;
+  setError(error, capacity, "commit cancelled; the previous scene is kept");
+  return MT_ERROR_CANCELLED;
 }
 
 uint32_t logSpp(uint32_t maxSamples) {
@@ -177,64 +214,12 @@ int32_t renderBlocking(Context &c, uint32_t samples) {
   return mtc_stream_run(table.data(), 1, &cfg, r.stream.ptr, nullptr, c.stream);
 }
 
-}  // namespace
-
-extern "C" {
-
-int32_t mt_render_settings_default(mt_render_settings *o) {
-  if (!o) return MT_ERROR_INVALID_ARGUMENT;
-  std::memset(o, 0, sizeof(*o));
-  o->struct_size = sizeof(mt_render_settings);
-  o->sampling_pattern = MT_SAMPLING_SOBOL;
-  o->seed = 12345;
-  o->max_samples = 64;
-  o->bounces = 6;
-  o->direct_light_candidates = 2;
-  o->bevel_samples = 8;
-  o->sample_sequence_offset = 0;
-  o->clamping = 0.0;
-  o->transmissive_output_alpha_min = 1.0;
-  return MT_OK;
-}
-
-int32_t mt_context_create(mt_context *output, char *error, size_t capacity) {
-  if (!output) { setError(error, capacity, "output is NULL"); return MT_ERROR_INVALID_ARGUMENT; }
-  int count = 0;
-  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
-    cudaGetLastError();
-    setError(error, capacity, "no CUDA device");
-    return MT_ERROR_UNAVAILABLE;
-  }
-  auto c = std::make_shared<Context>();
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->event, cudaEventDisableTiming) != cudaSuccess) {
-    cudaGetLastError();
-    setError(error, capacity, "stream creation failed");
-    return MT_ERROR_UNAVAILABLE;
-  }
-  std::lock_guard<std::mutex> g(gRegistry);
-  c->handle = gNextHandle++;
-  gContexts[c->handle] = c;
-  *output = c->handle;
-  return MT_OK;
-}
-
-int32_t mt_context_destroy(mt_context handle, char *error, size_t capacity) {
-  auto c = findContext(handle);
-  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
-  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
-  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
-  if (activeJob(*c)) { setError(error, capacity, "active render job: cancel/poll it first"); return MT_ERROR_INVALID_STATE; }
-  expireJob(*c);
-  std::lock_guard<std::mutex> g(gRegistry);
-  gContexts.erase(handle);
-  return MT_OK;
-}
-
-int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, const mt_render_settings *settings,
-                                 char *error, size_t capacity) {
-  auto c = findContext(handle);
-  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+// The publication step of every commit: validates the bundle, uploads it
+// into the context's (reused) device buffers and restarts accumulation.  A
+// cancellation requested before the first buffer is touched keeps the old
+// scene; once uploads begin, the commit completes.
+int32_t commitBundle(const std::shared_ptr<Context> &c, const mt_scene_bundle *b,
+                     const mt_render_settings *settings, char *error, size_t capacity) {
   if (!b || b->struct_size != sizeof(mt_scene_bundle)) { setError(error, capacity, "bundle struct_size"); return MT_ERROR_INVALID_ARGUMENT; }
   if (settings && settings->struct_size != sizeof(mt_render_settings)) { setError(error, capacity, "settings struct_size"); return MT_ERROR_INVALID_ARGUMENT; }
   if (b->width == 0 || b->height == 0 || b->width > 16384 || b->height > 16384 || !b->bvh || !b->instances ||
@@ -258,6 +243,7 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   }
   std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
   if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (int32_t st = commitCancelled(*c, error, capacity)) return st;
   // The previous job expires and nothing may still read the buffers that the
   // new scene reuses.
   expireJob(*c);
@@ -329,16 +315,192 @@ int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, co
   return MT_OK;
 }
 
+// ---------------------------------------------------------------- probe
+// Output files of mt_probe_render_scene (native/host/src/lib.rs:2227-2290):
+// the linear images as little-endian f32 RGBA, bottom row first, a Reinhard +
+// sRGB 8-bit preview PNG (top row first) and a small result.json.
+bool makeDirectories(const std::string &path) {
+  std::string part;
+  for (size_t i = 0; i <= path.size(); i++) {
+    if (i == path.size() || path[i] == '/') {
+      if (!part.empty() && mkdir(part.c_str(), 0777) != 0 && errno != EEXIST) return false;
+    }
+    if (i < path.size()) part.push_back(path[i]);
+  }
+  return true;
+}
+
+bool writeFile(const std::string &path, const void *data, size_t n) {
+  FILE *f = std::fopen(path.c_str(), "wb");
+  if (!f) return false;
+  bool ok = std::fwrite(data, 1, n, f) == n;
+  return std::fclose(f) == 0 && ok;
+}
+
+uint32_t crc32(const uint8_t *p, size_t n, uint32_t crc = 0) {
+  crc = ~crc;
+  for (size_t i = 0; i < n; i++) {
+    crc ^= p[i];
+    for (int k = 0; k < 8; k++) crc = (crc >> 1) ^ (0xedb88320u & (0u - (crc & 1u)));
+  }
+  return ~crc;
+}
+
+// An RGB8 PNG whose zlib stream uses stored (uncompressed) deflate blocks.
+std::vector<uint8_t> encodePng(const std::vector<uint8_t> &rgb, uint32_t width, uint32_t height) {
+  std::vector<uint8_t> raw;
+  raw.reserve(size_t(height) * (width * 3 + 1));
+  for (uint32_t y = 0; y < height; y++) {
+    raw.push_back(0);  // filter: none
+    raw.insert(raw.end(), rgb.begin() + size_t(y) * width * 3, rgb.begin() + size_t(y + 1) * width * 3);
+  }
+  std::vector<uint8_t> z = {0x78, 0x01};
+  uint32_t a = 1, b = 0;
+  for (uint8_t v : raw) { a = (a + v) % 65521u; b = (b + a) % 65521u; }
+  for (size_t at = 0; at < raw.size() || at == 0; at += 65535) {
+    size_t n = std::min<size_t>(65535, raw.size() - at);
+    z.push_back(at + n >= raw.size() ? 1 : 0);
+    z.push_back(uint8_t(n)); z.push_back(uint8_t(n >> 8));
+    z.push_back(uint8_t(~n)); z.push_back(uint8_t(~n >> 8));
+    z.insert(z.end(), raw.begin() + at, raw.begin() + at + n);
+    if (raw.empty()) break;
+  }
+  uint32_t adler = (b << 16) | a;
+  for (int k = 3; k >= 0; k--) z.push_back(uint8_t(adler >> (8 * k)));
+  std::vector<uint8_t> png = {0x89, 'P', 'N', 'G', 0x0d, 0x0a, 0x1a, 0x0a};
+  auto chunk = [&](const char *type, const std::vector<uint8_t> &data) {
+    uint32_t n = uint32_t(data.size());
+    for (int k = 3; k >= 0; k--) png.push_back(uint8_t(n >> (8 * k)));
+    std::vector<uint8_t> body(type, type + 4);
+    body.insert(body.end(), data.begin(), data.end());
+    png.insert(png.end(), body.begin(), body.end());
+    uint32_t c = crc32(body.data(), body.size());
+    for (int k = 3; k >= 0; k--) png.push_back(uint8_t(c >> (8 * k)));
+  };
+  std::vector<uint8_t> ihdr;
+  for (uint32_t v : {width, height})
+    for (int k = 3; k >= 0; k--) ihdr.push_back(uint8_t(v >> (8 * k)));
+  ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});  // 8-bit RGB, deflate, no filter method, no interlace
+  chunk("IHDR", ihdr);
+  chunk("IDAT", z);
+  chunk("IEND", {});
+  return png;
+}
+
+std::mutex gProbe;
+
+}  // namespace
+
+extern "C" {
+
+int32_t mt_render_settings_default(mt_render_settings *o) {
+  if (!o) return MT_ERROR_INVALID_ARGUMENT;
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = sizeof(mt_render_settings);
+  o->sampling_pattern = MT_SAMPLING_SOBOL;
+  o->seed = 12345;
+  o->max_samples = 64;
+  o->bounces = 6;
+  o->direct_light_candidates = 2;
+  o->bevel_samples = 8;
+  o->sample_sequence_offset = 0;
+  o->clamping = 0.0;
+  o->transmissive_output_alpha_min = 1.0;
+  return MT_OK;
+}
+
+int32_t mt_context_create(mt_context *output, char *error, size_t capacity) {
+  return mt_context_create_with_backend(MT_BACKEND_HWRT, output, error, capacity);
+}
+
+// mutracer-context.h:73 (context.rs:697-716, create_in :571-582): HWRT is
+// the reference's default request.  B200 has no ray-tracing cores, so every
+// context traverses in software (the CUDA kernels); mt_context_backend
+// reports that, with the reason when HWRT was asked for.
+int32_t mt_context_create_with_backend(uint32_t backend, mt_context *output, char *error, size_t capacity) {
+  if (!output) { setError(error, capacity, "output is NULL"); return MT_ERROR_INVALID_ARGUMENT; }
+  *output = 0;
+  if (backend > MT_BACKEND_HWRT) { setError(error, capacity, "Unknown native intersection backend"); return MT_ERROR_INVALID_ARGUMENT; }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    setError(error, capacity, "no CUDA device");
+    return MT_ERROR_UNAVAILABLE;
+  }
+  auto c = std::make_shared<Context>();
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->event, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    setError(error, capacity, "stream creation failed");
+    return MT_ERROR_UNAVAILABLE;
+  }
+  c->backend = backend;
+  std::lock_guard<std::mutex> g(gRegistry);
+  c->handle = gNextHandle++;
+  gContexts[c->handle] = c;
+  *output = c->handle;
+  return MT_OK;
+}
+
+// mutracer-context.h:79 mt_context_backend (context.rs:3516-3555): the
+// backend actually used for the committed scene, and why it differs from the
+// request.
+int32_t mt_context_backend(mt_context handle, uint32_t *active, char *reason, size_t reason_capacity, char *error,
+                           size_t capacity) {
+  if (!active || !reason || reason_capacity == 0) {
+    setError(error, capacity, "Invalid backend info output");
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (!c->scene || c->failed) { setError(error, capacity, "no healthy committed scene"); return MT_ERROR_INVALID_STATE; }
+  *active = MT_BACKEND_SOFTWARE;
+  setError(reason, reason_capacity,
+           c->backend == MT_BACKEND_HWRT ? "hardware ray tracing is unavailable on this device: software BVH traversal"
+                                         : "");
+  return MT_OK;
+}
+
+int32_t mt_context_destroy(mt_context handle, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
+  if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
+  if (activeJob(*c)) { setError(error, capacity, "active render job: cancel/poll it first"); return MT_ERROR_INVALID_STATE; }
+  if (c->committing.load()) c->cancelCommit.store(true);
+  expireJob(*c);
+  std::lock_guard<std::mutex> g(gRegistry);
+  gContexts.erase(handle);
+  return MT_OK;
+}
+
+int32_t mt_context_commit_bundle(mt_context handle, const mt_scene_bundle *b, const mt_render_settings *settings,
+                                 char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  CommitGuard guard(*c);
+  if (!guard.owned()) { setError(error, capacity, "another commit is in preparation"); return MT_ERROR_INVALID_STATE; }
+  return commitBundle(c, b, settings, error, capacity);
+}
+
+
 // mutracer-context.h:94 / :132-133: the scene descriptor v8 decoded (and
 // validated) on the host, then committed like a buffer bundle.  A rejected
 // descriptor leaves the previous scene committed.
 int32_t mt_context_commit_with_settings(mt_context handle, const uint8_t *input, size_t length,
                                         const mt_render_settings *settings, char *error, size_t capacity) {
-  if (!findContext(handle)) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
   if (settings && settings->struct_size != sizeof(mt_render_settings)) {
     setError(error, capacity, "settings struct_size");
     return MT_ERROR_INVALID_ARGUMENT;
   }
+  CommitGuard guard(*c);
+  if (!guard.owned()) { setError(error, capacity, "another commit is in preparation"); return MT_ERROR_INVALID_STATE; }
+  // Preparation on the calling thread: decode, validate and build the
+  // flattened buffers (BVHs, light tables) without touching the context.
   mtp::SceneHost scene;
   std::string message;
   int32_t st = mtp::decodeSceneDescriptor(input, length, scene, message);
@@ -346,6 +508,7 @@ int32_t mt_context_commit_with_settings(mt_context handle, const uint8_t *input,
     setError(error, capacity, message);
     return st;
   }
+  if ((st = commitCancelled(*c, error, capacity)) != MT_OK) return st;
   mt_render_settings defaults;
   if (!settings) {
     mt_render_settings_default(&defaults);
@@ -353,7 +516,17 @@ int32_t mt_context_commit_with_settings(mt_context handle, const uint8_t *input,
   }
   mt_scene_bundle bundle;
   mtp_scene_bundle(&scene, &bundle);
-  return mt_context_commit_bundle(handle, &bundle, settings, error, capacity);
+  return commitBundle(c, &bundle, settings, error, capacity);
+}
+
+// mutracer-context.h:87 mt_context_cancel_commit (context.rs:1409-1424):
+// idempotent; a commit in preparation returns MT_ERROR_CANCELLED at its next
+// preparation step and the previous scene stays; no commit, no effect.
+int32_t mt_context_cancel_commit(mt_context handle, char *error, size_t capacity) {
+  auto c = findContext(handle);
+  if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
+  if (c->committing.load()) c->cancelCommit.store(true);
+  return MT_OK;
 }
 
 int32_t mt_context_commit(mt_context handle, const uint8_t *input, size_t length, char *error, size_t capacity) {
@@ -434,19 +607,25 @@ int32_t mt_context_info(mt_context handle, mt_context_snapshot *info, char *erro
 
 int32_t mt_context_read_pixels(mt_context handle, uint32_t kind, void *pixels, size_t size, size_t *written,
                                char *error, size_t capacity) {
+  // Checks in the order of read_pixels_with (context.rs:1893-1960): the
+  // output length, the scene, an active job, the image kind, completed
+  // samples; then the size query and the destination.
+  if (!written) { setError(error, capacity, "Null pixel length output"); return MT_ERROR_INVALID_ARGUMENT; }
+  *written = 0;
   auto c = findContext(handle);
   if (!c) { setError(error, capacity, "unknown context"); return MT_ERROR_INVALID_HANDLE; }
-  if (!written || kind > MT_IMAGE_ALBEDO) { setError(error, capacity, "invalid argument"); return MT_ERROR_INVALID_ARGUMENT; }
   std::unique_lock<std::mutex> l(c->m, std::try_to_lock);
   if (!l) { setError(error, capacity, "context busy"); return MT_ERROR_BUSY; }
   if (!c->scene || c->failed) { setError(error, capacity, "no healthy committed scene"); return MT_ERROR_INVALID_STATE; }
+  if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
+  if (kind > MT_IMAGE_ALBEDO) { setError(error, capacity, "Unknown image kind"); return MT_ERROR_INVALID_ARGUMENT; }
+  if (c->samples == 0) { setError(error, capacity, "no completed samples"); return MT_ERROR_INVALID_STATE; }
   size_t px = size_t(c->scene->width) * c->scene->height;
   size_t need = px * 16;
   *written = need;
   if (!pixels && size == 0) return MT_OK;
-  if (activeJob(*c)) { setError(error, capacity, "active render job"); return MT_ERROR_INVALID_STATE; }
-  if (c->samples == 0) { setError(error, capacity, "no completed samples"); return MT_ERROR_INVALID_STATE; }
-  if (!pixels || size < need) { setError(error, capacity, "destination too small"); return MT_ERROR_BUFFER_TOO_SMALL; }
+  if (!pixels) { setError(error, capacity, "Null pixel destination"); return MT_ERROR_INVALID_ARGUMENT; }
+  if (size < need) { setError(error, capacity, "destination too small"); return MT_ERROR_BUFFER_TOO_SMALL; }
   // read_average (native/host/src/lib.rs:343-364): every value divided by the
   // completed sample count on the device, then one copy to the caller; a
   // non-finite value fails the read and marks the context failed.
@@ -566,6 +745,78 @@ int32_t mt_job_cancel(mt_render_job handle, char *error, size_t capacity) {
   if (!j || j->handle != handle) { setError(error, capacity, "unknown or expired job"); return MT_ERROR_INVALID_HANDLE; }
   if (j->state == MT_JOB_COMPLETE || j->state == MT_JOB_CANCELLED || j->state == MT_JOB_FAILED) return MT_OK;
   j->state = j->inflight ? MT_JOB_CANCELLING : MT_JOB_CANCELLED;
+  return MT_OK;
+}
+
+// mutracer-debug.h:24-25 (native/host/src/scene.rs:2506-2547), debug and
+// validation only: commits the descriptor into a fresh context with the
+// default settings (Sobol, seed 12345, 6 bounces), renders `samples`
+// samples, and writes render.rgba32f, normal.rgba32f, albedo.rgba32f,
+// render.png and result.json into output_directory (created if missing).
+int32_t mt_probe_render_scene(const uint8_t *input, size_t length, const char *output_directory, uint32_t samples,
+                              char *error, size_t capacity) {
+  if (!input || !output_directory) {
+    setError(error, capacity, "Null scene input or oversized descriptor");
+    return MT_ERROR_INVALID_ARGUMENT;
+  }
+  if (samples == 0 || samples > 16384) { setError(error, capacity, "Samples must be 1..16384"); return MT_ERROR_INVALID_ARGUMENT; }
+  std::unique_lock<std::mutex> l(gProbe, std::try_to_lock);
+  if (!l) { setError(error, capacity, "Native probe is already active"); return MT_ERROR_BUSY; }
+  mt_context ctx = 0;
+  int32_t st = mt_context_create_with_backend(MT_BACKEND_SOFTWARE, &ctx, error, capacity);
+  if (st != MT_OK) return st;
+  struct Destroy {
+    mt_context h;
+    ~Destroy() { mt_context_destroy(h, nullptr, 0); }
+  } destroy{ctx};
+  if ((st = mt_context_commit(ctx, input, length, error, capacity)) != MT_OK) return st;
+  if ((st = mt_context_render(ctx, samples, error, capacity)) != MT_OK) return st;
+  mt_context_snapshot info;
+  info.struct_size = sizeof(info);
+  if ((st = mt_context_info(ctx, &info, error, capacity)) != MT_OK) return st;
+  const std::string dir(output_directory);
+  if (!makeDirectories(dir)) { setError(error, capacity, "cannot create the output directory"); return MT_ERROR; }
+  const size_t n = size_t(info.width) * info.height * 4;
+  std::vector<float> image(n);
+  const char *names[] = {"render", "normal", "albedo"};
+  double lo = INFINITY, hi = -INFINITY, mean = 0.0;
+  std::vector<uint8_t> rgb;
+  for (uint32_t kind = MT_IMAGE_HDR; kind <= MT_IMAGE_ALBEDO; kind++) {
+    size_t written = 0;
+    if ((st = mt_context_read_pixels(ctx, kind, image.data(), n * 4, &written, error, capacity)) != MT_OK) return st;
+    if (!writeFile(dir + "/" + names[kind] + ".rgba32f", image.data(), n * 4)) {
+      setError(error, capacity, "cannot write the output files");
+      return MT_ERROR;
+    }
+    if (kind != MT_IMAGE_HDR) continue;
+    rgb.resize(size_t(info.width) * info.height * 3);
+    for (size_t p = 0; p < size_t(info.width) * info.height; p++) {
+      // Preview only: Reinhard plus sRGB, rows flipped to top-first.
+      size_t y = p / info.width, x = p % info.width, out = ((info.height - 1 - y) * info.width + x) * 3;
+      for (int ch = 0; ch < 3; ch++) {
+        float v = image[p * 4 + ch];
+        lo = std::min<double>(lo, v);
+        hi = std::max<double>(hi, v);
+        mean += v;
+        float linear = std::max(v, 0.0f) / (1.0f + std::max(v, 0.0f));
+        float srgb = linear <= 0.0031308f ? 12.92f * linear : 1.055f * std::pow(linear, 1.0f / 2.4f) - 0.055f;
+        rgb[out + ch] = uint8_t(std::min(std::max(srgb, 0.0f), 1.0f) * 255.0f + 0.5f);
+      }
+    }
+  }
+  std::vector<uint8_t> png = encodePng(rgb, info.width, info.height);
+  char json[1024];
+  int len = std::snprintf(json, sizeof(json),
+                          "{\n  \"width\": %u,\n  \"height\": %u,\n  \"samples\": %u,\n"
+                          "  \"intersectionBackend\": \"software BVH\",\n  \"rgbMin\": %.9g,\n"
+                          "  \"rgbMax\": %.9g,\n  \"rgbMean\": %.9g,\n"
+                          "  \"hdrLayout\": \"little-endian f32 RGBA, bottom row first; linear sample average\"\n}\n",
+                          info.width, info.height, samples, lo, hi,
+                          mean / (double(info.width) * info.height * 3.0));
+  if (!writeFile(dir + "/render.png", png.data(), png.size()) || !writeFile(dir + "/result.json", json, size_t(len))) {
+    setError(error, capacity, "cannot write the output files");
+    return MT_ERROR;
+  }
   return MT_OK;
 }
 

@@ -23,9 +23,10 @@
 // descriptors that use what this build does not render (displacement,
 // anisotropy and coat-normal maps, UDIM sets, textures the atlas would
 // downscale, alpha in spectral scenes, material
-// graphs, IES profiles, rect-light textures, background maps, meshes whose
-// triangles use several materials, bevel, shadow catchers, unlit materials,
-// the remaining material extensions) are refused with
+// graphs, IES profiles, rect-light textures, background maps and grounded
+// projection, anisotropic materials in scenes with vertex tangents or UVs,
+// bevel, shadow catchers, unlit materials, the remaining material
+// extensions) are refused with
 // MT_ERROR_UNAVAILABLE and a message naming the feature.
 //
 // Material textures (scene-records.ts:22-39 decodeTexture, MaterialData.ts

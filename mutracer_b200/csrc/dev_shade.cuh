@@ -1323,7 +1323,28 @@ struct SpectralState {
   // Texture coordinates of the current surface (kept from the last hit on a
   // miss, like the rest of the surface interaction) and of the primary one.
   SurfaceTexcoords tex, primaryTex;
+  // Shared spectral prefix (spectralPrefix.wgsl.ts): whether the current
+  // wavelength path still runs in RGB (spActive), whether the first one forked
+  // (spForkCall == 0), the channel and wavelength it forks to, and the loop
+  // state at the fork vertex (the flatPrefix checkpoint of
+  // rayTrace.compute.ts:145-148; the material is refetched from the surface).
+  bool spActive, spForked;
+  int spChannel;
+  float spWavelength;
+  Path forkPath;
+  SurfaceInteraction forkSi;
+  SurfaceTexcoords forkTex;
+  Aux forkAux;
+  int forkDepth, forkEvent;
+  bool forkIgnored, forkOpaque;
+  uint4 forkS0;
+  uint32_t forkHashed, forkBounce;
 };
+
+// spDisperses (spectralPrefix.wgsl.ts:29-31).
+MTD bool spDisperses(const Material &ma) {
+  return ma.transmissionDispersionScale > 0.0f && ma.specularIor != 1.0f;
+}
 
 // The alpha-split integrator runs for RGB scenes with a non-opaque material.
 MTD bool alphaSplit(const JobData &J) { return (J.s.flags & MTC_SCENE_HAS_ALPHA) && !isSpectral(J); }
@@ -1403,6 +1424,8 @@ static __device__ __noinline__ void beginSample(Ctx &c, uint32_t x, uint32_t y, 
   }
   if (isSpectral(J)) {
     sp.primaryReady = false;
+    sp.spActive = false;
+    sp.spForked = false;
     sp.primaryAux = {v3(0.0f), v3(0.0f), false};
     sp.cameraRay = cam;
     sp.wavelengthIndex = 0;
@@ -1581,8 +1604,13 @@ MTD bool finishAlphaSplit(const JobData &J, PathSample &ps, SpectralState &sp) {
 // its extension ray (if any) has been traced: at event 0 the first wavelength
 // path resolves and keeps the primary vertex, and every wavelength path
 // restarts there with its own wavelength, Cauchy IOR and the sampler state
-// saved after the wavelength draw.  Returns true when the current wavelength
-// path has ended (finishWavelength then decides whether the sample has).
+// saved after the wavelength draw.  With three wavelengths the path prefix is
+// shared (unless MTC_SCENE_SPECTRAL_INDEPENDENT): the first wavelength path
+// runs in RGB until its first dispersive transmissive vertex past the primary
+// one, saves its state there and forks; the later wavelength paths resume at
+// that vertex instead of the camera (:1001-1019).  Returns true when the
+// current wavelength path has ended (finishWavelength then decides whether
+// the sample has).
 static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, SpectralState &sp,
                                                       const TraversalHit &h) {
   Path &path = ps.path;
@@ -1590,8 +1618,15 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
   const mtc_trace_uniform &u = c.J.u;
   const int bounceLimit = max(u.bounces, 0);
   const int eventLimit = min(bounceLimit * 3, 20);
-  const int event = ps.event;
+  int event = ps.event;
   const bool singleWavelength = u.dispersion_wavelengths == 1;
+  const bool spEnabled = !singleWavelength && !(c.J.s.flags & MTC_SCENE_SPECTRAL_INDEPENDENT);
+  auto spFork = [&]() {  // spectralPrefix.wgsl.ts:32-36
+    sp.spActive = false;
+    path.li = spectralFilter(path.li, sp.spChannel);
+    si.spectralChannel = sp.spChannel;
+    si.wavelength = sp.spWavelength;
+  };
   Material ma;
   if (!reusesPrimary(c.J, ps, sp.primaryReady)) {
     si.hit = false;
@@ -1639,6 +1674,11 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
       int channel = singleWavelength ? sp.heroWavelengthIndex : sp.wavelengthIndex;
       si.spectralChannel = channel + 1;
       si.wavelength = spectrumCameraWavelength(uint32_t(channel), sp.wavelengthSample);
+      // spBegin (spectralPrefix.wgsl.ts:22-27)
+      sp.spChannel = channel + 1;
+      sp.spWavelength = si.wavelength;
+      sp.spActive = spEnabled && !spDisperses(ma);
+      if (sp.spActive) si.spectralChannel = 0;
       ma.specularIor = cauchyIor(si.wavelength, ma.specularIor, ma.transmissionDispersionScale,
                                  ma.dispersionAbbeNumber);
     }
@@ -1655,7 +1695,40 @@ static __device__ __noinline__ bool shadeStepSpectral(Ctx &c, PathSample &ps, Sp
     ps.depth = 0;
     ps.sampleIgnored = false;
     ps.isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
-  } else if (!path.abort) {
+    if (sp.spActive && sp.wavelengthIndex > 0 && sp.spForked) {
+      // Resume at the first wavelength path's fork vertex (:1010-1013).
+      path = sp.forkPath;
+      si = sp.forkSi;
+      sp.tex = sp.forkTex;
+      ps.aux = sp.forkAux;
+      ps.depth = sp.forkDepth;
+      event = sp.forkEvent;
+      ps.sampleIgnored = sp.forkIgnored;
+      ps.isNotTransparent = sp.forkOpaque;
+      c.smp.s0 = sp.forkS0;
+      c.smp.hashed = sp.forkHashed;
+      c.smp.bounce = sp.forkBounce;
+      getMaterial(c.J, si.materialIndex, si.instanceIndex, sp.tex.uv, sp.tex.uv1, sp.tex.vertexColor, ma);
+      spFork();
+    }
+  }
+  if (event > 0 && !path.abort) {
+    if (sp.spActive && ma.transmissionWeight > 0.001f && spDisperses(ma)) {
+      // The first dispersive transmission of the RGB prefix (:1015-1019).
+      sp.forkPath = path;
+      sp.forkSi = si;
+      sp.forkTex = sp.tex;
+      sp.forkAux = ps.aux;
+      sp.forkDepth = ps.depth;
+      sp.forkEvent = event;
+      sp.forkIgnored = ps.sampleIgnored;
+      sp.forkOpaque = ps.isNotTransparent;
+      sp.forkS0 = c.smp.s0;
+      sp.forkHashed = c.smp.hashed;
+      sp.forkBounce = c.smp.bounce;
+      sp.spForked = true;
+      spFork();
+    }
     completeVertex(c, path, ps.depth, si, ma, ps.sampleIgnored);
   }
   if (ps.isNotTransparent && event > bounceLimit) path.abort = true;
@@ -1673,6 +1746,14 @@ MTD bool finishWavelength(const JobData &J, PathSample &ps, SpectralState &sp) {
   if (J.u.dispersion_wavelengths == 1) {
     float scale = sp.dispersivePrimary ? 3.0f : 1.0f;
     ps.path.li = ps.path.li * scale;
+    return true;
+  }
+  if (sp.spActive) {
+    // The shared prefix never forked: its RGB path is the whole sample, with
+    // the guides of three identical wavelength paths (:1035-1041).
+    const V3 a = ps.aux.albedo, n = ps.aux.normal;
+    ps.aux.albedo = (a + a + a) / 3.0f;
+    ps.aux.normal = (n + n + n) / 3.0f;
     return true;
   }
   sp.color += ps.path.li;

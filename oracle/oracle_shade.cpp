@@ -1274,6 +1274,35 @@ static V4 integrateRgbAlpha(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
 // dispersionWavelengths == 1); each path restarts from the primary vertex with
 // the sampler state saved after the wavelength draw, refracts with a Cauchy
 // IOR at its wavelength, and its radiance is filtered to its RGB channel.
+// The path-prefix checkpoint of the shared-prefix spectral integrator
+// (rayTrace.compute.ts:145-148 flatPrefix, spectralPrefix.wgsl.ts:52-56): the
+// loop state at the fork vertex, and the sampler state (PCG words, hashed
+// counter, Sobol bounce) the wavelength paths after the first restart from.
+struct SpectralFlatPrefix {
+  Path path;
+  SurfaceInteraction si;
+  Material ma;
+  Aux aux;
+  int depth = 0, event = 0;
+  bool ignored = false, opaque = false;
+  u32 s0[4] = {0, 0, 0, 0};
+  u32 hashed = 0, bounce = 0;
+};
+
+// spDisperses (spectralPrefix.wgsl.ts:29-31).
+static inline bool spDisperses(const Material &ma) {
+  return ma.transmissionDispersionScale > 0.0f && ma.specularIor != 1.0f;
+}
+
+// The spectral integrator of rayTrace.compute.ts:947-1057.  With three
+// wavelengths it shares the path prefix (the reference's default,
+// WGPURayTracePass.ts:2113,2122): unless the primary surface disperses, the
+// first wavelength path runs in RGB (spectral channel 0) until it reaches a
+// dispersive transmissive surface past the primary vertex; there it saves
+// its state and forks (spFork), and the second and third wavelength paths
+// resume from that checkpoint with their own wavelength.  A path that never
+// forks is the whole sample.  MTC_SCENE_SPECTRAL_INDEPENDENT turns sharing
+// off: every wavelength path is spectral from the camera.
 static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
   SurfaceInteraction si, primarySi;
   Material ma, primaryMa;
@@ -1296,6 +1325,18 @@ static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
   float alpha = 0.0f;
   V3 guideAlbedo = v3(0.0f), guideNormal = v3(0.0f);
   bool allBlank = true;
+  // spectralPrefix.wgsl.ts:13-27 state.
+  const bool spEnabled = !singleWavelength && !(c.s.flags & MTC_SCENE_SPECTRAL_INDEPENDENT);
+  bool spActive = false;
+  int spChannel = 0, spForkCall = -1;
+  float spWavelength = 0.0f;
+  SpectralFlatPrefix spFlat;
+  auto spFork = [&]() {  // spectralPrefix.wgsl.ts:32-36
+    spActive = false;
+    path.li = spectralFilter(path.li, spChannel);
+    si.spectralChannel = spChannel;
+    si.wavelength = spWavelength;
+  };
   const int stepLimit = std::min((20 + 1) * 3, int(c.s.u->loop_unroll_guard * 16u));
   for (int step = 0; step < stepLimit; step++) {
     if (!primaryReady || (event != 0 && !path.abort)) {
@@ -1340,6 +1381,11 @@ static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
         int channel = singleWavelength ? heroWavelengthIndex : wavelengthIndex;
         si.spectralChannel = channel + 1;
         si.wavelength = spectrumCameraWavelength(u32(channel), wavelengthSample);
+        // spBegin (spectralPrefix.wgsl.ts:22-27)
+        spChannel = channel + 1;
+        spWavelength = si.wavelength;
+        spActive = spEnabled && !spDisperses(ma);
+        if (spActive) si.spectralChannel = 0;
         ma.specularIor = cauchyIor(si.wavelength, ma.specularIor, ma.transmissionDispersionScale,
                                    ma.dispersionAbbeNumber);
       }
@@ -1351,7 +1397,39 @@ static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
       depth = 0;
       sampleIgnored = false;
       isNotTransparent = ma.transmissionWeight < 0.001f && ma.subsurfaceWeight < 0.001f && ma.alpha > 0.99f;
-    } else if (!path.abort) {
+      if (spActive && wavelengthIndex > 0 && spForkCall == 0) {
+        // Resume at the first wavelength's fork vertex (:1010-1013).
+        path = spFlat.path;
+        si = spFlat.si;
+        ma = spFlat.ma;
+        wavelengthAux = spFlat.aux;
+        depth = spFlat.depth;
+        event = spFlat.event;
+        sampleIgnored = spFlat.ignored;
+        isNotTransparent = spFlat.opaque;
+        for (int k = 0; k < 4; k++) c.smp.s0[k] = spFlat.s0[k];
+        c.smp.hashed = spFlat.hashed;
+        c.smp.bounce = spFlat.bounce;
+        spFork();
+      }
+    }
+    if (event > 0 && !path.abort) {
+      if (spActive && ma.transmissionWeight > 0.001f && spDisperses(ma)) {
+        // The first dispersive transmission of the RGB prefix (:1015-1019).
+        spFlat.path = path;
+        spFlat.si = si;
+        spFlat.ma = ma;
+        spFlat.aux = wavelengthAux;
+        spFlat.depth = depth;
+        spFlat.event = event;
+        spFlat.ignored = sampleIgnored;
+        spFlat.opaque = isNotTransparent;
+        for (int k = 0; k < 4; k++) spFlat.s0[k] = c.smp.s0[k];
+        spFlat.hashed = c.smp.hashed;
+        spFlat.bounce = c.smp.bounce;
+        spForkCall = 0;
+        spFork();
+      }
       completeVertex(c, path, depth, si, ma, sampleIgnored);
     }
     if (isNotTransparent && event > bounceLimit) path.abort = true;
@@ -1361,6 +1439,13 @@ static V4 integrateSpectral(Ctx &c, V2 uv, const Ray &ray, Aux &outAux) {
         outAux = wavelengthAux;
         float scale = dispersivePrimary ? 3.0f : 1.0f;
         return {path.li.x * scale, path.li.y * scale, path.li.z * scale, path.alpha};
+      }
+      if (spActive) {
+        // No fork: the RGB path is the whole sample (:1035-1041).
+        outAux.isBlank = wavelengthAux.isBlank;
+        outAux.albedo = (wavelengthAux.albedo + wavelengthAux.albedo + wavelengthAux.albedo) / 3.0f;
+        outAux.normal = (wavelengthAux.normal + wavelengthAux.normal + wavelengthAux.normal) / 3.0f;
+        return {path.li.x, path.li.y, path.li.z, path.alpha};
       }
       color += path.li;
       alpha = std::max(alpha, path.alpha);

@@ -19,6 +19,8 @@ def _built_libraries():
     oracle_build.build()
     from mutracer_b200 import build as product_build
     product_build.build()
+    from oracle import ref_hosts
+    ref_hosts.build()
     yield
 
 

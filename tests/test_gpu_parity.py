@@ -88,6 +88,20 @@ def test_image_parity_cornell(cuda):
     assert np.array_equal(acc.normal[:, 3].cpu().numpy(), ref_acc.normal[:, 3])
 
 
+def test_image_parity_cornell_full_config(cuda):
+    """The small plain configuration at its full size: Cornell box 512x512,
+    64 spp, 8 bounces, Sobol seed 0, 16 SAH bins."""
+    host = scene.make_workload("cornell")
+    assert (host.width, host.height, host.bundle.uniform.bounces, host.bundle.uniform.sequence_seed) == \
+        (512, 512, 8, 0)
+    gpu, ref, acc, ref_acc = _render_pair(cuda, host, 64)
+    rel_mse, luma = _image_metrics(gpu, ref)
+    assert np.isfinite(gpu).all()
+    assert rel_mse <= REL_MSE_BAR, rel_mse
+    assert luma <= LUMA_BAR, luma
+    assert np.array_equal(acc.normal[:, 3].cpu().numpy(), ref_acc.normal[:, 3])
+
+
 def test_image_parity_instanced(cuda):
     host = scene.make_workload("instanced_spheres", width=160, height=90)
     gpu, ref, _, _ = _render_pair(cuda, host, 8)
@@ -108,23 +122,46 @@ def test_image_parity_zsobol_two_candidates(cuda):
     assert luma <= LUMA_BAR, luma
 
 
-@pytest.mark.parametrize("wavelengths", [3, 1])
-def test_image_parity_spectral_glass(cuda, wavelengths):
+@pytest.mark.parametrize("wavelengths,independent", [(3, False), (3, True), (1, False)])
+def test_image_parity_spectral_glass(cuda, wavelengths, independent):
     """Spectral integrator (rayTrace.compute.ts:947-1057): dispersive glass
-    spheres with homogeneous interiors, three wavelength paths per sample (or
-    one hero wavelength)."""
+    spheres with homogeneous interiors, three wavelength paths per sample
+    sharing their RGB prefix (the default), three independent ones, or one
+    hero wavelength."""
     host = scene.SceneHost("glass_spheres", 64, 48, 3, (8,))
     assert host.flags & abi.MTC_SCENE_SPECTRAL
-    if wavelengths == 1:
-        u = abi.TraceUniform.from_buffer_copy(host.uniform)
-        u.dispersion_wavelengths = 1
-        host.set_uniform(u)
+    u = abi.TraceUniform.from_buffer_copy(host.uniform)
+    u.dispersion_wavelengths = wavelengths
+    host.set_uniform(u, None, host.flags | (abi.MTC_SCENE_SPECTRAL_INDEPENDENT if independent else 0))
     gpu, ref, acc, ref_acc = _render_pair(cuda, host, 16)
     rel_mse, luma = _image_metrics(gpu, ref)
     assert np.isfinite(gpu).all()
     assert rel_mse <= REL_MSE_BAR, rel_mse
     assert luma <= LUMA_BAR, luma
     assert np.array_equal(acc.normal[:, 3].cpu().numpy(), ref_acc.normal[:, 3])
+
+
+def test_spectral_prefix_sharing_is_exact_on_the_device(cuda):
+    """The shared prefix (spectralPrefix.wgsl.ts) only skips work: the device
+    image is bit-identical to the independent-wavelength variant's, with
+    fewer extension and shadow rays (device counters)."""
+    import torch
+    out = {}
+    for independent in (False, True):
+        host = scene.SceneHost("glass_spheres", 56, 40, 5, (10,))
+        host.set_uniform(host.uniform, None,
+                         host.flags | (abi.MTC_SCENE_SPECTRAL_INDEPENDENT if independent else 0))
+        dev = scene.DeviceScene(host, cuda)
+        acc = trace.Accumulation(56, 40, cuda)
+        counters = trace.counters_tensor(cuda)
+        trace.trace_samples(dev, acc, 8, counters=counters)
+        torch.cuda.synchronize()
+        out[independent] = (acc, counters.cpu().numpy())
+    (a, ca), (b, cb) = out[False], out[True]
+    for x, y in ((a.color, b.color), (a.normal, b.normal), (a.albedo, b.albedo), (a.catcher, b.catcher)):
+        assert torch.equal(x, y)
+    assert ca[0] == cb[0]                          # path samples
+    assert ca[1] < 0.9 * cb[1] and ca[2] < cb[2]  # extension, shadow rays
 
 
 def test_refit_device_matches_host(cuda):
