@@ -337,6 +337,8 @@ def run_b200(args):
                          "form": "plain megakernel (mtc_trace_samples)" if args.form == "megakernel"
                          else f"wavefront (mtc_stream_run, {args.slots} slots)"},
               "mrays_per_s": round(rays_per_step / (ms_per_step / 1000.0) / 1e6, 2),
+              "mrays_per_s_extension": round(float(cnt[1]) / args.steps / (ms_per_step / 1000.0) / 1e6, 2),
+              "mrays_per_s_shadow": round(float(cnt[2]) / args.steps / (ms_per_step / 1000.0) / 1e6, 2),
               "gpu_launches": int(cnt[3]),
               "clocks": clocks.summary()}
     # End to end through the context API on every rank (its own replica); the

@@ -341,6 +341,53 @@ struct TraversalHit {
   int32_t triangleIndex, insIdx;
 };
 
+// Levels of the near path taken in one interior visit beyond the first.
+#ifndef MT_FUSED_LEVELS
+#define MT_FUSED_LEVELS 1
+#endif
+
+// The interior visit of getBVHTraverseCode at either level (intersect.wgsl.ts
+// :265-300, :439-624 for BVH2): box-test both children (boxes given), push
+// the nearer last (the `>` rule).  The node the reference pops next is the
+// child pushed last; when that child is an interior node (its header word
+// came with its box) its children are tested in the same visit instead of
+// going through the stack, for up to MT_FUSED_LEVELS more levels.  Nothing in
+// between could change tMax, so the boxes tested, their order and the stack
+// contents are those of one level per visit.  `base` is where node indices
+// start in the buffer (the BLAS base), `rightOffset` what a right pointer is
+// relative to (the BLAS offset; 0 in the TLAS).
+MTD void visitInterior(const float4 *bvh, int32_t base, int32_t rightOffset, bool fusable, V3 ro, V3 invDir,
+                       float tMax, int32_t left, int32_t right, float4 lmin, float4 lmax, float4 rmin, float4 rmax,
+                       int32_t *stack, int &top) {
+  for (int level = 0;; level++) {
+    const float d0 = intersectBox(ro, xyz(lmin), xyz(lmax), invDir, tMax);
+    const float d1 = intersectBox(ro, xyz(rmin), xyz(rmax), invDir, tMax);
+    int32_t first = right, second = left;
+    float df = d1, ds = d0;
+    float firstPtr = rmin.w, secondPtr = lmin.w;
+    if (d0 > d1) {
+      first = left; second = right;
+      df = d0; ds = d1;
+      firstPtr = lmin.w; secondPtr = rmin.w;
+    }
+    const bool pushFirst = df > 0.0f && top + 1 < MTC_MAX_STACK;
+    const bool pushSecond = ds > 0.0f && top + (pushFirst ? 2 : 1) < MTC_MAX_STACK;
+    // The node popped next: the second child if pushed, else the first.
+    const int32_t next = pushSecond ? second : first;
+    const int32_t nextPtr = asi(pushSecond ? secondPtr : firstPtr);
+    const bool fuse = fusable && level < MT_FUSED_LEVELS && (pushFirst || pushSecond) && nextPtr >= 0;
+    if (pushFirst && !(fuse && !pushSecond)) stack[++top] = first;
+    if (pushSecond && !fuse) stack[++top] = second;
+    if (!fuse) return;
+    left = next + 2;
+    right = nextPtr + rightOffset;
+    lmin = ld4(bvh + left + base);
+    lmax = ld4(bvh + left + 1 + base);
+    rmin = ld4(bvh + right + base);
+    rmax = ld4(bvh + right + 1 + base);
+  }
+}
+
 // getBVHTraverseCode, intersect.wgsl.ts:213-629 for the BVH2 layout.  With
 // `shadow` the first accepted hit ends the query (returns true).
 //
@@ -373,15 +420,8 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
     int32_t ptr = asi(r1.w);
     if (ptr >= 0) {
       int32_t left = tlasNode + 2, right = ptr;
-      float d0 = intersectBox(rayO, xyz(ld4(bvh + left)), xyz(ld4(bvh + left + 1)), invD, h.tMax);
-      float d1 = intersectBox(rayO, xyz(ld4(bvh + right)), xyz(ld4(bvh + right + 1)), invD, h.tMax);
-      if (d0 > d1) {
-        if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
-        if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
-      } else {
-        if (d1 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = right;
-        if (d0 > 0.0f && tlasTop + 1 < MTC_MAX_STACK) tlasStack[++tlasTop] = left;
-      }
+      visitInterior(bvh, 0, 0, true, rayO, invD, h.tMax, left, right, ld4(bvh + left), ld4(bvh + left + 1),
+                    ld4(bvh + right), ld4(bvh + right + 1), tlasStack, tlasTop);
       continue;
     }
     int32_t tlasCount = -ptr;
@@ -429,8 +469,10 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
           left = node + 2;
           right = p + blasOffset;
           if (p >= 0) {
-            d0 = intersectBox(o, xyz(ld4(bvh + left + blasBase)), xyz(ld4(bvh + left + 1 + blasBase)), linvD, h.tMax);
-            d1 = intersectBox(o, xyz(ld4(bvh + right + blasBase)), xyz(ld4(bvh + right + 1 + blasBase)), linvD, h.tMax);
+            visitInterior(bvh, blasBase, blasOffset, true, o, linvD, h.tMax, left, right, ld4(bvh + left + blasBase),
+                          ld4(bvh + left + 1 + blasBase), ld4(bvh + right + blasBase),
+                          ld4(bvh + right + 1 + blasBase), blasStack, blasTop);
+            continue;
           }
         }
         if (p >= 0) {
@@ -605,19 +647,9 @@ struct RayTraversal {
       }
     }
     if (interior) {
-      // Interior node at either level: box-test both children, push the
-      // nearer last (the `>` rule of intersect.wgsl.ts).
-      const V3 ro = blas ? o : rayO, id = blas ? linvD : invD;
-      float d0 = intersectBox(ro, xyz(lmin), xyz(lmax), id, h.tMax);
-      float d1 = intersectBox(ro, xyz(rmin), xyz(rmax), id, h.tMax);
-      int32_t first = right, second = left;
-      float df = d1, ds = d0;
-      if (d0 > d1) {
-        first = left; second = right;
-        df = d0; ds = d1;
-      }
-      if (df > 0.0f && top + 1 < MTC_MAX_STACK) stack[stackBase + (++top)] = first;
-      if (ds > 0.0f && top + 1 < MTC_MAX_STACK) stack[stackBase + (++top)] = second;
+      // Interior node at either level (one code path for both).
+      visitInterior(bvh, base, blas ? blasOffset : 0, !(kGpuLayout && blas && blasLayout == 2u), blas ? o : rayO,
+                    blas ? linvD : invD, h.tMax, left, right, lmin, lmax, rmin, rmax, stack + stackBase, top);
       if (blas) blasTop = top; else tlasTop = top;
       return false;
     }

@@ -564,9 +564,18 @@ bool streamShape(const mtc_stream_config *c, StreamShape &out) {
   return true;
 }
 
+// Every wavefront kernel asks for the largest L1 (no shared-memory carve-out
+// beyond the few words the sorts use): the traversal stacks, the spilled
+// shading state and the node reads all go through L1 (measured +1 % on the
+// 1080p instanced workload).
+cudaError_t carveout(const void *kernel) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+}
+
 cudaError_t gridFor(const void *kernel, uint32_t &grid) {
   int device = 0, sms = 0, perSm = 0;
-  cudaError_t e = cudaGetDevice(&device);
+  cudaError_t e = carveout(kernel);
+  if (e == cudaSuccess) e = cudaGetDevice(&device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kStreamThreads, 0);
   if (e != cudaSuccess) return e;
@@ -667,7 +676,11 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
       (e = gridFor((const void *)k_wf_shadow<false, false>, gShadow)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_finish, gFinish)) != cudaSuccess ||
       (e = gridFor((const void *)k_wf_regroup, gRegroup)) != cudaSuccess ||
-      (e = gridFor((const void *)k_wf_sort_rays, gSort)) != cudaSuccess)
+      (e = gridFor((const void *)k_wf_sort_rays, gSort)) != cudaSuccess ||
+      (e = carveout((const void *)k_wf_extend<true>)) != cudaSuccess ||
+      (e = carveout((const void *)k_wf_shadow<true, false>)) != cudaSuccess ||
+      (e = carveout((const void *)k_wf_shadow<false, true>)) != cudaSuccess ||
+      (e = carveout((const void *)k_wf_shadow<true, true>)) != cudaSuccess)
     return toStatus(e);
   if (shape.traversalCtasPerSm) {
     // Fewer resident traversal warps: a smaller local-memory footprint per SM.
