@@ -57,17 +57,21 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--mixed-jobs", type=int, default=64)
-    p.add_argument("--mixed-spp-divisor", type=int, default=16,
+    p.add_argument("--mixed-spp-divisor", type=int, default=4,
                    help="scale the mixed jobs' spp (log-uniform 4-256) down by this factor")
+    p.add_argument("--batch-all", action="store_true",
+                   help="also time the plain per-job launches and the persistent megakernel on the mixed jobs")
     p.add_argument("--deep-jobs", type=int, default=16)
     p.add_argument("--deep-spp-divisor", type=int, default=64,
                    help="scale the deep-transport jobs' 256 spp down by this factor")
     p.add_argument("--serve-requests", type=int, default=48)
-    p.add_argument("--serve-rate", type=float, default=20.0)
-    p.add_argument("--serve-scenes", type=int, default=8)
+    p.add_argument("--serve-rates", default="5,50,200", help="Poisson arrival rates (requests/s), one run each")
+    p.add_argument("--serve-scenes", type=int, default=32)
     p.add_argument("--serve-quantum", type=int, default=4, help="samples per job per served round")
-    p.add_argument("--serve-spp-divisor", type=int, default=16,
+    p.add_argument("--serve-spp-divisor", type=int, default=4,
                    help="scale the requests' target spp (uniform 16-128) down by this factor")
+    p.add_argument("--serve-budget-gb", type=float, default=24.0,
+                   help="HBM budget of the server: resident scenes + engine state + admitted accumulation")
     return p.parse_args()
 
 
@@ -535,12 +539,14 @@ def mixed_batch(args, dev_id):
     sb.set_jobs(jobs)
     res = {}
     ref = None
-    for name, fn in (("plain_per_sample", lambda: batch.run_plain(jobs, per_sample=True)),
-                     ("plain_per_job", lambda: batch.run_plain(jobs, per_sample=False)),
-                     ("persistent_graph", pb.replay),
-                     ("wavefront", sb.run)):
+    methods = [("plain_per_sample", lambda: batch.run_plain(jobs, per_sample=True), 1)]
+    if args.batch_all:
+        methods += [("plain_per_job", lambda: batch.run_plain(jobs, per_sample=False), 1),
+                    ("persistent_graph", pb.replay, 2)]
+    methods.append(("wavefront", sb.run, 2))
+    for name, fn, runs in methods:
         ms = []
-        for it in range(2):               # one warm-up, one timed
+        for it in range(runs):            # graph capture / first-run work in an untimed run; the last is timed
             zero()
             ms.append(_timed(fn, stream))
         res[name] = {"ms": round(ms[-1], 2), "mpaths_per_s": round(paths / ms[-1] / 1e3, 3)}
@@ -562,8 +568,9 @@ def mixed_batch(args, dev_id):
                              "traversal_ctas_per_sm": scfg.traversal_ctas_per_sm},
         "autotune_probe_ms": {k: round(v, 2) for k, v in timings.items()},
         "speedup_vs_plain_per_sample": round(res["plain_per_sample"]["ms"] / res["wavefront"]["ms"], 3),
-        "speedup_vs_plain_per_job": round(res["plain_per_job"]["ms"] / res["wavefront"]["ms"], 3),
     })
+    if args.batch_all:
+        res["speedup_vs_plain_per_job"] = round(res["plain_per_job"]["ms"] / res["wavefront"]["ms"], 3)
     del jobs
     torch.cuda.empty_cache()
     return res
@@ -677,25 +684,32 @@ def served_stream(args, dev_id):
     continuous batching; p50/p99 time-to-target-spp and sustained Mpaths/s."""
     import torch
     from mutracer_b200 import batch, scene, serve
+    t0 = time.perf_counter()
     pool = serve.build_pool(args.serve_scenes, seed=7, device=dev_id)
-    reqs = serve.poisson_requests(pool, args.serve_requests, args.serve_rate, seed=11,
-                                  spp_divisor=args.serve_spp_divisor)
-    budget = 12 * 1024 ** 3
+    build_s = time.perf_counter() - t0
+    budget = int(args.serve_budget_gb * 1024 ** 3)
     srv = serve.Server(pool, hbm_budget_bytes=budget, max_jobs=64, quantum=args.serve_quantum, device=dev_id)
     warm = serve.poisson_requests(pool, 4, 1000.0, seed=12, spp_divisor=args.serve_spp_divisor)
     srv.run(warm)
-    stats = srv.run(reqs)
+    rates = {}
+    for rate in (float(r) for r in args.serve_rates.split(",")):
+        reqs = serve.poisson_requests(pool, args.serve_requests, rate, seed=11, spp_divisor=args.serve_spp_divisor)
+        stats = srv.run(reqs)
+        stats["offered_s"] = reqs[-1].arrival
+        rates[f"{rate:g}"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in stats.items()
+                              if k != "resident_bytes"}
+    resident = srv.fixed_bytes
     srv.release()
-    stats.update({
-        "workload": f"{len(reqs)} requests, Poisson {args.serve_rate}/s, {len(pool)} resident scenes "
-                    f"({pool.device_bytes / 1e6:.0f} MB, 10k-8M tris), orbit cameras FOV 30-70, resolution from "
-                    f"{{256^2, 512^2, 1280x720, 1920x1080}}, target spp U[16,128] / {args.serve_spp_divisor}",
-        "hbm_budget_gb": budget / 1024 ** 3, "quantum_spp": args.serve_quantum, "max_jobs": 64,
+    return {
+        "rates_per_s": rates,
+        "workload": f"{args.serve_requests} requests per rate, Poisson arrivals, {len(pool)} resident scenes "
+                    f"({pool.device_bytes / 1e9:.2f} GB, 10k-8M instanced tris), orbit cameras FOV 30-70, "
+                    f"resolution from {{256^2, 512^2, 1280x720, 1920x1080}}, target spp U[16,128] / "
+                    f"{args.serve_spp_divisor}",
+        "hbm_budget_gb": args.serve_budget_gb, "resident_gb": round(resident / 1e9, 3),
+        "pool_build_s": round(build_s, 1), "quantum_spp": args.serve_quantum, "max_jobs": 64,
         "engine": "wavefront (mtc_stream_run per round)",
-    })
-    for k in ("mpaths_per_s", "p50_s", "p99_s", "mean_s", "device_seconds"):
-        stats[k] = round(stats[k], 4)
-    return stats
+    }
 
 
 def main():

@@ -200,6 +200,10 @@ class Batch(_JobTable):
             self.capture()
         self.graph.replay()
 
+    @property
+    def device_bytes(self):
+        return self.scratch.numel()
+
     def release(self):
         self.graph = None
 
@@ -222,6 +226,10 @@ class StreamBatch(_JobTable):
         abi.check(abi.lib().mtc_stream_run(C.c_void_p(self.table.data_ptr()), self.capacity,
                                            C.byref(self.stream_config), C.c_void_p(self.state.data_ptr()),
                                            C.c_void_p(self.counters.data_ptr()), _stream_ptr(stream)))
+
+    @property
+    def device_bytes(self):
+        return self.state.numel()
 
     def release(self):
         pass

@@ -123,16 +123,25 @@ def poisson_requests(pool, count, rate, seed=0, spp_range=(16, 128), resolutions
 
 
 class Server:
-    """Continuous-batching render server over a ScenePool."""
+    """Continuous-batching render server over a ScenePool.
 
-    def __init__(self, pool, hbm_budget_bytes, max_jobs=64, quantum=8, config=None, use_graph=True,
-                 engine="wavefront", stream_config=None, device="cuda"):
+    Admission is by HBM budget: the resident scenes and the engine's own
+    state (job tables, path slots and queues) are charged first, and a
+    request is admitted only while its accumulation buffers fit in what is
+    left, so the device never holds more than `hbm_budget_bytes` for the
+    pool, the engine and the admitted jobs together."""
+
+    def __init__(self, pool, hbm_budget_bytes=None, max_jobs=64, quantum=8, config=None, use_graph=True,
+                 engine="wavefront", stream_config=None, device="cuda", job_bytes=None):
         """engine "wavefront": each round is one mtc_stream_run over all
         admitted jobs; "persistent": each round replays the captured
         persistent-megakernel launch (two alternating tables, so the host
-        prepares round k+1 while round k runs)."""
+        prepares round k+1 while round k runs).  Give either the whole
+        budget (hbm_budget_bytes) or what is left for admitted jobs beyond
+        the resident scenes and engine state (job_bytes)."""
+        if (hbm_budget_bytes is None) == (job_bytes is None):
+            raise ValueError("give exactly one of hbm_budget_bytes and job_bytes")
         self.pool = pool
-        self.budget = int(hbm_budget_bytes)
         self.max_jobs = int(max_jobs)
         self.quantum = int(quantum)
         self.device = device
@@ -144,6 +153,12 @@ class Server:
             self.batches = [batch.Batch(max_jobs, config, device) for _ in range(2)]
         else:
             raise ValueError(f"engine {engine!r}")
+        # Resident scenes and engine state, charged before any request.
+        self.fixed_bytes = int(pool.device_bytes) + sum(int(b.device_bytes) for b in self.batches)
+        self.budget = int(hbm_budget_bytes) if job_bytes is None else self.fixed_bytes + int(job_bytes)
+        if self.fixed_bytes > self.budget:
+            raise ValueError(f"the resident scenes and engine state ({self.fixed_bytes} B) exceed the HBM budget "
+                             f"({self.budget} B)")
 
     def _bytes(self, req):
         return req.width * req.height * ACCUMULATION_BYTES_PER_PIXEL
@@ -155,7 +170,7 @@ class Server:
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()
         active = []
-        used = 0
+        used = self.fixed_bytes
         start = torch.cuda.Event(enable_timing=True)
         stream = torch.cuda.current_stream()
         torch.cuda.synchronize()
@@ -231,7 +246,7 @@ class Server:
             "requests": len(requests), "rounds": n_rounds, "paths": paths,
             "device_seconds": end, "mpaths_per_s": paths / end / 1e6,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "mean_s": float(lat.mean()),
+            "mean_s": float(lat.mean()), "resident_bytes": self.fixed_bytes,
         }
 
     def release(self):

@@ -73,7 +73,7 @@ def test_served_results_equal_alone(cuda):
         pool.add(sid, scene.SceneHost(kind, 32, 32, sid + 1, params))
     reqs = serve.poisson_requests(pool, 10, rate=400.0, seed=5, spp_range=(2, 9),
                                   resolutions=((24, 16), (40, 40), (13, 31)))
-    srv = serve.Server(pool, hbm_budget_bytes=3 * 40 * 40 * serve.ACCUMULATION_BYTES_PER_PIXEL, max_jobs=3,
+    srv = serve.Server(pool, job_bytes=3 * 40 * 40 * serve.ACCUMULATION_BYTES_PER_PIXEL, max_jobs=3,
                        quantum=2, device=cuda)
     stats = srv.run(reqs, keep_outputs=True)
     srv.release()
@@ -95,7 +95,7 @@ def test_served_results_equal_alone_both_engines(cuda, engine):
     pool.add(1, scene.SceneHost("glass_spheres", 32, 32, 2, (5,)))
     reqs = serve.poisson_requests(pool, 6, rate=300.0, seed=9, spp_range=(1, 7),
                                   resolutions=((20, 30), (33, 17)))
-    srv = serve.Server(pool, hbm_budget_bytes=1 << 30, max_jobs=4, quantum=3, engine=engine, device=cuda)
+    srv = serve.Server(pool, job_bytes=1 << 30, max_jobs=4, quantum=3, engine=engine, device=cuda)
     srv.run(reqs, keep_outputs=True)
     srv.release()
     for r in reqs:
@@ -110,13 +110,18 @@ def test_served_admission_respects_the_hbm_budget(cuda):
     pool.add(0, scene.SceneHost("cornell", 16, 16, 1))
     reqs = [serve.Request(i, 0, 64, 64, 3, 0.0) for i in range(6)]
     one = 64 * 64 * serve.ACCUMULATION_BYTES_PER_PIXEL
-    srv = serve.Server(pool, hbm_budget_bytes=2 * one, max_jobs=8, quantum=1, device=cuda)
+    srv = serve.Server(pool, job_bytes=2 * one, max_jobs=8, quantum=1, device=cuda)
+    # The resident scene and the engine's state are charged against the budget.
+    assert srv.fixed_bytes >= pool.device_bytes > 0 and srv.budget == srv.fixed_bytes + 2 * one
     stats = srv.run(reqs)
     srv.release()
     # At most two jobs fit at once, 3 samples each: 6 jobs need >= 9 rounds.
     assert stats["rounds"] >= 9
     with pytest.raises(RuntimeError):
-        serve.Server(pool, hbm_budget_bytes=one - 1, device=cuda).run([serve.Request(0, 0, 64, 64, 1, 0.0)])
+        serve.Server(pool, job_bytes=one - 1, device=cuda).run([serve.Request(0, 0, 64, 64, 1, 0.0)])
+    # A budget smaller than the resident scenes and engine state is refused.
+    with pytest.raises(ValueError):
+        serve.Server(pool, hbm_budget_bytes=pool.device_bytes, device=cuda)
 
 
 @pytest.mark.parametrize("slots,refill,regroup,sort", [(1024, 1, 1, 0), (1 << 16, 8, 1, 1), (4096, 32, 3, 1),
