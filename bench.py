@@ -51,8 +51,11 @@ def parse():
     p.add_argument("--form", default="wavefront", choices=["megakernel", "wavefront"],
                    help="engine of the headline step: the wavefront kernels (mtc_stream_run, the default, also "
                         "what mt_context_render runs) or the plain drop-in megakernel (mtc_trace_samples)")
-    p.add_argument("--slots", type=int, default=1 << 20, help="wavefront paths in flight")
+    p.add_argument("--slots", type=int, default=1 << 21, help="wavefront paths in flight")
     p.add_argument("--refill-lanes", type=int, default=0, help="wavefront traversal refill threshold (0: default)")
+    p.add_argument("--queue-trace", type=int, default=0,
+                   help="wavefront form: print the extension, shadow and finished-path counts of each of the first "
+                        "N event iterations of one run (runs stopped after 1..N iterations) and exit")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -267,6 +270,33 @@ def flush_l2(buf):
     buf.add_(1.0)
 
 
+def queue_trace(sb, counters, slots, iterations):
+    """Queue sizes of each event iteration of one wavefront run: the run is
+    repeated, stopped by its iteration limit after 1, 2, ... `iterations`
+    iterations, and the counter totals are differenced.  For an RGB
+    scene every queued extension ray is traced and every finished slot ends a
+    path, so the three counts are the queue lengths k_wf_extend (and
+    k_wf_shade), k_wf_shadow and k_wf_finish see in that iteration; they
+    normalise single-launch profiler captures to bytes per ray."""
+    import torch
+    from mutracer_b200 import abi
+    rows, last = [], [0, 0, 0]
+    for k in range(1, iterations + 1):
+        sb.stream_config = abi.StreamConfig.make(slots=slots, max_iterations=k)
+        counters.zero_()
+        try:
+            sb.run()
+        except abi.MtError as err:
+            if err.status != abi.MT_ERROR_TIMEOUT:
+                raise
+        torch.cuda.synchronize()
+        c = [int(x) for x in counters.cpu().tolist()[:3]]
+        rows.append({"iteration": k - 1, "extension": c[1] - last[1], "shadow": c[2] - last[2],
+                     "finished": c[0] - last[0]})
+        last = c
+    return {"queue_trace": rows, "slots": slots}
+
+
 def run_b200(args):
     import torch
     from mutracer_b200 import abi, scene, trace
@@ -293,6 +323,9 @@ def run_b200(args):
                                device=dev_id)
         sb.counters = counters
         sb.set_jobs([job])
+        if args.queue_trace:
+            print(json.dumps(queue_trace(sb, counters, args.slots, args.queue_trace)), flush=True)
+            return
 
         def step():
             acc.zero_()
@@ -502,7 +535,7 @@ def same_job_wavefront(dev, acc, spp, paths, dev_id, flush):
     ms = sum(times) / len(times)
     out = {"ms_per_step": round(ms, 2), "mpaths_per_s": round(paths / ms / 1e3, 3),
            "bit_identical_to_plain": bool(torch.equal(job.acc.color, plain)),
-           "config": "defaults: 1M slots, refill at 8 idle lanes, 8 steps per refill check, regroup every "
+           "config": "defaults: 2M slots, refill at 8 idle lanes, 8 steps per refill check, regroup every "
                      "iteration"}
     del sb, job
     return out

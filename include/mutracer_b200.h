@@ -449,14 +449,23 @@ mt_status mtc_batch_launch(const void *table, uint32_t capacity,
  * pixel until all of its samples are done, so outputs are bit-identical to
  * mtc_trace_samples and to mtc_trace_batch.  `table` is a HOST job table
  * written by mtc_batch_prepare for up to `capacity` jobs; `state` is device
- * memory of mtc_stream_state_bytes(capacity, config) bytes.  The call
- * enqueues the work on `stream` and returns once the queues have drained
- * (it waits on the stream); calls on one device are serialised.  No
- * counterpart in the reference. */
+ * memory of mtc_stream_state_bytes(capacity, config) bytes.  The event loop
+ * runs on the device: one CUDA graph whose WHILE node repeats an event
+ * iteration until the queues have drained or max_iterations iterations have
+ * run, so a run needs no host round trip after it is enqueued.
+ * mtc_stream_run enqueues the run on `stream` and waits for it (returning
+ * MT_ERROR_TIMEOUT when the iteration limit stopped it); mtc_stream_launch
+ * only enqueues it, and mtc_stream_status reports the outcome of the last run
+ * enqueued on `state` the same way (it waits on `stream`).  The table is
+ * uploaded with cudaMemcpyAsync on `stream`: a table in pinned memory must
+ * stay unchanged until the stream has passed the launch (pageable memory is
+ * read before the call returns).  One `state` buffer serves one run at a
+ * time.  No counterpart in the reference. */
 typedef struct mtc_stream_config {
   uint32_t struct_size;
-  uint32_t slots;                 /* paths in flight, 1024..2^25 (default 2^20) */
-  uint32_t iterations_per_check;  /* event iterations between queue polls (default 8) */
+  uint32_t slots;                 /* paths in flight, 1024..2^25 (default 2^21) */
+  uint32_t iterations_per_check;  /* accepted (0..256) and ignored: the device checks
+                                     the queue after every event iteration */
   uint32_t max_iterations;        /* MT_ERROR_TIMEOUT beyond this (default 2^20) */
   uint32_t refill_lanes;          /* idle lanes of a warp that trigger fetching new
                                      rays in the traversal kernels, 1..32 (default 8) */
@@ -476,6 +485,11 @@ size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config
 mt_status mtc_stream_run(const void *table, uint32_t capacity,
                          const mtc_stream_config *config, void *state,
                          mtc_counters *counters, void *stream);
+mt_status mtc_stream_launch(const void *table, uint32_t capacity,
+                            const mtc_stream_config *config, void *state,
+                            mtc_counters *counters, void *stream);
+mt_status mtc_stream_status(const void *state, uint32_t capacity,
+                            const mtc_stream_config *config, void *stream);
 
 /* No counterpart in the reference.  For callers that cannot let the library
  * allocate device memory (a host that owns a fixed device budget and its own

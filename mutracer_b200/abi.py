@@ -234,6 +234,8 @@ def _declare(lib):
         "mtc_average_output": (C.c_int32, [P, C.c_uint32, C.c_uint32, P, P, P]),
         "mtc_stream_state_bytes": (C.c_size_t, [C.c_uint32, C.POINTER(StreamConfig)]),
         "mtc_stream_run": (C.c_int32, [P, C.c_uint32, C.POINTER(StreamConfig), P, P, P]),
+        "mtc_stream_launch": (C.c_int32, [P, C.c_uint32, C.POINTER(StreamConfig), P, P, P]),
+        "mtc_stream_status": (C.c_int32, [P, C.c_uint32, C.POINTER(StreamConfig), P]),
         "mtc_batch_prepare": (C.c_int32, [C.POINTER(JobDesc), C.c_uint32, C.POINTER(BatchConfig), P,
                                            C.POINTER(C.c_uint32)]),
         "mtc_batch_launch": (C.c_int32, [P, C.c_uint32, C.POINTER(BatchConfig), P, P, P]),

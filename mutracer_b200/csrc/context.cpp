@@ -1,7 +1,8 @@
 // Persistent host API of native/include/mutracer-context.h:57-187 on CUDA:
 // contexts own device copies of a committed buffer bundle plus the four
-// accumulation buffers; render adds samples through mtc_trace_samples; jobs
-// are caller-polled with at most one batch in flight (a CUDA event), like
+// accumulation buffers; renders and job batches add samples through the
+// wavefront engine (mtc_trace_samples when its state cannot be allocated);
+// jobs are caller-polled with at most one batch in flight (a CUDA event), like
 // native/host/src/context.rs:2002-2256 (submit/poll_job/advance_job).
 #include <cuda_runtime.h>
 
@@ -77,6 +78,7 @@ struct Job {
   uint32_t state = MT_JOB_QUEUED;
   uint32_t requested = 0, submitted = 0, completed = 0, base = 0;
   uint32_t inflight = 0;
+  bool wavefront = false;  // the batch in flight runs in the wavefront engine
 };
 
 struct Context {
@@ -179,23 +181,31 @@ void applySettings(Context &c, const mt_render_settings &s) {
   c.uniform.zsobol_log_spp = logSpp(s.sampling_pattern == MT_SAMPLING_ZSOBOL ? std::max(1u, s.max_samples - 1) : s.max_samples);
 }
 
+mtc_stream_config streamConfig(size_t pixels) {
+  mtc_stream_config cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.struct_size = sizeof(cfg);
+  cfg.slots = uint32_t(std::max<size_t>(1024, std::min<size_t>(pixels, size_t(1) << 21)));
+  return cfg;
+}
+
 int32_t launch(Context &c, uint32_t samples) {
   mtc_outputs out{c.scene->color.ptr, c.scene->normal.ptr, c.scene->albedo.ptr, c.scene->catcher.ptr};
   return mtc_trace_samples(&c.scene->view, &c.camera, &c.uniform, &out, samples, nullptr, c.stream);
 }
 
-// Blocking renders run the same samples through the wavefront engine
-// (mtc_stream_run: queued traversal and material-regrouped shading), which
-// writes the same bits as mtc_trace_samples at about twice the throughput.
-// Path slots scale with the image, up to 2^20; the state buffer is kept with
-// the scene.  When it cannot be allocated the megakernel renders instead.
-int32_t renderBlocking(Context &c, uint32_t samples) {
+// Renders and job batches run their samples through the wavefront engine
+// (queued traversal and material-regrouped shading, its event loop on the
+// device), which writes the same bits as mtc_trace_samples at about twice the
+// throughput: mtc_stream_run for blocking renders, mtc_stream_launch for job
+// batches, which only enqueue.  Path slots scale with the image, up to 2^21;
+// the state buffer is kept with the scene.  When it cannot be allocated the
+// megakernel renders instead (*wavefront false).
+int32_t renderSamples(Context &c, uint32_t samples, bool wait, bool *wavefront) {
   SceneResources &r = *c.scene;
+  *wavefront = false;
   size_t px = size_t(r.width) * r.height;
-  mtc_stream_config cfg;
-  std::memset(&cfg, 0, sizeof(cfg));
-  cfg.struct_size = sizeof(cfg);
-  cfg.slots = uint32_t(std::max<size_t>(1024, std::min<size_t>(px, size_t(1) << 20)));
+  mtc_stream_config cfg = streamConfig(px);
   size_t bytes = mtc_stream_state_bytes(1, &cfg);
   if (bytes == 0 || r.stream.reserve(bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -211,7 +221,11 @@ int32_t renderBlocking(Context &c, uint32_t samples) {
   std::vector<char> table(mtc_batch_table_bytes(1));
   int32_t st = mtc_batch_prepare(&job, 1, nullptr, table.data(), nullptr);
   if (st != MT_OK) return st;
-  return mtc_stream_run(table.data(), 1, &cfg, r.stream.ptr, nullptr, c.stream);
+  *wavefront = true;
+  // The table is pageable host memory: the launch's upload has read it by
+  // the time the call returns.
+  return wait ? mtc_stream_run(table.data(), 1, &cfg, r.stream.ptr, nullptr, c.stream)
+              : mtc_stream_launch(table.data(), 1, &cfg, r.stream.ptr, nullptr, c.stream);
 }
 
 // The publication step of every commit: validates the bundle, uploads it
@@ -545,7 +559,8 @@ int32_t mt_context_render(mt_context handle, uint32_t additional, char *error, s
     return MT_ERROR_INVALID_ARGUMENT;
   }
   expireJob(*c);
-  int32_t st = renderBlocking(*c, additional);
+  bool wavefront = false;
+  int32_t st = renderSamples(*c, additional, true, &wavefront);
   if (st != MT_OK) { setError(error, capacity, "launch rejected"); return st; }
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return failContext(*c, e, error, capacity);
@@ -702,6 +717,19 @@ int32_t mt_job_poll(mt_render_job handle, uint32_t max_new_samples, char *error,
       j->inflight = 0;
       return failContext(*c, e, error, capacity);
     }
+    if (j->wavefront) {
+      // The batch has finished; its run drained every queue unless the
+      // iteration limit stopped it.
+      mtc_stream_config cfg = streamConfig(size_t(c->scene->width) * c->scene->height);
+      int32_t st = mtc_stream_status(c->scene->stream.ptr, 1, &cfg, c->stream);
+      if (st != MT_OK) {
+        j->state = MT_JOB_FAILED;
+        j->inflight = 0;
+        c->failed = true;
+        setError(error, capacity, "render batch did not complete");
+        return MT_ERROR_CONTEXT_FAILED;
+      }
+    }
     j->completed += j->inflight;
     c->samples += j->inflight;
     j->inflight = 0;
@@ -710,7 +738,7 @@ int32_t mt_job_poll(mt_render_job handle, uint32_t max_new_samples, char *error,
   if (j->state == MT_JOB_CANCELLING || j->state == MT_JOB_CANCELLED) { j->state = MT_JOB_CANCELLED; return MT_OK; }
   if (max_new_samples == 0) return MT_OK;
   uint32_t n = std::min(max_new_samples, j->requested - j->submitted);
-  int32_t st = launch(*c, n);
+  int32_t st = renderSamples(*c, n, false, &j->wavefront);
   if (st != MT_OK) { j->state = MT_JOB_FAILED; setError(error, capacity, "launch rejected"); return st; }
   cudaError_t e = cudaEventRecord(c->event, c->stream);
   if (e != cudaSuccess) { j->state = MT_JOB_FAILED; return failContext(*c, e, error, capacity); }

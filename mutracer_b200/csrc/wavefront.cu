@@ -40,6 +40,7 @@ struct Slot {
   ShadowQuery shadow;
   uint32_t job, x, y, left;  // pixel owned, samples still to start after the current one
 };
+static_assert(sizeof(Slot) % 16 == 0 && alignof(Slot) == 16, "slots keep their path sample 16-byte aligned");
 
 // Queue state at the start of the stream state buffer (256 bytes).
 struct StreamQueues {
@@ -49,7 +50,15 @@ struct StreamQueues {
   uint32_t finishCount;
   uint32_t extendNext;       // next extension ray to hand to a lane
   uint32_t shadowNext;       // next shadow ray to hand to a lane
-  uint32_t _pad[57];
+  // Event-iteration state, advanced on the device by k_wf_continue: the
+  // parity of the extension queue being traced, whether this iteration
+  // regroups the shading queue, iterations completed, and set when the
+  // iteration limit stopped a run with rays still queued.
+  uint32_t cur;
+  uint32_t regroup;
+  uint32_t iterations;
+  uint32_t limitHit;
+  uint32_t _pad[53];
 };
 static_assert(sizeof(StreamQueues) == 256, "queue header size");
 
@@ -83,6 +92,24 @@ constexpr uint32_t kStreamThreads = 128;
 
 __device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
 
+// Copies a path sample between its slot (16-byte aligned: slots start on
+// 256-byte boundaries and a Slot is a multiple of 16 bytes) and a 16-byte
+// aligned register copy with 128-bit accesses, the tail in 32-bit words:
+// a quarter of the load/store instructions of a field-by-field copy, whose
+// 4-byte accesses each touch one sector per lane of this array of structs.
+__device__ __forceinline__ void copyPathSample(PathSample &dst, const PathSample &src) {
+  constexpr int kWide = int(sizeof(PathSample) / 16), kTail = int(sizeof(PathSample) % 16) / 4;
+  static_assert(sizeof(PathSample) % 4 == 0, "path sample words");
+  const uint4 *s = reinterpret_cast<const uint4 *>(&src);
+  uint4 *d = reinterpret_cast<uint4 *>(&dst);
+#pragma unroll
+  for (int i = 0; i < kWide; i++) d[i] = s[i];
+  const uint32_t *st = reinterpret_cast<const uint32_t *>(s + kWide);
+  uint32_t *dt = reinterpret_cast<uint32_t *>(d + kWide);
+#pragma unroll
+  for (int i = 0; i < kTail; i++) dt[i] = st[i];
+}
+
 // Appends `value` to a queue with one atomic per converged group of lanes.
 __device__ __forceinline__ void enqueue(uint32_t *queue, uint32_t *count, uint32_t value) {
   unsigned m = __activemask();
@@ -104,9 +131,14 @@ __device__ __forceinline__ uint32_t takeUnit(uint32_t *counter) {
   return base + rank;
 }
 
+// Counts one launch of the calling kernel (block 0, thread 0).
+__device__ __forceinline__ void countLaunch(const StreamView &v) {
+  if (v.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&v.counters->kernel_launches, 1ull);
+}
+
 __device__ __forceinline__ void flush(const StreamView &v, uint32_t ext, uint32_t shadow, uint32_t paths) {
   if (!v.counters) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&v.counters->kernel_launches, 1ull);
+  countLaunch(v);
   unsigned m = __activemask();
   uint32_t e = __reduce_add_sync(m, ext), s = __reduce_add_sync(m, shadow), p = __reduce_add_sync(m, paths);
   if (int(laneId()) == __ffs(m) - 1) {
@@ -201,9 +233,9 @@ __device__ bool claimPixel(const StreamView &v, uint32_t s) {
     sl.y = y;
     sl.left = J.samples - 1u;
     Ctx c{J, Sampler(), bsdfContext(J), Counters(), ShadowQuery()};
-    PathSample ps;
+    alignas(16) PathSample ps;
     beginSample(c, x, y, ps, v.spectral[s]);
-    sl.ps = ps;
+    copyPathSample(sl.ps, ps);
     sl.smp = c.smp;
     sl.shadow.valid = false;
     return true;
@@ -211,7 +243,8 @@ __device__ bool claimPixel(const StreamView &v, uint32_t s) {
   return false;
 }
 
-__global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v) {
+__global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v, uint32_t regroup0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) v.q->regroup = regroup0;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.slotCount; s += gridDim.x * blockDim.x) {
     if (claimPixel(v, s)) enqueueRay(v, 0u, s);
   }
@@ -226,7 +259,8 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v) {
 #endif
 template <bool kGpuLayout>
 __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
-    k_wf_extend(StreamView v, uint32_t cur, uint32_t regroup) {
+    k_wf_extend(StreamView v) {
+  const uint32_t cur = v.q->cur, regroup = v.q->regroup;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     v.q->rayCount[cur ^ 1u] = 0;
     v.q->shadowCount = 0;
@@ -297,8 +331,10 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS)
 
 // Orders the extension queue by ray key (counting sort, keys counted when
 // the rays were queued).  Slot order never changes a result.
-__global__ void __launch_bounds__(kStreamThreads) k_wf_sort_rays(StreamView v, uint32_t cur) {
+__global__ void __launch_bounds__(kStreamThreads) k_wf_sort_rays(StreamView v) {
   __shared__ uint32_t offset[kRayKeys];
+  countLaunch(v);
+  const uint32_t cur = v.q->cur;
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (uint32_t k = 0; k < kRayKeys; k++) {
@@ -325,8 +361,11 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_sort_rays(StreamView v, u
 // counted by k_wf_extend), so that the warps shading at any one time run the
 // same BSDF code.  The order of slots inside a class is arbitrary; it cannot
 // change any result, since slots never share state.
-__global__ void __launch_bounds__(kStreamThreads) k_wf_regroup(StreamView v, uint32_t cur) {
+__global__ void __launch_bounds__(kStreamThreads) k_wf_regroup(StreamView v) {
   __shared__ uint32_t offset[kClasses];
+  countLaunch(v);
+  if (!v.q->regroup) return;
+  const uint32_t cur = v.q->cur;
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (uint32_t k = 0; k < kClasses; k++) {
@@ -353,7 +392,8 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_regroup(StreamView v, uin
 #define MT_SHADE_MIN_BLOCKS 4
 #endif
 __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
-    k_wf_shade(StreamView v, uint32_t cur, uint32_t regroup) {
+    k_wf_shade(StreamView v) {
+  const uint32_t cur = v.q->cur, regroup = v.q->regroup;
   if (blockIdx.x == 0) {
     if (threadIdx.x == 0) v.q->extendNext = 0;
     // The class counts of this iteration have been consumed by k_wf_regroup.
@@ -371,12 +411,13 @@ __global__ void __launch_bounds__(kStreamThreads, MT_SHADE_MIN_BLOCKS)
     const JobData &J = v.jobs[sl.job];
     Ctx c{J, sl.smp, bsdfContext(J), Counters(), ShadowQuery()};
     c.shadow.valid = false;
-    PathSample ps = sl.ps;
+    alignas(16) PathSample ps;
+    copyPathSample(ps, sl.ps);
     TraversalHit h = v.hits[s];
     bool ended = isSpectral(J)   ? shadeStepSpectral(c, ps, v.spectral[s], h)
                  : alphaSplit(J) ? shadeStepAlpha(c, ps, v.spectral[s], h)
                                  : shadeStep(c, ps, v.spectral[s], h);
-    sl.ps = ps;
+    copyPathSample(sl.ps, ps);
     sl.smp = c.smp;
     sl.shadow = c.shadow;
     if (c.shadow.valid) enqueue(v.shadowQueue, &v.q->shadowCount, s);
@@ -449,7 +490,8 @@ __global__ void __launch_bounds__(kStreamThreads, MT_TRAVERSE_MIN_BLOCKS) k_wf_s
   flush(v, 0, shadowRays, 0);
 }
 
-__global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint32_t cur) {
+__global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v) {
+  const uint32_t cur = v.q->cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) v.q->shadowNext = 0;
   const uint32_t n = v.q->finishCount;
   uint32_t paths = 0;
@@ -457,12 +499,13 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
     uint32_t s = v.finishQueue[t];
     Slot &sl = v.slots[s];
     const JobData &J = v.jobs[sl.job];
-    PathSample ps = sl.ps;
+    alignas(16) PathSample ps;
+    copyPathSample(ps, sl.ps);
     if ((isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) ||
         (alphaSplit(J) && !finishAlphaSplit(J, ps, v.spectral[s]))) {
       // The next wavelength path, or the front path, of this sample starts
       // at event 0.
-      sl.ps = ps;
+      copyPathSample(sl.ps, ps);
       enqueueRay(v, cur ^ 1u, s);
       continue;
     }
@@ -473,7 +516,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
       sl.left--;
       Ctx c{J, Sampler(), bsdfContext(J), Counters(), ShadowQuery()};
       beginSample(c, sl.x, sl.y, ps, v.spectral[s]);
-      sl.ps = ps;
+      copyPathSample(sl.ps, ps);
       sl.smp = c.smp;
       again = true;
     } else {
@@ -482,6 +525,26 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v, uint
     if (again) enqueueRay(v, cur ^ 1u, s);
   }
   flush(v, 0, 0, paths);
+}
+
+// The last node of the graph's loop body, one thread: ends event iteration
+// `iterations` (flips the queue parity, decides whether the next iteration
+// regroups the shading queue, as iteration % regroupInterval == 0) and keeps
+// the loop running while rays are queued and fewer than maxIterations
+// iterations have run.  An empty queue means every unit has been claimed and
+// every path finished.
+__global__ void k_wf_continue(StreamView v, cudaGraphConditionalHandle loop, uint32_t regroupInterval,
+                              uint32_t maxIterations) {
+  countLaunch(v);
+  StreamQueues *q = v.q;
+  const uint32_t it = q->iterations + 1u, cur = q->cur ^ 1u;
+  q->iterations = it;
+  q->cur = cur;
+  q->regroup = regroupInterval && (it % regroupInterval) == 0u ? 1u : 0u;
+  const bool pending = q->rayCount[cur] != 0u;
+  const bool more = pending && it < maxIterations;
+  if (pending && !more) q->limitHit = 1u;
+  cudaGraphSetConditional(loop, more ? 1u : 0u);
 }
 
 size_t roundUp(size_t x) { return (x + 255) / 256 * 256; }
@@ -531,7 +594,7 @@ struct StreamShape {
 };
 
 bool streamShape(const mtc_stream_config *c, StreamShape &out) {
-  out = StreamShape{1u << 20, 8u, 1u << 20, 8u, 1u, 0u, 8u, 0u};
+  out = StreamShape{1u << 21, 8u, 1u << 20, 8u, 1u, 0u, 8u, 0u};
   if (!c) return true;
   if (c->struct_size != sizeof(mtc_stream_config)) return false;
   if (c->slots) {
@@ -564,12 +627,27 @@ bool streamShape(const mtc_stream_config *c, StreamShape &out) {
   return true;
 }
 
-// Every wavefront kernel asks for the largest L1 (no shared-memory carve-out
-// beyond the few words the sorts use): the traversal stacks, the spilled
-// shading state and the node reads all go through L1 (measured +1 % on the
-// 1080p instanced workload).
+// Every wavefront kernel asks for the largest L1 that still holds the shared
+// memory of as many blocks per SM as its registers allow: the spilled
+// traversal and shading state and the node reads all go through L1 (measured
+// +1 % on the 1080p instanced workload).  A smaller carve-out than the
+// blocks need would cut the blocks per SM instead.
 cudaError_t carveout(const void *kernel) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+  if (e != cudaSuccess) return e;
+  if (a.sharedSizeBytes == 0) return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  int device = 0, perSm = 0, smemPerSm = 0, reserved = 0;
+  if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                int(cudaSharedmemCarveoutMaxShared))) != cudaSuccess ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kStreamThreads, 0)) != cudaSuccess ||
+      (e = cudaGetDevice(&device)) != cudaSuccess ||
+      (e = cudaDeviceGetAttribute(&smemPerSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device)) != cudaSuccess ||
+      (e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device)) != cudaSuccess)
+    return e;
+  const size_t need = size_t(std::max(1, perSm)) * (a.sharedSizeBytes + size_t(reserved));
+  const int percent = int(std::min<size_t>(100, (need * 100 + size_t(smemPerSm) - 1) / size_t(std::max(1, smemPerSm))));
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
 }
 
 cudaError_t gridFor(const void *kernel, uint32_t &grid) {
@@ -583,28 +661,120 @@ cudaError_t gridFor(const void *kernel, uint32_t &grid) {
   return cudaSuccess;
 }
 
-// Pinned words the host polls for the queue size (one pair per device), and
-// a per-device lock that serialises concurrent mtc_stream_run calls, which
-// share them.
+// Per device: a lock that serialises graph lookups and launches, the stream
+// the loop bodies are captured on, and the instantiated loop graphs of
+// recent launch shapes.
 constexpr int kMaxDevices = 64;
-uint32_t *g_pinned[kMaxDevices];
-std::mutex g_pinnedMutex;
-std::mutex g_runMutex[kMaxDevices];
+constexpr int kCachedGraphs = 4;
 
-cudaError_t pinnedWords(uint32_t **out) {
-  int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
+// Everything a loop graph bakes in: the kernels' view of the state buffer,
+// the grids, the kernel variants and the loop parameters.
+struct GraphKey {
+  StreamView v;
+  uint32_t grids[6];  // extend, shade, shadow, finish, ray sort, regroup
+  uint32_t gpuLayout, alpha, regroupInterval, maxIterations;
+};
+
+struct CachedGraph {
+  bool valid = false;
+  GraphKey key;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+struct DeviceRunState {
+  std::mutex m;
+  cudaStream_t capture = nullptr;
+  CachedGraph graphs[kCachedGraphs];
+  uint32_t nextSlot = 0;
+};
+DeviceRunState g_run[kMaxDevices];
+
+// The device-driven event loop: a graph whose one node is a WHILE
+// conditional; its body is one event iteration (optional ray sort,
+// extension, optional regroup, shading, shadow, finish) followed by
+// k_wf_continue, which sets the loop condition.  The iteration's queue parity
+// and regroup flag live in the queue header, so one body serves every
+// iteration.
+cudaError_t buildLoopGraph(DeviceRunState &d, const GraphKey &k, CachedGraph &out) {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
   if (e != cudaSuccess) return e;
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> g(g_pinnedMutex);
-  if (!g_pinned[device]) {
-    void *p = nullptr;
-    e = cudaHostAlloc(&p, 64, cudaHostAllocDefault);
-    if (e != cudaSuccess) return e;
-    std::memset(p, 0, 64);
-    g_pinned[device] = static_cast<uint32_t *>(p);
+  cudaGraphConditionalHandle loop;
+  e = cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = loop;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+  if (e == cudaSuccess) {
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    cudaStream_t cs = d.capture;
+    e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const StreamView &v = k.v;
+      const uint32_t gExtend = k.grids[0], gShade = k.grids[1], gShadow = k.grids[2], gFinish = k.grids[3],
+                     gSort = k.grids[4], gRegroup = k.grids[5];
+      if (v.sortRays) k_wf_sort_rays<<<gSort, kStreamThreads, 0, cs>>>(v);
+      if (k.gpuLayout) k_wf_extend<true><<<gExtend, kStreamThreads, 0, cs>>>(v);
+      else k_wf_extend<false><<<gExtend, kStreamThreads, 0, cs>>>(v);
+      if (k.regroupInterval) k_wf_regroup<<<gRegroup, kStreamThreads, 0, cs>>>(v);
+      k_wf_shade<<<gShade, kStreamThreads, 0, cs>>>(v);
+      if (k.alpha) {
+        if (k.gpuLayout) k_wf_shadow<true, true><<<gShadow, kStreamThreads, 0, cs>>>(v);
+        else k_wf_shadow<false, true><<<gShadow, kStreamThreads, 0, cs>>>(v);
+      } else {
+        if (k.gpuLayout) k_wf_shadow<true, false><<<gShadow, kStreamThreads, 0, cs>>>(v);
+        else k_wf_shadow<false, false><<<gShadow, kStreamThreads, 0, cs>>>(v);
+      }
+      k_wf_finish<<<gFinish, kStreamThreads, 0, cs>>>(v);
+      k_wf_continue<<<1, 1, 0, cs>>>(v, loop, k.regroupInterval, k.maxIterations);
+      cudaError_t launched = cudaGetLastError();
+      e = cudaStreamEndCapture(cs, &body);
+      if (e == cudaSuccess) e = launched;
+    }
   }
-  *out = g_pinned[device];
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (g) cudaGraphDestroy(g);
+    return e;
+  }
+  out.valid = true;
+  out.key = k;
+  out.graph = g;
+  out.exec = exec;
+  return cudaSuccess;
+}
+
+// The instantiated loop graph for `k`, built on first use (least recently
+// built one replaced).  Called with d.m held.
+cudaError_t loopGraph(DeviceRunState &d, const GraphKey &k, cudaGraphExec_t *exec) {
+  for (CachedGraph &c : d.graphs) {
+    if (c.valid && std::memcmp(&c.key, &k, sizeof(GraphKey)) == 0) {
+      *exec = c.exec;
+      return cudaSuccess;
+    }
+  }
+  if (!d.capture) {
+    cudaError_t e = cudaStreamCreateWithFlags(&d.capture, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+  }
+  CachedGraph &slot = d.graphs[d.nextSlot];
+  d.nextSlot = (d.nextSlot + 1) % kCachedGraphs;
+  if (slot.valid) {
+    // A launch of the old graph may still be running; the exec is released
+    // once that work has finished.
+    cudaGraphExecDestroy(slot.exec);
+    cudaGraphDestroy(slot.graph);
+    slot = CachedGraph();
+  }
+  cudaError_t e = buildLoopGraph(d, k, slot);
+  if (e != cudaSuccess) return e;
+  *exec = slot.exec;
   return cudaSuccess;
 }
 
@@ -624,18 +794,27 @@ size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config
   return layout(capacity, shape.slots).total;
 }
 
-mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_config *config, void *state,
-                         mtc_counters *counters, void *stream) {
+}  // extern "C"
+
+namespace {
+
+// Enqueues one wavefront run on `st`: the job table upload, the queue and
+// count resets, the seed kernel and one launch of the loop graph.  With
+// `wait`, blocks until the run has finished and reports MT_ERROR_TIMEOUT
+// when the iteration limit stopped it.
+mt_status streamLaunch(const void *table, uint32_t capacity, const mtc_stream_config *config, void *state,
+                       mtc_counters *counters, cudaStream_t st, bool wait) {
   if (!table || !state || capacity == 0) return MT_ERROR_INVALID_ARGUMENT;
   StreamShape shape;
   if (!streamShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
   TableHeader hdr;
   std::memcpy(&hdr, table, sizeof(hdr));
   if (hdr.jobCount > capacity || hdr.tileW == 0 || hdr.tileW > 32 || 32 % hdr.tileW) return MT_ERROR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
   StreamLayout L = layout(capacity, shape.slots);
   char *base = static_cast<char *>(state);
-  StreamView v;
+  GraphKey key;
+  std::memset(&key, 0, sizeof(key));  // padding included: keys compare bytewise
+  StreamView &v = key.v;
   v.header = reinterpret_cast<const TableHeader *>(base + L.table);
   v.jobs = reinterpret_cast<const JobData *>(base + L.table + sizeof(TableHeader));
   v.q = reinterpret_cast<StreamQueues *>(base + L.queues);
@@ -682,75 +861,73 @@ mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_
       (e = carveout((const void *)k_wf_shadow<false, true>)) != cudaSuccess ||
       (e = carveout((const void *)k_wf_shadow<true, true>)) != cudaSuccess)
     return toStatus(e);
+  int device = 0;
+  if ((e = cudaGetDevice(&device)) != cudaSuccess) return toStatus(e);
+  if (device < 0 || device >= kMaxDevices) return MT_ERROR_UNAVAILABLE;
   if (shape.traversalCtasPerSm) {
     // Fewer resident traversal warps: a smaller local-memory footprint per SM.
-    int device = 0, sms = 0;
-    if ((e = cudaGetDevice(&device)) != cudaSuccess ||
-        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+    int sms = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
       return toStatus(e);
     gExtend = std::min(gExtend, uint32_t(sms) * shape.traversalCtasPerSm);
     gShadow = std::min(gShadow, uint32_t(sms) * shape.traversalCtasPerSm);
   }
-  uint32_t *pinned = nullptr;
-  if ((e = pinnedWords(&pinned)) != cudaSuccess) return toStatus(e);
-  int device = 0;
-  if ((e = cudaGetDevice(&device)) != cudaSuccess) return toStatus(e);
-  std::lock_guard<std::mutex> runLock(g_runMutex[device]);
-  cudaEvent_t ev[2];
-  if ((e = cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming)) != cudaSuccess) return toStatus(e);
-  if ((e = cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming)) != cudaSuccess) {
-    cudaEventDestroy(ev[0]);
-    return toStatus(e);
-  }
+  // The BLAS-layout specialisation (blasLayoutMask) of the traversal kernels,
+  // and the coverage test of shadow rays in scenes with alpha.
+  key.gpuLayout = (hdr.flagsUnion & MTC_SCENE_BLAS_GPU_LAYOUT) != 0u ? 1u : 0u;
+  key.alpha = (hdr.flagsUnion & MTC_SCENE_HAS_ALPHA) != 0u ? 1u : 0u;
+  key.grids[0] = gExtend;
+  key.grids[1] = gShade;
+  key.grids[2] = gShadow;
+  key.grids[3] = gFinish;
+  key.grids[4] = gSort;
+  key.grids[5] = gRegroup;
+  key.regroupInterval = shape.regroupInterval;
+  key.maxIterations = shape.maxIterations;
 
-  // The BLAS-layout specialisation (blasLayoutMask) of the traversal kernels.
-  const bool gpuLayout = (hdr.flagsUnion & MTC_SCENE_BLAS_GPU_LAYOUT) != 0u;
-  const bool alpha = (hdr.flagsUnion & MTC_SCENE_HAS_ALPHA) != 0u;  // shadow rays test coverage
-  k_wf_seed<<<gSeed, kStreamThreads, 0, st>>>(v);
-  e = cudaGetLastError();
-  uint32_t cur = 0, iterations = 0, chunk = 0;
-  mt_status status = MT_OK;
-  while (e == cudaSuccess) {
-    for (uint32_t k = 0; k < shape.iterationsPerCheck && e == cudaSuccess; k++) {
-      const uint32_t regroup = shape.regroupInterval && (iterations % shape.regroupInterval) == 0u ? 1u : 0u;
-      if (v.sortRays) k_wf_sort_rays<<<gSort, kStreamThreads, 0, st>>>(v, cur);
-      if (gpuLayout) k_wf_extend<true><<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
-      else k_wf_extend<false><<<gExtend, kStreamThreads, 0, st>>>(v, cur, regroup);
-      if (regroup) k_wf_regroup<<<gRegroup, kStreamThreads, 0, st>>>(v, cur);
-      k_wf_shade<<<gShade, kStreamThreads, 0, st>>>(v, cur, regroup);
-      if (alpha) {
-        if (gpuLayout) k_wf_shadow<true, true><<<gShadow, kStreamThreads, 0, st>>>(v);
-        else k_wf_shadow<false, true><<<gShadow, kStreamThreads, 0, st>>>(v);
-      } else {
-        if (gpuLayout) k_wf_shadow<true, false><<<gShadow, kStreamThreads, 0, st>>>(v);
-        else k_wf_shadow<false, false><<<gShadow, kStreamThreads, 0, st>>>(v);
-      }
-      k_wf_finish<<<gFinish, kStreamThreads, 0, st>>>(v, cur);
-      e = cudaGetLastError();
-      cur ^= 1u;
-      iterations++;
-    }
-    if (e != cudaSuccess) break;
-    // Rays queued for the next iteration; zero means every slot is idle.
-    e = cudaMemcpyAsync(&pinned[chunk & 1u], &v.q->rayCount[cur], 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[chunk & 1u], st);
-    if (e != cudaSuccess) break;
-    if (chunk > 0) {
-      e = cudaEventSynchronize(ev[(chunk - 1) & 1u]);
-      if (e != cudaSuccess) break;
-      if (pinned[(chunk - 1) & 1u] == 0u) break;
-    }
-    chunk++;
-    if (iterations >= shape.maxIterations) {
-      status = MT_ERROR_TIMEOUT;
-      break;
-    }
+  k_wf_seed<<<gSeed, kStreamThreads, 0, st>>>(v, shape.regroupInterval ? 1u : 0u);
+  if ((e = cudaGetLastError()) != cudaSuccess) return toStatus(e);
+  {
+    DeviceRunState &d = g_run[device];
+    std::lock_guard<std::mutex> g(d.m);
+    cudaGraphExec_t exec = nullptr;
+    if ((e = loopGraph(d, key, &exec)) != cudaSuccess) return toStatus(e);
+    if ((e = cudaGraphLaunch(exec, st)) != cudaSuccess) return toStatus(e);
   }
-  if (e == cudaSuccess) e = cudaEventSynchronize(ev[(chunk) & 1u]);
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
+  if (!wait) return MT_OK;
+  uint32_t limitHit = 0;
+  e = cudaMemcpyAsync(&limitHit, &v.q->limitHit, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return toStatus(e);
-  return status;
+  return limitHit ? MT_ERROR_TIMEOUT : MT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mt_status mtc_stream_run(const void *table, uint32_t capacity, const mtc_stream_config *config, void *state,
+                         mtc_counters *counters, void *stream) {
+  return streamLaunch(table, capacity, config, state, counters, (cudaStream_t)stream, true);
+}
+
+mt_status mtc_stream_launch(const void *table, uint32_t capacity, const mtc_stream_config *config, void *state,
+                            mtc_counters *counters, void *stream) {
+  return streamLaunch(table, capacity, config, state, counters, (cudaStream_t)stream, false);
+}
+
+mt_status mtc_stream_status(const void *state, uint32_t capacity, const mtc_stream_config *config, void *stream) {
+  if (!state || capacity == 0) return MT_ERROR_INVALID_ARGUMENT;
+  StreamShape shape;
+  if (!streamShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
+  const StreamLayout L = layout(capacity, shape.slots);
+  const StreamQueues *q = reinterpret_cast<const StreamQueues *>(static_cast<const char *>(state) + L.queues);
+  cudaStream_t st = (cudaStream_t)stream;
+  uint32_t limitHit = 0;
+  cudaError_t e = cudaMemcpyAsync(&limitHit, &q->limitHit, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return toStatus(e);
+  return limitHit ? MT_ERROR_TIMEOUT : MT_OK;
 }
 
 }  // extern "C"

@@ -142,4 +142,8 @@ def test_plain_entry_points_validate_before_touching_the_device():
     cfg = abi.StreamConfig.make(slots=100)                # below the 1024-slot minimum
     assert L.mtc_stream_state_bytes(4, C.byref(cfg)) == 0
     assert L.mtc_stream_run(None, 4, None, C.c_void_p(16), None, None) == abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_stream_launch(None, 4, None, C.c_void_p(16), None, None) == abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_stream_launch(C.c_void_p(16), 0, None, C.c_void_p(16), None, None) == abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_stream_status(None, 4, None, None) == abi.MT_ERROR_INVALID_ARGUMENT
+    assert L.mtc_stream_status(C.c_void_p(16), 4, C.byref(cfg), None) == abi.MT_ERROR_INVALID_ARGUMENT
     assert L.mtc_stream_state_bytes(4, None) > (1 << 20) * 400

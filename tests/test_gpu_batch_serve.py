@@ -227,3 +227,62 @@ def test_empty_batches_and_empty_scene(cuda):
     torch.cuda.synchronize()
     assert _equal(a.acc, w.acc)
     assert int(sb.counters[1].item()) == 0               # no extension ray traced
+
+
+def test_stream_launch_is_asynchronous_and_reports_the_iteration_limit(cuda):
+    """mtc_stream_launch enqueues the device-driven event loop and returns;
+    mtc_stream_status reports the outcome.  An iteration limit below what the
+    jobs need stops the run with MT_ERROR_TIMEOUT; a full run of the same
+    state afterwards is complete and equals the jobs rendered alone."""
+    import ctypes as C
+
+    import torch
+    L = abi.lib()
+    alone = _small_jobs(cuda)
+    for j in alone:
+        j.render_alone()
+    jobs = _small_jobs(cuda)
+    sb = batch.StreamBatch(len(jobs), stream_config=abi.StreamConfig.make(slots=4096), device=cuda)
+    sb.set_jobs(jobs)
+    args = (C.c_void_p(sb.table.data_ptr()), sb.capacity)
+    state = C.c_void_p(sb.state.data_ptr())
+
+    limited = abi.StreamConfig.make(slots=4096, max_iterations=2)
+    assert L.mtc_stream_run(*args, C.byref(limited), state, None, None) == abi.MT_ERROR_TIMEOUT
+    assert L.mtc_stream_status(state, sb.capacity, C.byref(limited), None) == abi.MT_ERROR_TIMEOUT
+    side = torch.cuda.Stream(device=cuda)
+    for j in jobs:
+        j.acc.zero_()
+    torch.cuda.synchronize()
+    stream = C.c_void_p(side.cuda_stream)
+    assert L.mtc_stream_launch(*args, C.byref(sb.stream_config), state, C.c_void_p(sb.counters.data_ptr()),
+                               stream) == abi.MT_OK
+    assert L.mtc_stream_status(state, sb.capacity, C.byref(sb.stream_config), stream) == abi.MT_OK
+    torch.cuda.synchronize()
+    for a, j in zip(alone, jobs):
+        assert _equal(a.acc, j.acc), j.job_id
+    assert int(sb.counters[0].item()) == sum(j.pixels * j.spp for j in jobs)
+
+
+def test_loop_graphs_of_many_shapes_and_states(cuda):
+    """More launch shapes and state buffers than the per-device graph cache
+    holds, interleaved: every run equals the jobs rendered alone."""
+    import torch
+    alone = _small_jobs(cuda)
+    for j in alone:
+        j.render_alone()
+    batches = []
+    for slots, regroup in ((1024, 1), (2048, 2), (4096, 1), (8192, abi.MTC_REGROUP_OFF), (1 << 14, 5), (3072, 1)):
+        jobs = _small_jobs(cuda)
+        sb = batch.StreamBatch(len(jobs), stream_config=abi.StreamConfig.make(slots=slots, regroup_interval=regroup),
+                               device=cuda)
+        batches.append((sb, jobs))
+    for _ in range(2):
+        for sb, jobs in batches:
+            for j in jobs:
+                j.acc.zero_()
+            sb.set_jobs(jobs)
+            sb.run()
+            torch.cuda.synchronize()
+            for a, j in zip(alone, jobs):
+                assert _equal(a.acc, j.acc), (sb.stream_config.slots, j.job_id)

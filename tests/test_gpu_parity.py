@@ -248,6 +248,12 @@ def test_context_api_render_and_jobs(cuda):
         info = job.info()
         assert info.state == abi.MT_JOB_COMPLETE and info.completed_samples == 10 and info.base_samples == 4
         assert ctx.info().samples == 14
+        # The job's batches (asynchronous wavefront launches) continue each
+        # pixel's sample sequence: the image equals 14 samples traced at once.
+        acc14 = trace.Accumulation(48, 40, cuda)
+        trace.trace_samples(dev, acc14, 14)
+        torch.cuda.synchronize()
+        assert np.array_equal(ctx.read_pixels(), acc14.resolved().cpu().numpy())
         job2 = ctx.submit(8)
         job.__init__(job.handle)
         with pytest.raises(abi.MtError) as e:
