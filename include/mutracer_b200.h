@@ -476,8 +476,10 @@ typedef struct mtc_stream_config {
                                      octant) before traversal (default 0) */
   uint32_t steps_per_check;       /* traversal steps between refill checks, 1..64
                                      (default 8) */
-  uint32_t traversal_ctas_per_sm; /* resident CTAs of the persistent traversal
-                                     kernels, 1..8 (default 8: full occupancy) */
+  uint32_t traversal_ctas_per_sm; /* caps the resident CTAs per SM of the persistent
+                                     traversal kernels, 1..8 (default 0: as many as
+                                     their registers allow, 5 for closest-hit and 6
+                                     for shadow rays) */
   uint32_t _pad[3];
 } mtc_stream_config;
 #define MTC_REGROUP_OFF 0xffffffffu

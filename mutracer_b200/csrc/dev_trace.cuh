@@ -532,6 +532,8 @@ __device__ __noinline__ bool traverse(const DevScene &s, int32_t blasBase, V3 ra
 // current TLAS leaf.  Visit order, box tests, the `>` tie rule and the
 // self-hit and backface rules are those of traverse(), so the hits are
 // bit-identical to it.
+constexpr int kTraversalStackEntries = 2 * MTC_MAX_STACK;
+
 template <bool shadow, bool kGpuLayout, bool kAlpha = false>
 struct RayTraversal {
   const float4 *bvh, *ins, *mats;
@@ -544,9 +546,12 @@ struct RayTraversal {
   int32_t currentTri, currentIns;
   // TLAS entries at [0, MTC_MAX_STACK), the current instance's BLAS entries
   // at [MTC_MAX_STACK, 2 * MTC_MAX_STACK): two stacks of the reference's
-  // depth, addressed through one array so TLAS and BLAS node visits share
-  // one code path.
-  int32_t stack[2 * MTC_MAX_STACK];
+  // depth, addressed through one array of kTraversalStackEntries so TLAS and
+  // BLAS node visits share one code path.  The array belongs to the caller
+  // (a local array of the kernel): a dynamically indexed array inside this
+  // object would keep the whole object, ray and hit included, in local
+  // memory.
+  int32_t *stack;
   int tlasTop, blasTop;
   int32_t leafNode, io;
   V3 o, d, linvD, shear;
