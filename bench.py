@@ -53,6 +53,10 @@ def parse():
                         "what mt_context_render runs) or the plain drop-in megakernel (mtc_trace_samples)")
     p.add_argument("--slots", type=int, default=1 << 21, help="wavefront paths in flight")
     p.add_argument("--refill-lanes", type=int, default=0, help="wavefront traversal refill threshold (0: default)")
+    p.add_argument("--host-loop", type=int, default=0,
+                   help="wavefront form: drive the event loop from the host, checking the queue every N iterations "
+                        "(every kernel a separate launch, so that ncu sees each; default 0: the device-driven "
+                        "loop, one graph launch per run)")
     p.add_argument("--queue-trace", type=int, default=0,
                    help="wavefront form: print the extension, shadow and finished-path counts of each of the first "
                         "N event iterations of one run (runs stopped after 1..N iterations) and exit")
@@ -157,26 +161,48 @@ def oracle_traffic(host, rows=8, spp=2):
     return oracle_lib.algorithmic_bytes(total), total
 
 
-TRAFFIC_PROFILES = {
-    "megakernel": ("k_trace_dram_instanced_spheres_1080p_16spp.md", "traffic_bytes_per_launch:"),
-    "wavefront": ("wavefront_dram_instanced_spheres_1080p_16spp.md", "traffic_bytes_per_step:"),
-}
+# DRAM bytes (read + write) measured by ncu, per unit of work: the plain
+# megakernel per launch of the headline step; the wavefront kernels per queued
+# ray or finished path (small-case captures normalised by exact queue
+# lengths), scaled by the units this step processed.
+MEGAKERNEL_TRAFFIC = ("k_trace_dram_instanced_spheres_1080p_16spp.md", "traffic_bytes_per_launch:")
+WAVEFRONT_TRAFFIC = ("wavefront_dram_per_kernel_instanced_spheres_960x540_4spp.md",
+                     ("dram_bytes_per_extension_ray:", "dram_bytes_per_shaded_ray:", "dram_bytes_per_shadow_ray:",
+                      "dram_bytes_per_finished_path:"))
 
 
-def measured_traffic(form, args, host, spp):
-    """DRAM bytes (read + write) of one step of this exact workload in the
-    given engine, from the committed ncu summary; (None, None) otherwise."""
-    if args.workload != WORKLOAD or (host.width, host.height, spp) != (1920, 1080, 16):
-        return None, None
-    name, key = TRAFFIC_PROFILES[form]
-    path = os.path.join(ROOT, "profiles", name)
+def _profile_values(name, keys):
+    values = {}
     try:
-        for line in open(path):
-            if line.startswith(key):
-                return int(line.split(":")[1]), "profiles/" + name
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            for k in keys:
+                if line.startswith(k):
+                    values[k] = float(line.split(":")[1])
     except OSError:
         pass
-    return None, None
+    return values
+
+
+def measured_traffic(form, args, host, spp, units=None):
+    """DRAM bytes (read + write) of one step of this workload from the
+    committed ncu summaries; (None, None) where none applies.  `units`
+    (extension rays, shadow rays, paths of one step) scales the wavefront's
+    per-unit figures."""
+    if args.workload != WORKLOAD:
+        return None, None
+    if form == "megakernel":
+        if (host.width, host.height, spp) != (1920, 1080, 16):
+            return None, None
+        name, key = MEGAKERNEL_TRAFFIC
+        v = _profile_values(name, (key,))
+        return (int(v[key]), "profiles/" + name) if key in v else (None, None)
+    name, keys = WAVEFRONT_TRAFFIC
+    v = _profile_values(name, keys)
+    if units is None or len(v) != len(keys):
+        return None, None
+    ext, shadow, paths = units
+    total = (v[keys[0]] + v[keys[1]]) * ext + v[keys[2]] * shadow + v[keys[3]] * paths
+    return int(total), "profiles/" + name + " (per-unit figures x this step's rays and paths)"
 
 
 def cpu_baseline(host, spp, seconds, keep=None):
@@ -282,7 +308,8 @@ def queue_trace(sb, counters, slots, iterations):
     from mutracer_b200 import abi
     rows, last = [], [0, 0, 0]
     for k in range(1, iterations + 1):
-        sb.stream_config = abi.StreamConfig.make(slots=slots, max_iterations=k)
+        sb.stream_config = abi.StreamConfig.make(slots=slots, max_iterations=k,
+                                                 iterations_per_check=sb.stream_config.iterations_per_check)
         counters.zero_()
         try:
             sb.run()
@@ -319,7 +346,8 @@ def run_b200(args):
         from mutracer_b200 import batch
         job = batch.RenderJob(dev, spp, device=dev_id)
         acc = job.acc
-        sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=args.slots, refill_lanes=args.refill_lanes),
+        sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=args.slots, refill_lanes=args.refill_lanes,
+                                                                      iterations_per_check=args.host_loop),
                                device=dev_id)
         sb.counters = counters
         sb.set_jobs([job])
@@ -372,7 +400,9 @@ def run_b200(args):
                          "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                          "l2": "flushed between steps (256 MB write)",
                          "form": "plain megakernel (mtc_trace_samples)" if args.form == "megakernel"
-                         else f"wavefront (mtc_stream_run, {args.slots} slots)"},
+                         else f"wavefront (mtc_stream_run, {args.slots} slots, "
+                              + (f"host-driven loop, check every {args.host_loop} iterations)" if args.host_loop
+                                 else "device-driven loop)")},
               "mrays_per_s": round(rays_per_step / (ms_per_step / 1000.0) / 1e6, 2),
               "mrays_per_s_extension": round(float(cnt[1]) / args.steps / (ms_per_step / 1000.0) / 1e6, 2),
               "mrays_per_s_shadow": round(float(cnt[2]) / args.steps / (ms_per_step / 1000.0) / 1e6, 2),
@@ -399,7 +429,9 @@ def run_b200(args):
     try:
         bpp, traffic = oracle_traffic(host)
         achieved = bpp * paths_per_step / (ms_per_step / 1000.0) / 1e9
-        dram, source = measured_traffic(args.form, args, host, spp)
+        dram, source = measured_traffic(args.form, args, host, spp,
+                                        units=(float(cnt[1]) / args.steps, float(cnt[2]) / args.steps,
+                                               float(paths_per_step)))
         result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                               "frac": round(achieved / peak, 4), "traffic": dram,
                               "peak_source": peak_kind,

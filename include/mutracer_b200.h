@@ -452,7 +452,8 @@ mt_status mtc_batch_launch(const void *table, uint32_t capacity,
  * memory of mtc_stream_state_bytes(capacity, config) bytes.  The event loop
  * runs on the device: one CUDA graph whose WHILE node repeats an event
  * iteration until the queues have drained or max_iterations iterations have
- * run, so a run needs no host round trip after it is enqueued.
+ * run, so a run needs no host round trip after it is enqueued (unless
+ * iterations_per_check asks for the host-driven loop).
  * mtc_stream_run enqueues the run on `stream` and waits for it (returning
  * MT_ERROR_TIMEOUT when the iteration limit stopped it); mtc_stream_launch
  * only enqueues it, and mtc_stream_status reports the outcome of the last run
@@ -464,8 +465,13 @@ mt_status mtc_batch_launch(const void *table, uint32_t capacity,
 typedef struct mtc_stream_config {
   uint32_t struct_size;
   uint32_t slots;                 /* paths in flight, 1024..2^25 (default 2^21) */
-  uint32_t iterations_per_check;  /* accepted (0..256) and ignored: the device checks
-                                     the queue after every event iteration */
+  uint32_t iterations_per_check;  /* 0 (default): the device-driven loop (one graph
+                                     launch, the queue checked on the device after
+                                     every iteration); 1..256: a host-driven loop,
+                                     every kernel a separate launch and the host
+                                     checking the queue every N iterations (blocking
+                                     mtc_stream_run only; for profilers that cannot
+                                     look into conditional graphs) */
   uint32_t max_iterations;        /* MT_ERROR_TIMEOUT beyond this (default 2^20) */
   uint32_t refill_lanes;          /* idle lanes of a warp that trigger fetching new
                                      rays in the traversal kernels, 1..32 (default 8) */

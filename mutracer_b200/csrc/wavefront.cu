@@ -52,13 +52,15 @@ struct StreamQueues {
   uint32_t shadowNext;       // next shadow ray to hand to a lane
   // Event-iteration state, advanced on the device by k_wf_continue: the
   // parity of the extension queue being traced, whether this iteration
-  // regroups the shading queue, iterations completed, and set when the
-  // iteration limit stopped a run with rays still queued.
+  // regroups the shading queue, iterations completed, set when the
+  // iteration limit stopped a run with rays still queued, and whether the
+  // loop goes on (read by the host-driven loop).
   uint32_t cur;
   uint32_t regroup;
   uint32_t iterations;
   uint32_t limitHit;
-  uint32_t _pad[53];
+  uint32_t more;
+  uint32_t _pad[52];
 };
 static_assert(sizeof(StreamQueues) == 256, "queue header size");
 
@@ -544,8 +546,8 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v) {
 // the loop running while rays are queued and fewer than maxIterations
 // iterations have run.  An empty queue means every unit has been claimed and
 // every path finished.
-__global__ void k_wf_continue(StreamView v, cudaGraphConditionalHandle loop, uint32_t regroupInterval,
-                              uint32_t maxIterations) {
+__global__ void k_wf_continue(StreamView v, cudaGraphConditionalHandle loop, uint32_t inGraph,
+                              uint32_t regroupInterval, uint32_t maxIterations) {
   countLaunch(v);
   StreamQueues *q = v.q;
   const uint32_t it = q->iterations + 1u, cur = q->cur ^ 1u;
@@ -555,7 +557,8 @@ __global__ void k_wf_continue(StreamView v, cudaGraphConditionalHandle loop, uin
   const bool pending = q->rayCount[cur] != 0u;
   const bool more = pending && it < maxIterations;
   if (pending && !more) q->limitHit = 1u;
-  cudaGraphSetConditional(loop, more ? 1u : 0u);
+  q->more = more ? 1u : 0u;
+  if (inGraph) cudaGraphSetConditional(loop, more ? 1u : 0u);
 }
 
 size_t roundUp(size_t x) { return (x + 255) / 256 * 256; }
@@ -605,7 +608,7 @@ struct StreamShape {
 };
 
 bool streamShape(const mtc_stream_config *c, StreamShape &out) {
-  out = StreamShape{1u << 21, 8u, 1u << 20, 8u, 1u, 0u, 8u, 0u};
+  out = StreamShape{1u << 21, 0u, 1u << 20, 8u, 1u, 0u, 8u, 0u};
   if (!c) return true;
   if (c->struct_size != sizeof(mtc_stream_config)) return false;
   if (c->slots) {
@@ -672,9 +675,10 @@ cudaError_t gridFor(const void *kernel, uint32_t &grid) {
   return cudaSuccess;
 }
 
-// Per device: a lock that serialises graph lookups and launches, the stream
-// the loop bodies are captured on, and the instantiated loop graphs of
-// recent launch shapes.
+// Per device: a lock that serialises graph lookups and launches (and the
+// host-driven loop, which polls its pinned words), the stream the loop
+// bodies are captured on, and the instantiated loop graphs of recent launch
+// shapes.
 constexpr int kMaxDevices = 64;
 constexpr int kCachedGraphs = 4;
 
@@ -696,10 +700,33 @@ struct CachedGraph {
 struct DeviceRunState {
   std::mutex m;
   cudaStream_t capture = nullptr;
+  uint32_t *pinned = nullptr;  // loop-flag words of the host-driven loop
   CachedGraph graphs[kCachedGraphs];
   uint32_t nextSlot = 0;
 };
 DeviceRunState g_run[kMaxDevices];
+
+// One event iteration's kernels on `s` (captured into the loop body, or
+// launched directly by the host-driven loop), k_wf_continue last.
+void launchIteration(const GraphKey &k, cudaStream_t s, cudaGraphConditionalHandle loop, bool inGraph) {
+  const StreamView &v = k.v;
+  const uint32_t gExtend = k.grids[0], gShade = k.grids[1], gShadow = k.grids[2], gFinish = k.grids[3],
+                 gSort = k.grids[4], gRegroup = k.grids[5];
+  if (v.sortRays) k_wf_sort_rays<<<gSort, kStreamThreads, 0, s>>>(v);
+  if (k.gpuLayout) k_wf_extend<true><<<gExtend, kStreamThreads, 0, s>>>(v);
+  else k_wf_extend<false><<<gExtend, kStreamThreads, 0, s>>>(v);
+  if (k.regroupInterval) k_wf_regroup<<<gRegroup, kStreamThreads, 0, s>>>(v);
+  k_wf_shade<<<gShade, kStreamThreads, 0, s>>>(v);
+  if (k.alpha) {
+    if (k.gpuLayout) k_wf_shadow<true, true><<<gShadow, kStreamThreads, 0, s>>>(v);
+    else k_wf_shadow<false, true><<<gShadow, kStreamThreads, 0, s>>>(v);
+  } else {
+    if (k.gpuLayout) k_wf_shadow<true, false><<<gShadow, kStreamThreads, 0, s>>>(v);
+    else k_wf_shadow<false, false><<<gShadow, kStreamThreads, 0, s>>>(v);
+  }
+  k_wf_finish<<<gFinish, kStreamThreads, 0, s>>>(v);
+  k_wf_continue<<<1, 1, 0, s>>>(v, loop, inGraph ? 1u : 0u, k.regroupInterval, k.maxIterations);
+}
 
 // The device-driven event loop: a graph whose one node is a WHILE
 // conditional; its body is one event iteration (optional ray sort,
@@ -726,23 +753,7 @@ cudaError_t buildLoopGraph(DeviceRunState &d, const GraphKey &k, CachedGraph &ou
     cudaStream_t cs = d.capture;
     e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      const StreamView &v = k.v;
-      const uint32_t gExtend = k.grids[0], gShade = k.grids[1], gShadow = k.grids[2], gFinish = k.grids[3],
-                     gSort = k.grids[4], gRegroup = k.grids[5];
-      if (v.sortRays) k_wf_sort_rays<<<gSort, kStreamThreads, 0, cs>>>(v);
-      if (k.gpuLayout) k_wf_extend<true><<<gExtend, kStreamThreads, 0, cs>>>(v);
-      else k_wf_extend<false><<<gExtend, kStreamThreads, 0, cs>>>(v);
-      if (k.regroupInterval) k_wf_regroup<<<gRegroup, kStreamThreads, 0, cs>>>(v);
-      k_wf_shade<<<gShade, kStreamThreads, 0, cs>>>(v);
-      if (k.alpha) {
-        if (k.gpuLayout) k_wf_shadow<true, true><<<gShadow, kStreamThreads, 0, cs>>>(v);
-        else k_wf_shadow<false, true><<<gShadow, kStreamThreads, 0, cs>>>(v);
-      } else {
-        if (k.gpuLayout) k_wf_shadow<true, false><<<gShadow, kStreamThreads, 0, cs>>>(v);
-        else k_wf_shadow<false, false><<<gShadow, kStreamThreads, 0, cs>>>(v);
-      }
-      k_wf_finish<<<gFinish, kStreamThreads, 0, cs>>>(v);
-      k_wf_continue<<<1, 1, 0, cs>>>(v, loop, k.regroupInterval, k.maxIterations);
+      launchIteration(k, cs, loop, true);
       cudaError_t launched = cudaGetLastError();
       e = cudaStreamEndCapture(cs, &body);
       if (e == cudaSuccess) e = launched;
@@ -809,6 +820,47 @@ size_t mtc_stream_state_bytes(uint32_t capacity, const mtc_stream_config *config
 
 namespace {
 
+// The host-driven form of the event loop (iterations_per_check > 0): every
+// kernel of every iteration is a separate launch on `st`; every
+// `iterationsPerCheck` iterations the host reads the loop flag k_wf_continue
+// wrote, one check behind so the device never waits for the host, and stops
+// at max_iterations.  For tools that cannot look into conditional graphs.
+cudaError_t hostLoop(DeviceRunState &d, const GraphKey &key, const StreamShape &shape, cudaStream_t st) {
+  std::lock_guard<std::mutex> g(d.m);
+  cudaError_t e = cudaSuccess;
+  if (!d.pinned) {
+    void *p = nullptr;
+    if ((e = cudaHostAlloc(&p, 64, cudaHostAllocDefault)) != cudaSuccess) return e;
+    std::memset(p, 0, 64);
+    d.pinned = static_cast<uint32_t *>(p);
+  }
+  cudaEvent_t ev[2];
+  if ((e = cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming)) != cudaSuccess) return e;
+  if ((e = cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming)) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return e;
+  }
+  uint32_t iterations = 0, chunk = 0;
+  while (e == cudaSuccess && iterations < shape.maxIterations) {
+    const uint32_t n = std::min(shape.iterationsPerCheck, shape.maxIterations - iterations);
+    for (uint32_t k = 0; k < n; k++) launchIteration(key, st, 0, false);
+    iterations += n;
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    e = cudaMemcpyAsync(&d.pinned[chunk & 1u], &key.v.q->more, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[chunk & 1u], st);
+    if (e != cudaSuccess) break;
+    if (chunk > 0) {
+      if ((e = cudaEventSynchronize(ev[(chunk - 1) & 1u])) != cudaSuccess) break;
+      if (d.pinned[(chunk - 1) & 1u] == 0u) break;
+    }
+    chunk++;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  return e;
+}
+
 // Enqueues one wavefront run on `st`: the job table upload, the queue and
 // count resets, the seed kernel and one launch of the loop graph.  With
 // `wait`, blocks until the run has finished and reports MT_ERROR_TIMEOUT
@@ -818,6 +870,7 @@ mt_status streamLaunch(const void *table, uint32_t capacity, const mtc_stream_co
   if (!table || !state || capacity == 0) return MT_ERROR_INVALID_ARGUMENT;
   StreamShape shape;
   if (!streamShape(config, shape)) return MT_ERROR_INVALID_ARGUMENT;
+  if (shape.iterationsPerCheck && !wait) return MT_ERROR_INVALID_ARGUMENT;  // the host loop blocks
   TableHeader hdr;
   std::memcpy(&hdr, table, sizeof(hdr));
   if (hdr.jobCount > capacity || hdr.tileW == 0 || hdr.tileW > 32 || 32 % hdr.tileW) return MT_ERROR_INVALID_ARGUMENT;
@@ -898,12 +951,14 @@ mt_status streamLaunch(const void *table, uint32_t capacity, const mtc_stream_co
 
   k_wf_seed<<<gSeed, kStreamThreads, 0, st>>>(v, shape.regroupInterval ? 1u : 0u);
   if ((e = cudaGetLastError()) != cudaSuccess) return toStatus(e);
-  {
-    DeviceRunState &d = g_run[device];
+  DeviceRunState &d = g_run[device];
+  if (!shape.iterationsPerCheck) {
     std::lock_guard<std::mutex> g(d.m);
     cudaGraphExec_t exec = nullptr;
     if ((e = loopGraph(d, key, &exec)) != cudaSuccess) return toStatus(e);
     if ((e = cudaGraphLaunch(exec, st)) != cudaSuccess) return toStatus(e);
+  } else if ((e = hostLoop(d, key, shape, st)) != cudaSuccess) {
+    return toStatus(e);
   }
   if (!wait) return MT_OK;
   uint32_t limitHit = 0;

@@ -247,9 +247,13 @@ def test_stream_launch_is_asynchronous_and_reports_the_iteration_limit(cuda):
     args = (C.c_void_p(sb.table.data_ptr()), sb.capacity)
     state = C.c_void_p(sb.state.data_ptr())
 
-    limited = abi.StreamConfig.make(slots=4096, max_iterations=2)
-    assert L.mtc_stream_run(*args, C.byref(limited), state, None, None) == abi.MT_ERROR_TIMEOUT
-    assert L.mtc_stream_status(state, sb.capacity, C.byref(limited), None) == abi.MT_ERROR_TIMEOUT
+    for per_check in (0, 1, 8):                           # device-driven loop, host-driven loops
+        limited = abi.StreamConfig.make(slots=4096, max_iterations=2, iterations_per_check=per_check)
+        assert L.mtc_stream_run(*args, C.byref(limited), state, None, None) == abi.MT_ERROR_TIMEOUT
+        assert L.mtc_stream_status(state, sb.capacity, C.byref(limited), None) == abi.MT_ERROR_TIMEOUT
+    # The host-driven loop blocks, so it cannot be only enqueued.
+    host = abi.StreamConfig.make(slots=4096, iterations_per_check=8)
+    assert L.mtc_stream_launch(*args, C.byref(host), state, None, None) == abi.MT_ERROR_INVALID_ARGUMENT
     side = torch.cuda.Stream(device=cuda)
     for j in jobs:
         j.acc.zero_()
