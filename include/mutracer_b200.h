@@ -511,8 +511,9 @@ mt_status mtc_stream_status(const void *state, uint32_t capacity,
  * of mtc_trace_batch (same validation, every config field applied), and
  * status_out is used the same way.  The first call on a device (and the first
  * after its primary context was reset) looks up that array's device address
- * (cudaGetSymbolAddress) with the device current; make that first call
- * before any stream capture.  Every call on a
+ * (cudaGetSymbolAddress) with the device current.  Each call assembles the
+ * job table in host stack memory and uploads it with cudaMemcpyAsync on
+ * `stream` (pageable memory: read before the call returns).  Every call on a
  * device shares the one array (each call rewrites the table and clears the
  * counter), so calls whose work overlaps on the same device race: serialise
  * them, for example on one stream.  The array stays resident on every device
