@@ -513,16 +513,22 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_finish(StreamView v) {
     Slot &sl = v.slots[s];
     const JobData &J = v.jobs[sl.job];
     alignas(16) PathSample ps;
-    copyPathSample(ps, sl.ps);
-    if ((isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) ||
-        (alphaSplit(J) && !finishAlphaSplit(J, ps, v.spectral[s]))) {
-      // The next wavelength path, or the front path, of this sample starts
-      // at event 0.
-      copyPathSample(sl.ps, ps);
-      enqueueRay(v, cur ^ 1u, s);
-      continue;
+    if (isSpectral(J) || alphaSplit(J)) {
+      copyPathSample(ps, sl.ps);
+      if ((isSpectral(J) && !finishWavelength(J, ps, v.spectral[s])) ||
+          (alphaSplit(J) && !finishAlphaSplit(J, ps, v.spectral[s]))) {
+        // The next wavelength path, or the front path, of this sample starts
+        // at event 0.
+        copyPathSample(sl.ps, ps);
+        enqueueRay(v, cur ^ 1u, s);
+        continue;
+      }
+      endSample(J, sl.x + sl.y * J.width, ps);
+    } else {
+      // The accumulation reads a dozen words of the path sample: from the
+      // slot itself rather than a copy of all of it.
+      endSample(J, sl.x + sl.y * J.width, sl.ps);
     }
-    endSample(J, sl.x + sl.y * J.width, ps);
     paths++;
     bool again;
     if (sl.left > 0u) {
