@@ -53,6 +53,8 @@ def parse():
                         "what mt_context_render runs) or the plain drop-in megakernel (mtc_trace_samples)")
     p.add_argument("--slots", type=int, default=1 << 21, help="wavefront paths in flight")
     p.add_argument("--refill-lanes", type=int, default=0, help="wavefront traversal refill threshold (0: default)")
+    p.add_argument("--steps-per-check", type=int, default=0,
+                   help="wavefront traversal steps between refill checks (0: default)")
     p.add_argument("--host-loop", type=int, default=0,
                    help="wavefront form: drive the event loop from the host, checking the queue every N iterations "
                         "(every kernel a separate launch, so that ncu sees each; default 0: the device-driven "
@@ -347,7 +349,8 @@ def run_b200(args):
         job = batch.RenderJob(dev, spp, device=dev_id)
         acc = job.acc
         sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=args.slots, refill_lanes=args.refill_lanes,
-                                                                      iterations_per_check=args.host_loop),
+                                                                      iterations_per_check=args.host_loop,
+                                                                      steps_per_check=args.steps_per_check),
                                device=dev_id)
         sb.counters = counters
         sb.set_jobs([job])
@@ -567,7 +570,7 @@ def same_job_wavefront(dev, acc, spp, paths, dev_id, flush):
     ms = sum(times) / len(times)
     out = {"ms_per_step": round(ms, 2), "mpaths_per_s": round(paths / ms / 1e3, 3),
            "bit_identical_to_plain": bool(torch.equal(job.acc.color, plain)),
-           "config": "defaults: 2M slots, refill at 8 idle lanes, 8 steps per refill check, regroup every "
+           "config": "defaults: 2M slots, refill at 4 idle lanes, 8 steps per refill check, regroup every "
                      "iteration"}
     del sb, job
     return out

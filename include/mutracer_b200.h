@@ -474,7 +474,7 @@ typedef struct mtc_stream_config {
                                      look into conditional graphs) */
   uint32_t max_iterations;        /* MT_ERROR_TIMEOUT beyond this (default 2^20) */
   uint32_t refill_lanes;          /* idle lanes of a warp that trigger fetching new
-                                     rays in the traversal kernels, 1..32 (default 8) */
+                                     rays in the traversal kernels, 1..32 (default 4) */
   uint32_t regroup_interval;      /* order the shading queue by material class every
                                      N-th event iteration, 1..1024 (default 1);
                                      MTC_REGROUP_OFF never */

@@ -283,13 +283,13 @@ def autotune(jobs, probe_samples=1, space=AUTOTUNE_SPACE, repeats=2, device="cud
 # extension queue is ordered by (job, direction octant) before traversal, and
 # how many traversal steps a lane takes between refill checks.
 STREAM_SPACE = {
-    "refill_lanes": (4, 8, 16),
+    "refill_lanes": (2, 4, 8),
     "regroup_interval": (1, 2, abi.MTC_REGROUP_OFF),
     "sort_rays": (0, 1),
     "steps_per_check": (4, 8, 16),
     "slots": (1 << 20, 1 << 21, 1 << 22),
 }
-STREAM_DEFAULT = {"slots": 1 << 21, "refill_lanes": 8, "regroup_interval": 1, "sort_rays": 0, "steps_per_check": 8}
+STREAM_DEFAULT = {"slots": 1 << 21, "refill_lanes": 4, "regroup_interval": 1, "sort_rays": 0, "steps_per_check": 8}
 
 
 def autotune_stream(jobs, probe_samples=1, space=STREAM_SPACE, device="cuda", batch_config=None):

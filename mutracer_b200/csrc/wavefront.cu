@@ -614,7 +614,7 @@ struct StreamShape {
 };
 
 bool streamShape(const mtc_stream_config *c, StreamShape &out) {
-  out = StreamShape{1u << 21, 0u, 1u << 20, 8u, 1u, 0u, 8u, 0u};
+  out = StreamShape{1u << 21, 0u, 1u << 20, 4u, 1u, 0u, 8u, 0u};
   if (!c) return true;
   if (c->struct_size != sizeof(mtc_stream_config)) return false;
   if (c->slots) {
