@@ -300,8 +300,9 @@ def flush_l2(buf):
 
 def queue_trace(sb, counters, slots, iterations):
     """Queue sizes of each event iteration of one wavefront run: the run is
-    repeated, stopped by its iteration limit after 1, 2, ... `iterations`
-    iterations, and the counter totals are differenced.  For an RGB
+    repeated from zeroed accumulation (a pixel's sample index is its
+    accumulated count), stopped by its iteration limit after 1, 2, ...
+    `iterations` iterations, and the counter totals are differenced.  For an RGB
     scene every queued extension ray is traced and every finished slot ends a
     path, so the three counts are the queue lengths k_wf_extend (and
     k_wf_shade), k_wf_shadow and k_wf_finish see in that iteration; they
@@ -313,6 +314,8 @@ def queue_trace(sb, counters, slots, iterations):
         sb.stream_config = abi.StreamConfig.make(slots=slots, max_iterations=k,
                                                  iterations_per_check=sb.stream_config.iterations_per_check)
         counters.zero_()
+        for j in sb.jobs:                 # every run starts from sample 0 of every pixel
+            j.acc.zero_()
         try:
             sb.run()
         except abi.MtError as err:
