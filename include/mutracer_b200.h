@@ -460,9 +460,9 @@ mt_status mtc_batch_launch(const void *table, uint32_t capacity,
  * enqueued on `state` the same way (it waits on `stream`).  The table is
  * uploaded with cudaMemcpyAsync on `stream`: a table in pinned memory must
  * stay unchanged until the stream has passed the launch (pageable memory is
- * read before the call returns), so neither call can be captured into a
- * CUDA graph.  One `state` buffer serves one run at a time.  No counterpart
- * in the reference. */
+ * read before the call returns).  Neither call is for stream capture: a
+ * run launches its own graph.  One `state` buffer serves one run at a time.
+ * No counterpart in the reference. */
 typedef struct mtc_stream_config {
   uint32_t struct_size;
   uint32_t slots;                 /* paths in flight, 1024..2^25 (default 2^21) */
