@@ -701,6 +701,7 @@ struct CachedGraph {
   GraphKey key;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;  // recorded after each launch of `exec`
 };
 
 struct DeviceRunState {
@@ -771,19 +772,27 @@ cudaError_t buildLoopGraph(DeviceRunState &d, const GraphKey &k, CachedGraph &ou
     if (g) cudaGraphDestroy(g);
     return e;
   }
+  cudaEvent_t done = nullptr;
+  if ((e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming)) != cudaSuccess) {
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(g);
+    return e;
+  }
   out.valid = true;
   out.key = k;
   out.graph = g;
   out.exec = exec;
+  out.done = done;
   return cudaSuccess;
 }
 
-// The instantiated loop graph for `k`, built on first use (least recently
-// built one replaced).  Called with d.m held.
-cudaError_t loopGraph(DeviceRunState &d, const GraphKey &k, cudaGraphExec_t *exec) {
+// The cache entry of the loop graph for `k`, built on first use (the least
+// recently built one replaced once its last launch has finished).  Called
+// with d.m held.
+cudaError_t loopGraph(DeviceRunState &d, const GraphKey &k, CachedGraph **entry) {
   for (CachedGraph &c : d.graphs) {
     if (c.valid && std::memcmp(&c.key, &k, sizeof(GraphKey)) == 0) {
-      *exec = c.exec;
+      *entry = &c;
       return cudaSuccess;
     }
   }
@@ -794,15 +803,16 @@ cudaError_t loopGraph(DeviceRunState &d, const GraphKey &k, cudaGraphExec_t *exe
   CachedGraph &slot = d.graphs[d.nextSlot];
   d.nextSlot = (d.nextSlot + 1) % kCachedGraphs;
   if (slot.valid) {
-    // A launch of the old graph may still be running; the exec is released
-    // once that work has finished.
+    // The old graph's last launch (on whatever stream) finishes first.
+    cudaEventSynchronize(slot.done);
+    cudaEventDestroy(slot.done);
     cudaGraphExecDestroy(slot.exec);
     cudaGraphDestroy(slot.graph);
     slot = CachedGraph();
   }
   cudaError_t e = buildLoopGraph(d, k, slot);
   if (e != cudaSuccess) return e;
-  *exec = slot.exec;
+  *entry = &slot;
   return cudaSuccess;
 }
 
@@ -960,9 +970,10 @@ mt_status streamLaunch(const void *table, uint32_t capacity, const mtc_stream_co
   DeviceRunState &d = g_run[device];
   if (!shape.iterationsPerCheck) {
     std::lock_guard<std::mutex> g(d.m);
-    cudaGraphExec_t exec = nullptr;
-    if ((e = loopGraph(d, key, &exec)) != cudaSuccess) return toStatus(e);
-    if ((e = cudaGraphLaunch(exec, st)) != cudaSuccess) return toStatus(e);
+    CachedGraph *entry = nullptr;
+    if ((e = loopGraph(d, key, &entry)) != cudaSuccess) return toStatus(e);
+    if ((e = cudaGraphLaunch(entry->exec, st)) != cudaSuccess) return toStatus(e);
+    if ((e = cudaEventRecord(entry->done, st)) != cudaSuccess) return toStatus(e);
   } else if ((e = hostLoop(d, key, shape, st)) != cudaSuccess) {
     return toStatus(e);
   }
