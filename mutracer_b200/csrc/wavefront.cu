@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_wf_seed(StreamView v, uint32
 template <bool kGpuLayout>
 __global__ void __launch_bounds__(kStreamThreads, MT_EXTEND_MIN_BLOCKS)
     k_wf_extend(StreamView v) {
-  const uint32_t cur = v.q->cur, regroup = v.q->regroup;
+  const uint32_t cur = v.q->cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     v.q->rayCount[cur ^ 1u] = 0;
     v.q->shadowCount = 0;
@@ -314,7 +314,6 @@ __global__ void __launch_bounds__(kStreamThreads, MT_EXTEND_MIN_BLOCKS)
           none.triangleIndex = -1;
           none.insIdx = -1;
           v.hits[s] = none;
-          if (regroup) countClass(v, s, 0u);
         } else {
           ext++;
           if (rt.begin(J.s, J.u.blas_offset, sl.ps.path.ray.o, sl.ps.path.ray.d, sl.ps.depth, sl.ps.event != 0,
@@ -322,7 +321,6 @@ __global__ void __launch_bounds__(kStreamThreads, MT_EXTEND_MIN_BLOCKS)
             busy = true;
           } else {
             v.hits[s] = rt.h;
-            if (regroup) countClass(v, s, 0u);
           }
         }
       }
@@ -334,10 +332,26 @@ __global__ void __launch_bounds__(kStreamThreads, MT_EXTEND_MIN_BLOCKS)
     if (finished) {
       v.hits[s] = rt.h;
       busy = false;
-      if (regroup) countClass(v, s, materialClass(v.jobs[v.slots[s].job], rt.h));
     }
   }
   flush(v, ext, 0, 0);
+}
+
+// Material class of every traced ray of this iteration (read from its hit),
+// counted for k_wf_regroup; out of the traversal kernel, whose finishing
+// lanes would otherwise make these dependent loads while the rest of their
+// warp waits.
+__global__ void __launch_bounds__(kStreamThreads) k_wf_classify(StreamView v) {
+  countLaunch(v);
+  if (!v.q->regroup) return;
+  const uint32_t cur = v.q->cur;
+  const uint32_t n = v.q->rayCount[cur];
+  const uint32_t *queue = v.rayQueue[cur];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const uint32_t s = queue[t];
+    if (s >= v.slotCount) continue;
+    countClass(v, s, materialClass(v.jobs[v.slots[s].job], v.hits[s]));
+  }
 }
 
 // Orders the extension queue by ray key (counting sort, keys counted when
@@ -722,6 +736,7 @@ void launchIteration(const GraphKey &k, cudaStream_t s, cudaGraphConditionalHand
   if (v.sortRays) k_wf_sort_rays<<<gSort, kStreamThreads, 0, s>>>(v);
   if (k.gpuLayout) k_wf_extend<true><<<gExtend, kStreamThreads, 0, s>>>(v);
   else k_wf_extend<false><<<gExtend, kStreamThreads, 0, s>>>(v);
+  if (k.regroupInterval) k_wf_classify<<<gRegroup, kStreamThreads, 0, s>>>(v);
   if (k.regroupInterval) k_wf_regroup<<<gRegroup, kStreamThreads, 0, s>>>(v);
   k_wf_shade<<<gShade, kStreamThreads, 0, s>>>(v);
   if (k.alpha) {
