@@ -290,3 +290,28 @@ def test_loop_graphs_of_many_shapes_and_states(cuda):
             torch.cuda.synchronize()
             for a, j in zip(alone, jobs):
                 assert _equal(a.acc, j.acc), (sb.stream_config.slots, j.job_id)
+
+
+def test_queue_trace_adds_up_to_a_full_run(cuda):
+    """bench.py's queue trace (runs stopped by their iteration limit after
+    1, 2, ... iterations, from zeroed accumulation) gives per-iteration queue
+    lengths that sum to the counters of one complete run."""
+    import torch
+
+    import bench
+    host = scene.SceneHost("instanced_spheres", 48, 32, 2, (16, 4, 6, 64, 2))
+    dev = scene.DeviceScene(host, cuda)
+    job = batch.RenderJob(dev, 3, device=cuda)
+    sb = batch.StreamBatch(1, stream_config=abi.StreamConfig.make(slots=4096), device=cuda)
+    sb.set_jobs([job])
+    trace = bench.queue_trace(sb, sb.counters, 4096, 64)["queue_trace"]
+    job.acc.zero_()
+    sb.counters.zero_()
+    sb.stream_config = abi.StreamConfig.make(slots=4096)
+    sb.run()
+    torch.cuda.synchronize()
+    c = sb.counters.cpu().tolist()
+    assert trace[-1]["extension"] == 0                 # the queue drained within the traced iterations
+    assert sum(r["extension"] for r in trace) == c[1]
+    assert sum(r["shadow"] for r in trace) == c[2]
+    assert sum(r["finished"] for r in trace) == c[0] == 48 * 32 * 3
