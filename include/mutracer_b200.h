@@ -397,7 +397,7 @@ typedef struct mtc_batch_config {
   uint32_t block_threads;    /* threads per CTA: 32, 64, 96 or 128 (default 128) */
   uint32_t tile_width;       /* warp tile width in pixels: 1, 2, 4, 8, 16 or 32;
                                 height = 32 / width (default 8, an 8x4 tile) */
-  uint32_t ctas_per_sm;      /* grid = SM count * ctas_per_sm (default 2) */
+  uint32_t ctas_per_sm;      /* grid = SM count * ctas_per_sm (default 16) */
   uint32_t items_per_fetch;  /* warp tiles taken per queue atomic, 1..16 (default 1) */
   uint32_t _pad[3];
 } mtc_batch_config;

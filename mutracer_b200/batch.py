@@ -235,13 +235,13 @@ class StreamBatch(_JobTable):
         pass
 
 
-# Launch shapes the autotuner tries (block threads, CTAs per SM, warp tile
-# width, items per fetch).  The kernel holds 255 registers per thread, so at
-# most two 128-thread CTAs (8 warps) are resident per SM; larger grids only
-# queue CTAs behind them.
+# Launch shapes the autotuner tries, in BatchConfig.make's order (block
+# threads, warp tile width, CTAs per SM, items per fetch).  The kernel is
+# compiled for 16 resident 128-thread CTAs per SM (32 registers), so 16 fills
+# the SMs; larger grids only queue CTAs behind them.
 AUTOTUNE_SPACE = (
-    (128, 2, 8, 1), (128, 2, 8, 2), (128, 2, 4, 1), (128, 2, 16, 1),
-    (128, 2, 32, 1), (64, 4, 8, 1), (128, 1, 8, 1), (128, 4, 8, 1),
+    (128, 8, 16, 1), (128, 8, 16, 2), (128, 4, 16, 1), (128, 16, 16, 1),
+    (128, 32, 16, 1), (64, 8, 32, 1), (128, 8, 8, 1), (128, 8, 12, 1),
 )
 
 

@@ -90,7 +90,7 @@ cudaError_t scratchAddress(void **out) {
 
 // The persistent batched kernel of batch_table.cuh over the fixed scratch.
 template <bool kGpuLayout>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, MT_BATCH_MIN_BLOCKS)
     k_batch_noalloc(const BatchHeader *__restrict__ header, uint32_t *queue, uint32_t grain, uint32_t *status,
                     mtc_counters *counters) {
   Counters cnt;

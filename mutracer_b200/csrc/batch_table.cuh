@@ -109,13 +109,20 @@ inline JobData makeJob(const mtc_scene_view *scene, const mtc_camera_uniform *ca
   return J;
 }
 
+// Resident CTAs of 128 threads per SM the persistent batched kernels are
+// compiled for (32 registers; the default grid fills them): like the plain
+// kernel, latency-bound, so more warps beat fewer spills.
+#ifndef MT_BATCH_MIN_BLOCKS
+#define MT_BATCH_MIN_BLOCKS 16
+#endif
+
 struct BatchShape {
   uint32_t blockThreads, tileW, tileH, ctasPerSm, grain;
 };
 // Resolves a (possibly NULL) mtc_batch_config to launch parameters; false for
 // out-of-range values.
 inline bool batchShape(const mtc_batch_config *c, BatchShape &out) {
-  out = BatchShape{128u, 8u, 4u, 2u, 1u};
+  out = BatchShape{128u, 8u, 4u, uint32_t(MT_BATCH_MIN_BLOCKS), 1u};
   if (!c) return true;
   if (c->struct_size != sizeof(mtc_batch_config)) return false;
   if (c->block_threads) {

@@ -39,8 +39,12 @@ __device__ __forceinline__ void flushCounters(const Counters &cnt, uint32_t path
   }
 }
 
+// The plain kernel at 16 CTAs of 128 threads per SM (full occupancy, 32
+// registers): it is bound by dependent-load latency, and the warps hide more
+// of it than the spilled state costs (measured 11 % faster than 2 CTAs at
+// 255 registers; 4, 8 and 12 CTAs in between).
 #ifndef MT_TRACE_MIN_BLOCKS
-#define MT_TRACE_MIN_BLOCKS 2
+#define MT_TRACE_MIN_BLOCKS 16
 #endif
 template <bool kGpuLayout>
 __global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
@@ -58,7 +62,7 @@ __global__ void __launch_bounds__(kTileW *kTileH, MT_TRACE_MIN_BLOCKS)
 
 // Persistent batched kernel over a job table (batch_table.cuh).
 template <bool kGpuLayout>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, MT_BATCH_MIN_BLOCKS)
     k_batch(const BatchHeader *__restrict__ header, uint32_t *queue, mtc_counters *counters, uint32_t grain,
             uint32_t *status) {
   Counters cnt;

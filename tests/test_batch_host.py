@@ -147,3 +147,16 @@ def test_plain_entry_points_validate_before_touching_the_device():
     assert L.mtc_stream_status(None, 4, None, None) == abi.MT_ERROR_INVALID_ARGUMENT
     assert L.mtc_stream_status(C.c_void_p(16), 4, C.byref(cfg), None) == abi.MT_ERROR_INVALID_ARGUMENT
     assert L.mtc_stream_state_bytes(4, None) > (1 << 20) * 400
+
+
+def test_every_autotune_shape_is_a_valid_batch_config():
+    """The autotuner's launch shapes (BatchConfig.make order) all pass the
+    batched entry points' validation (batchShape)."""
+    from mutracer_b200 import batch
+    L = abi.lib()
+    table = (C.c_uint8 * L.mtc_batch_table_bytes(1))()
+    for shape in batch.AUTOTUNE_SPACE:
+        cfg = abi.BatchConfig.make(*shape)
+        assert L.mtc_batch_prepare(None, 0, C.byref(cfg), table, None) == abi.MT_OK, shape
+    bad = abi.BatchConfig.make(128, 12, 16, 1)           # a warp tile width that does not divide 32
+    assert L.mtc_batch_prepare(None, 0, C.byref(bad), table, None) == abi.MT_ERROR_INVALID_ARGUMENT
