@@ -164,10 +164,10 @@ def oracle_traffic(host, rows=8, spp=2):
 
 
 # DRAM bytes (read + write) measured by ncu, per unit of work: the plain
-# megakernel per launch of the headline step; the wavefront kernels per queued
-# ray or finished path (small-case captures normalised by exact queue
-# lengths), scaled by the units this step processed.
-MEGAKERNEL_TRAFFIC = ("k_trace_dram_instanced_spheres_1080p_16spp.md", "traffic_bytes_per_launch:")
+# megakernel per path sample, the wavefront kernels per queued ray or
+# finished path (small-case captures; the wavefront's normalised by exact
+# queue lengths), scaled by the units this step processed.
+MEGAKERNEL_TRAFFIC = ("k_trace_instanced_spheres_960x540_4spp.md", "dram_bytes_per_path:")
 WAVEFRONT_TRAFFIC = ("wavefront_dram_per_kernel_instanced_spheres_960x540_4spp.md",
                      ("dram_bytes_per_extension_ray:", "dram_bytes_per_shaded_ray:", "dram_bytes_per_shadow_ray:",
                       "dram_bytes_per_finished_path:"))
@@ -193,11 +193,11 @@ def measured_traffic(form, args, host, spp, units=None):
     if args.workload != WORKLOAD:
         return None, None
     if form == "megakernel":
-        if (host.width, host.height, spp) != (1920, 1080, 16):
-            return None, None
         name, key = MEGAKERNEL_TRAFFIC
         v = _profile_values(name, (key,))
-        return (int(v[key]), "profiles/" + name) if key in v else (None, None)
+        if key not in v:
+            return None, None
+        return int(v[key] * host.width * host.height * spp), "profiles/" + name + " (per path x this step's paths)"
     name, keys = WAVEFRONT_TRAFFIC
     v = _profile_values(name, keys)
     if units is None or len(v) != len(keys):
