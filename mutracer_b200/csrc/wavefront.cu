@@ -1,9 +1,9 @@
 // Wavefront form of the batched path tracer (mtc_stream_run).
 //
-// The megakernel keeps a whole path sample in one thread: every kernel
-// register budget is the shading code's (255 registers, 8 warps per SM), so
-// the traversal loops, which are latency-bound chains of dependent node
-// loads, run with too few warps to hide that latency.  Here the integrator's
+// The megakernel keeps a whole path sample in one thread, so its traversal
+// loops, latency-bound chains of dependent node loads, share one register
+// budget with the shading code: either few warps or heavy spills, and lanes
+// that drift between camera, traversal and shading code.  Here the integrator's
 // event loop (rayTrace.compute.ts:891-946) is cut at its traversals into
 // separate kernels that each see a queue of path slots:
 //
