@@ -22,7 +22,10 @@ using namespace mt;
 
 namespace {
 
-constexpr int kTileW = 16, kTileH = 8;       // plain kernel CTA tile
+#ifndef MT_TRACE_TILE_W
+#define MT_TRACE_TILE_W 16
+#endif
+constexpr int kTileW = MT_TRACE_TILE_W, kTileH = 128 / MT_TRACE_TILE_W;  // plain kernel CTA tile
 
 __device__ __forceinline__ void flushCounters(const Counters &cnt, uint32_t paths, mtc_counters *out) {
   if (!out) return;
